@@ -1,0 +1,324 @@
+"""Benchmark: worst-case topology-optimisation design iterations per second
+on a 256^3 voxel box (the adjoint-through-spline configuration): tricubic
+B-spline density (32^3 coefficients ~ N(0.5, 0.15)), Heaviside beta=8,
+bottom face clamped, free-force worst case over the top-face nodes (20
+Lanczos steps, each a multigrid solve to relative residual 1e-6), 45 degree
+self-support constraint, volume fraction 0.3, MMA update.
+
+One step = one full design iteration through the C ABI.  The mixed path
+(FP32 V-cycle inside FP64 CG) is the headline; the plain FP64 GPU path is
+measured beside it.  Data are synthetic and seeded.  Inputs (17M nodes)
+exceed the 126 MB L2, so no flush is inserted between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--size S]
+
+With torchrun each rank runs an independent replica (the path does not
+shard: one design problem per GPU), timing is max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "worst-case TO design iterations/s @256^3 (mixed FP32 V-cycle + FP64 CG, rel.resid 1e-6)"
+UNIT = "iter/s"
+
+
+def problem(n, seed=2026):
+    em = np.ones((n, n, n), np.uint8)
+    fa = np.zeros((n + 1,) * 3, np.uint8)
+    fa[0] = 1
+    la = np.zeros((n + 1,) * 3, np.uint8)
+    la[n] = 1
+    order = 4
+    parts = 32 - order
+    rng = np.random.default_rng(seed)
+    coeff = np.clip(rng.normal(0.5, 0.15, 32 ** 3), 0.0, 1.0)
+    return em, fa, la, order, parts, coeff
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms",
+                                          "200", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and "Active" in s[5 + i]
+                          and "Not" not in s[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier_max(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.barrier()
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, world, rank):
+    """CPU reference arm: the FP64 oracle restatement of the reference method
+    (the reference itself cannot be built here), one bounded design iteration
+    per step at args.ref_size^3, scaled to 256^3 by the element count."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    n = args.ref_size
+    em, fa, la, order, parts, coeff = problem(n)
+    cores = os.cpu_count()
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle_design_iteration(O, n, em, fa, la, order, parts, coeff)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(dt)
+    per_iter = statistics.mean(times) * (256.0 / n) ** 3
+    value = 1.0 / per_iter
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": per_iter * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "256^3 worst-case spline TO iteration (config 4 shape)", "sample_size": n},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"FP64 oracle design iteration at {n}^3 (20 Lanczos steps, MG-PCG to 1e-6), "
+                                       f"time scaled by (256/{n})^3"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def oracle_design_iteration(O, n, em, fa, la, order, parts, coeff, beta=8.0):
+    """The FP64 oracle's design iteration: spline -> Heaviside -> operators ->
+    Lanczos worst case -> self-support -> adjoint chain -> MMA."""
+    p = O.Problem(em, fa, la, None, nu=0.3, n_levels=0, first_factor=4)
+    p.spline_setup(order, (parts, parts, parts))
+    rh = p.coeff2density(coeff)
+    rho = O.heaviside(rh, beta, 1e-3)
+    p.set_density(rho)
+    p.update_stencil()
+    lam, fw, uw, _ = p.lanczos(20, 0, tol=1e-6)
+    ssv, _, dss, _, _ = p.selfsupport(coeff, beta, 4)
+    s = p.sensitivity(uw)
+    s = O.heaviside_chain(rh, beta, s)
+    v = O.heaviside_chain(rh, beta, np.full(p.ne, 1.0 / p.ne))
+    s = p.filter(2.0, s)
+    v = p.filter(2.0, v)
+    dc = p.density2coeff_adjoint(s)
+    dv = p.density2coeff_adjoint(v)
+    m = O.MMA(len(coeff), 2, 0.0, 1.0)
+    m.set_x(coeff)
+    m.update(dc * 1e6, np.stack([dv * 1e3, dss * 1e3]), np.array([1e3 * (rho.mean() - 0.3), 1e3 * ssv]))
+    return lam
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours")
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--ref-size", type=int, default=24)
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    import robustoptspline3d_b200 as R
+
+    n = args.size
+    em, fa, la, order, parts, coeff = problem(n)
+    prm = R.IterParams(lanczos_steps=20, solve_tol=1e-6, ss_mode=4)
+
+    def make(precision):
+        g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=precision, smoother=R.rso.SMOOTH_JACOBI, omega=0.6,
+                                                        pre=2, post=2, poisson_ratio=0.3))
+        nc = g.set_spline_partition(parts, parts, parts, order)
+        mma = R.MMA(nc, 2, 0.0, 1.0)
+        mma.set_x(coeff)
+        return g, mma
+
+    g, mma = make(R.rso.MIXED)
+    lib = g.lib
+    # warm-up (device path)
+    for _ in range(args.warmup):
+        g.design_iteration(mma, prm)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lib.rso_profile_reset(g.h)
+    lib.rso_set_profiling(g.h, 1)
+    launches0 = lib.rso_launch_count()
+    barrier_max(world, 0.0)
+    infos = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev0.record()
+        for _ in range(args.steps):
+            infos.append(g.design_iteration(mma, prm))
+        ev1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    launches = lib.rso_launch_count() - launches0
+    lib.rso_set_profiling(g.h, 0)
+    ms_dev = ev0.elapsed_time(ev1)
+    ms = barrier_max(world, max(ms_dev, wall * 1e3))
+    value = world * args.steps / (ms / 1e3)
+    # dominant-kernel roofline from the live event timings
+    import ctypes
+    kname = ctypes.create_string_buffer(64)
+    cnt = ctypes.c_longlong(0)
+    tot = ctypes.c_double(0)
+    bytes_per = ctypes.c_double(0)
+    flops_per = ctypes.c_double(0)
+    lib.rso_profile_top(g.h, kname, 64, ctypes.byref(cnt), ctypes.byref(tot), ctypes.byref(bytes_per),
+                        ctypes.byref(flops_per))
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    avg_ms = tot.value / max(cnt.value, 1)
+    achieved = bytes_per.value / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
+    roofline = {"kernel": kname.value.decode(), "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "launches": cnt.value, "avg_ms": avg_ms,
+                "algorithmic_bytes_per_launch": bytes_per.value,
+                "fp_flops_per_launch": flops_per.value,
+                "fp_tflops": flops_per.value / (avg_ms / 1e3) / 1e12 if avg_ms > 0 else 0.0,
+                "peak_source": "measured" if peaks else "fallback"}
+    # end-to-end through the host-buffer C ABI call
+    cin = np.ascontiguousarray(R.MMA.get(mma)[0])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps // 2)):
+        cout, _, _ = host_iteration(g, mma, cin, prm)
+        cin = cout
+    e2e_s = (time.perf_counter() - t0) / max(1, args.steps // 2)
+    e2e_s = barrier_max(world, e2e_s)
+    e2e = {"value": world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * len(cin),
+           "d2h_bytes_per_step": 8 * len(cin)}
+    g.close()
+    mma.close()
+    # plain FP64 GPU path for the mixed-vs-FP64 comparison
+    fp64 = None
+    if args.fp64_steps > 0:
+        g64, mma64 = make(R.rso.FP64)
+        g64.design_iteration(mma64, prm)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.fp64_steps):
+            g64.design_iteration(mma64, prm)
+        torch.cuda.synchronize()
+        fp64 = barrier_max(world, (time.perf_counter() - t0) / args.fp64_steps)
+        g64.close()
+        mma64.close()
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        nr = args.ref_size
+        emr, far, lar, _, _, _ = problem(nr)
+        t0 = time.perf_counter()
+        oracle_design_iteration(O, nr, emr, far, lar, order, parts, coeff)
+        dt = time.perf_counter() - t0
+        cpu = {"value": 1.0 / (dt * (256.0 / nr) ** 3), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"one FP64 oracle design iteration at {nr}^3 took {dt:.2f} s, scaled by (256/{nr})^3"}
+    if rank == 0:
+        last = infos[-1]
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 V-cycle + f64 CG/Lanczos/MMA", "data": "synthetic",
+                "config": {"workload": f"{n}^3 worst-case spline TO iteration (config 4 shape)", "elements": n ** 3,
+                           "spline": "order 4, 32^3 coefficients", "lanczos_steps": 20, "solve_tol": 1e-6,
+                           "levels": g_levels(n), "parallelism": f"replicas x{world}",
+                           "l2_flush": "inputs larger than L2"},
+                "fp64_iters_per_s": (1.0 / fp64) if fp64 else None,
+                "mixed_vs_fp64": (fp64 / (ms / 1e3 / args.steps)) if fp64 else None,
+                "last_iteration": {k: last[k] for k in ("c_worst", "lam", "volume", "ss_value", "solve_iterations",
+                                                        "ms_operators", "ms_worst", "ms_selfsupport", "ms_adjoint",
+                                                        "ms_mma")},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def g_levels(n):
+    lv = [n]
+    m = n
+    while (m ** 3) > 400:
+        m = (m + 1) // 2
+        lv.append(m)
+    return [lv[0]] + lv[2:]
+
+
+def host_iteration(g, mma, cin, prm):
+    return g.design_iteration_host(mma, cin, prm)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,289 @@
+/*
+ * rso.h - C ABI of the B200-native voxel-FEM worst-case topology-optimisation
+ * path (capabilities of NanXYZH/RobustOptSpline3D).
+ *
+ * Conventions
+ *  - Box of ex*ey*ez hexahedral voxels with unit edge, origin 0.  Elements are
+ *    numbered e = x + ex*(y + ey*z); nodes n = x + nx*(y + ny*z), nx = ex+1.
+ *  - Nodal vectors are structure-of-arrays: v[c*Nn + n], c = 0,1,2, double.
+ *  - Element fields (densities, sensitivities) and spline coefficients are
+ *    float, as in the reference (rho_e, g_sens, coeffs are float there).
+ *  - Pointers named *_dev are CUDA device pointers owned by the caller and
+ *    borrowed for the duration of the call; *_host are host pointers.
+ *  - Every call returns rso_status and never aborts; rso_last_error() gives a
+ *    message.  Calls on one handle are ordered on the handle's stream; handles
+ *    are not thread-safe, distinct handles are independent.
+ *  - Dirichlet (support) DOFs are homogeneous: entries of f and u at support
+ *    nodes are ignored on input and returned as zero.
+ *
+ * Each entry point cites the reference interface it replaces (file:line in
+ * the reference project).
+ */
+#ifndef RSO_H
+#define RSO_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  RSO_OK = 0,
+  RSO_ERR_INVALID_ARG = 1,
+  RSO_ERR_OOM = 2,
+  RSO_ERR_CUDA = 3,
+  RSO_ERR_DIVERGED = 4,
+  RSO_ERR_NONFINITE = 5,
+  RSO_ERR_BUDGET_EXCEEDED = 6,
+  RSO_ERR_UNSUPPORTED = 7,
+  RSO_ERR_STATE = 8
+} rso_status;
+
+/* smoothers */
+enum { RSO_SMOOTH_GS = 0, RSO_SMOOTH_JACOBI = 1 };
+/* V-cycle arithmetic */
+enum { RSO_FP64 = 0, RSO_MIXED = 1 };
+/* solve methods */
+enum { RSO_SOLVE_VCYCLE = 0, RSO_SOLVE_PCG = 1 };
+/* worst-case modes: grid/Grid.h:170-175 HierarchyGrid::Mode */
+enum {
+  RSO_NO_SUPPORT_CONSTRAIN_FORCE_DIRECTION = 0,
+  RSO_NO_SUPPORT_FREE_FORCE = 1,
+  RSO_WITH_SUPPORT_CONSTRAIN_FORCE_DIRECTION = 2,
+  RSO_WITH_SUPPORT_FREE_FORCE = 3
+};
+
+typedef struct rso_handle rso_handle;
+typedef struct rso_mma rso_mma;
+
+/* Problem parameters; replaces the Parameter struct and HierarchySetting
+ * (optimization/optimization.h:15-35, grid/Grid.h:836-862). */
+typedef struct {
+  double youngs_modulus;   /* E  (reference default 1e6) */
+  double poisson_ratio;    /* nu */
+  double penal;            /* SIMP power p */
+  double rho_min;          /* density floor */
+  int n_levels;            /* 0: reference policy, coarsen while > 400 active elements */
+  int first_factor;        /* 4: non-dyadic first coarsening (skip layer 1, reference); 2: dyadic */
+  int smoother;            /* RSO_SMOOTH_* */
+  double omega;            /* damped Jacobi factor relative to the bound 2/lambda_max(D^-1 K) */
+  int pre, post;           /* smoothing sweeps */
+  int precision;           /* RSO_FP64 or RSO_MIXED (FP32 V-cycle inside FP64 outer iteration) */
+  int mode;                /* RSO_WITH_SUPPORT_* / RSO_NO_SUPPORT_* */
+} rso_config;
+
+typedef struct {
+  int iterations;
+  double rel_res;
+  double ms;
+} rso_solve_info;
+
+/* ---------------------------------------------------------------- setup */
+void rso_default_config(rso_config* cfg);
+
+/* Build the hierarchy, topology, support/load node sets and all device
+ * buffers.  emask: ex*ey*ez bytes (1 = solid voxel).  fixed_area/load_area:
+ * node masks (Nn bytes) that play the role of the reference's
+ * _inFixedArea/_inLoadArea predicates; load_normals: 3*Nn unit normals used
+ * in constrained-direction modes (may be NULL otherwise).
+ * Replaces HierarchyGrid::genFromMesh(solid_bit, reso) (grid/Grid.cpp:978-1237),
+ * Grid::build (grid/Grid.cpp:2973-3215), computeProjectionMatrix
+ * (grid/Grid.cpp:2694-2836), setNodes/setLoadNodes (optimization/projection.cpp:46-269)
+ * and uploadTemplateMatrix (optimization/optimization.cu:815-827). */
+rso_status rso_create(const rso_config* cfg, int ex, int ey, int ez, const uint8_t* emask_host,
+                      const uint8_t* fixed_area_host, const uint8_t* load_area_host,
+                      const double* load_normals_host, rso_handle** out);
+void rso_destroy(rso_handle* h);
+const char* rso_last_error(const rso_handle* h);
+/* stream is a cudaStream_t; NULL = the handle's own stream */
+rso_status rso_set_stream(rso_handle* h, void* stream);
+rso_status rso_synchronize(rso_handle* h);
+
+/* element stiffness matrix (24x24 row-major, host); element/templateMatrix.cpp:31-124 */
+rso_status rso_element_matrix(double E, double nu, double h, double* K0_host);
+
+/* ---------------------------------------------------------------- topology */
+/* HierarchyGrid::n_grid (grid/Grid.h:1000) */
+int rso_n_levels(const rso_handle* h);
+/* dims[0..2] element dims, dims[3..5] node dims of a level */
+rso_status rso_level_dims(const rso_handle* h, int level, int* dims_host);
+/* per-level element/vertex masks; elesatlist/vrtsatlist (grid/Grid.cpp:1011-1034) */
+rso_status rso_level_masks(rso_handle* h, int level, uint8_t* emask_host, uint8_t* vmask_host);
+/* per-level masks as 32-bit words, the BitSAT bit arrays (grid/Grid.h:116-158) */
+rso_status rso_level_bitwords(rso_handle* h, int level, uint32_t* ebits_host, uint32_t* vbits_host);
+/* BitSAT rank of every set bit and -1 elsewhere (gBitSAT operator(), culib/lib.cuh:1474-1550) */
+rso_status rso_bitsat_rank(rso_handle* h, const uint32_t* words_dev, int64_t nbits, int32_t* rank_dev);
+/* fine-level node classes: bit0 active, bit1 surface, bit2 support, bit3 load;
+ * mark_surface_nodes_kernel (grid/Grid.cu:2824-2858) + computeProjectionMatrix */
+rso_status rso_node_class(rso_handle* h, uint8_t* class_host);
+/* reference compact numbering of a level: lexicographic vertex/element ids,
+ * GS colour order padded to 32 per colour, flag words (padding -1).
+ * compute_gscolor (grid/Grid.cu:1310-1385), enumerate_gs_subset
+ * (grid/Grid.cpp:4187-4248), lexico2gsorder_g (grid/Grid.cu:1465-1495).
+ * counts[4] = {n_vertices, n_elements, n_gs_vertices, n_gs_elements};
+ * any output may be NULL (call once with NULL arrays to size them). */
+rso_status rso_ref_numbering(rso_handle* h, int level, int* counts_host, int* gs_num_host,
+                             int* vlexi2gs_host, int* elexi2gs_host, int* vflag_host, int* eflag_host);
+/* load nodes (dense node ids) in the reference's order (sorted by GS id);
+ * getLoadNodes (optimization/projection.cpp:272) */
+rso_status rso_load_nodes(rso_handle* h, int* nodes_host, int* n_load);
+
+/* ---------------------------------------------------------------- operator and multigrid */
+/* element densities (ex*ey*ez floats, inactive entries ignored); Grid rho_e buffer */
+rso_status rso_set_density(rso_handle* h, const float* rho_dev);
+/* Galerkin coarse operators and coarsest factorisation; update_stencil
+ * (grid/Grid.cpp:4250-4261, grid/Grid.cu:882-1308, grid/Grid.cpp:3697-3752) */
+rso_status rso_update_operators(rso_handle* h);
+/* f = K(rho) u with support rows passing u; Grid::applyK (grid/Grid.cu:4358-4450) */
+rso_status rso_apply_K(rso_handle* h, const double* u_dev, double* f_dev);
+/* r = f - K u; Grid::update_residual (grid/Grid.cu:2463-2497) */
+rso_status rso_residual(rso_handle* h, const double* u_dev, const double* f_dev, double* r_dev);
+/* coarse-level stencil (243 x Nn_level doubles, [d][row][col][node]); rxStencil */
+rso_status rso_get_stencil(rso_handle* h, int level, double* out_dev);
+/* coarse residual on stored stencils; update_residual_kernel_1 (grid/Grid.cu:2169-2267) */
+rso_status rso_coarse_residual(rso_handle* h, int level, const double* u_dev, const double* f_dev,
+                               double* r_dev);
+/* smoothing sweeps on a level (omega absolute for Jacobi); Grid::gs_relax (grid/Grid.cu:1887-1930) */
+rso_status rso_smooth(rso_handle* h, int level, double* u_dev, const double* f_dev, int kind,
+                      double omega, int sweeps, int reverse);
+/* Grid::restrict_residual (grid/Grid.cu:2615-2635) */
+rso_status rso_restrict(rso_handle* h, int coarse_level, const double* rf_dev, double* fc_dev);
+/* Grid::prolongate_correction (grid/Grid.cu:2717-2734) */
+rso_status rso_prolong(rso_handle* h, int coarse_level, const double* uc_dev, double* uf_dev);
+/* coarsest dense solve; Grid::solve_fem_host (grid/Grid.cpp:4123-4185) */
+rso_status rso_coarsest_solve(rso_handle* h, const double* f_dev, double* u_dev);
+/* lambda_max(D^-1 K) estimate of a level used by damped Jacobi */
+rso_status rso_level_lambda(rso_handle* h, int level, double* lambda);
+/* one V-cycle updating u in place; HierarchyGrid::v_cycle (grid/Grid.cpp:2431-2476).
+ * symmetric=1 reverses the post-smoothing order (needed for PCG). */
+rso_status rso_vcycle(rso_handle* h, double* u_dev, const double* f_dev, int pre, int post,
+                      int symmetric, double* rel_res);
+/* solve K u = f to tol; u holds the initial guess.  method RSO_SOLVE_VCYCLE
+ * repeats V-cycles (solveFEM, optimization/optimization.cpp:178-184),
+ * RSO_SOLVE_PCG runs FP64 CG preconditioned by one V-cycle (FP32 in mixed mode). */
+rso_status rso_solve(rso_handle* h, const double* f_dev, double* u_dev, double tol, int max_iter,
+                     int method, rso_solve_info* info);
+/* Grid::compliance (grid/Grid.cpp:4118-4121): c = f . u */
+rso_status rso_dot(rso_handle* h, const double* a_dev, const double* b_dev, double* out);
+
+/* ---------------------------------------------------------------- design variables and sensitivities */
+/* dC/drho_e = -p rho^(p-1) u_e^T K0 u_e; computeSensitivity_kernel (optimization/optimization.cu:102-165) */
+rso_status rso_sensitivity(rso_handle* h, const double* u_dev, float* sens_dev);
+/* rho^p u_e^T K0 u_e; elementCompliance_kernel (grid/Grid.cu:5569-5610) */
+rso_status rso_element_energy(rso_handle* h, const double* u_dev, float* energy_dev);
+/* rho_out = clamp(H_beta(rho_in), rho_min, 1), shell -> 1; computeProjection_kernel
+ * (optimization/optimization.cu:324-348) */
+rso_status rso_heaviside(rso_handle* h, const float* rho_in_dev, double beta, const uint8_t* shell_dev,
+                         float* rho_out_dev);
+/* g_out = g_in * H'(rho_in); computeProjectionSensitivity_kernel (optimization/optimization.cu:167-189) */
+rso_status rso_heaviside_chain(rso_handle* h, const float* rho_in_dev, double beta, const float* g_in_dev,
+                               float* g_out_dev);
+/* sensitivity filter; filterSensitivity_kernel (grid/Grid.cu:4210-4326) */
+rso_status rso_filter(rso_handle* h, double radius, const float* in_dev, float* out_dev);
+/* consistent density filter (same weights) and its adjoint (build mode) */
+rso_status rso_density_filter(rso_handle* h, double radius, const float* in_dev, float* out_dev);
+rso_status rso_density_filter_adjoint(rso_handle* h, double radius, const float* in_dev, float* out_dev);
+/* volume fraction sum(rho)/n_gs_elements; Grid::volumeRatio (grid/Grid.cu:5642-5650) */
+rso_status rso_volume(rso_handle* h, const float* rho_dev, double* vol);
+
+/* B-spline map: HierarchyGrid::set_spline_partition (grid/Grid.cu:3187-3256),
+ * Grid::set_spline_knot_series (grid/Grid.cpp:3307-3431).  Returns n_coeff. */
+rso_status rso_spline_setup(rso_handle* h, int order, int px, int py, int pz, int* n_coeff);
+/* per-axis tables: first-knot index (-1 outside) and order basis values/derivatives (host) */
+rso_status rso_spline_axis(rso_handle* h, int axis, int* idx_host, double* N_host, double* dN_host);
+/* Grid::coeff2density (grid/Grid.cu:3405-3536) */
+rso_status rso_coeff2density(rso_handle* h, const float* coeff_dev, const uint8_t* shell_dev,
+                             float* rho_hat_dev);
+/* race-free adjoint; Grid::ddensity2dcoeff (grid/Grid.cu:3566-3721),
+ * ddensity2dcoeff_update (:3723-3828), dvol2dcoeff (:3830-3939) */
+rso_status rso_density2coeff_adjoint(rso_handle* h, const float* g_dev, const uint8_t* shell_dev,
+                                     float* dc_dev);
+/* self-support constraint on element centres; deal_background_points
+ * (optimization/optimization.cpp:1223-1242) -> grid/Grid.cu:7449-8250.
+ * per_element (ex*ey*ez) and dc (n_coeff, already divided by the count) may be NULL. */
+rso_status rso_selfsupport(rso_handle* h, const float* coeff_dev, double beta, int mode, double opt_angle,
+                           double default_angle, float* per_element_dev, float* dc_dev, double* value,
+                           double* count, double* direction_sum);
+
+/* ---------------------------------------------------------------- worst case */
+/* forceProject (optimization/projection.cu:165-231, projection.cpp:289-360) */
+rso_status rso_force_project(rso_handle* h, double* f_dev, int constrain_direction);
+/* worst-case load: lambda_max of P K^-1 P by Lanczos with full FP64
+ * reorthogonalisation, one multigrid solve (to tol) per step.  Replaces
+ * modifiedPM (optimization/optimization.cpp:215-353).  ritz_host may be NULL. */
+rso_status rso_worst_case(rso_handle* h, int steps, int constrain_direction, double tol, uint64_t seed,
+                          double* f_worst_dev, double* u_worst_dev, double* lambda, double* ritz_host);
+/* the reference's modified power method itself (optimization/optimization.cpp:215-353) */
+rso_status rso_modified_pm(rso_handle* h, int constrain_direction, uint64_t seed, int max_itn,
+                           double* f_dev, double* u_dev, double* c_worst, int* itn);
+
+/* ---------------------------------------------------------------- MMA */
+/* MMA::mma_t (optimization/mma_t.h:159-266) in FP64 on the device */
+rso_status rso_mma_create(int n, int m, const double* xmin_host, const double* xmax_host, rso_mma** out);
+/* start from a given design (host); the reference starts from the box midpoint */
+rso_status rso_mma_set_x(rso_mma* s, const double* x_host);
+rso_status rso_mma_get(rso_mma* s, double* x_host, double* L_host, double* U_host, double* alpha_host,
+                       double* beta_host);
+/* device x (n doubles) of the current design */
+const double* rso_mma_x_dev(rso_mma* s);
+/* mma_t::update(df, dg, g) (optimization/mma_t.cpp:18-51, mma_t.cu:330-499).
+ * df_dev: n doubles, dg_dev: m*n doubles (constraint-major), g_host: m doubles.
+ * info_host[4] = {kkt inf-norm, last step, sub-iterations, overflowed}. */
+rso_status rso_mma_update(rso_mma* s, const double* df_dev, const double* dg_dev, const double* g_host,
+                          int* converged, double* info_host);
+void rso_mma_destroy(rso_mma* s);
+
+/* ---------------------------------------------------------------- design iteration */
+typedef struct {
+  double beta;             /* Heaviside sharpness */
+  double volume_ratio;     /* V* */
+  double filter_radius;    /* sensitivity filter radius (elements) */
+  int filter_mode;         /* 0 reference sensitivity filter, 1 none */
+  int lanczos_steps;
+  double solve_tol;        /* relative residual of each multigrid solve */
+  int constrain_direction; /* 1: cf mode, 0: ff mode */
+  int ss_mode;             /* GlobalSSMode, -1 disables the self-support constraint */
+  double opt_angle, default_angle;
+  double sens_scale, vol_scale, ss_scale;  /* driver scalings (optimization.cpp:1008-1024) */
+  uint64_t seed;
+} rso_iter_params;
+
+typedef struct {
+  double c_worst, lambda, volume, ss_value;
+  double ms_total, ms_operators, ms_worst, ms_adjoint, ms_selfsupport, ms_mma;
+  int solve_iterations;
+  int mma_converged;
+} rso_iter_info;
+
+void rso_default_iter_params(rso_iter_params* p);
+/* one robust spline design iteration: coefficients -> density -> Heaviside ->
+ * operators -> worst case -> self-support -> adjoint chain -> MMA update of
+ * the coefficients (optimization_ss loop body, optimization/optimization.cpp:859-1075).
+ * The coefficients live in the MMA state (rso_mma_x_dev). */
+rso_status rso_design_iteration(rso_handle* h, rso_mma* mma, const rso_iter_params* prm, rso_iter_info* info);
+/* the same call with host buffers: copies coeff_host in, runs the iteration
+ * and copies the updated coefficients and the density field out. */
+rso_status rso_design_iteration_host(rso_handle* h, rso_mma* mma, const rso_iter_params* prm,
+                                     const double* coeff_in_host, double* coeff_out_host,
+                                     float* rho_out_host, rso_iter_info* info);
+
+/* ---------------------------------------------------------------- instrumentation */
+/* Number of kernels this library has launched in the process (all handles).
+ * The reference has no counterpart (it prints tictoc timers, utils/tictoc.h:78-80). */
+long long rso_launch_count(void);
+/* CUDA-event timing of the operator kernels on the handle's stream
+ * (replaces the _TIC/_TOC phase timers of test_vcycle, grid/Grid.cpp:2349-2388) */
+rso_status rso_set_profiling(rso_handle* h, int on);
+rso_status rso_profile_reset(rso_handle* h);
+/* per kernel class: launches, total device ms, algorithmic bytes and flops per launch */
+rso_status rso_profile_class(rso_handle* h, int cls, char* name, int name_len, long long* launches,
+                             double* total_ms, double* bytes_per_launch, double* flops_per_launch);
+/* the class with the largest total device time */
+rso_status rso_profile_top(rso_handle* h, char* name, int name_len, long long* launches, double* total_ms,
+                           double* bytes_per_launch, double* flops_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RSO_H */

@@ -1,0 +1,532 @@
+// Coarse levels: Galerkin operators, stencil smoothing/residuals, transfer
+// operators and the coarsest dense FP64 solve.
+//
+// Galerkin operators are built element by element: a coarse element matrix
+// is K_E = sum_children P_c^T K_c P_c with P_c the trilinear interpolation
+// from the 8 coarse corners to a child's 8 nodes.  For the first coarsening
+// the children are fine voxels, K_c = rho^p K0 with the rows/columns of
+// support DOFs zeroed and 1e6 on their diagonal (the matrix behind
+// restrict_stencil_nondyadic_OTFA_WS_kernel, grid/Grid.cu:1154-1268); for
+// unconstrained voxels P^T (rho^p K0) P = rho^p T_pos with T_pos tabulated
+// once per coarsening factor.  Deeper levels recurse on the coarse element
+// matrices (equivalent to restrict_stencil_dyadic_kernel, grid/Grid.cu:882-939,
+// which applies R K P to assembled stencils).  Stencils are then assembled
+// from the element matrices, in FP64 and FP32.
+#include "rso_internal.cuh"
+#include <cmath>
+#include <cstdio>
+
+namespace rso {
+
+static const double DIRICHLET_W = 1e6;  // grid/Grid.cu:14
+
+// ---------------------------------------------------------------- stencil kernels
+template <typename T>
+__device__ __forceinline__ void stencil_apply(const Level& L, const T* __restrict__ st, const T* __restrict__ u,
+                                              long long n, bool skip_centre, T acc[3]) {
+  const long long NP = L.NP, px = L.px, pxy = (long long)L.px * L.py;
+#pragma unroll
+  for (int d = 0; d < 27; d++) {
+    if (skip_centre && d == 13) continue;
+    const long long nb = n + (d % 3 - 1) + (d / 3 % 3 - 1) * px + (d / 9 - 1) * pxy;
+    const T u0 = u[nb], u1 = u[nb + NP], u2 = u[nb + 2 * NP];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+      acc[r] += st[(d * 9 + r * 3 + 0) * NP + n] * u0 + st[(d * 9 + r * 3 + 1) * NP + n] * u1 +
+                st[(d * 9 + r * 3 + 2) * NP + n] * u2;
+  }
+}
+
+// MODE 0 residual, MODE 2 damped block Jacobi (out of place)
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) k_coarse(const Level L, const T* __restrict__ st, const T* __restrict__ u,
+                                                const T* __restrict__ f, T* __restrict__ out, T omega) {
+  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+  if (x >= L.nx || y >= L.ny) return;
+  const long long NP = L.NP;
+  const long long n = L.nidx(x, y, z);
+  const bool act = (L.vclass[n] & NC_ACTIVE) != 0;
+  T acc[3] = {0, 0, 0};
+  if (act) stencil_apply<T>(L, st, u, n, false, acc);
+  if (MODE == 0) {
+#pragma unroll
+    for (int r = 0; r < 3; r++) out[n + r * NP] = f[n + r * NP] - acc[r];
+  } else {
+    if (!act) { out[n] = 0; out[n + NP] = 0; out[n + 2 * NP] = 0; return; }
+    T S[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) S[i] = st[(13 * 9 + i) * NP + n];
+    const T r0 = f[n] - acc[0], r1 = f[n + NP] - acc[1], r2 = f[n + 2 * NP] - acc[2];
+    const T A = S[4] * S[8] - S[5] * S[7], B = -(S[3] * S[8] - S[5] * S[6]), C = S[3] * S[7] - S[4] * S[6];
+    const T det = S[0] * A + S[1] * B + S[2] * C;
+    const T id = omega / det;
+    const T i01 = -(S[1] * S[8] - S[2] * S[7]), i02 = S[1] * S[5] - S[2] * S[4];
+    const T i11 = S[0] * S[8] - S[2] * S[6], i12 = -(S[0] * S[5] - S[2] * S[3]);
+    const T i21 = -(S[0] * S[7] - S[1] * S[6]), i22 = S[0] * S[4] - S[1] * S[3];
+    out[n] = u[n] + id * (A * r0 + i01 * r1 + i02 * r2);
+    out[n + NP] = u[n + NP] + id * (B * r0 + i11 * r1 + i12 * r2);
+    out[n + 2 * NP] = u[n + 2 * NP] + id * (C * r0 + i21 * r1 + i22 * r2);
+  }
+}
+
+// one colour of the point Gauss-Seidel sweep on stored stencils (gs_relax_kernel grid/Grid.cu:1497-1609)
+template <typename T>
+__global__ void __launch_bounds__(256) k_coarse_gs(const Level L, const T* __restrict__ st, T* __restrict__ u,
+                                                   const T* __restrict__ f, int cx, int cy, int cz, int rev) {
+  const int x = 2 * (blockIdx.x * 32 + threadIdx.x) + cx;
+  const int y = 2 * (blockIdx.y * 8 + threadIdx.y) + cy;
+  const int z = 2 * blockIdx.z + cz;
+  if (x >= L.nx || y >= L.ny || z >= L.nz) return;
+  const long long NP = L.NP;
+  const long long n = L.nidx(x, y, z);
+  if (!(L.vclass[n] & NC_ACTIVE)) return;
+  T acc[3] = {0, 0, 0};
+  stencil_apply<T>(L, st, u, n, true, acc);
+  T v[3] = {u[n], u[n + NP], u[n + 2 * NP]};
+#pragma unroll
+  for (int t = 0; t < 3; t++) {
+    const int r = rev ? 2 - t : t;
+    T s = f[n + r * NP] - acc[r];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      if (c != r) s -= st[(13 * 9 + r * 3 + c) * NP + n] * v[c];
+    v[r] = s / st[(13 * 9 + r * 3 + r) * NP + n];
+  }
+  u[n] = v[0]; u[n + NP] = v[1]; u[n + 2 * NP] = v[2];
+}
+
+// ---------------------------------------------------------------- transfers
+// f_c(X) = sum_x w(x - F X) r_f(x), w = prod (F-|d|)/F  (R = P^T)
+template <typename T>
+__global__ void k_restrict(const Level Fl, const Level C, int F, const T* __restrict__ rf, T* __restrict__ fc) {
+  const int X = blockIdx.x * 32 + threadIdx.x, Y = blockIdx.y * 8 + threadIdx.y, Z = blockIdx.z;
+  if (X >= C.nx || Y >= C.ny) return;
+  const long long nC = C.nidx(X, Y, Z);
+  T s0 = 0, s1 = 0, s2 = 0;
+  if (C.vclass[nC] & NC_ACTIVE) {
+    const T inv = T(1) / (T)(F * F * F);
+    for (int dz = -F + 1; dz < F; dz++) {
+      const int z = F * Z + dz;
+      if (z < 0 || z >= Fl.nz) continue;
+      for (int dy = -F + 1; dy < F; dy++) {
+        const int y = F * Y + dy;
+        if (y < 0 || y >= Fl.ny) continue;
+        const T wyz = (T)((F - abs(dy)) * (F - abs(dz)));
+        for (int dx = -F + 1; dx < F; dx++) {
+          const int x = F * X + dx;
+          if (x < 0 || x >= Fl.nx) continue;
+          const long long n = Fl.nidx(x, y, z);
+          const T w = wyz * (T)(F - abs(dx)) * inv;
+          s0 += w * rf[n]; s1 += w * rf[n + Fl.NP]; s2 += w * rf[n + 2 * Fl.NP];
+        }
+      }
+    }
+  }
+  fc[nC] = s0; fc[nC + C.NP] = s1; fc[nC + 2 * C.NP] = s2;
+}
+
+// u_f += P u_c at active, non-support fine nodes
+template <typename T>
+__global__ void k_prolong(const Level Fl, const Level C, int F, const T* __restrict__ uc, T* __restrict__ uf) {
+  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+  if (x >= Fl.nx || y >= Fl.ny) return;
+  const long long n = Fl.nidx(x, y, z);
+  const uint8_t cls = Fl.vclass[n];
+  if (!(cls & NC_ACTIVE) || (cls & NC_SUPPORT)) return;
+  const int X0 = x / F, Y0 = y / F, Z0 = z / F;
+  const int ox = x - F * X0, oy = y - F * Y0, oz = z - F * Z0;
+  const T inv = T(1) / (T)(F * F * F);
+  T s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll
+  for (int A = 0; A < 8; A++) {
+    const int ax = A & 1, ay = (A >> 1) & 1, az = A >> 2;
+    const int wx = ax ? ox : F - ox, wy = ay ? oy : F - oy, wz = az ? oz : F - oz;
+    if (wx == 0 || wy == 0 || wz == 0) continue;
+    const long long nC = C.nidx(X0 + ax, Y0 + ay, Z0 + az);
+    const T w = (T)(wx * wy * wz) * inv;
+    s0 += w * uc[nC]; s1 += w * uc[nC + C.NP]; s2 += w * uc[nC + 2 * C.NP];
+  }
+  uf[n] += s0; uf[n + Fl.NP] += s1; uf[n + 2 * Fl.NP] += s2;
+}
+
+// ---------------------------------------------------------------- Galerkin
+__device__ __forceinline__ double pw(int F, int o, int A) { return A ? (double)o / F : (double)(F - o) / F; }
+
+// first coarsening: one block per coarse element, 288 threads x 2 entries
+__global__ void __launch_bounds__(288) k_galerkin_first(const Level Fl, const Level C, int F,
+                                                        const double* __restrict__ rp, const double* __restrict__ T1,
+                                                        const double* __restrict__ K0g, double* __restrict__ KE) {
+  const long long E = blockIdx.x;
+  const int X = E % C.ex, Y = (E / C.ex) % C.ey, Z = E / ((long long)C.ex * C.ey);
+  const int t = threadIdx.x;
+  double acc[2] = {0, 0};
+  if (C.emask[C.eidx(X, Y, Z)]) {
+    for (int pz = 0; pz < F; pz++)
+      for (int py = 0; py < F; py++)
+        for (int px = 0; px < F; px++) {
+          const int x = X * F + px, y = Y * F + py, z = Z * F + pz;
+          if (x >= Fl.ex || y >= Fl.ey || z >= Fl.ez) continue;
+          const long long e = Fl.eidx(x, y, z);
+          if (!Fl.emask[e]) continue;
+          const double r = rp[e];
+          unsigned fixmask = 0;
+#pragma unroll
+          for (int a = 0; a < 8; a++)
+            if (Fl.vclass[Fl.nidx(x + (a & 1), y + ((a >> 1) & 1), z + (a >> 2))] & NC_SUPPORT) fixmask |= 1u << a;
+          const int pos = px + F * (py + F * pz);
+          if (!fixmask) {
+            acc[0] += r * T1[(long long)pos * 576 + t];
+            acc[1] += r * T1[(long long)pos * 576 + t + 288];
+          } else {
+            for (int h2 = 0; h2 < 2; h2++) {
+              const int ent = t + 288 * h2;
+              const int row = ent / 24, col = ent % 24;
+              const int A = row / 3, i = row % 3, B = col / 3, j = col % 3;
+              double s = 0;
+              for (int a = 0; a < 8; a++) {
+                const double wa = pw(F, px + (a & 1), A & 1) * pw(F, py + ((a >> 1) & 1), (A >> 1) & 1) *
+                                  pw(F, pz + (a >> 2), A >> 2);
+                if (wa == 0) continue;
+                for (int b = 0; b < 8; b++) {
+                  const double wb = pw(F, px + (b & 1), B & 1) * pw(F, py + ((b >> 1) & 1), (B >> 1) & 1) *
+                                    pw(F, pz + (b >> 2), B >> 2);
+                  if (wb == 0) continue;
+                  double kv;
+                  if ((fixmask >> a & 1u) || (fixmask >> b & 1u)) kv = (a == b && i == j) ? DIRICHLET_W : 0.0;
+                  else kv = r * K0g[(a * 3 + i) * 24 + b * 3 + j];
+                  s += wa * wb * kv;
+                }
+              }
+              acc[h2] += s;
+            }
+          }
+        }
+  }
+  KE[E * 576 + t] = acc[0];
+  KE[E * 576 + t + 288] = acc[1];
+}
+
+// dyadic recursion on element matrices
+__global__ void __launch_bounds__(288) k_galerkin_next(const Level Fl, const Level C, const double* __restrict__ KEf,
+                                                       double* __restrict__ KEc) {
+  __shared__ double K[576];
+  __shared__ double Tm[576];
+  const long long E = blockIdx.x;
+  const int X = E % C.ex, Y = (E / C.ex) % C.ey, Z = E / ((long long)C.ex * C.ey);
+  const int t = threadIdx.x;
+  double acc[2] = {0, 0};
+  if (C.emask[C.eidx(X, Y, Z)]) {
+    for (int c = 0; c < 8; c++) {
+      const int px = c & 1, py = (c >> 1) & 1, pz = c >> 2;
+      const int x = 2 * X + px, y = 2 * Y + py, z = 2 * Z + pz;
+      if (x >= Fl.ex || y >= Fl.ey || z >= Fl.ez) continue;
+      if (!Fl.emask[Fl.eidx(x, y, z)]) continue;
+      const long long ef = x + (long long)Fl.ex * (y + (long long)Fl.ey * z);
+      __syncthreads();
+      K[t] = KEf[ef * 576 + t];
+      K[t + 288] = KEf[ef * 576 + t + 288];
+      __syncthreads();
+      // Tm[(a,i),(B,j)] = sum_b K[(a,i),(b,j)] P[b][B]
+      for (int h2 = 0; h2 < 2; h2++) {
+        const int ent = t + 288 * h2;
+        const int row = ent / 24, col = ent % 24, B = col / 3, j = col % 3;
+        double s = 0;
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+          const double wb = pw(2, px + (b & 1), B & 1) * pw(2, py + ((b >> 1) & 1), (B >> 1) & 1) *
+                            pw(2, pz + (b >> 2), B >> 2);
+          s += K[row * 24 + b * 3 + j] * wb;
+        }
+        Tm[ent] = s;
+      }
+      __syncthreads();
+      for (int h2 = 0; h2 < 2; h2++) {
+        const int ent = t + 288 * h2;
+        const int row = ent / 24, col = ent % 24, A = row / 3, i = row % 3;
+        double s = 0;
+#pragma unroll
+        for (int a = 0; a < 8; a++) {
+          const double wa = pw(2, px + (a & 1), A & 1) * pw(2, py + ((a >> 1) & 1), (A >> 1) & 1) *
+                            pw(2, pz + (a >> 2), A >> 2);
+          s += wa * Tm[(a * 3 + i) * 24 + col];
+        }
+        acc[h2] += s;
+      }
+    }
+  }
+  KEc[E * 576 + t] = acc[0];
+  KEc[E * 576 + t + 288] = acc[1];
+}
+
+// stencil assembly from element matrices: one thread per (node, neighbour d),
+// summing the 3x3 blocks of the incident elements that contain both nodes
+__global__ void k_assemble(const Level C, const double* __restrict__ KE, double* __restrict__ st64,
+                           float* __restrict__ st32) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= 27 * C.nn) return;
+  const int d = t / C.nn;
+  const long long nl = t % C.nn;
+  const int x = nl % C.nx, y = (nl / C.nx) % C.ny, z = nl / ((long long)C.nx * C.ny);
+  const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
+  const long long NP = C.NP;
+  const long long n = C.nidx(x, y, z);
+  double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int k = 0; k < 8; k++) {
+    const int kx = k & 1, ky = (k >> 1) & 1, kz = k >> 2;
+    if (!((dx == kx - 1 || dx == kx) && (dy == ky - 1 || dy == ky) && (dz == kz - 1 || dz == kz))) continue;
+    const int ex = x - 1 + kx, ey = y - 1 + ky, ez = z - 1 + kz;
+    if (!C.emask[C.eidx(ex, ey, ez)]) continue;
+    const long long E = ex + (long long)C.ex * (ey + (long long)C.ey * ez);
+    const int a = 7 - k;
+    const int b = (dx - kx + 1) + 2 * (dy - ky + 1) + 4 * (dz - kz + 1);
+    const double* K = KE + E * 576;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) s[r * 3 + c] += K[(a * 3 + r) * 24 + b * 3 + c];
+  }
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    st64[(d * 9 + i) * NP + n] = s[i];
+    st32[(d * 9 + i) * NP + n] = (float)s[i];
+  }
+}
+
+// ---------------------------------------------------------------- coarsest dense solve
+__global__ void k_coarse_dense(const Level C, const double* __restrict__ st, const int* __restrict__ cnodes,
+                               const int* __restrict__ crow, int nc, double* __restrict__ K) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long tot = (long long)nc * 243;
+  if (t >= tot) return;
+  const int i = t / 243, rem = t % 243, d = rem / 9, r = (rem % 9) / 3, c = rem % 3;
+  const long long n = cnodes[i];
+  const long long nb = n + (d % 3 - 1) + (d / 3 % 3 - 1) * (long long)C.px + (d / 9 - 1) * (long long)C.px * C.py;
+  const int j = crow[nb];
+  if (j < 0) return;
+  const int N = 3 * nc;
+  K[(long long)(3 * i + r) * N + 3 * j + c] = st[(long long)(d * 9 + r * 3 + c) * C.NP + n];
+}
+
+// in-place Cholesky (lower) in a single block; flag != 0 on a non-positive pivot
+__global__ void __launch_bounds__(1024) k_cholesky(double* A, int N, int* flag) {
+  // symmetrise first
+  for (long long idx = threadIdx.x; idx < (long long)N * N; idx += blockDim.x) {
+    const int i = idx / N, j = idx % N;
+    if (j > i) {
+      const double v = 0.5 * (A[(long long)i * N + j] + A[(long long)j * N + i]);
+      A[(long long)i * N + j] = v;
+      A[(long long)j * N + i] = v;
+    }
+  }
+  __syncthreads();
+  __shared__ double dsh;
+  for (int j = 0; j < N; j++) {
+    if (threadIdx.x == 0) {
+      double s = A[(long long)j * N + j];
+      if (!(s > 0)) { *flag = 1; s = 1e-300; }
+      s = sqrt(s);
+      A[(long long)j * N + j] = s;
+      dsh = s;
+    }
+    __syncthreads();
+    const double d = dsh;
+    for (int i = j + 1 + threadIdx.x; i < N; i += blockDim.x) A[(long long)i * N + j] /= d;
+    __syncthreads();
+    const int m = N - j - 1;
+    for (long long idx = threadIdx.x; idx < (long long)m * m; idx += blockDim.x) {
+      const int i = j + 1 + idx / m, k = j + 1 + idx % m;
+      if (k <= i) A[(long long)i * N + k] -= A[(long long)i * N + j] * A[(long long)k * N + j];
+    }
+    __syncthreads();
+  }
+}
+
+// X = (L L^T)^-1, one column per thread
+__global__ void k_chol_inverse(const double* __restrict__ Lc, int N, double* __restrict__ X) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= N) return;
+  for (int i = 0; i < N; i++) {
+    double t = (i == col) ? 1.0 : 0.0;
+    for (int k = 0; k < i; k++) t -= Lc[(long long)i * N + k] * X[(long long)k * N + col];
+    X[(long long)i * N + col] = t / Lc[(long long)i * N + i];
+  }
+  for (int i = N - 1; i >= 0; i--) {
+    double t = X[(long long)i * N + col];
+    for (int k = i + 1; k < N; k++) t -= Lc[(long long)k * N + i] * X[(long long)k * N + col];
+    X[(long long)i * N + col] = t / Lc[(long long)i * N + i];
+  }
+}
+
+template <typename T>
+__global__ void k_gather_coarse(const Level C, const T* __restrict__ f, const int* __restrict__ cnodes, int nc,
+                                double* __restrict__ b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nc) return;
+  const long long n = cnodes[i];
+  b[3 * i + 0] = (double)f[n];
+  b[3 * i + 1] = (double)f[n + C.NP];
+  b[3 * i + 2] = (double)f[n + 2 * C.NP];
+}
+
+// u = Kinv b, one warp per row; result scattered to the padded coarsest vector
+template <typename T>
+__global__ void k_gemv_scatter(const Level C, const double* __restrict__ Kinv, const double* __restrict__ b, int nc,
+                               const int* __restrict__ cnodes, T* __restrict__ u) {
+  const int N = 3 * nc;
+  const int row = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (row >= N) return;
+  double s = 0;
+  for (int j = lane; j < N; j += 32) s += Kinv[(long long)row * N + j] * b[j];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) u[cnodes[row / 3] + (row % 3) * C.NP] = (T)s;
+}
+
+// ---------------------------------------------------------------- host wrappers
+static inline dim3 node_grid(const Level& l) { return dim3(cdiv(l.nx, 32), cdiv(l.ny, 8), l.nz); }
+
+template <typename T>
+static const T* stencil_of(const Level& l);
+template <>
+const double* stencil_of<double>(const Level& l) { return l.st64; }
+template <>
+const float* stencil_of<float>(const Level& l) { return l.st32; }
+
+template <typename T>
+rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* r) {
+  const Level& l = h->L[level];
+  if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
+  k_coarse<T, 0><<<node_grid(l), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0)); rso::note_launch();
+  if (h->prof_on) prof_end(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64));
+  return launch_check(h, "coarse_residual");
+}
+template <typename T>
+rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T* u_out, double omega) {
+  const Level& l = h->L[level];
+  if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
+  k_coarse<T, 2><<<node_grid(l), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega); rso::note_launch();
+  if (h->prof_on) prof_end(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64));
+  return launch_check(h, "coarse_jacobi");
+}
+template <typename T>
+rso_status coarse_gs(rso_handle* h, int level, T* u, const T* f, int colour, int reverse) {
+  const Level& l = h->L[level];
+  int cx = colour & 1, cy = (colour >> 1) & 1, cz = colour >> 2;
+  dim3 g(cdiv((l.nx - cx + 1) / 2, 32), cdiv((l.ny - cy + 1) / 2, 8), (l.nz - cz + 1) / 2);
+  if (g.x == 0 || g.y == 0 || g.z == 0) return RSO_OK;
+  if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn / 8);
+  k_coarse_gs<T><<<g, dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, cx, cy, cz, reverse); rso::note_launch();
+  if (h->prof_on) prof_end(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64));
+  return launch_check(h, "coarse_gs");
+}
+template <typename T>
+rso_status restrict_(rso_handle* h, int cl, const T* rf, T* fc) {
+  const Level& c = h->L[cl];
+  k_restrict<T><<<node_grid(c), dim3(32, 8), 0, h->stream>>>(h->L[cl - 1], c, c.factor, rf, fc); rso::note_launch();
+  return launch_check(h, "restrict");
+}
+template <typename T>
+rso_status prolong(rso_handle* h, int cl, const T* uc, T* uf) {
+  const Level& f = h->L[cl - 1];
+  k_prolong<T><<<node_grid(f), dim3(32, 8), 0, h->stream>>>(f, h->L[cl], h->L[cl].factor, uc, uf); rso::note_launch();
+  return launch_check(h, "prolong");
+}
+template <typename T>
+rso_status coarsest_solve(rso_handle* h, const T* f, T* u) {
+  const Level& c = h->L.back();
+  if (h->nc == 0) return RSO_OK;
+  k_gather_coarse<T><<<cdiv(h->nc, 128), 128, 0, h->stream>>>(c, f, h->c_nodes, h->nc, h->c_f); rso::note_launch();
+  const int N = 3 * h->nc;
+  k_gemv_scatter<T><<<cdiv(N, 8), 256, 0, h->stream>>>(c, h->c_K + (size_t)N * N, h->c_f, h->nc, h->c_nodes, u); rso::note_launch();
+  return launch_check(h, "coarsest_solve");
+}
+
+rso_status galerkin(rso_handle* h) {
+  for (size_t li = 1; li < h->L.size(); li++) {
+    Level& c = h->L[li];
+    const Level& f = h->L[li - 1];
+    if (li == 1)
+      k_galerkin_first<<<(unsigned)c.ne, 288, 0, h->stream>>>(f, c, c.factor, h->rp64, h->T1, h->K0_dev, c.KE);
+    else
+      k_galerkin_next<<<(unsigned)c.ne, 288, 0, h->stream>>>(f, c, f.KE, c.KE);
+    rso::note_launch();
+    RSO_TRY(launch_check(h, "galerkin"));
+    k_assemble<<<cdiv(27 * c.nn, 256), 256, 0, h->stream>>>(c, c.KE, c.st64, c.st32); rso::note_launch();
+    RSO_TRY(launch_check(h, "assemble"));
+  }
+  return RSO_OK;
+}
+
+rso_status coarsest_factor(rso_handle* h) {
+  if (h->L.size() < 2 || h->nc == 0) return RSO_OK;
+  const Level& c = h->L.back();
+  const int N = 3 * h->nc;
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(h->c_K, 0, sizeof(double) * (size_t)N * N, h->stream));
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(h->c_flag, 0, sizeof(int), h->stream));
+  // crow map lives right after the c_nodes list (see capi set-up)
+  k_coarse_dense<<<cdiv((long long)h->nc * 243, 256), 256, 0, h->stream>>>(c, c.st64, h->c_nodes,
+                                                                           h->c_nodes + h->nc, h->nc, h->c_K); rso::note_launch();
+  k_cholesky<<<1, 1024, 0, h->stream>>>(h->c_K, N, h->c_flag); rso::note_launch();
+  k_chol_inverse<<<cdiv(N, 64), 64, 0, h->stream>>>(h->c_K, N, h->c_K + (size_t)N * N); rso::note_launch();
+  RSO_TRY(launch_check(h, "coarsest_factor"));
+  int flag = 0;
+  RSO_CHECK_CUDA(h, cudaMemcpyAsync(&flag, h->c_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (flag) {
+    h->err = "coarsest operator is not positive definite (a support-free mode needs the pseudo-inverse path)";
+    return RSO_ERR_UNSUPPORTED;
+  }
+  return RSO_OK;
+}
+
+// lambda_max(D^-1 K) per level: power iteration on the Jacobi operator
+__global__ void k_seed_vec(double* v, long long n, uint64_t seed) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) v[i] = rso_urand(seed, (uint64_t)i);
+}
+__global__ void k_sub_scale(const double* u, const double* v, double* w, long long n, const double* nrm) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) w[i] = (u[i] - v[i]);
+}
+
+rso_status estimate_lambda(rso_handle* h) {
+  const int iters = 12;
+  for (size_t li = 0; li + 1 < h->L.size() || (li == 0 && h->L.size() == 1); li++) {
+    Level& l = h->L[li];
+    const long long n3 = 3 * l.NP;
+    k_seed_vec<<<cdiv(n3, 256), 256, 0, h->stream>>>(l.u64, n3, 777 + li); rso::note_launch();
+    if (li == 0) RSO_TRY(zero_support(h, l.u64));
+    RSO_CHECK_CUDA(h, cudaMemsetAsync(l.f64, 0, sizeof(double) * n3, h->stream));
+    double lam = 1.0;
+    for (int it = 0; it < iters; it++) {
+      // t = u - D^-1 K u  ->  r = D^-1 K u
+      if (li == 0) RSO_TRY(fine_jacobi<double>(h, l.u64, l.f64, l.t64, h->rp64, 1.0));
+      else RSO_TRY(coarse_jacobi<double>(h, (int)li, l.u64, l.f64, l.t64, 1.0));
+      k_sub_scale<<<cdiv(n3, 256), 256, 0, h->stream>>>(l.u64, l.t64, l.r64, n3, nullptr); rso::note_launch();
+      double nu = 0, nw = 0;
+      RSO_TRY(dot_host(h, l.u64, l.u64, n3, &nu));
+      RSO_TRY(dot_host(h, l.r64, l.r64, n3, &nw));
+      lam = std::sqrt(nw / nu);
+      RSO_CHECK_CUDA(h, cudaMemcpyAsync(l.u64, l.r64, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    l.lam = 1.05 * lam;
+    if (h->L.size() == 1) break;
+  }
+  return RSO_OK;
+}
+
+template rso_status coarse_residual<double>(rso_handle*, int, const double*, const double*, double*);
+template rso_status coarse_residual<float>(rso_handle*, int, const float*, const float*, float*);
+template rso_status coarse_jacobi<double>(rso_handle*, int, const double*, const double*, double*, double);
+template rso_status coarse_jacobi<float>(rso_handle*, int, const float*, const float*, float*, double);
+template rso_status coarse_gs<double>(rso_handle*, int, double*, const double*, int, int);
+template rso_status coarse_gs<float>(rso_handle*, int, float*, const float*, int, int);
+template rso_status restrict_<double>(rso_handle*, int, const double*, double*);
+template rso_status restrict_<float>(rso_handle*, int, const float*, float*);
+template rso_status prolong<double>(rso_handle*, int, const double*, double*);
+template rso_status prolong<float>(rso_handle*, int, const float*, float*);
+template rso_status coarsest_solve<double>(rso_handle*, const double*, double*);
+template rso_status coarsest_solve<float>(rso_handle*, const float*, float*);
+
+}  // namespace rso

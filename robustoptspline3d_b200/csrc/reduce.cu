@@ -1,0 +1,171 @@
+// FP64 reductions (warp-shuffle trees, deterministic two-pass), layout
+// conversions between the public dense layout and the padded device layout,
+// and small elementwise helpers.
+#include "rso_internal.cuh"
+
+namespace rso {
+
+constexpr int RED_BLOCKS = 592;  // 4 x 148 SMs
+constexpr int RED_THREADS = 512;
+
+rso_status launch_check(rso_handle* h, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    h->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return RSO_ERR_CUDA;
+  }
+  return RSO_OK;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double ws[32];
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  v = (threadIdx.x < blockDim.x / 32) ? ws[lane] : 0.0;
+  if (w == 0) v = warp_sum(v);
+  __syncthreads();
+  return v;
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_dot_partial(const double* __restrict__ a, const double* __restrict__ b,
+                                                             long long n, double* __restrict__ part) {
+  double s = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s += a[i] * b[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_sumf_partial(const float* __restrict__ a, long long n,
+                                                              double* __restrict__ part) {
+  double s = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s += (double)a[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_final(const double* __restrict__ part, int np, double* out) {
+  double s = 0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) s += part[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) *out = s;
+}
+
+rso_status dot(rso_handle* h, const double* a, const double* b, long long n, double* dev_out) {
+  k_dot_partial<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(a, b, n, h->red); rso::note_launch();
+  k_final<<<1, RED_THREADS, 0, h->stream>>>(h->red, RED_BLOCKS, dev_out); rso::note_launch();
+  return launch_check(h, "dot");
+}
+
+rso_status dot_host(rso_handle* h, const double* a, const double* b, long long n, double* out) {
+  RSO_TRY(dot(h, a, b, n, h->scal + 15));
+  RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->h_scal + 15, h->scal + 15, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  *out = h->h_scal[15];
+  return RSO_OK;
+}
+
+rso_status sum_float(rso_handle* h, const float* a, long long n, double* dev_out) {
+  k_sumf_partial<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(a, n, h->red); rso::note_launch();
+  k_final<<<1, RED_THREADS, 0, h->stream>>>(h->red, RED_BLOCKS, dev_out); rso::note_launch();
+  return launch_check(h, "sum_float");
+}
+
+// ---------------------------------------------------------------- layouts
+__global__ void k_pad_nodes(Level L, const double* __restrict__ dense, double* __restrict__ pad, int to_pad) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= L.nn) return;
+  int x = i % L.nx, y = (i / L.nx) % L.ny, z = i / ((long long)L.nx * L.ny);
+  long long j = L.nidx(x, y, z);
+  for (int c = 0; c < 3; c++) {
+    if (to_pad) pad[j + c * L.NP] = dense[i + c * L.nn];
+    else pad[i + c * L.nn] = dense[j + c * L.NP];  // 'dense' is the padded source here
+  }
+}
+
+rso_status pad_nodes(rso_handle* h, int level, const double* dense, double* padded) {
+  const Level& l = h->L[level];
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(padded, 0, sizeof(double) * 3 * l.NP, h->stream));
+  k_pad_nodes<<<cdiv(l.nn, 256), 256, 0, h->stream>>>(l, dense, padded, 1); rso::note_launch();
+  return launch_check(h, "pad_nodes");
+}
+
+rso_status unpad_nodes(rso_handle* h, int level, const double* padded, double* dense) {
+  const Level& l = h->L[level];
+  k_pad_nodes<<<cdiv(l.nn, 256), 256, 0, h->stream>>>(l, padded, dense, 0); rso::note_launch();
+  return launch_check(h, "unpad_nodes");
+}
+
+__global__ void k_pad_elems(Level L, const float* __restrict__ src, float* __restrict__ dst, int to_pad) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= L.ne) return;
+  int x = i % L.ex, y = (i / L.ex) % L.ey, z = i / ((long long)L.ex * L.ey);
+  long long j = L.eidx(x, y, z);
+  if (to_pad) dst[j] = L.emask[j] ? src[i] : 0.f;
+  else dst[i] = L.emask[j] ? src[j] : 0.f;
+}
+
+rso_status pad_elems_f(rso_handle* h, const float* dense, float* padded) {
+  const Level& l = h->L[0];
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(padded, 0, sizeof(float) * l.NQ, h->stream));
+  k_pad_elems<<<cdiv(l.ne, 256), 256, 0, h->stream>>>(l, dense, padded, 1); rso::note_launch();
+  return launch_check(h, "pad_elems");
+}
+
+rso_status unpad_elems_f(rso_handle* h, const float* padded, float* dense) {
+  const Level& l = h->L[0];
+  k_pad_elems<<<cdiv(l.ne, 256), 256, 0, h->stream>>>(l, padded, dense, 0); rso::note_launch();
+  return launch_check(h, "unpad_elems");
+}
+
+// zero the support DOFs (and inactive nodes) of a padded fine vector
+__global__ void k_zero_support(Level L, double* v) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= L.NP) return;
+  uint8_t c = L.vclass[i];
+  if (!(c & NC_ACTIVE) || (c & NC_SUPPORT)) { v[i] = 0; v[i + L.NP] = 0; v[i + 2 * L.NP] = 0; }
+}
+
+rso_status zero_support(rso_handle* h, double* padded) {
+  const Level& l = h->L[0];
+  k_zero_support<<<cdiv(l.NP, 256), 256, 0, h->stream>>>(l, padded); rso::note_launch();
+  return launch_check(h, "zero_support");
+}
+
+// ---------------------------------------------------------------- elementwise
+__global__ void k_axpby(long long n, double a, const double* __restrict__ x, double b, double* __restrict__ y) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) y[i] = a * x[i] + b * y[i];
+}
+rso_status axpby(rso_handle* h, long long n, double a, const double* x, double b, double* y) {
+  k_axpby<<<cdiv(n, 256), 256, 0, h->stream>>>(n, a, x, b, y); rso::note_launch();
+  return launch_check(h, "axpby");
+}
+
+__global__ void k_fill_d(double* p, long long n, double v) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+__global__ void k_fill_f(float* p, long long n, float v) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+rso_status fill_d(rso_handle* h, double* p, long long n, double v) {
+  k_fill_d<<<cdiv(n, 256), 256, 0, h->stream>>>(p, n, v); rso::note_launch();
+  return launch_check(h, "fill_d");
+}
+rso_status fill_f(rso_handle* h, float* p, long long n, float v) {
+  k_fill_f<<<cdiv(n, 256), 256, 0, h->stream>>>(p, n, v); rso::note_launch();
+  return launch_check(h, "fill_f");
+}
+
+}  // namespace rso

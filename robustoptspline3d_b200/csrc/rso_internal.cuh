@@ -1,0 +1,247 @@
+// Internal definitions of the B200 voxel-FEM library (librso).
+//
+// Device data layout ("padded box"): every level stores its nodes on a box
+// padded by one zero node on each side, x fastest, the padded x extent
+// rounded up to a multiple of 4 so that rows stay 32-byte aligned:
+//   node (x,y,z), x in [-1, nx] -> (x+1) + px*((y+1) + py*(z+1))
+// Element fields use the same scheme with their own extents.  Halo entries
+// are zero, so the matrix-free operator needs no bounds tests, and a padded
+// element with zero density contributes nothing.  Nodal vectors are three
+// consecutive component planes of NP entries each.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "../../include/rso.h"
+
+namespace rso {
+
+enum : uint8_t { NC_ACTIVE = 1, NC_SURFACE = 2, NC_SUPPORT = 4, NC_LOAD = 8 };
+
+struct Level {
+  int ex = 0, ey = 0, ez = 0;     // element extents
+  int nx = 0, ny = 0, nz = 0;     // node extents
+  int px = 0, py = 0, pz = 0;     // padded node extents
+  int qx = 0, qy = 0, qz = 0;     // padded element extents
+  long long NP = 0, NQ = 0;       // padded node / element counts
+  long long nn = 0, ne = 0;       // unpadded counts
+  int factor = 0;                 // coarsening factor from the finer level
+  long long n_active_e = 0, n_active_v = 0;
+  std::vector<uint8_t> h_emask, h_vmask;   // host copies (unpadded), set-up only
+  uint8_t* emask = nullptr;       // padded element mask
+  uint8_t* vclass = nullptr;      // padded node class
+  double* KE = nullptr;           // coarse element matrices, 576 per unpadded element
+  double* st64 = nullptr;         // stencil [243][NP]
+  float* st32 = nullptr;
+  double *u64 = nullptr, *f64 = nullptr, *r64 = nullptr, *t64 = nullptr;
+  float *u32 = nullptr, *f32 = nullptr, *r32 = nullptr, *t32 = nullptr;
+  double lam = 1.0;               // lambda_max(D^-1 K) estimate
+  __host__ __device__ long long nidx(int x, int y, int z) const {
+    return (long long)(x + 1) + (long long)px * ((y + 1) + (long long)py * (z + 1));
+  }
+  __host__ __device__ long long eidx(int x, int y, int z) const {
+    return (long long)(x + 1) + (long long)qx * ((y + 1) + (long long)qy * (z + 1));
+  }
+};
+
+struct Spline {
+  int order = 0, part[3] = {0, 0, 0}, nb[3] = {0, 0, 0};
+  float bmin[3], bmax[3], step[3];
+  std::vector<float> knots[3];
+  std::vector<int> h_idx[3];
+  std::vector<double> h_N[3], h_dN[3];
+  int* idx[3] = {nullptr, nullptr, nullptr};       // per element coordinate, -1 outside
+  double* N[3] = {nullptr, nullptr, nullptr};      // order values per coordinate
+  double* dN[3] = {nullptr, nullptr, nullptr};
+  long long n_coeff = 0;
+  float* knots_dev = nullptr;                      // the three knot vectors back to back
+  int* ranges[3] = {nullptr, nullptr, nullptr};    // per basis index: first/last element coordinate in its support
+  double* work[10] = {};                           // adjoint and self-support scratch
+};
+
+}  // namespace rso
+
+struct rso_handle {
+  rso_config cfg;
+  std::string err;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+  std::vector<rso::Level> L;
+  double K0[576];
+  double* K0_dev = nullptr;
+  // fine-level design fields (padded elements)
+  float* rho = nullptr;
+  float* rp32 = nullptr;
+  double* rp64 = nullptr;
+  bool operators_ready = false;
+  // load nodes
+  std::vector<int> h_load_nodes;      // dense node ids, reference order
+  int n_load = 0;
+  int* load_nodes = nullptr;          // padded node ids
+  double* load_normals = nullptr;     // 3 per load node
+  // Galerkin tables
+  double* T1 = nullptr;               // F^3 x 576 table for the first coarsening
+  // coarsest dense solve
+  int nc = 0;                         // active coarsest nodes
+  int* c_nodes = nullptr;             // padded node ids of active coarsest nodes
+  double* c_K = nullptr;              // N x N workspace / inverse
+  double* c_f = nullptr;
+  int* c_flag = nullptr;              // factorisation status
+  // reductions
+  double* red = nullptr;              // partials
+  double* scal = nullptr;             // device scalars
+  double* h_scal = nullptr;           // pinned host mirror
+  // PCG / solver vectors (fine, FP64, padded)
+  double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *w = nullptr;
+  // public-layout staging
+  double* stage_a = nullptr;
+  double* stage_b = nullptr;
+  // spline
+  rso::Spline sp;
+  // worst case storage
+  std::vector<double*> lanczos_u;
+  long long n_gs_elements = 0;
+  // design-iteration scratch
+  float *e_a = nullptr, *e_b = nullptr, *e_c = nullptr, *e_d = nullptr, *e_rhohat = nullptr;
+  double *coef_a = nullptr, *coef_b = nullptr, *coef_c = nullptr;
+  double *coef_df = nullptr, *coef_dg = nullptr;   // MMA inputs
+  double *fw = nullptr, *uw = nullptr;             // worst-case force / displacement (padded)
+  int prof_on = 0;                                 // per-kernel event timing (prof.cu)
+  void* prof = nullptr;
+};
+
+namespace rso {
+// launch accounting and profiling (prof.cu)
+enum ProfClass {
+  PC_FINE_JAC32, PC_FINE_RES32, PC_FINE_GS32, PC_FINE_APPLYK64, PC_FINE_RES64, PC_FINE_JAC64, PC_FINE_GS64,
+  PC_COARSE32, PC_COARSE64, PC_N
+};
+void note_launch();
+void prof_begin(rso_handle* h, int cls, double nodes);
+void prof_end(rso_handle* h, int cls);
+void prof_free(rso_handle* h);
+}  // namespace rso
+
+// ---------------------------------------------------------------- helpers
+#define RSO_CHECK_CUDA(h, call)                                                          \
+  do {                                                                                   \
+    cudaError_t _e = (call);                                                             \
+    if (_e != cudaSuccess) {                                                             \
+      (h)->err = std::string(#call) + ": " + cudaGetErrorString(_e);                      \
+      return RSO_ERR_CUDA;                                                               \
+    }                                                                                    \
+  } while (0)
+
+#define RSO_TRY(call)                 \
+  do {                                \
+    rso_status _s = (call);           \
+    if (_s != RSO_OK) return _s;      \
+  } while (0)
+
+namespace rso {
+
+inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+rso_status launch_check(rso_handle* h, const char* what);
+
+// reductions (reduce.cu)
+rso_status dot(rso_handle* h, const double* a, const double* b, long long n, double* dev_out);
+rso_status dot_host(rso_handle* h, const double* a, const double* b, long long n, double* out);
+rso_status sum_float(rso_handle* h, const float* a, long long n, double* dev_out);
+
+// conversion between the public dense layout and padded layout
+rso_status pad_nodes(rso_handle* h, int level, const double* dense, double* padded);
+rso_status unpad_nodes(rso_handle* h, int level, const double* padded, double* dense);
+rso_status pad_elems_f(rso_handle* h, const float* dense, float* padded);
+rso_status unpad_elems_f(rso_handle* h, const float* padded, float* dense);
+rso_status zero_support(rso_handle* h, double* padded);
+
+// topology (topology.cu)
+Level make_level(int ex, int ey, int ez, int factor);
+rso_status build_topology(rso_handle* h, const uint8_t* emask, const uint8_t* fixed_area,
+                          const uint8_t* load_area, const double* load_normals);
+
+// fine operator (fine_op.cu)
+template <typename T>
+rso_status fine_residual(rso_handle* h, const T* u, const T* f, T* r, const T* rp);
+template <typename T>
+rso_status fine_applyK(rso_handle* h, const T* u, T* f, const T* rp);
+template <typename T>
+rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega);
+template <typename T>
+rso_status fine_gs(rso_handle* h, T* u, const T* f, const T* rp, int colour, int reverse);
+rso_status upload_K0(rso_handle* h);
+rso_status penalise(rso_handle* h);
+
+// coarse levels (coarse_op.cu)
+template <typename T>
+rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* r);
+template <typename T>
+rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T* u_out, double omega);
+template <typename T>
+rso_status coarse_gs(rso_handle* h, int level, T* u, const T* f, int colour, int reverse);
+template <typename T>
+rso_status restrict_(rso_handle* h, int coarse_level, const T* rf, T* fc);
+template <typename T>
+rso_status prolong(rso_handle* h, int coarse_level, const T* uc, T* uf);
+template <typename T>
+rso_status coarsest_solve(rso_handle* h, const T* f, T* u);
+rso_status galerkin(rso_handle* h);
+rso_status coarsest_factor(rso_handle* h);
+rso_status estimate_lambda(rso_handle* h);
+
+// solver (solver.cu)
+template <typename T>
+rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric);
+rso_status precondition(rso_handle* h, const double* r, double* z);
+rso_status solve_pcg(rso_handle* h, const double* f, double* u, double tol, int max_iter, rso_solve_info* info);
+rso_status solve_vcycles(rso_handle* h, const double* f, double* u, double tol, int max_iter,
+                         rso_solve_info* info);
+rso_status vcycle_fp64(rso_handle* h, double* u, const double* f, int pre, int post, int symmetric,
+                       double* rel_res);
+
+// elementwise kernels shared by several files
+rso_status axpby(rso_handle* h, long long n, double a, const double* x, double b, double* y);
+rso_status fill_d(rso_handle* h, double* p, long long n, double v);
+rso_status fill_f(rso_handle* h, float* p, long long n, float v);
+
+// design (design.cu)
+rso_status sensitivity(rso_handle* h, const double* u_pad, float* sens_pad, int energy);
+rso_status heaviside(rso_handle* h, const float* in_pad, double beta, const uint8_t* shell_pad, float* out_pad);
+rso_status heaviside_chain(rso_handle* h, const float* rho_pad, double beta, const float* gin, float* gout);
+rso_status filter(rso_handle* h, double radius, const float* in_pad, float* out_pad, int adjoint);
+rso_status coeff2density(rso_handle* h, const double* c, const uint8_t* shell_pad, float* out_pad);
+rso_status density2coeff(rso_handle* h, const float* g_pad, const uint8_t* shell_pad, double* dc);
+rso_status selfsupport(rso_handle* h, const double* c, double beta, int mode, double opt_angle,
+                       double default_angle, float* per_pad, double* dc, double* value, double* count,
+                       double* dirsum);
+rso_status volume(rso_handle* h, const float* rho_pad, double* vol);
+rso_status spline_setup(rso_handle* h, int order, int px, int py, int pz);
+
+// worst case (worst.cu)
+rso_status force_project(rso_handle* h, double* f_pad, int cf);
+rso_status worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t seed, double* f_pad,
+                      double* u_pad, double* lambda, double* ritz, int* iters);
+rso_status modified_pm(rso_handle* h, int cf, uint64_t seed, int max_itn, double* f_pad, double* u_pad,
+                       double* c_worst, int* itn);
+
+// MMA state accessors (mma.cu)
+double* mma_x(rso_mma* s);
+int mma_n(rso_mma* s);
+int mma_m(rso_mma* s);
+
+}  // namespace rso
+
+// deterministic uniform [-1,1) stream shared with the oracle
+__host__ __device__ inline uint64_t rso_splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+__host__ __device__ inline double rso_urand(uint64_t seed, uint64_t i) {
+  uint64_t h = rso_splitmix64(seed * 0x100000001B3ull ^ rso_splitmix64(i));
+  return (double)(h >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+}

@@ -1,0 +1,221 @@
+// Multigrid V-cycle (templated on the arithmetic type), the FP64 outer
+// iterations (defect correction and V-cycle preconditioned CG) and the
+// reference-sequenced V-cycle on a caller vector.
+//
+// HierarchyGrid::v_cycle (grid/Grid.cpp:2431-2476): down-sweep computes the
+// finer residual, restricts it, zeroes u and pre-smooths; the coarsest level
+// is solved directly; the up-sweep prolongates and post-smooths.  In mixed
+// precision the V-cycle runs in FP32 on FP32 copies of rho^p and of the
+// coarse stencils, while the outer residual, the CG vectors and scalars and
+// the coarsest solve stay FP64.
+#include "rso_internal.cuh"
+#include <cmath>
+#include <utility>
+
+namespace rso {
+
+template <typename T>
+struct LV;
+template <>
+struct LV<double> {
+  static double*& u(Level& l) { return l.u64; }
+  static double*& f(Level& l) { return l.f64; }
+  static double*& r(Level& l) { return l.r64; }
+  static double*& t(Level& l) { return l.t64; }
+  static const double* rp(rso_handle* h) { return h->rp64; }
+};
+template <>
+struct LV<float> {
+  static float*& u(Level& l) { return l.u32; }
+  static float*& f(Level& l) { return l.f32; }
+  static float*& r(Level& l) { return l.r32; }
+  static float*& t(Level& l) { return l.t32; }
+  static const float* rp(rso_handle* h) { return h->rp32; }
+};
+
+template <typename T>
+static rso_status smooth(rso_handle* h, int li, int sweeps, int reverse) {
+  Level& l = h->L[li];
+  if (h->cfg.smoother == RSO_SMOOTH_GS) {
+    for (int s = 0; s < sweeps; s++)
+      for (int ci = 0; ci < 8; ci++) {
+        const int c = reverse ? 7 - ci : ci;
+        if (li == 0) RSO_TRY(fine_gs<T>(h, LV<T>::u(l), LV<T>::f(l), LV<T>::rp(h), c, reverse));
+        else RSO_TRY(coarse_gs<T>(h, li, LV<T>::u(l), LV<T>::f(l), c, reverse));
+      }
+  } else {
+    const double om = h->cfg.omega * 2.0 / l.lam;
+    for (int s = 0; s < sweeps; s++) {
+      if (li == 0) RSO_TRY(fine_jacobi<T>(h, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om));
+      else RSO_TRY(coarse_jacobi<T>(h, li, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), om));
+      std::swap(LV<T>::u(l), LV<T>::t(l));
+    }
+  }
+  return RSO_OK;
+}
+
+template <typename T>
+static rso_status level_residual(rso_handle* h, int li) {
+  Level& l = h->L[li];
+  if (li == 0) return fine_residual<T>(h, LV<T>::u(l), LV<T>::f(l), LV<T>::r(l), LV<T>::rp(h));
+  return coarse_residual<T>(h, li, LV<T>::u(l), LV<T>::f(l), LV<T>::r(l));
+}
+
+// V-cycle on the level work vectors: L[0].f holds the right-hand side and
+// L[0].u the initial iterate; the result is left in L[0].u.
+template <typename T>
+rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric) {
+  const int nl = (int)h->L.size();
+  for (int li = 0; li < nl; li++) {
+    Level& l = h->L[li];
+    if (li > 0) {
+      RSO_TRY(level_residual<T>(h, li - 1));
+      RSO_TRY(restrict_<T>(h, li, LV<T>::r(h->L[li - 1]), LV<T>::f(l)));
+      RSO_CHECK_CUDA(h, cudaMemsetAsync(LV<T>::u(l), 0, sizeof(T) * 3 * l.NP, h->stream));
+    }
+    if (li < nl - 1 || nl == 1) RSO_TRY(smooth<T>(h, li, pre, 0));
+    else RSO_TRY(coarsest_solve<T>(h, LV<T>::f(l), LV<T>::u(l)));
+  }
+  for (int li = nl - 2; li >= 0; li--) {
+    RSO_TRY(prolong<T>(h, li + 1, LV<T>::u(h->L[li + 1]), LV<T>::u(h->L[li])));
+    RSO_TRY(smooth<T>(h, li, post, symmetric ? 1 : 0));
+  }
+  return RSO_OK;
+}
+
+template rso_status vcycle_levels<double>(rso_handle*, int, int, int);
+template rso_status vcycle_levels<float>(rso_handle*, int, int, int);
+
+__global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+__global__ void k_f2d(const float* __restrict__ a, double* __restrict__ b, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (double)a[i];
+}
+
+// z = M r: one V-cycle from a zero iterate (FP32 in mixed precision)
+rso_status precondition(rso_handle* h, const double* r, double* z) {
+  Level& l0 = h->L[0];
+  const long long n3 = 3 * l0.NP;
+  const int pre = h->cfg.pre, post = h->cfg.post;
+  if (h->cfg.precision == RSO_MIXED) {
+    k_d2f<<<cdiv(n3, 256), 256, 0, h->stream>>>(r, l0.f32, n3); rso::note_launch();
+    RSO_CHECK_CUDA(h, cudaMemsetAsync(l0.u32, 0, sizeof(float) * n3, h->stream));
+    RSO_TRY(vcycle_levels<float>(h, pre, post, 1));
+    k_f2d<<<cdiv(n3, 256), 256, 0, h->stream>>>(l0.u32, z, n3); rso::note_launch();
+  } else {
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(l0.f64, r, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
+    RSO_CHECK_CUDA(h, cudaMemsetAsync(l0.u64, 0, sizeof(double) * n3, h->stream));
+    RSO_TRY(vcycle_levels<double>(h, pre, post, 1));
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(z, l0.u64, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
+  }
+  return launch_check(h, "precondition");
+}
+
+// x += a p; r -= a q; partial sums of r.r
+__global__ void k_cg_update(long long n, const double* __restrict__ alpha, const double* __restrict__ p,
+                            const double* __restrict__ q, double* __restrict__ x, double* __restrict__ r) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = *alpha;
+  x[i] += a * p[i];
+  r[i] -= a * q[i];
+}
+__global__ void k_cg_dir(long long n, const double* __restrict__ beta, const double* __restrict__ z,
+                         double* __restrict__ p) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) p[i] = z[i] + (*beta) * p[i];
+}
+// scalar updates on the device: s[0]=rz, s[1]=pq, s[2]=alpha, s[3]=rz_new, s[4]=beta
+__global__ void k_cg_alpha(double* s) { s[2] = s[0] / s[1]; }
+__global__ void k_cg_beta(double* s) {
+  s[4] = s[3] / s[0];
+  s[0] = s[3];
+}
+
+rso_status solve_pcg(rso_handle* h, const double* f, double* x, double tol, int max_iter, rso_solve_info* info) {
+  Level& l0 = h->L[0];
+  const long long n3 = 3 * l0.NP;
+  double* s = h->scal;
+  RSO_TRY(fine_residual<double>(h, x, f, h->r, h->rp64));
+  double fn2 = 0, rn2 = 0;
+  RSO_TRY(dot_host(h, f, f, n3, &fn2));
+  RSO_TRY(dot_host(h, h->r, h->r, n3, &rn2));
+  const double fn = std::sqrt(fn2);
+  int it = 0;
+  double rel = fn > 0 ? std::sqrt(rn2) / fn : 0.0;
+  if (fn == 0) {
+    RSO_CHECK_CUDA(h, cudaMemsetAsync(x, 0, sizeof(double) * n3, h->stream));
+    rel = 0;
+  }
+  if (rel >= tol && fn > 0) {
+    RSO_TRY(precondition(h, h->r, h->z));
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->p, h->z, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
+    RSO_TRY(dot(h, h->r, h->z, n3, s + 0));
+    while (it < max_iter) {
+      RSO_TRY(fine_applyK<double>(h, h->p, h->q, h->rp64));
+      RSO_TRY(dot(h, h->p, h->q, n3, s + 1));
+      k_cg_alpha<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
+      k_cg_update<<<cdiv(n3, 256), 256, 0, h->stream>>>(n3, s + 2, h->p, h->q, x, h->r); rso::note_launch();
+      RSO_TRY(dot_host(h, h->r, h->r, n3, &rn2));
+      it++;
+      rel = std::sqrt(rn2) / fn;
+      if (!std::isfinite(rel)) { h->err = "non-finite residual in PCG"; return RSO_ERR_NONFINITE; }
+      if (rel < tol) break;
+      RSO_TRY(precondition(h, h->r, h->z));
+      RSO_TRY(dot(h, h->r, h->z, n3, s + 3));
+      k_cg_beta<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
+      k_cg_dir<<<cdiv(n3, 256), 256, 0, h->stream>>>(n3, s + 4, h->z, h->p); rso::note_launch();
+      RSO_TRY(launch_check(h, "pcg"));
+    }
+  }
+  if (info) { info->iterations = it; info->rel_res = rel; }
+  if (rel >= tol && fn > 0) { h->err = "PCG did not reach the tolerance within max_iter"; return RSO_ERR_BUDGET_EXCEEDED; }
+  return RSO_OK;
+}
+
+// x <- x + M (f - K x) repeated (defect correction; plain V-cycles in FP64 mode)
+rso_status solve_vcycles(rso_handle* h, const double* f, double* x, double tol, int max_iter, rso_solve_info* info) {
+  Level& l0 = h->L[0];
+  const long long n3 = 3 * l0.NP;
+  double fn2 = 0, rn2 = 0;
+  RSO_TRY(dot_host(h, f, f, n3, &fn2));
+  const double fn = std::sqrt(fn2);
+  int it = 0;
+  double rel = 0;
+  RSO_TRY(fine_residual<double>(h, x, f, h->r, h->rp64));
+  RSO_TRY(dot_host(h, h->r, h->r, n3, &rn2));
+  rel = fn > 0 ? std::sqrt(rn2) / fn : 0;
+  while (rel >= tol && it < max_iter && fn > 0) {
+    RSO_TRY(precondition(h, h->r, h->z));
+    RSO_TRY(axpby(h, n3, 1.0, h->z, 1.0, x));
+    RSO_TRY(fine_residual<double>(h, x, f, h->r, h->rp64));
+    RSO_TRY(dot_host(h, h->r, h->r, n3, &rn2));
+    rel = std::sqrt(rn2) / fn;
+    it++;
+    if (!std::isfinite(rel) || rel > 1e4) { h->err = "defect correction diverged"; return RSO_ERR_DIVERGED; }
+  }
+  if (info) { info->iterations = it; info->rel_res = rel; }
+  if (rel >= tol && fn > 0) { h->err = "V-cycle iteration did not reach the tolerance"; return RSO_ERR_BUDGET_EXCEEDED; }
+  return RSO_OK;
+}
+
+// reference-sequenced FP64 V-cycle on a caller iterate (padded vectors)
+rso_status vcycle_fp64(rso_handle* h, double* u, const double* f, int pre, int post, int symmetric, double* rel) {
+  Level& l0 = h->L[0];
+  const long long n3 = 3 * l0.NP;
+  RSO_CHECK_CUDA(h, cudaMemcpyAsync(l0.u64, u, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
+  RSO_CHECK_CUDA(h, cudaMemcpyAsync(l0.f64, f, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
+  RSO_TRY(vcycle_levels<double>(h, pre, post, symmetric));
+  RSO_CHECK_CUDA(h, cudaMemcpyAsync(u, h->L[0].u64, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
+  RSO_TRY(fine_residual<double>(h, u, f, h->r, h->rp64));
+  double rn2 = 0, fn2 = 0;
+  RSO_TRY(dot_host(h, h->r, h->r, n3, &rn2));
+  RSO_TRY(dot_host(h, f, f, n3, &fn2));
+  if (rel) *rel = fn2 > 0 ? std::sqrt(rn2 / fn2) : std::sqrt(rn2);
+  return RSO_OK;
+}
+
+}  // namespace rso

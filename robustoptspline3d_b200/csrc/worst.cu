@@ -1,0 +1,267 @@
+// Worst-case load machinery: admissible-load projection on the load nodes,
+// Lanczos for lambda_max of P K^-1 P with full FP64 reorthogonalisation
+// (each step one multigrid solve), and the reference's modified power method.
+#include "rso_internal.cuh"
+#include <cmath>
+#include <vector>
+
+namespace rso {
+
+// gather the load-node forces into a load-space vector (3 per load node),
+// optionally keeping only the component along the load normal
+// (forceProject: f -= Nd^T Nd f, optimization/projection.cpp:289-360)
+__global__ void k_gather_load(const double* __restrict__ f, long long NP, const int* __restrict__ nodes,
+                              const double* __restrict__ nrm, int nl, int cf, double* __restrict__ v) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nl) return;
+  const long long n = nodes[k];
+  double a = f[n], b = f[n + NP], c = f[n + 2 * NP];
+  if (cf) {
+    const double s = a * nrm[3 * k] + b * nrm[3 * k + 1] + c * nrm[3 * k + 2];
+    a = s * nrm[3 * k]; b = s * nrm[3 * k + 1]; c = s * nrm[3 * k + 2];
+  }
+  v[3 * k] = a; v[3 * k + 1] = b; v[3 * k + 2] = c;
+}
+
+__global__ void k_scatter_load(const double* __restrict__ v, const int* __restrict__ nodes, int nl, long long NP,
+                               double a, double* __restrict__ f) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nl) return;
+  const long long n = nodes[k];
+  f[n] += a * v[3 * k]; f[n + NP] += a * v[3 * k + 1]; f[n + 2 * NP] += a * v[3 * k + 2];
+}
+
+__global__ void k_rand_load(double* v, int nl, uint64_t seed) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 3 * nl) v[i] = rso_urand(seed, (uint64_t)i);
+}
+
+__global__ void k_project_ls(double* v, const double* __restrict__ nrm, int nl) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nl) return;
+  const double s = v[3 * k] * nrm[3 * k] + v[3 * k + 1] * nrm[3 * k + 1] + v[3 * k + 2] * nrm[3 * k + 2];
+  v[3 * k] = s * nrm[3 * k]; v[3 * k + 1] = s * nrm[3 * k + 1]; v[3 * k + 2] = s * nrm[3 * k + 2];
+}
+
+rso_status force_project(rso_handle* h, double* f, int cf) {
+  const Level& l = h->L[0];
+  const int nl = h->n_load;
+  double* v = nullptr;
+  RSO_CHECK_CUDA(h, cudaMallocAsync(&v, sizeof(double) * 3 * (nl > 0 ? nl : 1), h->stream));
+  if (nl) { k_gather_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(f, l.NP, h->load_nodes, h->load_normals, nl, cf, v); rso::note_launch(); }
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(f, 0, sizeof(double) * 3 * l.NP, h->stream));
+  if (nl) { k_scatter_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(v, h->load_nodes, nl, l.NP, 1.0, f); rso::note_launch(); }
+  RSO_TRY(launch_check(h, "force_project"));
+  RSO_CHECK_CUDA(h, cudaFreeAsync(v, h->stream));
+  return RSO_OK;
+}
+
+// symmetric tridiagonal eigenproblem of the Lanczos matrix (tiny, host)
+static void tri_eig(int m, const std::vector<double>& al, const std::vector<double>& be, std::vector<double>& w,
+                    std::vector<double>& V) {
+  std::vector<double> A((size_t)m * m, 0.0);
+  for (int i = 0; i < m; i++) {
+    A[(size_t)i * m + i] = al[i];
+    if (i + 1 < m) A[(size_t)i * m + i + 1] = A[(size_t)(i + 1) * m + i] = be[i];
+  }
+  V.assign((size_t)m * m, 0.0);
+  for (int i = 0; i < m; i++) V[(size_t)i * m + i] = 1;
+  for (int sweep = 0; sweep < 100; sweep++) {
+    double off = 0;
+    for (int i = 0; i < m; i++)
+      for (int j = i + 1; j < m; j++) off += A[(size_t)i * m + j] * A[(size_t)i * m + j];
+    if (off < 1e-30) break;
+    for (int p = 0; p < m; p++)
+      for (int q = p + 1; q < m; q++) {
+        const double apq = A[(size_t)p * m + q];
+        if (std::fabs(apq) < 1e-300) continue;
+        const double th = (A[(size_t)q * m + q] - A[(size_t)p * m + p]) / (2 * apq);
+        const double t = (th >= 0 ? 1 : -1) / (std::fabs(th) + std::sqrt(th * th + 1));
+        const double c = 1 / std::sqrt(t * t + 1), s = t * c;
+        for (int k = 0; k < m; k++) {
+          const double akp = A[(size_t)k * m + p], akq = A[(size_t)k * m + q];
+          A[(size_t)k * m + p] = c * akp - s * akq;
+          A[(size_t)k * m + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < m; k++) {
+          const double apk = A[(size_t)p * m + k], aqk = A[(size_t)q * m + k];
+          A[(size_t)p * m + k] = c * apk - s * aqk;
+          A[(size_t)q * m + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < m; k++) {
+          const double vkp = V[(size_t)k * m + p], vkq = V[(size_t)k * m + q];
+          V[(size_t)k * m + p] = c * vkp - s * vkq;
+          V[(size_t)k * m + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  w.resize(m);
+  for (int i = 0; i < m; i++) w[i] = A[(size_t)i * m + i];
+}
+
+rso_status worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t seed, double* f_out, double* u_out,
+                      double* lambda, double* ritz, int* iters) {
+  const Level& l0 = h->L[0];
+  const int nl = h->n_load;
+  if (nl == 0) { h->err = "no load nodes"; return RSO_ERR_STATE; }
+  if (steps < 1) return RSO_ERR_INVALID_ARG;
+  const long long n3 = 3 * l0.NP;
+  const long long ls = 3LL * nl;
+  while ((int)h->lanczos_u.size() < steps) {
+    double* p = nullptr;
+    RSO_CHECK_CUDA(h, cudaMalloc(&p, sizeof(double) * n3));
+    h->lanczos_u.push_back(p);
+  }
+  double* V = nullptr;  // (steps+1) load-space vectors
+  double* wv = nullptr;
+  RSO_CHECK_CUDA(h, cudaMallocAsync(&V, sizeof(double) * ls * (steps + 1), h->stream));
+  RSO_CHECK_CUDA(h, cudaMallocAsync(&wv, sizeof(double) * ls, h->stream));
+  k_rand_load<<<cdiv(ls, 128), 128, 0, h->stream>>>(V, nl, seed); rso::note_launch();
+  if (cf) { k_project_ls<<<cdiv(nl, 128), 128, 0, h->stream>>>(V, h->load_normals, nl); rso::note_launch(); }
+  double nv = 0;
+  RSO_TRY(dot_host(h, V, V, ls, &nv));
+  RSO_TRY(axpby(h, ls, 0.0, V, 1.0 / std::sqrt(nv), V));
+  std::vector<double> al, be;
+  int total_it = 0;
+  for (int it = 0; it < steps; it++) {
+    double* v = V + ls * it;
+    RSO_CHECK_CUDA(h, cudaMemsetAsync(h->w, 0, sizeof(double) * n3, h->stream));
+    k_scatter_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(v, h->load_nodes, nl, l0.NP, 1.0, h->w); rso::note_launch();
+    double* u = h->lanczos_u[it];
+    RSO_CHECK_CUDA(h, cudaMemsetAsync(u, 0, sizeof(double) * n3, h->stream));
+    rso_solve_info si = {0, 0, 0};
+    RSO_TRY(solve_pcg(h, h->w, u, tol, 500, &si));
+    total_it += si.iterations;
+    k_gather_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(u, l0.NP, h->load_nodes, h->load_normals, nl, cf, wv); rso::note_launch();
+    double a = 0;
+    RSO_TRY(dot_host(h, v, wv, ls, &a));
+    al.push_back(a);
+    for (int pass = 0; pass < 2; pass++)
+      for (int j = 0; j <= it; j++) {
+        double s = 0;
+        RSO_TRY(dot_host(h, V + ls * j, wv, ls, &s));
+        RSO_TRY(axpby(h, ls, -s, V + ls * j, 1.0, wv));
+      }
+    double b2 = 0;
+    RSO_TRY(dot_host(h, wv, wv, ls, &b2));
+    const double b = std::sqrt(b2);
+    if (it == steps - 1 || b < 1e-14 * std::fabs(a)) break;
+    be.push_back(b);
+    RSO_TRY(axpby(h, ls, 1.0 / b, wv, 0.0, V + ls * (it + 1)));
+  }
+  const int m = (int)al.size();
+  std::vector<double> w, EV;
+  tri_eig(m, al, be, w, EV);
+  int best = 0;
+  for (int i = 1; i < m; i++) if (w[i] > w[best]) best = i;
+  if (ritz) for (int i = 0; i < m; i++) ritz[i] = w[i];
+  if (lambda) *lambda = w[best];
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(f_out, 0, sizeof(double) * n3, h->stream));
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(u_out, 0, sizeof(double) * n3, h->stream));
+  for (int k = 0; k < m; k++) {
+    const double y = EV[(size_t)k * m + best];
+    k_scatter_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(V + ls * k, h->load_nodes, nl, l0.NP, y, f_out); rso::note_launch();
+    RSO_TRY(axpby(h, n3, y, h->lanczos_u[k], 1.0, u_out));
+  }
+  RSO_TRY(launch_check(h, "worst_case"));
+  RSO_CHECK_CUDA(h, cudaFreeAsync(V, h->stream));
+  RSO_CHECK_CUDA(h, cudaFreeAsync(wv, h->stream));
+  if (iters) *iters = total_it;
+  return RSO_OK;
+}
+
+rso_status modified_pm(rso_handle* h, int cf, uint64_t seed, int max_itn, double* f, double* u, double* c_worst,
+                       int* itn_out) {
+  const Level& l0 = h->L[0];
+  const int nl = h->n_load;
+  if (nl == 0) { h->err = "no load nodes"; return RSO_ERR_STATE; }
+  const long long n3 = 3 * l0.NP, ls = 3LL * nl;
+  double *fs = nullptr, *fs_old = nullptr;
+  RSO_CHECK_CUDA(h, cudaMallocAsync(&fs, sizeof(double) * ls, h->stream));
+  RSO_CHECK_CUDA(h, cudaMallocAsync(&fs_old, sizeof(double) * ls, h->stream));
+  k_rand_load<<<cdiv(ls, 128), 128, 0, h->stream>>>(fs, nl, seed); rso::note_launch();
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(f, 0, sizeof(double) * n3, h->stream));
+  k_scatter_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(fs, h->load_nodes, nl, l0.NP, 1.0, f); rso::note_launch();
+  RSO_TRY(force_project(h, f, cf));
+  double fn2 = 0;
+  RSO_TRY(dot_host(h, f, f, n3, &fn2));
+  RSO_TRY(axpby(h, n3, 0.0, f, 1.0 / std::sqrt(fn2), f));
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(u, 0, sizeof(double) * n3, h->stream));
+  k_gather_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(f, l0.NP, h->load_nodes, h->load_normals, nl, 0, fs_old); rso::note_launch();
+  double fch = 1, rr = 1;
+  int itn = 0;
+  while (itn++ < max_itn && (fch > 1e-4 || rr > 1e-2)) {
+    RSO_TRY(vcycle_fp64(h, u, f, 1, 1, 0, &rr));
+    if (!std::isfinite(rr) || rr > 1e4) { h->err = "modified power method diverged"; return RSO_ERR_DIVERGED; }
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(f, u, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
+    RSO_TRY(force_project(h, f, cf));
+    RSO_TRY(dot_host(h, f, f, n3, &fn2));
+    RSO_TRY(axpby(h, n3, 0.0, f, 1.0 / std::sqrt(fn2), f));
+    k_gather_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(f, l0.NP, h->load_nodes, h->load_normals, nl, 0, fs); rso::note_launch();
+    double so = 0;
+    RSO_TRY(dot_host(h, fs_old, fs_old, ls, &so));
+    RSO_TRY(axpby(h, ls, 1.0, fs, -1.0, fs_old));  // fs_old <- fs - fs_old
+    double d2 = 0;
+    RSO_TRY(dot_host(h, fs_old, fs_old, ls, &d2));
+    fch = std::sqrt(d2) / std::sqrt(so);
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(fs_old, fs, sizeof(double) * ls, cudaMemcpyDeviceToDevice, h->stream));
+  }
+  if (itn_out) *itn_out = itn;
+  if (c_worst) RSO_TRY(dot_host(h, f, u, n3, c_worst));
+  RSO_CHECK_CUDA(h, cudaFreeAsync(fs, h->stream));
+  RSO_CHECK_CUDA(h, cudaFreeAsync(fs_old, h->stream));
+  return RSO_OK;
+}
+
+}  // namespace rso
+
+using namespace rso;
+
+extern "C" rso_status rso_force_project(rso_handle* h, double* f, int cf) {
+  if (!h || !f) return RSO_ERR_INVALID_ARG;
+  RSO_TRY(pad_nodes(h, 0, f, h->w));
+  RSO_TRY(force_project(h, h->w, cf));
+  RSO_TRY(unpad_nodes(h, 0, h->w, f));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  return RSO_OK;
+}
+
+extern "C" rso_status rso_worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t seed, double* f_worst,
+                                     double* u_worst, double* lambda, double* ritz) {
+  if (!h || !f_worst || !u_worst || steps < 1 || !(tol > 0)) return RSO_ERR_INVALID_ARG;
+  if (!h->operators_ready) { h->err = "call rso_update_operators first"; return RSO_ERR_STATE; }
+  double* fo = nullptr;
+  double* uo = nullptr;
+  const long long n3 = 3 * h->L[0].NP;
+  RSO_CHECK_CUDA(h, cudaMallocAsync(&fo, sizeof(double) * n3, h->stream));
+  RSO_CHECK_CUDA(h, cudaMallocAsync(&uo, sizeof(double) * n3, h->stream));
+  rso_status s = worst_case(h, steps, cf, tol, seed, fo, uo, lambda, ritz, nullptr);
+  if (s == RSO_OK) {
+    RSO_TRY(unpad_nodes(h, 0, fo, f_worst));
+    RSO_TRY(unpad_nodes(h, 0, uo, u_worst));
+  }
+  cudaFreeAsync(fo, h->stream);
+  cudaFreeAsync(uo, h->stream);
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  return s;
+}
+
+extern "C" rso_status rso_modified_pm(rso_handle* h, int cf, uint64_t seed, int max_itn, double* f, double* u,
+                                      double* c_worst, int* itn) {
+  if (!h || !f || !u || max_itn < 1) return RSO_ERR_INVALID_ARG;
+  if (!h->operators_ready) { h->err = "call rso_update_operators first"; return RSO_ERR_STATE; }
+  double* fo = nullptr;
+  double* uo = nullptr;
+  const long long n3 = 3 * h->L[0].NP;
+  RSO_CHECK_CUDA(h, cudaMallocAsync(&fo, sizeof(double) * n3, h->stream));
+  RSO_CHECK_CUDA(h, cudaMallocAsync(&uo, sizeof(double) * n3, h->stream));
+  rso_status s = modified_pm(h, cf, seed, max_itn, fo, uo, c_worst, itn);
+  if (s == RSO_OK) {
+    RSO_TRY(unpad_nodes(h, 0, fo, f));
+    RSO_TRY(unpad_nodes(h, 0, uo, u));
+  }
+  cudaFreeAsync(fo, h->stream);
+  cudaFreeAsync(uo, h->stream);
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  return s;
+}

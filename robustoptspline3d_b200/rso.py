@@ -1,0 +1,618 @@
+"""ctypes binding of librso.so and a Python mirror of the reference's
+Grid / optimization / mma_t call surface.
+
+Device arrays are torch CUDA tensors (PyTorch is only the allocator and
+stream plumbing here); the arithmetic runs in librso's CUDA kernels.
+Names follow the reference:
+
+  HierarchyGrid.genFromMesh      -> rso_create            (grid/Grid.cpp:978)
+  HierarchyGrid.update_stencil   -> rso_update_operators  (grid/Grid.cpp:4250)
+  Grid.applyK / update_residual  -> rso_apply_K / rso_residual
+  HierarchyGrid.v_cycle          -> rso_vcycle            (grid/Grid.cpp:2431)
+  computeSensitivity             -> rso_sensitivity       (optimization/optimization.cu:191)
+  projectDensities               -> rso_heaviside         (optimization/optimization.cu:350)
+  Grid.filterSensitivity         -> rso_filter            (grid/Grid.cu:4298)
+  Grid.coeff2density             -> rso_coeff2density     (grid/Grid.cu:3441)
+  Grid.ddensity2dcoeff           -> rso_density2coeff_adjoint (grid/Grid.cu:3566)
+  deal_background_points         -> rso_selfsupport       (optimization/optimization.cpp:1223)
+  forceProject / modifiedPM      -> rso_force_project / rso_modified_pm / rso_worst_case
+  MMA::mma_t::update             -> rso_mma_update        (optimization/mma_t.cpp:18)
+"""
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_NAME = "librso.so"
+
+
+def library_path():
+    return os.path.join(_HERE, _LIB_NAME)
+
+
+class RSOError(RuntimeError):
+    pass
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("youngs_modulus", ctypes.c_double), ("poisson_ratio", ctypes.c_double),
+                ("penal", ctypes.c_double), ("rho_min", ctypes.c_double), ("n_levels", ctypes.c_int),
+                ("first_factor", ctypes.c_int), ("smoother", ctypes.c_int), ("omega", ctypes.c_double),
+                ("pre", ctypes.c_int), ("post", ctypes.c_int), ("precision", ctypes.c_int), ("mode", ctypes.c_int)]
+
+
+class _SolveInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("rel_res", ctypes.c_double), ("ms", ctypes.c_double)]
+
+
+class _IterParams(ctypes.Structure):
+    _fields_ = [("beta", ctypes.c_double), ("volume_ratio", ctypes.c_double), ("filter_radius", ctypes.c_double),
+                ("filter_mode", ctypes.c_int), ("lanczos_steps", ctypes.c_int), ("solve_tol", ctypes.c_double),
+                ("constrain_direction", ctypes.c_int), ("ss_mode", ctypes.c_int), ("opt_angle", ctypes.c_double),
+                ("default_angle", ctypes.c_double), ("sens_scale", ctypes.c_double), ("vol_scale", ctypes.c_double),
+                ("ss_scale", ctypes.c_double), ("seed", ctypes.c_uint64)]
+
+
+class _IterInfo(ctypes.Structure):
+    _fields_ = [("c_worst", ctypes.c_double), ("lam", ctypes.c_double), ("volume", ctypes.c_double),
+                ("ss_value", ctypes.c_double), ("ms_total", ctypes.c_double), ("ms_operators", ctypes.c_double),
+                ("ms_worst", ctypes.c_double), ("ms_adjoint", ctypes.c_double), ("ms_selfsupport", ctypes.c_double),
+                ("ms_mma", ctypes.c_double), ("solve_iterations", ctypes.c_int), ("mma_converged", ctypes.c_int)]
+
+
+_vp = ctypes.c_void_p
+_ci = ctypes.c_int
+_cd = ctypes.c_double
+_pd = ctypes.POINTER(ctypes.c_double)
+_pi = ctypes.POINTER(ctypes.c_int)
+_pu8 = ctypes.POINTER(ctypes.c_uint8)
+_pu32 = ctypes.POINTER(ctypes.c_uint32)
+
+# every entry point of include/rso.h with its ctypes signature
+SIGNATURES = {
+    "rso_default_config": (None, [ctypes.POINTER(_Config)]),
+    "rso_create": (_ci, [ctypes.POINTER(_Config), _ci, _ci, _ci, _pu8, _pu8, _pu8, _pd, ctypes.POINTER(_vp)]),
+    "rso_destroy": (None, [_vp]),
+    "rso_last_error": (ctypes.c_char_p, [_vp]),
+    "rso_set_stream": (_ci, [_vp, _vp]),
+    "rso_synchronize": (_ci, [_vp]),
+    "rso_element_matrix": (_ci, [_cd, _cd, _cd, _pd]),
+    "rso_n_levels": (_ci, [_vp]),
+    "rso_level_dims": (_ci, [_vp, _ci, _pi]),
+    "rso_level_masks": (_ci, [_vp, _ci, _pu8, _pu8]),
+    "rso_level_bitwords": (_ci, [_vp, _ci, _pu32, _pu32]),
+    "rso_bitsat_rank": (_ci, [_vp, _vp, ctypes.c_int64, _vp]),
+    "rso_node_class": (_ci, [_vp, _pu8]),
+    "rso_ref_numbering": (_ci, [_vp, _ci, _pi, _pi, _pi, _pi, _pi, _pi]),
+    "rso_load_nodes": (_ci, [_vp, _pi, _pi]),
+    "rso_set_density": (_ci, [_vp, _vp]),
+    "rso_update_operators": (_ci, [_vp]),
+    "rso_apply_K": (_ci, [_vp, _vp, _vp]),
+    "rso_residual": (_ci, [_vp, _vp, _vp, _vp]),
+    "rso_get_stencil": (_ci, [_vp, _ci, _vp]),
+    "rso_coarse_residual": (_ci, [_vp, _ci, _vp, _vp, _vp]),
+    "rso_smooth": (_ci, [_vp, _ci, _vp, _vp, _ci, _cd, _ci, _ci]),
+    "rso_restrict": (_ci, [_vp, _ci, _vp, _vp]),
+    "rso_prolong": (_ci, [_vp, _ci, _vp, _vp]),
+    "rso_coarsest_solve": (_ci, [_vp, _vp, _vp]),
+    "rso_level_lambda": (_ci, [_vp, _ci, _pd]),
+    "rso_vcycle": (_ci, [_vp, _vp, _vp, _ci, _ci, _ci, _pd]),
+    "rso_solve": (_ci, [_vp, _vp, _vp, _cd, _ci, _ci, ctypes.POINTER(_SolveInfo)]),
+    "rso_dot": (_ci, [_vp, _vp, _vp, _pd]),
+    "rso_sensitivity": (_ci, [_vp, _vp, _vp]),
+    "rso_element_energy": (_ci, [_vp, _vp, _vp]),
+    "rso_heaviside": (_ci, [_vp, _vp, _cd, _vp, _vp]),
+    "rso_heaviside_chain": (_ci, [_vp, _vp, _cd, _vp, _vp]),
+    "rso_filter": (_ci, [_vp, _cd, _vp, _vp]),
+    "rso_density_filter": (_ci, [_vp, _cd, _vp, _vp]),
+    "rso_density_filter_adjoint": (_ci, [_vp, _cd, _vp, _vp]),
+    "rso_volume": (_ci, [_vp, _vp, _pd]),
+    "rso_spline_setup": (_ci, [_vp, _ci, _ci, _ci, _ci, _pi]),
+    "rso_spline_axis": (_ci, [_vp, _ci, _pi, _pd, _pd]),
+    "rso_coeff2density": (_ci, [_vp, _vp, _vp, _vp]),
+    "rso_density2coeff_adjoint": (_ci, [_vp, _vp, _vp, _vp]),
+    "rso_selfsupport": (_ci, [_vp, _vp, _cd, _ci, _cd, _cd, _vp, _vp, _pd, _pd, _pd]),
+    "rso_force_project": (_ci, [_vp, _vp, _ci]),
+    "rso_worst_case": (_ci, [_vp, _ci, _ci, _cd, ctypes.c_uint64, _vp, _vp, _pd, _pd]),
+    "rso_modified_pm": (_ci, [_vp, _ci, ctypes.c_uint64, _ci, _vp, _vp, _pd, _pi]),
+    "rso_mma_create": (_ci, [_ci, _ci, _pd, _pd, ctypes.POINTER(_vp)]),
+    "rso_mma_set_x": (_ci, [_vp, _pd]),
+    "rso_mma_get": (_ci, [_vp, _pd, _pd, _pd, _pd, _pd]),
+    "rso_mma_x_dev": (_vp, [_vp]),
+    "rso_mma_update": (_ci, [_vp, _vp, _vp, _pd, _pi, _pd]),
+    "rso_mma_destroy": (None, [_vp]),
+    "rso_default_iter_params": (None, [ctypes.POINTER(_IterParams)]),
+    "rso_design_iteration": (_ci, [_vp, _vp, ctypes.POINTER(_IterParams), ctypes.POINTER(_IterInfo)]),
+    "rso_design_iteration_host": (_ci, [_vp, _vp, ctypes.POINTER(_IterParams), _pd, _pd,
+                                        ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_IterInfo)]),
+    "rso_launch_count": (ctypes.c_longlong, []),
+    "rso_set_profiling": (_ci, [_vp, _ci]),
+    "rso_profile_reset": (_ci, [_vp]),
+    "rso_profile_class": (_ci, [_vp, _ci, ctypes.c_char_p, _ci, ctypes.POINTER(ctypes.c_longlong), _pd, _pd, _pd]),
+    "rso_profile_top": (_ci, [_vp, ctypes.c_char_p, _ci, ctypes.POINTER(ctypes.c_longlong), _pd, _pd, _pd]),
+}
+
+_lib = None
+
+
+def load_library():
+    """Load librso.so; raises if it has not been built (no CPU fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise RSOError(f"{path} is missing: build it with `python -m robustoptspline3d_b200.build` "
+                       "(the CUDA library is the only implementation)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+_STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA", 4: "DIVERGED", 5: "NONFINITE", 6: "BUDGET_EXCEEDED",
+           7: "UNSUPPORTED", 8: "STATE"}
+
+SMOOTH_GS, SMOOTH_JACOBI = 0, 1
+FP64, MIXED = 0, 1
+SOLVE_VCYCLE, SOLVE_PCG = 0, 1
+NO_SUPPORT_CF, NO_SUPPORT_FF, WITH_SUPPORT_CF, WITH_SUPPORT_FF = 0, 1, 2, 3
+
+
+def _np_ptr(a, t):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+def _dev(t, dtype=None):
+    """Device pointer of a contiguous CUDA tensor (None -> NULL)."""
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise RSOError("expected a CUDA tensor")
+    if dtype is not None and t.dtype != dtype:
+        raise RSOError(f"expected {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise RSOError("expected a contiguous tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def element_matrix(E=1e6, nu=0.3, h=1.0):
+    out = np.zeros(576)
+    st = load_library().rso_element_matrix(E, nu, h, _np_ptr(out, _pd))
+    if st:
+        raise RSOError(f"rso_element_matrix: {_STATUS.get(st, st)}")
+    return out.reshape(24, 24)
+
+
+@dataclass
+class Config:
+    youngs_modulus: float = 1e6
+    poisson_ratio: float = 0.3
+    penal: float = 3.0
+    rho_min: float = 1e-3
+    n_levels: int = 0
+    first_factor: int = 4
+    smoother: int = SMOOTH_JACOBI
+    omega: float = 0.6
+    pre: int = 2
+    post: int = 2
+    precision: int = MIXED
+    mode: int = WITH_SUPPORT_FF
+
+    def _c(self):
+        c = _Config()
+        for f in _Config._fields_:
+            setattr(c, f[0], getattr(self, f[0]))
+        return c
+
+
+@dataclass
+class IterParams:
+    beta: float = 8.0
+    volume_ratio: float = 0.3
+    filter_radius: float = 2.0
+    filter_mode: int = 0
+    lanczos_steps: int = 20
+    solve_tol: float = 1e-6
+    constrain_direction: int = 0
+    ss_mode: int = 4
+    opt_angle: float = 0.75 * np.pi
+    default_angle: float = 0.75 * np.pi
+    sens_scale: float = 1e6
+    vol_scale: float = 1e3
+    ss_scale: float = 1e3
+    seed: int = 1234
+
+    def _c(self):
+        c = _IterParams()
+        for f in _IterParams._fields_:
+            setattr(c, f[0], getattr(self, f[0]))
+        return c
+
+
+class HierarchyGrid:
+    """The multigrid hierarchy and fine-level design state of one voxel box.
+
+    Arrays: nodal vectors are float64 CUDA tensors of shape (3, nz+1, ny+1, nx+1)
+    (or flat 3*Nn); element fields float32 of shape (ez, ey, ex) or flat.
+    """
+
+    def __init__(self, emask, fixed_area, load_area, load_normals=None, config=None):
+        import torch  # noqa: F401  (CUDA context / allocator)
+        self.lib = load_library()
+        self.cfg = config or Config()
+        emask = np.ascontiguousarray(emask, dtype=np.uint8)
+        self.ez, self.ey, self.ex = emask.shape
+        self.nx, self.ny, self.nz = self.ex + 1, self.ey + 1, self.ez + 1
+        self.nn = self.nx * self.ny * self.nz
+        self.ne = self.ex * self.ey * self.ez
+        fa = np.ascontiguousarray(fixed_area, dtype=np.uint8).ravel()
+        la = np.ascontiguousarray(load_area, dtype=np.uint8).ravel()
+        ln = None if load_normals is None else np.ascontiguousarray(load_normals, dtype=np.float64).ravel()
+        h = ctypes.c_void_p()
+        c = self.cfg._c()
+        st = self.lib.rso_create(ctypes.byref(c), self.ex, self.ey, self.ez, _np_ptr(emask.ravel(), _pu8),
+                                 _np_ptr(fa, _pu8), _np_ptr(la, _pu8), _np_ptr(ln, _pd), ctypes.byref(h))
+        if st:
+            raise RSOError(f"rso_create: {_STATUS.get(st, st)}: {self.lib.rso_last_error(None).decode()}")
+        self.h = h
+        self.n_coeff = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.rso_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _chk(self, st, what):
+        if st:
+            raise RSOError(f"{what}: {_STATUS.get(st, st)}: {self.lib.rso_last_error(self.h).decode()}")
+
+    # ------------------------------------------------------------ topology
+    def n_levels(self):
+        return self.lib.rso_n_levels(self.h)
+
+    def level_dims(self, level):
+        d = np.zeros(6, dtype=np.int32)
+        self._chk(self.lib.rso_level_dims(self.h, level, _np_ptr(d, _pi)), "rso_level_dims")
+        return d
+
+    def level_masks(self, level):
+        d = self.level_dims(level)
+        em = np.zeros(int(d[0] * d[1] * d[2]), np.uint8)
+        vm = np.zeros(int(d[3] * d[4] * d[5]), np.uint8)
+        self._chk(self.lib.rso_level_masks(self.h, level, _np_ptr(em, _pu8), _np_ptr(vm, _pu8)), "rso_level_masks")
+        return em, vm
+
+    def level_bitwords(self, level):
+        d = self.level_dims(level)
+        eb = np.zeros((int(d[0] * d[1] * d[2]) + 31) // 32, np.uint32)
+        vb = np.zeros((int(d[3] * d[4] * d[5]) + 31) // 32, np.uint32)
+        self._chk(self.lib.rso_level_bitwords(self.h, level, _np_ptr(eb, _pu32), _np_ptr(vb, _pu32)), "bitwords")
+        return eb, vb
+
+    def bitsat_rank(self, words, nbits):
+        import torch
+        w = torch.as_tensor(np.asarray(words, np.uint32).view(np.int32), device="cuda")
+        out = torch.empty(nbits, dtype=torch.int32, device="cuda")
+        self._chk(self.lib.rso_bitsat_rank(self.h, _dev(w), nbits, _dev(out)), "rso_bitsat_rank")
+        return out.cpu().numpy()
+
+    def node_class(self):
+        out = np.zeros(self.nn, np.uint8)
+        self._chk(self.lib.rso_node_class(self.h, _np_ptr(out, _pu8)), "rso_node_class")
+        return out
+
+    def ref_numbering(self, level):
+        counts = np.zeros(4, np.int32)
+        gs = np.zeros(8, np.int32)
+        self._chk(self.lib.rso_ref_numbering(self.h, level, _np_ptr(counts, _pi), _np_ptr(gs, _pi), None, None, None,
+                                             None), "rso_ref_numbering")
+        nv, ne, nvgs, negs = [int(v) for v in counts]
+        vl, el = np.zeros(nv, np.int32), np.zeros(ne, np.int32)
+        vf, ef = np.zeros(nvgs, np.int32), np.zeros(negs, np.int32)
+        self._chk(self.lib.rso_ref_numbering(self.h, level, None, None, _np_ptr(vl, _pi), _np_ptr(el, _pi),
+                                             _np_ptr(vf, _pi), _np_ptr(ef, _pi)), "rso_ref_numbering")
+        return dict(counts=counts, gs_num=gs, vlexi2gs=vl, elexi2gs=el, vflag=vf, eflag=ef)
+
+    def load_nodes(self):
+        n = ctypes.c_int(0)
+        self._chk(self.lib.rso_load_nodes(self.h, None, ctypes.byref(n)), "rso_load_nodes")
+        out = np.zeros(max(n.value, 1), np.int32)
+        self._chk(self.lib.rso_load_nodes(self.h, _np_ptr(out, _pi), ctypes.byref(n)), "rso_load_nodes")
+        return out[:n.value]
+
+    # ------------------------------------------------------------ operator
+    def set_density(self, rho):
+        import torch
+        r = rho if isinstance(rho, torch.Tensor) else torch.as_tensor(np.asarray(rho, np.float32), device="cuda")
+        r = r.to(device="cuda", dtype=torch.float32).contiguous()
+        self._chk(self.lib.rso_set_density(self.h, _dev(r)), "rso_set_density")
+
+    def update_stencil(self):
+        self._chk(self.lib.rso_update_operators(self.h), "rso_update_operators")
+
+    def _vec(self, level=0):
+        import torch
+        d = self.level_dims(level)
+        return torch.zeros(3 * int(d[3] * d[4] * d[5]), dtype=torch.float64, device="cuda")
+
+    def applyK(self, u):
+        import torch
+        f = torch.empty_like(u)
+        self._chk(self.lib.rso_apply_K(self.h, _dev(u, torch.float64), _dev(f)), "rso_apply_K")
+        return f
+
+    def update_residual(self, u, f):
+        import torch
+        r = torch.empty_like(u)
+        self._chk(self.lib.rso_residual(self.h, _dev(u, torch.float64), _dev(f, torch.float64), _dev(r)), "rso_residual")
+        return r
+
+    def stencil(self, level):
+        import torch
+        d = self.level_dims(level)
+        nn = int(d[3] * d[4] * d[5])
+        out = torch.empty(243 * nn, dtype=torch.float64, device="cuda")
+        self._chk(self.lib.rso_get_stencil(self.h, level, _dev(out)), "rso_get_stencil")
+        return out.view(27, 3, 3, nn)
+
+    def coarse_residual(self, level, u, f):
+        import torch
+        r = torch.empty_like(u)
+        self._chk(self.lib.rso_coarse_residual(self.h, level, _dev(u, torch.float64), _dev(f, torch.float64), _dev(r)),
+                  "rso_coarse_residual")
+        return r
+
+    def gs_relax(self, level, u, f, kind=SMOOTH_GS, omega=1.0, sweeps=1, reverse=0):
+        import torch
+        u = u.clone()
+        self._chk(self.lib.rso_smooth(self.h, level, _dev(u, torch.float64), _dev(f, torch.float64), kind, omega, sweeps,
+                                      reverse), "rso_smooth")
+        return u
+
+    def restrict_residual(self, coarse_level, rf):
+        import torch
+        fc = self._vec(coarse_level)
+        self._chk(self.lib.rso_restrict(self.h, coarse_level, _dev(rf, torch.float64), _dev(fc)), "rso_restrict")
+        return fc
+
+    def prolongate_correction(self, coarse_level, uc, uf):
+        import torch
+        uf = uf.clone()
+        self._chk(self.lib.rso_prolong(self.h, coarse_level, _dev(uc, torch.float64), _dev(uf)), "rso_prolong")
+        return uf
+
+    def solve_coarsest(self, f):
+        import torch
+        u = torch.empty_like(f)
+        self._chk(self.lib.rso_coarsest_solve(self.h, _dev(f, torch.float64), _dev(u)), "rso_coarsest_solve")
+        return u
+
+    def level_lambda(self, level):
+        v = ctypes.c_double(0)
+        self._chk(self.lib.rso_level_lambda(self.h, level, ctypes.byref(v)), "rso_level_lambda")
+        return v.value
+
+    def v_cycle(self, u, f, pre=1, post=1, symmetric=0):
+        import torch
+        u = u.clone()
+        rr = ctypes.c_double(0)
+        self._chk(self.lib.rso_vcycle(self.h, _dev(u, torch.float64), _dev(f, torch.float64), pre, post, symmetric,
+                                      ctypes.byref(rr)), "rso_vcycle")
+        return u, rr.value
+
+    def solve(self, f, u0=None, tol=1e-10, max_iter=200, method=SOLVE_PCG):
+        import torch
+        u = torch.zeros_like(f) if u0 is None else u0.clone()
+        info = _SolveInfo()
+        self._chk(self.lib.rso_solve(self.h, _dev(f, torch.float64), _dev(u), tol, max_iter, method, ctypes.byref(info)),
+                  "rso_solve")
+        return u, info.iterations, info.rel_res, info.ms
+
+    def compliance(self, f, u):
+        v = ctypes.c_double(0)
+        self._chk(self.lib.rso_dot(self.h, _dev(f), _dev(u), ctypes.byref(v)), "rso_dot")
+        return v.value
+
+    # ------------------------------------------------------------ design variables
+    def _efield(self, x):
+        import torch
+        x = x if isinstance(x, torch.Tensor) else torch.as_tensor(np.asarray(x, np.float32))
+        return x.to(device="cuda", dtype=torch.float32).contiguous().view(-1)
+
+    def _shell(self, shell):
+        import torch
+        if shell is None:
+            return None
+        return torch.as_tensor(np.ascontiguousarray(shell, np.uint8).ravel(), device="cuda")
+
+    def computeSensitivity(self, u):
+        import torch
+        out = torch.empty(self.ne, dtype=torch.float32, device="cuda")
+        self._chk(self.lib.rso_sensitivity(self.h, _dev(u, torch.float64), _dev(out)), "rso_sensitivity")
+        return out
+
+    def elementCompliance(self, u):
+        import torch
+        out = torch.empty(self.ne, dtype=torch.float32, device="cuda")
+        self._chk(self.lib.rso_element_energy(self.h, _dev(u, torch.float64), _dev(out)), "rso_element_energy")
+        return out
+
+    def projectDensities(self, rho, beta, shell=None):
+        import torch
+        rho = self._efield(rho)
+        sh = self._shell(shell)
+        out = torch.empty_like(rho)
+        self._chk(self.lib.rso_heaviside(self.h, _dev(rho), beta, _dev(sh), _dev(out)), "rso_heaviside")
+        return out
+
+    def projectSensitivity(self, rho, beta, g):
+        import torch
+        rho, g = self._efield(rho), self._efield(g)
+        out = torch.empty_like(g)
+        self._chk(self.lib.rso_heaviside_chain(self.h, _dev(rho), beta, _dev(g), _dev(out)), "rso_heaviside_chain")
+        return out
+
+    def filterSensitivity(self, radius, g):
+        import torch
+        g = self._efield(g)
+        out = torch.empty_like(g)
+        self._chk(self.lib.rso_filter(self.h, radius, _dev(g), _dev(out)), "rso_filter")
+        return out
+
+    def densityFilter(self, radius, x, adjoint=False):
+        import torch
+        x = self._efield(x)
+        out = torch.empty_like(x)
+        fn = self.lib.rso_density_filter_adjoint if adjoint else self.lib.rso_density_filter
+        self._chk(fn(self.h, radius, _dev(x), _dev(out)), "rso_density_filter")
+        return out
+
+    def volumeRatio(self, rho):
+        v = ctypes.c_double(0)
+        self._chk(self.lib.rso_volume(self.h, _dev(self._efield(rho)), ctypes.byref(v)), "rso_volume")
+        return v.value
+
+    def set_spline_partition(self, px, py, pz, order):
+        n = ctypes.c_int(0)
+        self._chk(self.lib.rso_spline_setup(self.h, order, px, py, pz, ctypes.byref(n)), "rso_spline_setup")
+        self.n_coeff = n.value
+        self.order = order
+        return n.value
+
+    def spline_axis(self, axis):
+        n = [self.ex, self.ey, self.ez][axis]
+        idx = np.zeros(n, np.int32)
+        N = np.zeros(n * self.order)
+        dN = np.zeros(n * self.order)
+        self._chk(self.lib.rso_spline_axis(self.h, axis, _np_ptr(idx, _pi), _np_ptr(N, _pd), _np_ptr(dN, _pd)),
+                  "rso_spline_axis")
+        return idx, N.reshape(n, self.order), dN.reshape(n, self.order)
+
+    def coeff2density(self, coeff, shell=None):
+        import torch
+        c = self._efield(coeff)
+        out = torch.empty(self.ne, dtype=torch.float32, device="cuda")
+        self._chk(self.lib.rso_coeff2density(self.h, _dev(c), _dev(self._shell(shell)), _dev(out)), "rso_coeff2density")
+        return out
+
+    def ddensity2dcoeff(self, g, shell=None):
+        import torch
+        g = self._efield(g)
+        out = torch.empty(self.n_coeff, dtype=torch.float32, device="cuda")
+        self._chk(self.lib.rso_density2coeff_adjoint(self.h, _dev(g), _dev(self._shell(shell)), _dev(out)),
+                  "rso_density2coeff_adjoint")
+        return out
+
+    def deal_background_points(self, coeff, beta, mode=4, opt_angle=0.75 * np.pi, default_angle=0.75 * np.pi):
+        import torch
+        c = self._efield(coeff)
+        per = torch.empty(self.ne, dtype=torch.float32, device="cuda")
+        dc = torch.empty(self.n_coeff, dtype=torch.float32, device="cuda")
+        val, cnt, ds = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_double(0)
+        self._chk(self.lib.rso_selfsupport(self.h, _dev(c), beta, mode, opt_angle, default_angle, _dev(per), _dev(dc),
+                                           ctypes.byref(val), ctypes.byref(cnt), ctypes.byref(ds)), "rso_selfsupport")
+        return val.value, per, dc, cnt.value, ds.value
+
+    # ------------------------------------------------------------ worst case
+    def forceProject(self, f, constrain_direction):
+        import torch
+        f = f.clone()
+        self._chk(self.lib.rso_force_project(self.h, _dev(f, torch.float64), int(constrain_direction)), "rso_force_project")
+        return f
+
+    def worst_case(self, steps=20, constrain_direction=0, tol=1e-6, seed=1234):
+        import torch
+        fw = self._vec()
+        uw = self._vec()
+        lam = ctypes.c_double(0)
+        ritz = np.zeros(steps)
+        self._chk(self.lib.rso_worst_case(self.h, steps, int(constrain_direction), tol, seed, _dev(fw), _dev(uw),
+                                          ctypes.byref(lam), _np_ptr(ritz, _pd)), "rso_worst_case")
+        return lam.value, fw, uw, ritz
+
+    def modifiedPM(self, constrain_direction=0, seed=1234, max_itn=500):
+        fw = self._vec()
+        uw = self._vec()
+        c = ctypes.c_double(0)
+        itn = ctypes.c_int(0)
+        self._chk(self.lib.rso_modified_pm(self.h, int(constrain_direction), seed, max_itn, _dev(fw), _dev(uw),
+                                           ctypes.byref(c), ctypes.byref(itn)), "rso_modified_pm")
+        return c.value, fw, uw, itn.value
+
+    # ------------------------------------------------------------ design iteration
+    def design_iteration(self, mma, params=None):
+        p = (params or IterParams())._c()
+        info = _IterInfo()
+        self._chk(self.lib.rso_design_iteration(self.h, mma.s, ctypes.byref(p), ctypes.byref(info)),
+                  "rso_design_iteration")
+        return {f[0]: getattr(info, f[0]) for f in _IterInfo._fields_}
+
+    def design_iteration_host(self, mma, coeff_in, params=None):
+        p = (params or IterParams())._c()
+        info = _IterInfo()
+        cin = np.ascontiguousarray(coeff_in, np.float64)
+        cout = np.zeros(self.n_coeff)
+        rho = np.zeros(self.ne, np.float32)
+        self._chk(self.lib.rso_design_iteration_host(self.h, mma.s, ctypes.byref(p), _np_ptr(cin, _pd),
+                                                     _np_ptr(cout, _pd), rho.ctypes.data_as(
+                                                         ctypes.POINTER(ctypes.c_float)), ctypes.byref(info)),
+                  "rso_design_iteration_host")
+        return cout, rho, {f[0]: getattr(info, f[0]) for f in _IterInfo._fields_}
+
+
+class MMA:
+    """MMA::mma_t (optimization/mma_t.h:159) on the device in FP64."""
+
+    def __init__(self, n, m, xmin, xmax):
+        self.lib = load_library()
+        self.n, self.m = n, m
+        lo = np.broadcast_to(np.asarray(xmin, np.float64), (n,)).copy()
+        hi = np.broadcast_to(np.asarray(xmax, np.float64), (n,)).copy()
+        s = ctypes.c_void_p()
+        st = self.lib.rso_mma_create(n, m, _np_ptr(lo, _pd), _np_ptr(hi, _pd), ctypes.byref(s))
+        if st:
+            raise RSOError(f"rso_mma_create: {_STATUS.get(st, st)}")
+        self.s = s
+
+    def close(self):
+        if getattr(self, "s", None):
+            self.lib.rso_mma_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        self.close()
+
+    def set_x(self, x):
+        st = self.lib.rso_mma_set_x(self.s, _np_ptr(np.ascontiguousarray(x, np.float64), _pd))
+        if st:
+            raise RSOError(f"rso_mma_set_x: {_STATUS.get(st, st)}")
+
+    def get(self):
+        x, L, U, a, b = [np.zeros(self.n) for _ in range(5)]
+        st = self.lib.rso_mma_get(self.s, _np_ptr(x, _pd), _np_ptr(L, _pd), _np_ptr(U, _pd), _np_ptr(a, _pd),
+                                  _np_ptr(b, _pd))
+        if st:
+            raise RSOError(f"rso_mma_get: {_STATUS.get(st, st)}")
+        return x, L, U, a, b
+
+    def update(self, df, dg, g):
+        import torch
+        df = df.to(device="cuda", dtype=torch.float64).contiguous()
+        dg = dg.to(device="cuda", dtype=torch.float64).contiguous()
+        gv = np.ascontiguousarray(g, np.float64)
+        conv = ctypes.c_int(0)
+        info = np.zeros(4)
+        st = self.lib.rso_mma_update(self.s, _dev(df), _dev(dg), _np_ptr(gv, _pd), ctypes.byref(conv),
+                                     _np_ptr(info, _pd))
+        if st:
+            raise RSOError(f"rso_mma_update: {_STATUS.get(st, st)}")
+        return bool(conv.value), info

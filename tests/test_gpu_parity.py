@@ -1,0 +1,302 @@
+"""CUDA path (through the C ABI) against the FP64 CPU oracle.
+
+Tolerances: integer work bit-exact; FP64 operator pieces 1e-12 relative;
+converged solves 1e-5 relative in displacement and 1e-6 in compliance and
+lambda_max; FP32 element fields 1e-5 relative (sensitivities 1e-4).
+"""
+import numpy as np
+import pytest
+
+import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def make(oracle, prob, n_levels=0, first_factor=4, smoother=0, precision=0, nu=0.3, omega=0.6, pre=1, post=1):
+    from robustoptspline3d_b200 import Config, HierarchyGrid
+    cfg = Config(poisson_ratio=nu, n_levels=n_levels, first_factor=first_factor, smoother=smoother,
+                 precision=precision, omega=omega, pre=pre, post=post)
+    g = HierarchyGrid(prob["emask"], prob["fixed"], prob["load"], prob["normals"], cfg)
+    o = oracle.Problem(prob["emask"], prob["fixed"], prob["load"], prob["normals"], nu=nu, n_levels=n_levels,
+                       first_factor=first_factor)
+    rho32 = prob["rho"].astype(np.float32)
+    g.set_density(rho32.ravel())
+    o.set_density(rho32.astype(np.float64).ravel())
+    return g, o
+
+
+def t(x, torch):
+    return torch.as_tensor(np.ascontiguousarray(x), device="cuda")
+
+
+@pytest.mark.parametrize("gen,nl,ff", [(lambda: P.ellipsoid(24, 16, 12), 0, 4),
+                                       (lambda: P.voids_box(20, 12, 12, 3), 3, 2),
+                                       (lambda: P.cantilever(16, 8, 8), 3, 2)])
+def test_topology_bit_exact(oracle, cuda, gen, nl, ff):
+    prob = gen()
+    g, o = make(oracle, prob, n_levels=nl, first_factor=ff)
+    assert g.n_levels() == o.n_levels()
+    for lvl in range(o.n_levels()):
+        assert np.array_equal(g.level_dims(lvl), o.level_dims(lvl))
+        for a, b in zip(g.level_masks(lvl), o.level_masks(lvl)):
+            assert np.array_equal(a, b)
+        for a, b in zip(g.level_bitwords(lvl), o.level_bitwords(lvl)):
+            assert np.array_equal(a, b)
+        rg, ro = g.ref_numbering(lvl), o.ref_numbering(lvl)
+        for k in ro:
+            assert np.array_equal(rg[k], ro[k]), (lvl, k)
+    assert np.array_equal(g.node_class(), o.node_class())
+    assert np.array_equal(g.load_nodes(), o.load_nodes())
+
+
+def test_bitsat_rank(oracle, cuda):
+    # selfTest (optimization/optimization.cu:712-765): rank of every set bit of 0xaaaaaaaa words
+    prob = P.cantilever(8, 4, 4)
+    g, _ = make(oracle, prob, n_levels=2, first_factor=2)
+    words = np.full(10000, 0xAAAAAAAA, dtype=np.uint32)
+    rank = g.bitsat_rank(words, 32 * 10000)
+    bits = np.unpackbits(words.view(np.uint8), bitorder="little").astype(bool)
+    expect = np.where(bits, np.cumsum(bits) - 1, -1)
+    assert np.array_equal(rank, expect)
+
+
+@pytest.mark.parametrize("gen", [lambda: P.ellipsoid(24, 16, 12), lambda: P.voids_box(20, 12, 12, 3)])
+def test_operator_fp64(oracle, cuda, gen):
+    prob = gen()
+    g, o = make(oracle, prob)
+    rng = np.random.default_rng(5)
+    u = rng.standard_normal(3 * o.nn)
+    f = rng.standard_normal(3 * o.nn)
+    cls = o.node_class()
+    fix = np.tile((cls & 4) > 0, 3) | np.tile((cls & 1) == 0, 3)
+    u[fix] = 0
+    f[fix] = 0
+    Ku_o = o.apply_K(u)
+    Ku_g = g.applyK(t(u, cuda)).cpu().numpy()
+    assert rel(Ku_g, Ku_o) < 1e-13
+    r_o = o.residual(u, f)
+    r_g = g.update_residual(t(u, cuda), t(f, cuda)).cpu().numpy()
+    assert rel(r_g, r_o) < 1e-13
+
+
+@pytest.mark.parametrize("gen,nl,ff", [(lambda: P.ellipsoid(24, 16, 12), 0, 4),
+                                       (lambda: P.cantilever(16, 8, 8), 3, 2)])
+def test_galerkin_stencils_and_transfers(oracle, cuda, gen, nl, ff):
+    prob = gen()
+    g, o = make(oracle, prob, n_levels=nl, first_factor=ff)
+    g.update_stencil()
+    o.update_stencil()
+    rng = np.random.default_rng(6)
+    for lvl in range(1, o.n_levels()):
+        sg = g.stencil(lvl).cpu().numpy()
+        so = o.stencil(lvl)
+        assert rel(sg, so) < 1e-12, lvl
+        d = o.level_dims(lvl)
+        nn = int(d[3] * d[4] * d[5])
+        df = o.level_dims(lvl - 1)
+        nnf = int(df[3] * df[4] * df[5])
+        _, vm = o.level_masks(lvl)
+        _, vmf = o.level_masks(lvl - 1)
+        uc = rng.standard_normal(3 * nn) * np.tile(vm, 3)
+        fc = rng.standard_normal(3 * nn) * np.tile(vm, 3)
+        assert rel(g.coarse_residual(lvl, t(uc, cuda), t(fc, cuda)).cpu().numpy(), o.coarse_residual(lvl, uc, fc)) < 1e-12
+        rf = rng.standard_normal(3 * nnf) * np.tile(vmf, 3)
+        assert rel(g.restrict_residual(lvl, t(rf, cuda)).cpu().numpy(), o.restrict(lvl, rf)) < 1e-13
+        uf = rng.standard_normal(3 * nnf) * np.tile(vmf, 3)
+        if lvl == 1:
+            cls = o.node_class()
+            uf[np.tile((cls & 4) > 0, 3)] = 0
+        pg = g.prolongate_correction(lvl, t(uc, cuda), t(uf, cuda)).cpu().numpy()
+        po = o.prolong(lvl, uc, uf)
+        if lvl == 1:
+            po[np.tile((o.node_class() & 4) > 0, 3)] = 0  # support DOFs stay zero on the device
+        assert rel(pg, po) < 1e-13
+        if lvl < o.n_levels() - 1:
+            for kind, om in [(0, 1.0), (1, 0.3)]:
+                sg1 = g.gs_relax(lvl, t(uc, cuda), t(fc, cuda), kind=kind, omega=om, sweeps=2).cpu().numpy()
+                so1 = o.smooth(lvl, uc, fc, kind=kind, omega=om, sweeps=2)
+                assert rel(sg1, so1) < 1e-11, (lvl, kind)
+    last = o.n_levels() - 1
+    d = o.level_dims(last)
+    nn = int(d[3] * d[4] * d[5])
+    _, vm = o.level_masks(last)
+    fc = rng.standard_normal(3 * nn) * np.tile(vm, 3)
+    assert rel(g.solve_coarsest(t(fc, cuda)).cpu().numpy(), o.coarsest_solve(fc)) < 1e-9
+
+
+def test_fine_smoothers(oracle, cuda):
+    prob = P.ellipsoid(20, 14, 12)
+    g, o = make(oracle, prob)
+    rng = np.random.default_rng(7)
+    cls = o.node_class()
+    dead = np.tile(((cls & 4) > 0) | ((cls & 1) == 0), 3)
+    u = rng.standard_normal(3 * o.nn)
+    f = rng.standard_normal(3 * o.nn)
+    u[dead] = 0
+    f[dead] = 0
+    for kind, om, rev in [(0, 1.0, 0), (0, 1.0, 1), (1, 0.25, 0)]:
+        ug = g.gs_relax(0, t(u, cuda), t(f, cuda), kind=kind, omega=om, sweeps=2, reverse=rev).cpu().numpy()
+        uo = o.smooth(0, u, f, kind=kind, omega=om, sweeps=2, reverse=rev)
+        assert rel(ug, uo) < 1e-12, (kind, rev)
+
+
+def test_vcycle_reference_sequence(oracle, cuda):
+    prob = P.ellipsoid(24, 16, 12)
+    g, o = make(oracle, prob, smoother=0)
+    g.update_stencil()
+    o.update_stencil()
+    f = np.zeros(3 * o.nn)
+    rng = np.random.default_rng(8)
+    ln = o.load_nodes()
+    for c in range(3):
+        f[c * o.nn + ln] = rng.standard_normal(len(ln))
+    u = np.zeros(3 * o.nn)
+    ug = t(u, cuda)
+    for _ in range(3):
+        ug, rg = g.v_cycle(ug, t(f, cuda), 1, 1)
+        u, ro = o.vcycle(u, f, 1, 1, 0, 1.0, 0)
+        assert abs(rg - ro) <= 1e-9 * ro
+    assert rel(ug.cpu().numpy(), u) < 1e-10
+
+
+@pytest.mark.parametrize("precision,smoother", [(0, 0), (0, 1), (1, 1), (1, 0)])
+def test_solve_cantilever(oracle, cuda, precision, smoother):
+    prob = P.cantilever(32, 16, 16)
+    g, o = make(oracle, prob, n_levels=3, first_factor=2, smoother=smoother, precision=precision, nu=0.4, pre=2,
+                post=2)
+    g.update_stencil()
+    o.update_stencil()
+    f = prob["f"]
+    uo, _, _ = o.solve(f, tol=1e-12, method=1)
+    ug, it, rr, _ = g.solve(t(f, cuda), tol=1e-10, method=1, max_iter=300)
+    ug = ug.cpu().numpy()
+    assert rr < 1e-10
+    assert rel(ug, uo) < 1e-5
+    assert abs(f @ ug - f @ uo) <= 1e-6 * abs(f @ uo)
+    if precision == 1:
+        ug2, it2, rr2, _ = g.solve(t(f, cuda), tol=1e-10, method=0, max_iter=400)
+        assert rr2 < 1e-10
+        assert rel(ug2.cpu().numpy(), uo) < 1e-5
+
+
+def test_design_fields(oracle, cuda):
+    prob = P.ellipsoid(24, 16, 12)
+    g, o = make(oracle, prob)
+    rng = np.random.default_rng(9)
+    u = rng.standard_normal(3 * o.nn)
+    cls = o.node_class()
+    u[np.tile(((cls & 4) > 0) | ((cls & 1) == 0), 3)] = 0
+    em = prob["emask"].ravel() > 0
+    assert rel(g.computeSensitivity(t(u, cuda)).cpu().numpy(), o.sensitivity(u)) < 1e-6
+    assert rel(g.elementCompliance(t(u, cuda)).cpu().numpy(), o.element_energy(u)) < 1e-6
+    rho = rng.uniform(0, 1, o.ne).astype(np.float32)
+    shell = (rng.uniform(size=o.ne) < 0.05).astype(np.uint8)
+    out = oracle.heaviside(rho.astype(np.float64), 8.0, o.rhomin, shell)
+    hg = g.projectDensities(rho, 8.0, shell).cpu().numpy()
+    assert rel(hg[em], out[em]) < 1e-6
+    gin = rng.standard_normal(o.ne).astype(np.float32)
+    ho = oracle.heaviside_chain(rho.astype(np.float64), 8.0, gin.astype(np.float64))
+    assert rel(g.projectSensitivity(rho, 8.0, gin).cpu().numpy()[em], ho[em]) < 1e-5
+    for R in (1.5, 2.0, 2.6):
+        assert rel(g.filterSensitivity(R, gin).cpu().numpy(), o.filter(R, gin.astype(np.float64))) < 1e-5
+        assert rel(g.densityFilter(R, gin, adjoint=True).cpu().numpy(),
+                   o.density_filter_adjoint(R, gin.astype(np.float64))) < 1e-5
+
+
+@pytest.mark.parametrize("order,parts", [(3, (6, 4, 3)), (4, (5, 5, 4))])
+def test_spline_and_selfsupport(oracle, cuda, order, parts):
+    prob = P.ellipsoid(24, 16, 12)
+    g, o = make(oracle, prob)
+    nco = o.spline_setup(order, parts)
+    ncg = g.set_spline_partition(*parts, order)
+    assert nco == ncg
+    for ax in range(3):
+        ig, Ng, dNg = g.spline_axis(ax)
+        io, No, dNo = o.spline_axis(ax)
+        assert np.array_equal(ig, io)  # spline support indices: bit-exact
+        assert np.allclose(Ng, No, rtol=0, atol=1e-13)
+        assert np.allclose(dNg, dNo, rtol=0, atol=1e-12)
+    rng = np.random.default_rng(10)
+    c = np.clip(rng.normal(0.5, 0.15, nco), 0.0, 1.0).astype(np.float32)
+    em = prob["emask"].ravel() > 0
+    shell = (rng.uniform(size=o.ne) < 0.03).astype(np.uint8)
+    rg = g.coeff2density(c, shell).cpu().numpy()
+    ro = o.coeff2density(c.astype(np.float64), shell)
+    assert rel(rg[em], ro[em]) < 1e-6
+    gg = rng.standard_normal(o.ne).astype(np.float32)
+    assert rel(g.ddensity2dcoeff(gg, shell).cpu().numpy(), o.density2coeff_adjoint(gg.astype(np.float64), shell)) < 1e-6
+    for mode in (4, 5, 2):
+        vg, perg, dcg, cntg, dsg = g.deal_background_points(c, 8.0, mode)
+        vo, pero, dco, cnto, dso = o.selfsupport(c.astype(np.float64), 8.0, mode)
+        assert cntg == cnto and dsg == dso
+        assert abs(vg - vo) <= 1e-5 * max(abs(vo), 1e-12)
+        assert rel(perg.cpu().numpy(), pero) < 1e-5
+        assert rel(dcg.cpu().numpy(), dco) < 1e-4
+
+
+def test_worst_case_lanczos_vs_dense(oracle, cuda):
+    prob = P.top_loaded_cube(8)
+    g, o = make(oracle, prob, n_levels=3, first_factor=2, smoother=1, precision=1, pre=2, post=2)
+    g.update_stencil()
+    o.update_stencil()
+    lam_o, fo, uo = o.dense_worst(0, tol=1e-12)
+    lam_g, fg, ug, ritz = g.worst_case(steps=40, constrain_direction=0, tol=1e-10)
+    assert abs(lam_g - lam_o) <= 1e-6 * lam_o
+    fg = fg.cpu().numpy()
+    ug = ug.cpu().numpy()
+    s = np.sign(fg @ fo)
+    assert rel(s * fg, fo) < 1e-3
+    assert abs(fg @ ug - lam_o) <= 1e-6 * lam_o
+    # same Lanczos on the oracle (seeded start vector shared)
+    lam_l, _, _, _ = o.lanczos(40, 0, tol=1e-11)
+    assert abs(lam_l - lam_o) <= 1e-6 * lam_o
+
+
+def test_worst_case_cf_mode(oracle, cuda):
+    prob = P.ellipsoid(20, 12, 12, shell=2)
+    g, o = make(oracle, prob, smoother=1, precision=1, pre=2, post=2)
+    g.update_stencil()
+    o.update_stencil()
+    lam_o, _, _ = o.dense_worst(1, tol=1e-12)
+    lam_g, fg, ug, _ = g.worst_case(steps=60, constrain_direction=1, tol=1e-10)
+    assert abs(lam_g - lam_o) <= 1e-6 * lam_o
+    f = np.random.default_rng(11).standard_normal(3 * o.nn)
+    assert rel(g.forceProject(t(f, cuda), 1).cpu().numpy(), o.force_project(f, 1)) < 1e-14
+
+
+def test_modified_pm(oracle, cuda):
+    prob = P.top_loaded_cube(8)
+    g, o = make(oracle, prob, n_levels=3, first_factor=2, smoother=0)
+    g.update_stencil()
+    o.update_stencil()
+    cg, fg, ug, itg = g.modifiedPM(0, seed=42, max_itn=300)
+    co, fo, uo, ito = o.modified_pm(0, seed=42, max_itn=300)
+    assert itg == ito
+    assert abs(cg - co) <= 1e-8 * abs(co)
+
+
+def test_mma_matches_oracle(oracle, cuda):
+    import torch
+    from robustoptspline3d_b200 import MMA
+    rng = np.random.default_rng(12)
+    n, m = 500, 2
+    xo = oracle.MMA(n, m, 0.0, 1.0)
+    xg = MMA(n, m, 0.0, 1.0)
+    x0 = rng.uniform(0.2, 0.8, n)
+    xo.set_x(x0)
+    xg.set_x(x0)
+    for k in range(4):
+        x = xo.get()[0]
+        df = -np.exp(-x) * (1 + rng.uniform(0, 0.1, n))
+        dg = np.stack([np.full(n, 1.0 / n), rng.standard_normal(n) * 0.1])
+        gval = np.array([x.mean() - 0.4, 0.05 * np.sin(k)])
+        xo.update(df, dg, gval)
+        xg.update(torch.as_tensor(df, device="cuda"), torch.as_tensor(dg, device="cuda"), gval)
+        for a, b in zip(xg.get(), xo.get()):
+            assert np.allclose(a, b, rtol=1e-8, atol=1e-10)

@@ -223,6 +223,8 @@ rso_status rso_modified_pm(rso_handle* h, int constrain_direction, uint64_t seed
 rso_status rso_mma_create(int n, int m, const double* xmin_host, const double* xmax_host, rso_mma** out);
 /* start from a given design (host); the reference starts from the box midpoint */
 rso_status rso_mma_set_x(rso_mma* s, const double* x_host);
+/* the same from a device array (n doubles) */
+rso_status rso_mma_set_x_dev(rso_mma* s, const double* x_dev);
 rso_status rso_mma_get(rso_mma* s, double* x_host, double* L_host, double* U_host, double* alpha_host,
                        double* beta_host);
 /* device x (n doubles) of the current design */

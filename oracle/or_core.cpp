@@ -115,6 +115,9 @@ void orc::build_topology(or_problem* p, int n_levels, int first_factor) {
         out.back().factor = 2;
       }
     }
+    // the coarsest level is solved directly from its stencil, so at least one
+    // coarse level is kept (the reference would be left with only a dummy layer)
+    if (out.size() == 1) out.push_back(coarsen(l0, 2));
     p->L = out;
   } else {
     std::vector<Level> out;
@@ -820,7 +823,10 @@ extern "C" double or_vcycle(or_problem* p, double* u, const double* f, int pre, 
     double om = kind == 1 ? omega * 2.0 / p->lam[l] : omega;
     if (l < nl - 1) or_smooth(p, l, w.u[l].data(), w.f[l].data(), kind, om, pre, 0);
     else if (nl > 1) or_coarsest_solve(p, w.f[l].data(), w.u[l].data());
-    else or_smooth(p, l, w.u[l].data(), w.f[l].data(), kind, om, pre, 0);
+    else {  // single level: smoothing only, kept symmetric
+      or_smooth(p, l, w.u[l].data(), w.f[l].data(), kind, om, pre, 0);
+      or_smooth(p, l, w.u[l].data(), w.f[l].data(), kind, om, post, symmetric ? 1 : 0);
+    }
   }
   for (int l = nl - 2; l >= 0; l--) {
     or_prolong(p, l + 1, w.u[l + 1].data(), w.u[l].data());

@@ -339,6 +339,14 @@ extern "C" rso_status rso_mma_create(int n, int m, const double* xmin, const dou
   return RSO_OK;
 }
 
+extern "C" rso_status rso_mma_set_x_dev(rso_mma* s, const double* x) {
+  if (!s || !x) return RSO_ERR_INVALID_ARG;
+  MMA_CHECK(s, cudaMemcpyAsync(s->x, x, sizeof(double) * s->n, cudaMemcpyDeviceToDevice, s->stream));
+  k_clamp_asym<<<MMA_BLOCKS, MMA_THREADS, 0, s->stream>>>(s->n, s->x, s->L, s->U, s->alpha, s->beta, s->xmin, s->xmax); rso::note_launch();
+  MMA_CHECK(s, cudaStreamSynchronize(s->stream));
+  return RSO_OK;
+}
+
 extern "C" rso_status rso_mma_set_x(rso_mma* s, const double* x) {
   if (!s || !x) return RSO_ERR_INVALID_ARG;
   MMA_CHECK(s, cudaMemcpyAsync(s->x, x, sizeof(double) * s->n, cudaMemcpyHostToDevice, s->stream));

@@ -73,8 +73,12 @@ rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric) {
       RSO_TRY(restrict_<T>(h, li, LV<T>::r(h->L[li - 1]), LV<T>::f(l)));
       RSO_CHECK_CUDA(h, cudaMemsetAsync(LV<T>::u(l), 0, sizeof(T) * 3 * l.NP, h->stream));
     }
-    if (li < nl - 1 || nl == 1) RSO_TRY(smooth<T>(h, li, pre, 0));
-    else RSO_TRY(coarsest_solve<T>(h, LV<T>::f(l), LV<T>::u(l)));
+    if (li < nl - 1) RSO_TRY(smooth<T>(h, li, pre, 0));
+    else if (nl > 1) RSO_TRY(coarsest_solve<T>(h, LV<T>::f(l), LV<T>::u(l)));
+    else {  // single level: smoothing only, kept symmetric
+      RSO_TRY(smooth<T>(h, li, pre, 0));
+      RSO_TRY(smooth<T>(h, li, post, symmetric ? 1 : 0));
+    }
   }
   for (int li = nl - 2; li >= 0; li--) {
     RSO_TRY(prolong<T>(h, li + 1, LV<T>::u(h->L[li + 1]), LV<T>::u(h->L[li])));

@@ -360,6 +360,13 @@ rso_status build_topology(rso_handle* h, const uint8_t* emask, const uint8_t* fi
       }
     }
     for (size_t i = 1; i < halves.size(); i++) free_level_masks(halves[i]);
+    // keep at least one coarse level: the coarsest level is solved directly
+    // from its stencil (the reference would be left with only a dummy layer)
+    if (h->L.size() == 1) {
+      Level c;
+      RSO_TRY(coarsen_level(h, h->L[0], 2, c));
+      h->L.push_back(c);
+    }
   }
   for (auto& l : h->L) RSO_TRY(host_masks(h, l));
   // h->L may have been reallocated by push_back: take the finest level afresh

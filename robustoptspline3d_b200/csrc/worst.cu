@@ -130,7 +130,8 @@ rso_status worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t see
     double* u = h->lanczos_u[it];
     RSO_CHECK_CUDA(h, cudaMemsetAsync(u, 0, sizeof(double) * n3, h->stream));
     rso_solve_info si = {0, 0, 0};
-    RSO_TRY(solve_pcg(h, h->w, u, tol, 500, &si));
+    // high-contrast designs (void at rho_min^p = 1e-9) can need hundreds of CG steps
+    RSO_TRY(solve_pcg(h, h->w, u, tol, 4000, &si));
     total_it += si.iterations;
     k_gather_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(u, l0.NP, h->load_nodes, h->load_normals, nl, cf, wv); rso::note_launch();
     double a = 0;

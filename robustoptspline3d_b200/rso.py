@@ -119,6 +119,7 @@ SIGNATURES = {
     "rso_modified_pm": (_ci, [_vp, _ci, ctypes.c_uint64, _ci, _vp, _vp, _pd, _pi]),
     "rso_mma_create": (_ci, [_ci, _ci, _pd, _pd, ctypes.POINTER(_vp)]),
     "rso_mma_set_x": (_ci, [_vp, _pd]),
+    "rso_mma_set_x_dev": (_ci, [_vp, _vp]),
     "rso_mma_get": (_ci, [_vp, _pd, _pd, _pd, _pd, _pd]),
     "rso_mma_x_dev": (_vp, [_vp]),
     "rso_mma_update": (_ci, [_vp, _vp, _vp, _pd, _pi, _pd]),
@@ -592,7 +593,11 @@ class MMA:
         self.close()
 
     def set_x(self, x):
-        st = self.lib.rso_mma_set_x(self.s, _np_ptr(np.ascontiguousarray(x, np.float64), _pd))
+        import torch
+        if isinstance(x, torch.Tensor) and x.is_cuda:
+            st = self.lib.rso_mma_set_x_dev(self.s, _dev(x.contiguous(), torch.float64))
+        else:
+            st = self.lib.rso_mma_set_x(self.s, _np_ptr(np.ascontiguousarray(x, np.float64), _pd))
         if st:
             raise RSOError(f"rso_mma_set_x: {_STATUS.get(st, st)}")
 

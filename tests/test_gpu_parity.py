@@ -85,7 +85,8 @@ def test_operator_fp64(oracle, cuda, gen):
     assert rel(r_g, r_o) < 1e-13
 
 
-@pytest.mark.parametrize("gen,nl,ff", [(lambda: P.ellipsoid(24, 16, 12), 0, 4),
+@pytest.mark.parametrize("gen,nl,ff", [(lambda: P.ellipsoid(40, 24, 24), 0, 4),
+                                       (lambda: P.ellipsoid(24, 16, 12), 0, 4),
                                        (lambda: P.cantilever(16, 8, 8), 3, 2)])
 def test_galerkin_stencils_and_transfers(oracle, cuda, gen, nl, ff):
     prob = gen()

@@ -31,9 +31,13 @@ __device__ __forceinline__ void stencil_apply(const Level& L, const T* __restric
     const long long nb = n + (d % 3 - 1) + (d / 3 % 3 - 1) * px + (d / 9 - 1) * pxy;
     const T u0 = u[nb], u1 = u[nb + NP], u2 = u[nb + 2 * NP];
 #pragma unroll
-    for (int r = 0; r < 3; r++)
-      acc[r] += st[(d * 9 + r * 3 + 0) * NP + n] * u0 + st[(d * 9 + r * 3 + 1) * NP + n] * u1 +
-                st[(d * 9 + r * 3 + 2) * NP + n] * u2;
+    for (int r = 0; r < 3; r++) {
+      T s = acc[r];
+      s = fma(st[(d * 9 + r * 3 + 0) * NP + n], u0, s);
+      s = fma(st[(d * 9 + r * 3 + 1) * NP + n], u1, s);
+      s = fma(st[(d * 9 + r * 3 + 2) * NP + n], u2, s);
+      acc[r] = s;
+    }
   }
 }
 

@@ -171,6 +171,8 @@ rso_status fine_applyK(rso_handle* h, const T* u, T* f, const T* rp);
 template <typename T>
 rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega);
 template <typename T>
+rso_status fine_jacobi0(rso_handle* h, const T* f, T* u_out, const T* rp, double omega);
+template <typename T>
 rso_status fine_gs(rso_handle* h, T* u, const T* f, const T* rp, int colour, int reverse);
 rso_status upload_K0(rso_handle* h);
 rso_status penalise(rso_handle* h);
@@ -194,7 +196,7 @@ rso_status estimate_lambda(rso_handle* h);
 
 // solver (solver.cu)
 template <typename T>
-rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric);
+rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric, bool u0_zero);
 rso_status precondition(rso_handle* h, const double* r, double* z);
 rso_status solve_pcg(rso_handle* h, const double* f, double* u, double tol, int max_iter, rso_solve_info* info);
 rso_status solve_vcycles(rso_handle* h, const double* f, double* u, double tol, int max_iter,

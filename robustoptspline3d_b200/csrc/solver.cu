@@ -33,8 +33,10 @@ struct LV<float> {
   static const float* rp(rso_handle* h) { return h->rp32; }
 };
 
+// zero: the iterate is known to be zero before the first sweep (the first
+// damped-Jacobi sweep on the fine level then needs no operator application)
 template <typename T>
-static rso_status smooth(rso_handle* h, int li, int sweeps, int reverse) {
+static rso_status smooth(rso_handle* h, int li, int sweeps, int reverse, bool zero = false) {
   Level& l = h->L[li];
   if (h->cfg.smoother == RSO_SMOOTH_GS) {
     for (int s = 0; s < sweeps; s++)
@@ -46,7 +48,8 @@ static rso_status smooth(rso_handle* h, int li, int sweeps, int reverse) {
   } else {
     const double om = h->cfg.omega * 2.0 / l.lam;
     for (int s = 0; s < sweeps; s++) {
-      if (li == 0) RSO_TRY(fine_jacobi<T>(h, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om));
+      if (li == 0 && zero && s == 0) RSO_TRY(fine_jacobi0<T>(h, LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om));
+      else if (li == 0) RSO_TRY(fine_jacobi<T>(h, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om));
       else RSO_TRY(coarse_jacobi<T>(h, li, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), om));
       std::swap(LV<T>::u(l), LV<T>::t(l));
     }
@@ -64,7 +67,7 @@ static rso_status level_residual(rso_handle* h, int li) {
 // V-cycle on the level work vectors: L[0].f holds the right-hand side and
 // L[0].u the initial iterate; the result is left in L[0].u.
 template <typename T>
-rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric) {
+rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric, bool u0_zero) {
   const int nl = (int)h->L.size();
   for (int li = 0; li < nl; li++) {
     Level& l = h->L[li];
@@ -73,10 +76,11 @@ rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric) {
       RSO_TRY(restrict_<T>(h, li, LV<T>::r(h->L[li - 1]), LV<T>::f(l)));
       RSO_CHECK_CUDA(h, cudaMemsetAsync(LV<T>::u(l), 0, sizeof(T) * 3 * l.NP, h->stream));
     }
-    if (li < nl - 1) RSO_TRY(smooth<T>(h, li, pre, 0));
+    const bool zero = li > 0 || u0_zero;
+    if (li < nl - 1) RSO_TRY(smooth<T>(h, li, pre, 0, zero));
     else if (nl > 1) RSO_TRY(coarsest_solve<T>(h, LV<T>::f(l), LV<T>::u(l)));
     else {  // single level: smoothing only, kept symmetric
-      RSO_TRY(smooth<T>(h, li, pre, 0));
+      RSO_TRY(smooth<T>(h, li, pre, 0, zero));
       RSO_TRY(smooth<T>(h, li, post, symmetric ? 1 : 0));
     }
   }
@@ -87,8 +91,8 @@ rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric) {
   return RSO_OK;
 }
 
-template rso_status vcycle_levels<double>(rso_handle*, int, int, int);
-template rso_status vcycle_levels<float>(rso_handle*, int, int, int);
+template rso_status vcycle_levels<double>(rso_handle*, int, int, int, bool);
+template rso_status vcycle_levels<float>(rso_handle*, int, int, int, bool);
 
 __global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, long long n) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -107,12 +111,12 @@ rso_status precondition(rso_handle* h, const double* r, double* z) {
   if (h->cfg.precision == RSO_MIXED) {
     k_d2f<<<cdiv(n3, 256), 256, 0, h->stream>>>(r, l0.f32, n3); rso::note_launch();
     RSO_CHECK_CUDA(h, cudaMemsetAsync(l0.u32, 0, sizeof(float) * n3, h->stream));
-    RSO_TRY(vcycle_levels<float>(h, pre, post, 1));
+    RSO_TRY(vcycle_levels<float>(h, pre, post, 1, true));
     k_f2d<<<cdiv(n3, 256), 256, 0, h->stream>>>(l0.u32, z, n3); rso::note_launch();
   } else {
     RSO_CHECK_CUDA(h, cudaMemcpyAsync(l0.f64, r, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
     RSO_CHECK_CUDA(h, cudaMemsetAsync(l0.u64, 0, sizeof(double) * n3, h->stream));
-    RSO_TRY(vcycle_levels<double>(h, pre, post, 1));
+    RSO_TRY(vcycle_levels<double>(h, pre, post, 1, true));
     RSO_CHECK_CUDA(h, cudaMemcpyAsync(z, l0.u64, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
   }
   return launch_check(h, "precondition");
@@ -212,7 +216,7 @@ rso_status vcycle_fp64(rso_handle* h, double* u, const double* f, int pre, int p
   const long long n3 = 3 * l0.NP;
   RSO_CHECK_CUDA(h, cudaMemcpyAsync(l0.u64, u, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
   RSO_CHECK_CUDA(h, cudaMemcpyAsync(l0.f64, f, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
-  RSO_TRY(vcycle_levels<double>(h, pre, post, symmetric));
+  RSO_TRY(vcycle_levels<double>(h, pre, post, symmetric, false));
   RSO_CHECK_CUDA(h, cudaMemcpyAsync(u, h->L[0].u64, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
   RSO_TRY(fine_residual<double>(h, u, f, h->r, h->rp64));
   double rn2 = 0, fn2 = 0;

@@ -92,14 +92,19 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def dist_setup():
+def dist_setup(backend=None):
+    """One process per GPU (torchrun env); replicas exchange only barriers and
+    the max of their timings.  NCCL on GPUs, gloo for host-only runs."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import datetime
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -108,7 +113,8 @@ def barrier_max(world, value):
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.barrier()
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
@@ -179,10 +185,12 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
-    world, rank, local = dist_setup()
     if args.impl == "reference":
-        run_reference(args, world, rank)
+        # host-only arm: rank 0 times the CPU path, other ranks exit at once
+        # (no process group is needed for that)
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
         return
+    world, rank, local = dist_setup()
     import torch
     torch.cuda.set_device(local)
     import robustoptspline3d_b200 as R

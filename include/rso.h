@@ -184,6 +184,22 @@ rso_status rso_filter(rso_handle* h, double radius, const float* in_dev, float* 
 /* consistent density filter (same weights) and its adjoint (build mode) */
 rso_status rso_density_filter(rso_handle* h, double radius, const float* in_dev, float* out_dev);
 rso_status rso_density_filter_adjoint(rso_handle* h, double radius, const float* in_dev, float* out_dev);
+/* The sensitivity filter of rso_filter, computed without any device memory
+ * allocation; it has no counterpart in the reference.  rso_filter copies its
+ * tap table into a stream-ordered allocation made on every call; this entry
+ * point keeps the table in a fixed array of the library instead (52,728 bytes
+ * per device), for callers that cannot allocate device memory inside their
+ * loop: all free memory already handed to their own pool, a fixed device
+ * footprint, or no room for the pool growth and synchronisation an allocation
+ * can bring.  Limits: int(radius + 0.5) <= RSO_FILTER_NOALLOC_MAX_REACH
+ * (radius < 6.5); larger radii return RSO_ERR_INVALID_ARG with a message.
+ * The first call on a device looks the array up on that device (this may
+ * load the module there), so make it before any stream capture.  All calls
+ * on one device share the array: each call rewrites the entries it reads,
+ * and calls that overlap on one device (other threads or unordered streams)
+ * race and must be serialised by the caller.  Synchronises h's stream. */
+#define RSO_FILTER_NOALLOC_MAX_REACH 6
+rso_status rso_filter_noalloc(rso_handle* h, double radius, const float* in_dev, float* out_dev);
 /* volume fraction sum(rho)/n_gs_elements; Grid::volumeRatio (grid/Grid.cu:5642-5650) */
 rso_status rso_volume(rso_handle* h, const float* rho_dev, double* vol);
 

@@ -108,6 +108,7 @@ SIGNATURES = {
     "rso_filter": (_ci, [_vp, _cd, _vp, _vp]),
     "rso_density_filter": (_ci, [_vp, _cd, _vp, _vp]),
     "rso_density_filter_adjoint": (_ci, [_vp, _cd, _vp, _vp]),
+    "rso_filter_noalloc": (_ci, [_vp, _cd, _vp, _vp]),
     "rso_volume": (_ci, [_vp, _vp, _pd]),
     "rso_spline_setup": (_ci, [_vp, _ci, _ci, _ci, _ci, _pi]),
     "rso_spline_axis": (_ci, [_vp, _ci, _pi, _pd, _pd]),

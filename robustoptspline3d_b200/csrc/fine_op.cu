@@ -4,18 +4,15 @@
 // (update_residual_OTFA_WS_kernel grid/Grid.cu:2320-2376, applyK_OTFA_kernel
 // grid/Grid.cu:4358-4436, gs_relax_OTFA_WS_kernel grid/Grid.cu:1742-1885).
 //
-// Residual / apply / damped-Jacobi kernels march along z.  A CTA owns a
-// TX x TY column of nodes and a chunk of z planes; it keeps a rolling window
-// of four node planes of u (three in use, one being filled) and three element
-// planes of rho^p in shared memory, filled with cp.async while the previous
-// plane is computed, so every value is read from HBM about once per CTA
-// (halo overhead (TX+2)(TY+2)/(TX*TY)).  Each thread computes one node per
-// plane: the 27 neighbour displacements are multiplied by the K0 blocks of
-// the incident elements that contain both nodes, accumulated per element and
-// scaled by rho_e^p at the end (576 + 24 FMA per node).  K0 lives in constant
-// memory; with every loop unrolled each entry is a compile-time constant-bank
-// operand.  Support DOFs hold zero by construction, so neighbours need no
-// Dirichlet test; support rows are handled from the node-class byte.
+// The residual / apply / damped-Jacobi kernel (k_fine_w) evaluates every
+// element product K0 u_e in the sum/difference ("Walsh") basis of the
+// element's nodes, where K0 is block diagonal (8 blocks of 3x3, 45 non-zero
+// entries), and shares the face transforms between the two elements on
+// either side of a node plane, so a fine node costs about 200 additions and
+// multiplications instead of 576 multiply-adds.  Support DOFs hold zero by
+// construction, so neighbours need no Dirichlet test; support rows are
+// handled from the node-class byte.  The point Gauss-Seidel colour sweep and
+// the first Jacobi sweep from a zero iterate use K0 directly.
 #include "rso_internal.cuh"
 #include <cmath>
 #include <cuda_pipeline.h>
@@ -32,7 +29,10 @@ __device__ __forceinline__ double k0<double>(int i) { return cK0d[i]; }
 template <>
 __device__ __forceinline__ float k0<float>(int i) { return cK0f[i]; }
 
+rso_status upload_walsh(rso_handle* h);
+
 rso_status upload_K0(rso_handle* h) {
+  RSO_TRY(upload_walsh(h));
   float kf[576];
   for (int i = 0; i < 576; i++) kf[i] = (float)h->K0[i];
   RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cK0d, h->K0, sizeof(double) * 576, 0, cudaMemcpyHostToDevice, h->stream));
@@ -56,159 +56,327 @@ rso_status penalise(rso_handle* h) {
   return launch_check(h, "penalise");
 }
 
-constexpr int FTX = 32, FTY = 8, FZC = 32;
+// ---------------------------------------------------------------- Walsh-basis element operator
+//
+// Along each axis the two nodes of an element are combined into a sum and a
+// difference (H = [[1, 1], [-1, 1]]); over the 8 nodes this is W = H (x) H (x) H,
+// with W^T W = 8 I.  The reflections of the cube commute with K0, so in this
+// basis K0 splits into 8 symmetric 3x3 blocks: block c couples the entries
+// (mode c ^ (1 << j), component j), j = 0..2, and
+//   K0 u = W^T B W u,  B = (W K0 W^T) / 64  (45 non-zeros instead of 576).
+// Structural zeros (exact for the isotropic cube; checked on the host):
+// for one-bit c the translation row/column (c >> i & 1), for two-bit c the
+// entries coupling the axis outside c with the two inside it.
+__constant__ double cBd[72];  // [c][i][j]
+__constant__ float cBf[72];
+__constant__ double cD0d[9];  // diagonal 3x3 block of local node 0
+__constant__ float cD0f[9];
 
 template <typename T>
-constexpr int fine_smem_bytes() {
-  return (int)sizeof(T) * (4 * 3 * (FTX + 2) * (FTY + 2) + 3 * (FTX + 1) * (FTY + 1));
+__device__ __forceinline__ T bw(int i);
+template <>
+__device__ __forceinline__ double bw<double>(int i) { return cBd[i]; }
+template <>
+__device__ __forceinline__ float bw<float>(int i) { return cBf[i]; }
+template <typename T>
+__device__ __forceinline__ T d0(int i);
+template <>
+__device__ __forceinline__ double d0<double>(int i) { return cD0d[i]; }
+template <>
+__device__ __forceinline__ float d0<float>(int i) { return cD0f[i]; }
+
+__host__ __device__ constexpr bool b_zero(int c, int i, int j) {
+  const int pc = (c & 1) + ((c >> 1) & 1) + ((c >> 2) & 1);
+  if (pc == 1) return ((c >> i) & 1) || ((c >> j) & 1);
+  if (pc == 2) {
+    const int out = ~c & 7;
+    return (((out >> i) & 1) != 0) != (((out >> j) & 1) != 0);
+  }
+  return false;
+}
+
+rso_status upload_walsh(rso_handle* h) {
+  const double* K = h->K0;
+  // W[m][a] = prod_axis H[m_axis][a_axis]
+  auto Hh = [](int m, int b) { return m == 0 ? 1.0 : (b ? 1.0 : -1.0); };
+  double W[8][8];
+  for (int m = 0; m < 8; m++)
+    for (int a = 0; a < 8; a++) W[m][a] = Hh(m & 1, a & 1) * Hh((m >> 1) & 1, (a >> 1) & 1) * Hh(m >> 2, a >> 2);
+  double B[72], kmax = 0;
+  for (int i = 0; i < 576; i++) kmax = std::fmax(kmax, std::fabs(K[i]));
+  for (int c = 0; c < 8; c++)
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        const int mi = c ^ (1 << i), mj = c ^ (1 << j);
+        double s = 0;
+        for (int a = 0; a < 8; a++)
+          for (int b = 0; b < 8; b++) s += W[mi][a] * K[(a * 3 + i) * 24 + b * 3 + j] * W[mj][b];
+        s /= 64.0;
+        if (b_zero(c, i, j)) {
+          if (std::fabs(s) > 1e-12 * kmax) {
+            h->err = "element matrix lacks the reflection symmetry of the cube";
+            return RSO_ERR_INVALID_ARG;
+          }
+          s = 0;
+        }
+        B[c * 9 + i * 3 + j] = s;
+      }
+  // diagonal blocks: K0[a][a](i, j) = D0(i, j) * sigma_i(a) * sigma_j(a), sigma = 1 - 2 bit
+  double D0[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) D0[i * 3 + j] = K[i * 24 + j];
+  for (int a = 0; a < 8; a++)
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        const double si = ((a >> i) & 1) ? -1.0 : 1.0, sj = ((a >> j) & 1) ? -1.0 : 1.0;
+        if (std::fabs(K[(a * 3 + i) * 24 + a * 3 + j] - D0[i * 3 + j] * si * sj) > 1e-12 * kmax) {
+          h->err = "element matrix diagonal blocks lack the reflection symmetry of the cube";
+          return RSO_ERR_INVALID_ARG;
+        }
+      }
+  float Bf[72], Df[9];
+  for (int i = 0; i < 72; i++) Bf[i] = (float)B[i];
+  for (int i = 0; i < 9; i++) Df[i] = (float)D0[i];
+  RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cBd, B, sizeof(B), 0, cudaMemcpyHostToDevice, h->stream));
+  RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cBf, Bf, sizeof(Bf), 0, cudaMemcpyHostToDevice, h->stream));
+  RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cD0d, D0, sizeof(D0), 0, cudaMemcpyHostToDevice, h->stream));
+  RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cD0f, Df, sizeof(Df), 0, cudaMemcpyHostToDevice, h->stream));
+  // the host copies are stack arrays: finish the copies before returning
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  return RSO_OK;
+}
+
+// Residual / apply / damped-Jacobi kernel.  A CTA of 32 x TY threads marches
+// along z through FZC node planes.  Thread (tx, ty) owns the element column
+// (ex, ey) = (x0 - 1 + tx, y0 - 1 + ty) and the node (ex + 1, ey + 1), so a
+// CTA computes 32 x TY element columns and writes the 31 x (TY - 1) nodes
+// whose four surrounding columns it holds.  Per element layer z (between node
+// planes z and z+1) a thread
+//   1. forms the xy sum/difference modes of the 4 nodes of its top face
+//      (plane z+1) from the staged plane, the bottom face coming from the
+//      previous layer,
+//   2. combines them along z, applies the 8 blocks of B and scales by rho^p,
+//   3. splits the result into its bottom- and top-face parts, adds the bottom
+//      part to the top part of layer z-1 (both act on plane z), and
+//   4. transforms that face back to its 4 corner nodes; the node sums the
+//      corners of its 4 columns through shared memory.
+// Node planes of u (3 components, 33 x (TY+1)) and element layers of rho^p are
+// staged with cp.async WPD stages ahead in WNSLOT slots.
+constexpr int WTX = 32, FZC = 32, WPD = 2, WNSLOT = 4;
+
+template <typename T, int TY>
+constexpr int walsh_smem_bytes() {
+  return (int)sizeof(T) * (WNSLOT * (3 * (WTX + 1) * (TY + 1) + WTX * TY) + 9 * WTX * TY);
 }
 
 // MODE 0: out = f - K u;  MODE 1: out = K u (support rows pass u);
 // MODE 2: out = u + omega D^-1 (f - K u)  (damped block Jacobi, D = 3x3 diagonal block)
-template <typename T, int MODE>
-__global__ void __launch_bounds__(FTX* FTY, sizeof(T) == 8 ? 2 : 3)
-    k_fine(const Level L, const T* __restrict__ u, const T* __restrict__ f,
-                                                   T* __restrict__ out, const T* __restrict__ rp, T omega) {
-  constexpr int SX = FTX + 2, SY = FTY + 2, SP = SX * SY;  // one component of a node plane
-  constexpr int EX = FTX + 1, EY = FTY + 1, EP = EX * EY;  // an element plane
-  constexpr int NT = FTX * FTY;
+template <typename T, int MODE, int TY>
+__global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
+    k_fine_w(const Level L, const T* __restrict__ u, const T* __restrict__ f, T* __restrict__ out,
+             const T* __restrict__ rp, T omega) {
+  constexpr int NX = WTX + 1, NPL = NX * (TY + 1), NE = WTX * TY, SLOT = 3 * NPL + NE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* su = reinterpret_cast<T*>(smem_raw);  // [4 slots][3 comps][SP]
-  T* sr = su + 4 * 3 * SP;                 // [3 slots][EP]
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * FTX + tx;
-  const int x0 = blockIdx.x * FTX, y0 = blockIdx.y * FTY;
-  const int z0 = blockIdx.z * FZC;
-  const int z1 = min(z0 + FZC, L.nz);
+  T* ss = reinterpret_cast<T*>(smem_raw);  // [WNSLOT][SLOT]: u plane (3 comps) + rho layer
+  T* sx = ss + WNSLOT * SLOT;              // [9][NE]: corners (0,0), (1,0), (0,1)
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * WTX + tx;
+  const int x0 = blockIdx.x * (WTX - 1), y0 = blockIdx.y * (TY - 1);
+  const int z0 = blockIdx.z * FZC, z1 = min(z0 + FZC, L.nz);
+  const int ex = x0 - 1 + tx, ey = y0 - 1 + ty;
   const long long NP = L.NP;
 
-  // node plane zp (in [-1, nz]) -> slot; element plane ep (in [-1, ez]) -> slot
-  auto load_u = [&](int zp, int slot) {
-    for (int i = tid; i < 3 * SP; i += NT) {
-      const int c = i / SP, r = i - c * SP, sy = r / SX, sx = r - sy * SX;
-      const int gx = x0 - 1 + sx, gy = y0 - 1 + sy;
-      T* dst = su + (slot * 3 + c) * SP + r;
-      if (gx <= L.nx && gy <= L.ny && zp <= L.nz)
-        __pipeline_memcpy_async(dst, u + L.nidx(gx, gy, zp) + c * NP, sizeof(T));
-      else
-        *dst = T(0);
+  // per-thread staging slots: entry i = tid + k*NE of the plane tile, as an
+  // in-plane offset (component plane included; -1 outside the padded box)
+  constexpr int KU = (3 * NPL + NE - 1) / NE;
+  int ioff[KU];
+#pragma unroll
+  for (int k = 0; k < KU; k++) {
+    const int i = tid + k * NE;
+    const int c = i / NPL, r = i - c * NPL, sy = r / NX, sxx = r - sy * NX;
+    const int gx = x0 - 1 + sxx, gy = y0 - 1 + sy;
+    ioff[k] = (i < 3 * NPL && gx <= L.nx && gy <= L.ny) ? (int)(c * NP + (gx + 1) + (long long)L.px * (gy + 1)) : -1;
+  }
+  const bool rvalid = ex <= L.ex && ey <= L.ey;
+  const long long roff = rvalid ? L.eidx(ex, ey, -1) : 0;
+  const long long pxy = (long long)L.px * L.py, qxy = (long long)L.qx * L.qy;
+  // stage s: node plane s of u and element layer s of rho^p (zero outside)
+  auto issue = [&](int s) {
+    T* dst = ss + ((s + WNSLOT) % WNSLOT) * SLOT;
+    const long long po = pxy * (s + 1);
+#pragma unroll
+    for (int k = 0; k < KU; k++) {
+      const int i = tid + k * NE;
+      if (i < 3 * NPL) {
+        if (ioff[k] >= 0 && s <= L.nz)
+          __pipeline_memcpy_async(dst + i, u + po + ioff[k], sizeof(T));
+        else
+          dst[i] = T(0);
+      }
     }
-  };
-  auto load_r = [&](int ep, int slot) {
-    for (int i = tid; i < EP; i += NT) {
-      const int sy = i / EX, sx = i - sy * EX;
-      const int gx = x0 - 1 + sx, gy = y0 - 1 + sy;
-      T* dst = sr + slot * EP + i;
-      if (gx <= L.ex && gy <= L.ey && ep <= L.ez)
-        __pipeline_memcpy_async(dst, rp + L.eidx(gx, gy, ep), sizeof(T));
-      else
-        *dst = T(0);
-    }
-  };
-
-  // prologue: node planes z0-1, z0, z0+1 and element planes z0-1, z0
-  load_u(z0 - 1, (z0 + 3) & 3);
-  load_u(z0, z0 & 3);
-  load_r(z0 - 1, (z0 + 2) % 3);
-  __pipeline_commit();
-  load_u(z0 + 1, (z0 + 1) & 3);
-  load_r(z0, z0 % 3);
-  __pipeline_commit();
-
-  const int x = x0 + tx, y = y0 + ty;
-  const bool inside = x < L.nx && y < L.ny;
-  for (int z = z0; z < z1; z++) {
-    // stage the next planes while this one is computed
-    if (z + 2 <= L.nz && z + 1 < z1 + 1) load_u(z + 2, (z + 2) & 3);
-    if (z + 1 <= L.ez) load_r(z + 1, (z + 1) % 3);
+    if (rvalid && s <= L.ez)
+      __pipeline_memcpy_async(dst + 3 * NPL + tid, rp + roff + qxy * (s + 1), sizeof(T));
+    else
+      dst[3 * NPL + tid] = T(0);
     __pipeline_commit();
-    __pipeline_wait_prior(1);
-    __syncthreads();
-    if (inside) {
-      const long long n = L.nidx(x, y, z);
-      const uint8_t cls = L.vclass[n];
-      const bool work = (cls & NC_ACTIVE) && !(cls & NC_SUPPORT);
-      T acc0 = 0, acc1 = 0, acc2 = 0;
-      T D[6] = {0, 0, 0, 0, 0, 0};
-      if (work) {
-        const T* pu[3] = {su + ((z + 3) & 3) * 3 * SP, su + (z & 3) * 3 * SP, su + ((z + 1) & 3) * 3 * SP};
-        const T* pr[2] = {sr + ((z + 2) % 3) * EP, sr + (z % 3) * EP};
-        T r[8];
+  };
+  // xy modes of the 4 face nodes of this column on a staged plane; also the
+  // own node (corner (1,1)) values
+  auto face = [&](const T* pl, T (&F)[4][3], T (&own)[3]) {
 #pragma unroll
-        for (int k = 0; k < 8; k++) r[k] = pr[k >> 2][(ty + ((k >> 1) & 1)) * EX + tx + (k & 1)];
-        T a[8][3];
-#pragma unroll
-        for (int k = 0; k < 8; k++) a[k][0] = a[k][1] = a[k][2] = 0;
-#pragma unroll
-        for (int d = 0; d < 27; d++) {
-          const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
-          const T* q = pu[dz + 1] + (ty + 1 + dy) * SX + (tx + 1 + dx);
-          const T u0 = q[0], u1 = q[SP], u2 = q[2 * SP];
-#pragma unroll
-          for (int k = 0; k < 8; k++) {
-            const int kx = k & 1, ky = (k >> 1) & 1, kz = k >> 2;
-            if ((dx == kx - 1 || dx == kx) && (dy == ky - 1 || dy == ky) && (dz == kz - 1 || dz == kz)) {
-              const int vi = 7 - k;
-              const int vj = (dx - kx + 1) + 2 * (dy - ky + 1) + 4 * (dz - kz + 1);
-#pragma unroll
-              for (int rr = 0; rr < 3; rr++) {
-                // explicit fused chain: one FMA per matrix entry
-                T s = a[k][rr];
-                s = fma(k0<T>((vi * 3 + rr) * 24 + vj * 3 + 0), u0, s);
-                s = fma(k0<T>((vi * 3 + rr) * 24 + vj * 3 + 1), u1, s);
-                s = fma(k0<T>((vi * 3 + rr) * 24 + vj * 3 + 2), u2, s);
-                a[k][rr] = s;
-              }
-            }
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          acc0 += r[k] * a[k][0];
-          acc1 += r[k] * a[k][1];
-          acc2 += r[k] * a[k][2];
-        }
-        if (MODE == 2) {
-#pragma unroll
-          for (int k = 0; k < 8; k++) {
-            const int vi = 7 - k;
-            D[0] += r[k] * k0<T>((vi * 3 + 0) * 24 + vi * 3 + 0);
-            D[1] += r[k] * k0<T>((vi * 3 + 0) * 24 + vi * 3 + 1);
-            D[2] += r[k] * k0<T>((vi * 3 + 0) * 24 + vi * 3 + 2);
-            D[3] += r[k] * k0<T>((vi * 3 + 1) * 24 + vi * 3 + 1);
-            D[4] += r[k] * k0<T>((vi * 3 + 1) * 24 + vi * 3 + 2);
-            D[5] += r[k] * k0<T>((vi * 3 + 2) * 24 + vi * 3 + 2);
-          }
-        }
-      }
-      if (MODE == 0) {
-        out[n] = f[n] - acc0;
-        out[n + NP] = f[n + NP] - acc1;
-        out[n + 2 * NP] = f[n + 2 * NP] - acc2;
-      } else if (MODE == 1) {
-        const bool pass = (cls & NC_SUPPORT) != 0;
-        const T* c0 = su + (z & 3) * 3 * SP + (ty + 1) * SX + (tx + 1);
-        out[n] = pass ? c0[0] : acc0;
-        out[n + NP] = pass ? c0[SP] : acc1;
-        out[n + 2 * NP] = pass ? c0[2 * SP] : acc2;
-      } else {
-        if (!work) {
-          out[n] = 0; out[n + NP] = 0; out[n + 2 * NP] = 0;
-        } else {
-          const T* c0 = su + (z & 3) * 3 * SP + (ty + 1) * SX + (tx + 1);
-          const T r0 = f[n] - acc0, r1 = f[n + NP] - acc1, r2 = f[n + 2 * NP] - acc2;
-          // symmetric 3x3 inverse
-          const T a = D[0], b = D[1], c = D[2], d = D[3], e = D[4], g = D[5];
-          const T A = d * g - e * e, B = c * e - b * g, C = b * e - c * d;
-          const T det = a * A + b * B + c * C;
-          const T id = omega / det;
-          const T E = a * g - c * c, F = b * c - a * e, I = a * d - b * b;
-          out[n] = c0[0] + id * (A * r0 + B * r1 + C * r2);
-          out[n + NP] = c0[SP] + id * (B * r0 + E * r1 + F * r2);
-          out[n + 2 * NP] = c0[2 * SP] + id * (C * r0 + F * r1 + I * r2);
-        }
-      }
+    for (int c = 0; c < 3; c++) {
+      const T* p = pl + c * NPL + ty * NX + tx;
+      const T a00 = p[0], a10 = p[1], a01 = p[NX], a11 = p[NX + 1];
+      const T s0 = a00 + a10, d0 = a10 - a00, s1 = a01 + a11, d1 = a11 - a01;
+      F[0][c] = s0 + s1;  // (mx, my) = (0, 0)
+      F[1][c] = d0 + d1;  // (1, 0)
+      F[2][c] = s1 - s0;  // (0, 1)
+      F[3][c] = d1 - d0;  // (1, 1)
+      own[c] = a11;
     }
+  };
+
+  for (int s = z0 - 1; s <= z0 - 1 + WPD; s++) issue(s);
+  __pipeline_wait_prior(WPD);
+  __syncthreads();
+  T F[4][3], Gt[4][3], uc[3], rprev[4];
+  face(ss + ((z0 - 1 + WNSLOT) % WNSLOT) * SLOT, F, uc);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    Gt[q][0] = Gt[q][1] = Gt[q][2] = T(0);
+    rprev[q] = T(0);
+  }
+  const bool writer = tx < WTX - 1 && ty < TY - 1 && ex + 1 < L.nx && ey + 1 < L.ny;
+
+  for (int z = z0 - 1; z < z1; z++) {
+    issue(z + 1 + WPD);
+    __pipeline_wait_prior(WPD);
     __syncthreads();
+    const T* su = ss + ((z + 1 + WNSLOT) % WNSLOT) * SLOT;
+    const T* sr = ss + ((z + WNSLOT) % WNSLOT) * SLOT + 3 * NPL;
+    T v[8][3], un[3];
+    {
+      T Fn[4][3];
+      face(su, Fn, un);
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          v[q][c] = F[q][c] + Fn[q][c];
+          v[q + 4][c] = Fn[q][c] - F[q][c];
+          F[q][c] = Fn[q][c];
+        }
+    }
+    // blocks of B, in place (block c maps its three entries onto themselves), times rho^p
+    const T re = sr[tid];
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      T in[3], o[3];
+#pragma unroll
+      for (int j = 0; j < 3; j++) in[j] = v[c ^ (1 << j)][j];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        T s = T(0);
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+          if (!b_zero(c, i, j)) s = fma(bw<T>(c * 9 + i * 3 + j), in[j], s);
+        o[i] = s * re;
+      }
+#pragma unroll
+      for (int i = 0; i < 3; i++) v[c ^ (1 << i)][i] = o[i];
+    }
+    // bottom face (plane z) = S - D, top face (plane z+1) = S + D
+    T tot[4][3];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        tot[q][c] = Gt[q][c] + (v[q][c] - v[q + 4][c]);
+        Gt[q][c] = v[q][c] + v[q + 4][c];
+      }
+    if (z >= z0) {
+      // back to the 4 corners of plane z: corner (bx, by)
+      T cor[4][3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const T e0 = tot[0][c] - tot[1][c], e1 = tot[0][c] + tot[1][c];  // my = 0: bx = 0, 1
+        const T g0 = tot[2][c] - tot[3][c], g1 = tot[2][c] + tot[3][c];  // my = 1
+        cor[0][c] = e0 - g0;  // (0, 0)
+        cor[1][c] = e1 - g1;  // (1, 0)
+        cor[2][c] = e0 + g0;  // (0, 1)
+        cor[3][c] = e1 + g1;  // (1, 1)
+      }
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) sx[(k * 3 + c) * NE + tid] = cor[k][c];
+      T rl[4];
+      if (MODE == 2) {
+        rl[0] = re;
+        rl[1] = writer ? sr[tid + 1] : T(0);
+        rl[2] = writer ? sr[tid + WTX] : T(0);
+        rl[3] = writer ? sr[tid + WTX + 1] : T(0);
+      }
+      __syncthreads();
+      if (writer) {
+        T acc[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+          acc[c] = cor[3][c] + sx[(2 * 3 + c) * NE + tid + 1] + sx[(1 * 3 + c) * NE + tid + WTX] +
+                   sx[(0 * 3 + c) * NE + tid + WTX + 1];
+        const long long n = L.nidx(ex + 1, ey + 1, z);
+        const uint8_t cls = L.vclass[n];
+        const bool work = (cls & NC_ACTIVE) && !(cls & NC_SUPPORT);
+        if (MODE == 0) {
+#pragma unroll
+          for (int c = 0; c < 3; c++) out[n + c * NP] = f[n + c * NP] - (work ? acc[c] : T(0));
+        } else if (MODE == 1) {
+          const bool pass = (cls & NC_SUPPORT) != 0;
+#pragma unroll
+          for (int c = 0; c < 3; c++) out[n + c * NP] = pass ? uc[c] : (work ? acc[c] : T(0));
+        } else {
+          if (!work) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) out[n + c * NP] = T(0);
+          } else {
+            // D = sum_e rho_e K0[a_e][a_e]; node bits in column (ex + a, ey + b), layer z - 1 + l
+            // are (1 - a, 1 - b, 1 - l), so sigma = (2a - 1, 2b - 1, 2l - 1)
+            const T lo = rprev[0] + rprev[1] + rprev[2] + rprev[3];
+            const T hi = rl[0] + rl[1] + rl[2] + rl[3];
+            const T R = lo + hi;
+            // sigma_x sigma_y = +1 for (a, b) = (0,0), (1,1)
+            const T pxy_ = (rprev[0] + rprev[3] - rprev[1] - rprev[2]) + (rl[0] + rl[3] - rl[1] - rl[2]);
+            const T xlo = rprev[1] + rprev[3] - rprev[0] - rprev[2], xhi = rl[1] + rl[3] - rl[0] - rl[2];
+            const T ylo = rprev[2] + rprev[3] - rprev[0] - rprev[1], yhi = rl[2] + rl[3] - rl[0] - rl[1];
+            const T pxz = xhi - xlo, pyz = yhi - ylo;
+            const T a = d0<T>(0) * R, b = d0<T>(1) * pxy_, cc = d0<T>(2) * pxz;
+            const T d = d0<T>(4) * R, e = d0<T>(5) * pyz, g = d0<T>(8) * R;
+            const T r0 = f[n] - acc[0], r1 = f[n + NP] - acc[1], r2 = f[n + 2 * NP] - acc[2];
+            const T A = d * g - e * e, B = cc * e - b * g, C = b * e - cc * d;
+            const T det = a * A + b * B + cc * C;
+            const T id = omega / det;
+            const T E = a * g - cc * cc, Fm = b * cc - a * e, I = a * d - b * b;
+            out[n] = uc[0] + id * (A * r0 + B * r1 + C * r2);
+            out[n + NP] = uc[1] + id * (B * r0 + E * r1 + Fm * r2);
+            out[n + 2 * NP] = uc[2] + id * (C * r0 + Fm * r1 + I * r2);
+          }
+        }
+      }
+      if (MODE == 2) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) rprev[q] = rl[q];
+      }
+    } else {
+      if (MODE == 2) {
+        rprev[0] = re;
+        rprev[1] = writer ? sr[tid + 1] : T(0);
+        rprev[2] = writer ? sr[tid + WTX] : T(0);
+        rprev[3] = writer ? sr[tid + WTX + 1] : T(0);
+      }
+      // the next issue() refills the slot read in this (first) step
+      __syncthreads();
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) uc[c] = un[c];
   }
   __pipeline_wait_prior(0);
 }
@@ -325,7 +493,8 @@ __global__ void __launch_bounds__(256) k_fine_gs(const Level L, T* __restrict__ 
 }
 
 static inline dim3 plane_grid(const Level& l) { return dim3(cdiv(l.nx, 32), cdiv(l.ny, 8), l.nz); }
-static inline dim3 march_grid(const Level& l) { return dim3(cdiv(l.nx, FTX), cdiv(l.ny, FTY), cdiv(l.nz, FZC)); }
+constexpr int WTY = 8;
+static inline dim3 march_grid(const Level& l) { return dim3(cdiv(l.nx, WTX - 1), cdiv(l.ny, WTY - 1), cdiv(l.nz, FZC)); }
 
 template <typename T>
 static inline int pcls(int c32, int c64) { return sizeof(T) == 4 ? c32 : c64; }
@@ -334,14 +503,18 @@ template <typename T, int MODE>
 static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, const T* rp, double omega, int cls,
                               const char* what) {
   const Level& l = h->L[0];
-  constexpr int smem = fine_smem_bytes<T>();
+  if (3 * l.NP >= (1LL << 31)) {
+    h->err = "fine level too large for 32-bit in-plane offsets";
+    return RSO_ERR_UNSUPPORTED;
+  }
+  constexpr int smem = walsh_smem_bytes<T, WTY>();
   static bool attr = false;
   if (!attr) {
-    RSO_CHECK_CUDA(h, cudaFuncSetAttribute(k_fine<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    RSO_CHECK_CUDA(h, cudaFuncSetAttribute(k_fine_w<T, MODE, WTY>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr = true;
   }
   if (h->prof_on) prof_begin(h, cls, (double)l.nn);
-  k_fine<T, MODE><<<march_grid(l), dim3(FTX, FTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega);
+  k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega);
   rso::note_launch();
   if (h->prof_on) prof_end(h, cls);
   return launch_check(h, what);

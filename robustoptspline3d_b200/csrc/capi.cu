@@ -191,13 +191,14 @@ static rso_status setup(rso_handle* h, int ex, int ey, int ez, const uint8_t* em
     RSO_CHECK_CUDA(h, cudaMemcpy(h->T1, T.data(), sizeof(double) * T.size(), cudaMemcpyHostToDevice));
     // coarsest node list + node->row map
     const Level& c = h->L.back();
+    const std::vector<uint8_t>& cvm = h->h_vmask.back();
     std::vector<int> nodes;
     std::vector<int> crow(c.NP, -1);
     for (int z = 0; z < c.nz; z++)
       for (int y = 0; y < c.ny; y++)
         for (int x = 0; x < c.nx; x++) {
           const long long i = x + (long long)c.nx * (y + (long long)c.ny * z);
-          if (!c.h_vmask[i]) continue;
+          if (!cvm[i]) continue;
           crow[c.nidx(x, y, z)] = (int)nodes.size();
           nodes.push_back((int)c.nidx(x, y, z));
         }

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <type_traits>
 #include <vector>
 #include "../../include/rso.h"
 
@@ -28,7 +29,6 @@ struct Level {
   long long nn = 0, ne = 0;       // unpadded counts
   int factor = 0;                 // coarsening factor from the finer level
   long long n_active_e = 0, n_active_v = 0;
-  std::vector<uint8_t> h_emask, h_vmask;   // host copies (unpadded), set-up only
   uint8_t* emask = nullptr;       // padded element mask
   uint8_t* vclass = nullptr;      // padded node class
   double* KE = nullptr;           // coarse element matrices, 576 per unpadded element
@@ -44,6 +44,11 @@ struct Level {
     return (long long)(x + 1) + (long long)qx * ((y + 1) + (long long)qy * (z + 1));
   }
 };
+
+// Level is passed to kernels by value: it must stay a plain, trivially
+// copyable record (host-side data such as the unpadded masks lives in the
+// handle), or every launch would copy it member by member on the host.
+static_assert(std::is_trivially_copyable<Level>::value, "Level must be trivially copyable");
 
 struct Spline {
   int order = 0, part[3] = {0, 0, 0}, nb[3] = {0, 0, 0};
@@ -69,6 +74,7 @@ struct rso_handle {
   bool own_stream = false;
   int device = 0;
   std::vector<rso::Level> L;
+  std::vector<std::vector<uint8_t>> h_emask, h_vmask;  // per level, unpadded host copies (set-up only)
   double K0[576];
   double* K0_dev = nullptr;
   // fine-level design fields (padded elements)

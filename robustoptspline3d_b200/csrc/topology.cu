@@ -292,17 +292,20 @@ static void free_level_masks(Level& l) {
   l.vclass = nullptr;
 }
 
-static rso_status host_masks(rso_handle* h, Level& l) {
+static rso_status host_masks(rso_handle* h, int li) {
+  const Level& l = h->L[li];
+  std::vector<uint8_t>& hem = h->h_emask[li];
+  std::vector<uint8_t>& hvm = h->h_vmask[li];
   uint8_t* d = nullptr;
   long long n = std::max(l.ne, l.nn);
   RSO_CHECK_CUDA(h, cudaMallocAsync(&d, n, h->stream));
-  l.h_emask.resize(l.ne);
-  l.h_vmask.resize(l.nn);
+  hem.resize(l.ne);
+  hvm.resize(l.nn);
   k_unpad_u8<<<cdiv(l.ne, 256), 256, 0, h->stream>>>(l.emask, l.ne, l.ex, l.ey, l.qx, l.qy, 0xff, d); rso::note_launch();
-  RSO_CHECK_CUDA(h, cudaMemcpyAsync(l.h_emask.data(), d, l.ne, cudaMemcpyDeviceToHost, h->stream));
+  RSO_CHECK_CUDA(h, cudaMemcpyAsync(hem.data(), d, l.ne, cudaMemcpyDeviceToHost, h->stream));
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   k_unpad_u8<<<cdiv(l.nn, 256), 256, 0, h->stream>>>(l.vclass, l.nn, l.nx, l.ny, l.px, l.py, NC_ACTIVE, d); rso::note_launch();
-  RSO_CHECK_CUDA(h, cudaMemcpyAsync(l.h_vmask.data(), d, l.nn, cudaMemcpyDeviceToHost, h->stream));
+  RSO_CHECK_CUDA(h, cudaMemcpyAsync(hvm.data(), d, l.nn, cudaMemcpyDeviceToHost, h->stream));
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   RSO_CHECK_CUDA(h, cudaFreeAsync(d, h->stream));
   return RSO_OK;
@@ -368,7 +371,9 @@ rso_status build_topology(rso_handle* h, const uint8_t* emask, const uint8_t* fi
       h->L.push_back(c);
     }
   }
-  for (auto& l : h->L) RSO_TRY(host_masks(h, l));
+  h->h_emask.assign(h->L.size(), {});
+  h->h_vmask.assign(h->L.size(), {});
+  for (int li = 0; li < (int)h->L.size(); li++) RSO_TRY(host_masks(h, li));
   // h->L may have been reallocated by push_back: take the finest level afresh
   Level& lf = h->L[0];
 
@@ -484,8 +489,8 @@ extern "C" rso_status rso_bitsat_rank(rso_handle* h, const uint32_t* words, int6
 extern "C" rso_status rso_level_masks(rso_handle* h, int level, uint8_t* em, uint8_t* vm) {
   if (!h || level < 0 || level >= (int)h->L.size()) return RSO_ERR_INVALID_ARG;
   Level& l = h->L[level];
-  if (em) std::memcpy(em, l.h_emask.data(), l.ne);
-  if (vm) std::memcpy(vm, l.h_vmask.data(), l.nn);
+  if (em) std::memcpy(em, h->h_emask[level].data(), l.ne);
+  if (vm) std::memcpy(vm, h->h_vmask[level].data(), l.nn);
   return RSO_OK;
 }
 
@@ -494,11 +499,13 @@ extern "C" rso_status rso_level_bitwords(rso_handle* h, int level, uint32_t* eb,
   Level& l = h->L[level];
   if (eb) {
     std::memset(eb, 0, sizeof(uint32_t) * ((l.ne + 31) / 32));
-    for (long long i = 0; i < l.ne; i++) if (l.h_emask[i]) eb[i >> 5] |= 1u << (i & 31);
+    const uint8_t* m = h->h_emask[level].data();
+    for (long long i = 0; i < l.ne; i++) if (m[i]) eb[i >> 5] |= 1u << (i & 31);
   }
   if (vb) {
     std::memset(vb, 0, sizeof(uint32_t) * ((l.nn + 31) / 32));
-    for (long long i = 0; i < l.nn; i++) if (l.h_vmask[i]) vb[i >> 5] |= 1u << (i & 31);
+    const uint8_t* m = h->h_vmask[level].data();
+    for (long long i = 0; i < l.nn; i++) if (m[i]) vb[i >> 5] |= 1u << (i & 31);
   }
   return RSO_OK;
 }

@@ -166,7 +166,7 @@ constexpr int WTX = 32, FZC = 32, WPD = 2, WNSLOT = 4;
 
 template <typename T, int TY>
 constexpr int walsh_smem_bytes() {
-  return (int)sizeof(T) * (WNSLOT * (3 * (WTX + 1) * (TY + 1) + WTX * TY) + 9 * WTX * TY);
+  return (int)sizeof(T) * (WNSLOT * (3 * (WTX + 1) * (TY + 1) + WTX * TY) + 2 * 9 * WTX * TY);
 }
 
 // MODE 0: out = f - K u;  MODE 1: out = K u (support rows pass u);
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
   constexpr int NX = WTX + 1, NPL = NX * (TY + 1), NE = WTX * TY, SLOT = 3 * NPL + NE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* ss = reinterpret_cast<T*>(smem_raw);  // [WNSLOT][SLOT]: u plane (3 comps) + rho layer
-  T* sx = ss + WNSLOT * SLOT;              // [9][NE]: corners (0,0), (1,0), (0,1)
+  T* sx = ss + WNSLOT * SLOT;              // [2][9][NE]: corners (0,0), (1,0), (0,1), by plane parity
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * WTX + tx;
   const int x0 = blockIdx.x * (WTX - 1), y0 = blockIdx.y * (TY - 1);
   const int z0 = blockIdx.z * FZC, z1 = min(z0 + FZC, L.nz);
@@ -238,19 +238,81 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
   for (int s = z0 - 1; s <= z0 - 1 + WPD; s++) issue(s);
   __pipeline_wait_prior(WPD);
   __syncthreads();
-  T F[4][3], Gt[4][3], uc[3], rprev[4];
+  const bool writer = tx < WTX - 1 && ty < TY - 1 && ex + 1 < L.nx && ey + 1 < L.ny;
+  // per-plane registers: F face modes of plane z; Gt top-face part of layer
+  // z-1; uc/uo u at the own node on planes z / z-1; own corner, f and class
+  // of the plane being emitted; ra/rb rho^p of the 4 columns in the two
+  // layers around it
+  T F[4][3], Gt[4][3], uc[3], uo[3], own[3], fo[3], ra[4], rb[4];
+  uint8_t clo = 0;
   face(ss + ((z0 - 1 + WNSLOT) % WNSLOT) * SLOT, F, uc);
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     Gt[q][0] = Gt[q][1] = Gt[q][2] = T(0);
-    rprev[q] = T(0);
+    ra[q] = rb[q] = T(0);
   }
-  const bool writer = tx < WTX - 1 && ty < TY - 1 && ex + 1 < L.nx && ey + 1 < L.ny;
+#pragma unroll
+  for (int c = 0; c < 3; c++) uo[c] = own[c] = fo[c] = T(0);
+
+  // node plane zo from the corners its 4 columns left in exchange buffer xb
+  auto emit = [&](int zo, const T* xb) {
+    if (!writer) return;
+    T acc[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      acc[c] = own[c] + xb[(2 * 3 + c) * NE + tid + 1] + xb[(1 * 3 + c) * NE + tid + WTX] +
+               xb[(0 * 3 + c) * NE + tid + WTX + 1];
+    const long long n = L.nidx(ex + 1, ey + 1, zo);
+    const bool work = (clo & NC_ACTIVE) && !(clo & NC_SUPPORT);
+    if (MODE == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) out[n + c * NP] = fo[c] - (work ? acc[c] : T(0));
+    } else if (MODE == 1) {
+      const bool pass = (clo & NC_SUPPORT) != 0;
+#pragma unroll
+      for (int c = 0; c < 3; c++) out[n + c * NP] = pass ? uo[c] : (work ? acc[c] : T(0));
+    } else {
+      if (!work) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) out[n + c * NP] = T(0);
+      } else {
+        // D = sum_e rho_e K0[a_e][a_e]; node bits in column (ex + a, ey + b), layer zo - 1 + l
+        // are (1 - a, 1 - b, 1 - l), so sigma = (2a - 1, 2b - 1, 2l - 1); ra: l = 0, rb: l = 1
+        const T R = (ra[0] + ra[1] + ra[2] + ra[3]) + (rb[0] + rb[1] + rb[2] + rb[3]);
+        const T pxy_ = (ra[0] + ra[3] - ra[1] - ra[2]) + (rb[0] + rb[3] - rb[1] - rb[2]);
+        const T xlo = ra[1] + ra[3] - ra[0] - ra[2], xhi = rb[1] + rb[3] - rb[0] - rb[2];
+        const T ylo = ra[2] + ra[3] - ra[0] - ra[1], yhi = rb[2] + rb[3] - rb[0] - rb[1];
+        const T pxz = xhi - xlo, pyz = yhi - ylo;
+        const T a = d0<T>(0) * R, b = d0<T>(1) * pxy_, cc = d0<T>(2) * pxz;
+        const T d = d0<T>(4) * R, e = d0<T>(5) * pyz, g = d0<T>(8) * R;
+        const T r0 = fo[0] - acc[0], r1 = fo[1] - acc[1], r2 = fo[2] - acc[2];
+        const T A = d * g - e * e, B = cc * e - b * g, C = b * e - cc * d;
+        const T det = a * A + b * B + cc * C;
+        const T id = omega / det;
+        const T E = a * g - cc * cc, Fm = b * cc - a * e, I = a * d - b * b;
+        out[n] = uo[0] + id * (A * r0 + B * r1 + C * r2);
+        out[n + NP] = uo[1] + id * (B * r0 + E * r1 + Fm * r2);
+        out[n + 2 * NP] = uo[2] + id * (C * r0 + Fm * r1 + I * r2);
+      }
+    }
+  };
 
   for (int z = z0 - 1; z < z1; z++) {
-    issue(z + 1 + WPD);
-    __pipeline_wait_prior(WPD);
+    // one barrier per layer: stage z+1 is staged, the corners of plane z-1
+    // are visible, and the slot of stage z-1 is free for refilling
+    __pipeline_wait_prior(WPD - 1);
     __syncthreads();
+    issue(z + 1 + WPD);
+    if (z - 1 >= z0) emit(z - 1, sx + ((z - 1) & 1) * 9 * NE);
+    if (writer && z >= z0) {
+      // operands of plane z, used when it is emitted in the next step
+      const long long n = L.nidx(ex + 1, ey + 1, z);
+      clo = L.vclass[n];
+      if (MODE != 1) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) fo[c] = f[n + c * NP];
+      }
+    }
     const T* su = ss + ((z + 1 + WNSLOT) % WNSLOT) * SLOT;
     const T* sr = ss + ((z + WNSLOT) % WNSLOT) * SLOT + 3 * NPL;
     T v[8][3], un[3];
@@ -284,6 +346,14 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
 #pragma unroll
       for (int i = 0; i < 3; i++) v[c ^ (1 << i)][i] = o[i];
     }
+    if (MODE == 2) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) ra[q] = rb[q];
+      rb[0] = re;
+      rb[1] = writer ? sr[tid + 1] : T(0);
+      rb[2] = writer ? sr[tid + WTX] : T(0);
+      rb[3] = writer ? sr[tid + WTX + 1] : T(0);
+    }
     // bottom face (plane z) = S - D, top face (plane z+1) = S + D
     T tot[4][3];
 #pragma unroll
@@ -294,90 +364,26 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
         Gt[q][c] = v[q][c] + v[q + 4][c];
       }
     if (z >= z0) {
-      // back to the 4 corners of plane z: corner (bx, by)
-      T cor[4][3];
+      // back to the 4 corners of plane z: corner (bx, by); (1,1) stays here
+      T* xb = sx + (z & 1) * 9 * NE;
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const T e0 = tot[0][c] - tot[1][c], e1 = tot[0][c] + tot[1][c];  // my = 0: bx = 0, 1
         const T g0 = tot[2][c] - tot[3][c], g1 = tot[2][c] + tot[3][c];  // my = 1
-        cor[0][c] = e0 - g0;  // (0, 0)
-        cor[1][c] = e1 - g1;  // (1, 0)
-        cor[2][c] = e0 + g0;  // (0, 1)
-        cor[3][c] = e1 + g1;  // (1, 1)
+        xb[(0 * 3 + c) * NE + tid] = e0 - g0;  // (0, 0)
+        xb[(1 * 3 + c) * NE + tid] = e1 - g1;  // (1, 0)
+        xb[(2 * 3 + c) * NE + tid] = e0 + g0;  // (0, 1)
+        own[c] = e1 + g1;                      // (1, 1)
       }
-#pragma unroll
-      for (int k = 0; k < 3; k++)
-#pragma unroll
-        for (int c = 0; c < 3; c++) sx[(k * 3 + c) * NE + tid] = cor[k][c];
-      T rl[4];
-      if (MODE == 2) {
-        rl[0] = re;
-        rl[1] = writer ? sr[tid + 1] : T(0);
-        rl[2] = writer ? sr[tid + WTX] : T(0);
-        rl[3] = writer ? sr[tid + WTX + 1] : T(0);
-      }
-      __syncthreads();
-      if (writer) {
-        T acc[3];
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-          acc[c] = cor[3][c] + sx[(2 * 3 + c) * NE + tid + 1] + sx[(1 * 3 + c) * NE + tid + WTX] +
-                   sx[(0 * 3 + c) * NE + tid + WTX + 1];
-        const long long n = L.nidx(ex + 1, ey + 1, z);
-        const uint8_t cls = L.vclass[n];
-        const bool work = (cls & NC_ACTIVE) && !(cls & NC_SUPPORT);
-        if (MODE == 0) {
-#pragma unroll
-          for (int c = 0; c < 3; c++) out[n + c * NP] = f[n + c * NP] - (work ? acc[c] : T(0));
-        } else if (MODE == 1) {
-          const bool pass = (cls & NC_SUPPORT) != 0;
-#pragma unroll
-          for (int c = 0; c < 3; c++) out[n + c * NP] = pass ? uc[c] : (work ? acc[c] : T(0));
-        } else {
-          if (!work) {
-#pragma unroll
-            for (int c = 0; c < 3; c++) out[n + c * NP] = T(0);
-          } else {
-            // D = sum_e rho_e K0[a_e][a_e]; node bits in column (ex + a, ey + b), layer z - 1 + l
-            // are (1 - a, 1 - b, 1 - l), so sigma = (2a - 1, 2b - 1, 2l - 1)
-            const T lo = rprev[0] + rprev[1] + rprev[2] + rprev[3];
-            const T hi = rl[0] + rl[1] + rl[2] + rl[3];
-            const T R = lo + hi;
-            // sigma_x sigma_y = +1 for (a, b) = (0,0), (1,1)
-            const T pxy_ = (rprev[0] + rprev[3] - rprev[1] - rprev[2]) + (rl[0] + rl[3] - rl[1] - rl[2]);
-            const T xlo = rprev[1] + rprev[3] - rprev[0] - rprev[2], xhi = rl[1] + rl[3] - rl[0] - rl[2];
-            const T ylo = rprev[2] + rprev[3] - rprev[0] - rprev[1], yhi = rl[2] + rl[3] - rl[0] - rl[1];
-            const T pxz = xhi - xlo, pyz = yhi - ylo;
-            const T a = d0<T>(0) * R, b = d0<T>(1) * pxy_, cc = d0<T>(2) * pxz;
-            const T d = d0<T>(4) * R, e = d0<T>(5) * pyz, g = d0<T>(8) * R;
-            const T r0 = f[n] - acc[0], r1 = f[n + NP] - acc[1], r2 = f[n + 2 * NP] - acc[2];
-            const T A = d * g - e * e, B = cc * e - b * g, C = b * e - cc * d;
-            const T det = a * A + b * B + cc * C;
-            const T id = omega / det;
-            const T E = a * g - cc * cc, Fm = b * cc - a * e, I = a * d - b * b;
-            out[n] = uc[0] + id * (A * r0 + B * r1 + C * r2);
-            out[n + NP] = uc[1] + id * (B * r0 + E * r1 + Fm * r2);
-            out[n + 2 * NP] = uc[2] + id * (C * r0 + Fm * r1 + I * r2);
-          }
-        }
-      }
-      if (MODE == 2) {
-#pragma unroll
-        for (int q = 0; q < 4; q++) rprev[q] = rl[q];
-      }
-    } else {
-      if (MODE == 2) {
-        rprev[0] = re;
-        rprev[1] = writer ? sr[tid + 1] : T(0);
-        rprev[2] = writer ? sr[tid + WTX] : T(0);
-        rprev[3] = writer ? sr[tid + WTX + 1] : T(0);
-      }
-      // the next issue() refills the slot read in this (first) step
-      __syncthreads();
     }
 #pragma unroll
-    for (int c = 0; c < 3; c++) uc[c] = un[c];
+    for (int c = 0; c < 3; c++) {
+      uo[c] = uc[c];
+      uc[c] = un[c];
+    }
   }
+  __syncthreads();
+  emit(z1 - 1, sx + ((z1 - 1) & 1) * 9 * NE);
   __pipeline_wait_prior(0);
 }
 

@@ -66,6 +66,50 @@ rso_status dot(rso_handle* h, const double* a, const double* b, long long n, dou
   return launch_check(h, "dot");
 }
 
+// CG step fused with the norm of the new residual: x += a p, r -= a q,
+// sum r.r, and (mixed precision) the FP32 copy of r that the V-cycle smooths
+__global__ void __launch_bounds__(RED_THREADS) k_cg_update_rr(long long n, const double* __restrict__ alpha,
+                                                              const double* __restrict__ p,
+                                                              const double* __restrict__ q, double* __restrict__ x,
+                                                              double* __restrict__ r, float* __restrict__ r32,
+                                                              double* __restrict__ part) {
+  const double a = *alpha;
+  double s = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    x[i] += a * p[i];
+    const double ri = r[i] - a * q[i];
+    r[i] = ri;
+    if (r32) r32[i] = (float)ri;
+    s += ri * ri;
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// sum a.b with b in FP32 (the mixed-precision preconditioned residual)
+__global__ void __launch_bounds__(RED_THREADS) k_dot_df_partial(const double* __restrict__ a,
+                                                                const float* __restrict__ b, long long n,
+                                                                double* __restrict__ part) {
+  double s = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s += a[i] * (double)b[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+rso_status cg_update_rr(rso_handle* h, long long n, const double* alpha, const double* p, const double* q, double* x,
+                        double* r, float* r32, double* rr_dev) {
+  k_cg_update_rr<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, alpha, p, q, x, r, r32, h->red); rso::note_launch();
+  k_final<<<1, RED_THREADS, 0, h->stream>>>(h->red, RED_BLOCKS, rr_dev); rso::note_launch();
+  return launch_check(h, "cg_update_rr");
+}
+
+rso_status dot_df(rso_handle* h, const double* a, const float* b, long long n, double* dev_out) {
+  k_dot_df_partial<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(a, b, n, h->red); rso::note_launch();
+  k_final<<<1, RED_THREADS, 0, h->stream>>>(h->red, RED_BLOCKS, dev_out); rso::note_launch();
+  return launch_check(h, "dot_df");
+}
+
 rso_status dot_host(rso_handle* h, const double* a, const double* b, long long n, double* out) {
   RSO_TRY(dot(h, a, b, n, h->scal + 15));
   RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->h_scal + 15, h->scal + 15, sizeof(double), cudaMemcpyDeviceToHost, h->stream));

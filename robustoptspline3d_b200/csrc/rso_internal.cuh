@@ -155,6 +155,9 @@ rso_status launch_check(rso_handle* h, const char* what);
 // reductions (reduce.cu)
 rso_status dot(rso_handle* h, const double* a, const double* b, long long n, double* dev_out);
 rso_status dot_host(rso_handle* h, const double* a, const double* b, long long n, double* out);
+rso_status cg_update_rr(rso_handle* h, long long n, const double* alpha, const double* p, const double* q, double* x,
+                        double* r, float* r32, double* rr_dev);
+rso_status dot_df(rso_handle* h, const double* a, const float* b, long long n, double* dev_out);
 rso_status sum_float(rso_handle* h, const float* a, long long n, double* dev_out);
 
 // conversion between the public dense layout and padded layout

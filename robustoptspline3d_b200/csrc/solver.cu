@@ -143,9 +143,30 @@ __global__ void k_cg_beta(double* s) {
   s[0] = s[3];
 }
 
+__global__ void k_cg_dir_f(long long n, const double* __restrict__ beta, const float* __restrict__ z,
+                           double* __restrict__ p) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) p[i] = (double)z[i] + (*beta) * p[i];
+}
+
+// mixed precision: one FP32 V-cycle from a zero iterate on L[0].f32 (already
+// holding the FP32 residual); the result is left in L[0].u32
+static rso_status vcycle_mixed(rso_handle* h) {
+  Level& l0 = h->L[0];
+  // the first damped-Jacobi sweep from zero reads no iterate; Gauss-Seidel does
+  if (h->cfg.smoother == RSO_SMOOTH_GS || h->cfg.pre == 0)
+    RSO_CHECK_CUDA(h, cudaMemsetAsync(l0.u32, 0, sizeof(float) * 3 * l0.NP, h->stream));
+  return vcycle_levels<float>(h, h->cfg.pre, h->cfg.post, 1, true);
+}
+
+// CG preconditioned by one V-cycle.  In mixed precision the preconditioned
+// residual z stays FP32 (it only enters r.z and the direction update), the
+// FP32 copy of r is written by the fused residual update, and the norm of r
+// comes out of the same pass.
 rso_status solve_pcg(rso_handle* h, const double* f, double* x, double tol, int max_iter, rso_solve_info* info) {
   Level& l0 = h->L[0];
   const long long n3 = 3 * l0.NP;
+  const bool mixed = h->cfg.precision == RSO_MIXED;
   double* s = h->scal;
   RSO_TRY(fine_residual<double>(h, x, f, h->r, h->rp64));
   double fn2 = 0, rn2 = 0;
@@ -159,23 +180,39 @@ rso_status solve_pcg(rso_handle* h, const double* f, double* x, double tol, int 
     rel = 0;
   }
   if (rel >= tol && fn > 0) {
-    RSO_TRY(precondition(h, h->r, h->z));
-    RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->p, h->z, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
-    RSO_TRY(dot(h, h->r, h->z, n3, s + 0));
+    if (mixed) {
+      k_d2f<<<cdiv(n3, 256), 256, 0, h->stream>>>(h->r, h->L[0].f32, n3); rso::note_launch();
+      RSO_TRY(vcycle_mixed(h));
+      k_f2d<<<cdiv(n3, 256), 256, 0, h->stream>>>(h->L[0].u32, h->p, n3); rso::note_launch();
+      RSO_TRY(dot_df(h, h->r, h->L[0].u32, n3, s + 0));
+    } else {
+      RSO_TRY(precondition(h, h->r, h->z));
+      RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->p, h->z, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
+      RSO_TRY(dot(h, h->r, h->z, n3, s + 0));
+    }
     while (it < max_iter) {
       RSO_TRY(fine_applyK<double>(h, h->p, h->q, h->rp64));
       RSO_TRY(dot(h, h->p, h->q, n3, s + 1));
       k_cg_alpha<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
-      k_cg_update<<<cdiv(n3, 256), 256, 0, h->stream>>>(n3, s + 2, h->p, h->q, x, h->r); rso::note_launch();
-      RSO_TRY(dot_host(h, h->r, h->r, n3, &rn2));
+      RSO_TRY(cg_update_rr(h, n3, s + 2, h->p, h->q, x, h->r, mixed ? h->L[0].f32 : nullptr, s + 5));
+      RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->h_scal + 5, s + 5, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+      rn2 = h->h_scal[5];
       it++;
       rel = std::sqrt(rn2) / fn;
       if (!std::isfinite(rel)) { h->err = "non-finite residual in PCG"; return RSO_ERR_NONFINITE; }
       if (rel < tol) break;
-      RSO_TRY(precondition(h, h->r, h->z));
-      RSO_TRY(dot(h, h->r, h->z, n3, s + 3));
-      k_cg_beta<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
-      k_cg_dir<<<cdiv(n3, 256), 256, 0, h->stream>>>(n3, s + 4, h->z, h->p); rso::note_launch();
+      if (mixed) {
+        RSO_TRY(vcycle_mixed(h));
+        RSO_TRY(dot_df(h, h->r, h->L[0].u32, n3, s + 3));
+        k_cg_beta<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
+        k_cg_dir_f<<<cdiv(n3, 256), 256, 0, h->stream>>>(n3, s + 4, h->L[0].u32, h->p); rso::note_launch();
+      } else {
+        RSO_TRY(precondition(h, h->r, h->z));
+        RSO_TRY(dot(h, h->r, h->z, n3, s + 3));
+        k_cg_beta<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
+        k_cg_dir<<<cdiv(n3, 256), 256, 0, h->stream>>>(n3, s + 4, h->z, h->p); rso::note_launch();
+      }
       RSO_TRY(launch_check(h, "pcg"));
     }
   }

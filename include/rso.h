@@ -285,6 +285,18 @@ rso_status rso_design_iteration(rso_handle* h, rso_mma* mma, const rso_iter_para
 rso_status rso_design_iteration_host(rso_handle* h, rso_mma* mma, const rso_iter_params* prm,
                                      const double* coeff_in_host, double* coeff_out_host,
                                      float* rho_out_host, rso_iter_info* info);
+/* Objective values and coefficient gradients of the design at coeff_dev
+ * (n_coeff doubles on the device), without an MMA step: values_host[3] =
+ * {lambda_max of the worst case, volume fraction, self-support value} and
+ * their gradients with respect to the coefficients (device, n_coeff doubles
+ * each, any may be NULL).  This is the objective/gradient part of the
+ * optimization_ss loop body (computeSensitivity2,
+ * optimization/optimization.cu:249-322, and deal_background_points,
+ * optimization/optimization.cpp:1223-1242), unscaled.  With
+ * prm->filter_mode == 1 (no sensitivity filter) the gradients are exact. */
+rso_status rso_design_gradient(rso_handle* h, const double* coeff_dev, const rso_iter_params* prm,
+                               double* values_host, double* dlambda_dc_dev, double* dvolume_dc_dev,
+                               double* dss_dc_dev);
 
 /* ---------------------------------------------------------------- instrumentation */
 /* Number of kernels this library has launched in the process (all handles).
@@ -293,6 +305,9 @@ long long rso_launch_count(void);
 /* CUDA-event timing of the operator kernels on the handle's stream
  * (replaces the _TIC/_TOC phase timers of test_vcycle, grid/Grid.cpp:2349-2388) */
 rso_status rso_set_profiling(rso_handle* h, int on);
+/* the same for a subset of kernel classes (bit cls of mask), so that a timed
+ * run can record only the kernel whose roofline it reports */
+rso_status rso_set_profiling_classes(rso_handle* h, unsigned mask);
 rso_status rso_profile_reset(rso_handle* h);
 /* per kernel class: launches, total device ms, algorithmic bytes and flops per launch */
 rso_status rso_profile_class(rso_handle* h, int cls, char* name, int name_len, long long* launches,

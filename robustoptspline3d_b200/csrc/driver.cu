@@ -22,31 +22,29 @@ static double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-rso_status design_iteration(rso_handle* h, rso_mma* mma, const rso_iter_params* prm, rso_iter_info* info) {
+// Objective values and unscaled coefficient gradients at coefficients c:
+// h->coef_a = d lambda / dc, h->coef_c = d volume / dc, h->coef_b = d ss / dc.
+struct DesignEval {
+  double lambda = 0, c_worst = 0, volume = 0, ss = 0;
+  int iters = 0;
+  double t_ops = 0, t_worst = 0, t_ss = 0, t_adj = 0;  // ms per phase
+};
+
+static rso_status evaluate_design(rso_handle* h, const double* c, const rso_iter_params* prm, DesignEval* ev) {
   const Level& l0 = h->L[0];
   if (!h->sp.order) { h->err = "spline not set up"; return RSO_ERR_STATE; }
-  const long long nc = h->sp.n_coeff;
-  if (mma_n(mma) != nc) { h->err = "MMA size differs from the number of spline coefficients"; return RSO_ERR_INVALID_ARG; }
-  const int m = mma_m(mma);
-  const bool ss = prm->ss_mode >= 0;
-  if (m != (ss ? 2 : 1)) { h->err = "MMA needs 1 constraint (volume) or 2 (volume, self-support)"; return RSO_ERR_INVALID_ARG; }
   const long long n3 = 3 * l0.NP;
+  const bool ss = prm->ss_mode >= 0;
   if (!h->fw) {
     RSO_CHECK_CUDA(h, cudaMalloc(&h->fw, sizeof(double) * n3));
     RSO_CHECK_CUDA(h, cudaMalloc(&h->uw, sizeof(double) * n3));
   }
-  if (!h->coef_df) {
-    RSO_CHECK_CUDA(h, cudaMalloc(&h->coef_df, sizeof(double) * nc));
-    RSO_CHECK_CUDA(h, cudaMalloc(&h->coef_dg, sizeof(double) * nc * 2));
-  }
-  const double* c = mma_x(mma);
   const double t0 = now_ms();
   // density: spline -> clamp -> Heaviside -> clamp (Grid.cu:3428-3435, optimization.cu:336-347)
   RSO_TRY(coeff2density(h, c, nullptr, h->e_rhohat));
   RSO_TRY(heaviside(h, h->e_rhohat, prm->beta, nullptr, h->rho));
   RSO_TRY(penalise(h));
-  double vol = 0;
-  RSO_TRY(volume(h, h->rho, &vol));
+  RSO_TRY(volume(h, h->rho, &ev->volume));
   // operators (update_stencil)
   RSO_TRY(galerkin(h));
   RSO_TRY(coarsest_factor(h));
@@ -55,17 +53,14 @@ rso_status design_iteration(rso_handle* h, rso_mma* mma, const rso_iter_params* 
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   const double t1 = now_ms();
   // worst case
-  double lambda = 0;
-  int iters = 0;
-  RSO_TRY(worst_case(h, prm->lanczos_steps, prm->constrain_direction, prm->solve_tol, prm->seed, h->fw, h->uw, &lambda,
-                     nullptr, &iters));
-  double cw = 0;
-  RSO_TRY(dot_host(h, h->fw, h->uw, n3, &cw));
+  RSO_TRY(worst_case(h, prm->lanczos_steps, prm->constrain_direction, prm->solve_tol, prm->seed, h->fw, h->uw,
+                     &ev->lambda, nullptr, &ev->iters));
+  RSO_TRY(dot_host(h, h->fw, h->uw, n3, &ev->c_worst));
   const double t2 = now_ms();
   // self-support (deal_background_points)
-  double ssv = 0;
+  ev->ss = 0;
   if (ss) {
-    RSO_TRY(selfsupport(h, c, prm->beta, prm->ss_mode, prm->opt_angle, prm->default_angle, nullptr, h->coef_b, &ssv,
+    RSO_TRY(selfsupport(h, c, prm->beta, prm->ss_mode, prm->opt_angle, prm->default_angle, nullptr, h->coef_b, &ev->ss,
                         nullptr, nullptr));
     RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   }
@@ -85,24 +80,44 @@ rso_status design_iteration(rso_handle* h, rso_mma* mma, const rso_iter_params* 
   }
   RSO_TRY(density2coeff(h, gs, nullptr, h->coef_a));
   RSO_TRY(density2coeff(h, gv, nullptr, h->coef_c));
+  RSO_TRY(launch_check(h, "adjoint chain"));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  const double t4 = now_ms();
+  ev->t_ops = t1 - t0; ev->t_worst = t2 - t1; ev->t_ss = t3 - t2; ev->t_adj = t4 - t3;
+  return RSO_OK;
+}
+
+rso_status design_iteration(rso_handle* h, rso_mma* mma, const rso_iter_params* prm, rso_iter_info* info) {
+  if (!h->sp.order) { h->err = "spline not set up"; return RSO_ERR_STATE; }
+  const long long nc = h->sp.n_coeff;
+  if (mma_n(mma) != nc) { h->err = "MMA size differs from the number of spline coefficients"; return RSO_ERR_INVALID_ARG; }
+  const int m = mma_m(mma);
+  const bool ss = prm->ss_mode >= 0;
+  if (m != (ss ? 2 : 1)) { h->err = "MMA needs 1 constraint (volume) or 2 (volume, self-support)"; return RSO_ERR_INVALID_ARG; }
+  if (!h->coef_df) {
+    RSO_CHECK_CUDA(h, cudaMalloc(&h->coef_df, sizeof(double) * nc));
+    RSO_CHECK_CUDA(h, cudaMalloc(&h->coef_dg, sizeof(double) * nc * 2));
+  }
+  DesignEval ev;
+  RSO_TRY(evaluate_design(h, mma_x(mma), prm, &ev));
+  const double t4 = now_ms();
   // driver scalings (optimization.cpp:1008-1024) and the MMA inputs
   k_scale_into<<<cdiv(nc, 256), 256, 0, h->stream>>>(nc, prm->sens_scale, h->coef_a, h->coef_df); rso::note_launch();
   k_scale_into<<<cdiv(nc, 256), 256, 0, h->stream>>>(nc, prm->vol_scale, h->coef_c, h->coef_dg); rso::note_launch();
   if (ss) { k_scale_into<<<cdiv(nc, 256), 256, 0, h->stream>>>(nc, prm->ss_scale, h->coef_b, h->coef_dg + nc); rso::note_launch(); }
-  RSO_TRY(launch_check(h, "adjoint chain"));
-  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
-  const double t4 = now_ms();
-  double g[2] = {prm->vol_scale * (vol - prm->volume_ratio), prm->ss_scale * ssv};
+  RSO_TRY(launch_check(h, "MMA inputs"));
+  double g[2] = {prm->vol_scale * (ev.volume - prm->volume_ratio), prm->ss_scale * ev.ss};
   int conv = 0;
   double minfo[4];
   rso_status s = rso_mma_update(mma, h->coef_df, h->coef_dg, g, &conv, minfo);
   if (s != RSO_OK) { h->err = "MMA update failed"; return s; }
   const double t5 = now_ms();
   if (info) {
-    info->c_worst = cw; info->lambda = lambda; info->volume = vol; info->ss_value = ssv;
-    info->ms_operators = t1 - t0; info->ms_worst = t2 - t1; info->ms_selfsupport = t3 - t2;
-    info->ms_adjoint = t4 - t3; info->ms_mma = t5 - t4; info->ms_total = t5 - t0;
-    info->solve_iterations = iters; info->mma_converged = conv;
+    info->c_worst = ev.c_worst; info->lambda = ev.lambda; info->volume = ev.volume; info->ss_value = ev.ss;
+    info->ms_operators = ev.t_ops; info->ms_worst = ev.t_worst; info->ms_selfsupport = ev.t_ss;
+    info->ms_adjoint = ev.t_adj; info->ms_mma = t5 - t4;
+    info->ms_total = ev.t_ops + ev.t_worst + ev.t_ss + ev.t_adj + (t5 - t4);
+    info->solve_iterations = ev.iters; info->mma_converged = conv;
   }
   return RSO_OK;
 }
@@ -149,5 +164,27 @@ extern "C" rso_status rso_design_iteration_host(rso_handle* h, rso_mma* mma, con
     RSO_CHECK_CUDA(h, cudaMemcpyAsync(rho_out, d, sizeof(float) * h->L[0].ne, cudaMemcpyDeviceToHost, h->stream));
   }
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  return RSO_OK;
+}
+
+extern "C" rso_status rso_design_gradient(rso_handle* h, const double* coeff_dev, const rso_iter_params* prm,
+                                          double* values_host, double* dlambda_dc_dev, double* dvolume_dc_dev,
+                                          double* dss_dc_dev) {
+  if (!h || !coeff_dev || !prm) return RSO_ERR_INVALID_ARG;
+  DesignEval ev;
+  RSO_TRY(evaluate_design(h, coeff_dev, prm, &ev));
+  const size_t nb = sizeof(double) * h->sp.n_coeff;
+  if (dlambda_dc_dev) RSO_CHECK_CUDA(h, cudaMemcpyAsync(dlambda_dc_dev, h->coef_a, nb, cudaMemcpyDeviceToDevice, h->stream));
+  if (dvolume_dc_dev) RSO_CHECK_CUDA(h, cudaMemcpyAsync(dvolume_dc_dev, h->coef_c, nb, cudaMemcpyDeviceToDevice, h->stream));
+  if (dss_dc_dev) {
+    if (prm->ss_mode >= 0) RSO_CHECK_CUDA(h, cudaMemcpyAsync(dss_dc_dev, h->coef_b, nb, cudaMemcpyDeviceToDevice, h->stream));
+    else RSO_CHECK_CUDA(h, cudaMemsetAsync(dss_dc_dev, 0, nb, h->stream));
+  }
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (values_host) {
+    values_host[0] = ev.lambda;
+    values_host[1] = ev.volume;
+    values_host[2] = ev.ss;
+  }
   return RSO_OK;
 }

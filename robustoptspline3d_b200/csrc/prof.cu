@@ -42,6 +42,7 @@ struct Prof {
 };
 
 void prof_begin(rso_handle* h, int cls, double nodes) {
+  if (!((h->prof_on >> cls) & 1)) return;
   Prof* p = (Prof*)h->prof;
   if (!p) { p = new Prof(); h->prof = p; }
   size_t k = p->used[cls];
@@ -56,6 +57,7 @@ void prof_begin(rso_handle* h, int cls, double nodes) {
 }
 
 void prof_end(rso_handle* h, int cls) {
+  if (!((h->prof_on >> cls) & 1)) return;
   Prof* p = (Prof*)h->prof;
   size_t k = p->used[cls];
   cudaEventRecord(p->ev[cls][k + 1], h->stream);
@@ -79,7 +81,13 @@ extern "C" long long rso_launch_count(void) { return g_launches.load(); }
 
 extern "C" rso_status rso_set_profiling(rso_handle* h, int on) {
   if (!h) return RSO_ERR_INVALID_ARG;
-  h->prof_on = on ? 1 : 0;
+  h->prof_on = on ? (1u << PC_N) - 1 : 0u;
+  return RSO_OK;
+}
+
+extern "C" rso_status rso_set_profiling_classes(rso_handle* h, unsigned mask) {
+  if (!h) return RSO_ERR_INVALID_ARG;
+  h->prof_on = mask & ((1u << PC_N) - 1);
   return RSO_OK;
 }
 

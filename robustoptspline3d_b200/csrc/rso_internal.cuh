@@ -114,7 +114,7 @@ struct rso_handle {
   double *coef_a = nullptr, *coef_b = nullptr, *coef_c = nullptr;
   double *coef_df = nullptr, *coef_dg = nullptr;   // MMA inputs
   double *fw = nullptr, *uw = nullptr;             // worst-case force / displacement (padded)
-  int prof_on = 0;                                 // per-kernel event timing (prof.cu)
+  unsigned prof_on = 0;                            // classes with per-kernel event timing (prof.cu)
   void* prof = nullptr;
 };
 

@@ -129,8 +129,10 @@ SIGNATURES = {
     "rso_design_iteration": (_ci, [_vp, _vp, ctypes.POINTER(_IterParams), ctypes.POINTER(_IterInfo)]),
     "rso_design_iteration_host": (_ci, [_vp, _vp, ctypes.POINTER(_IterParams), _pd, _pd,
                                         ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_IterInfo)]),
+    "rso_design_gradient": (_ci, [_vp, _vp, ctypes.POINTER(_IterParams), _pd, _vp, _vp, _vp]),
     "rso_launch_count": (ctypes.c_longlong, []),
     "rso_set_profiling": (_ci, [_vp, _ci]),
+    "rso_set_profiling_classes": (_ci, [_vp, ctypes.c_uint]),
     "rso_profile_reset": (_ci, [_vp]),
     "rso_profile_class": (_ci, [_vp, _ci, ctypes.c_char_p, _ci, ctypes.POINTER(ctypes.c_longlong), _pd, _pd, _pd]),
     "rso_profile_top": (_ci, [_vp, ctypes.c_char_p, _ci, ctypes.POINTER(ctypes.c_longlong), _pd, _pd, _pd]),
@@ -569,6 +571,19 @@ class HierarchyGrid:
                                                          ctypes.POINTER(ctypes.c_float)), ctypes.byref(info)),
                   "rso_design_iteration_host")
         return cout, rho, {f[0]: getattr(info, f[0]) for f in _IterInfo._fields_}
+
+    def design_gradient(self, coeff, params=None):
+        """Objective values {lambda, volume, ss} and their gradients with respect
+        to the spline coefficients (float64 CUDA tensors) at `coeff`, with no
+        MMA step (rso_design_gradient)."""
+        import torch
+        p = (params or IterParams())._c()
+        c = torch.as_tensor(coeff, dtype=torch.float64, device="cuda").contiguous()
+        gl, gv, gs = (torch.empty_like(c) for _ in range(3))
+        vals = np.zeros(3)
+        self._chk(self.lib.rso_design_gradient(self.h, _dev(c, torch.float64), ctypes.byref(p), _np_ptr(vals, _pd),
+                                               _dev(gl), _dev(gv), _dev(gs)), "rso_design_gradient")
+        return {"lambda": vals[0], "volume": vals[1], "ss": vals[2]}, gl, gv, gs
 
 
 class MMA:

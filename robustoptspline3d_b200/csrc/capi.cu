@@ -109,7 +109,7 @@ static void free_handle(rso_handle* h) {
   cudaFree(h->K0_dev); cudaFree(h->rho); cudaFree(h->rp32); cudaFree(h->rp64);
   cudaFree(h->load_nodes); cudaFree(h->load_normals); cudaFree(h->T1);
   cudaFree(h->c_nodes); cudaFree(h->c_K); cudaFree(h->c_f); cudaFree(h->c_flag);
-  cudaFree(h->red); cudaFree(h->scal);
+  cudaFree(h->red); cudaFree(h->scal); cudaFree(h->xfer); cudaFree(h->fpart);
   if (h->h_scal) cudaFreeHost(h->h_scal);
   cudaFree(h->x); cudaFree(h->r); cudaFree(h->p); cudaFree(h->q); cudaFree(h->z); cudaFree(h->w);
   cudaFree(h->stage_a); cudaFree(h->stage_b);
@@ -144,6 +144,22 @@ static rso_status setup(rso_handle* h, int ex, int ey, int ez, const uint8_t* em
   RSO_CHECK_CUDA(h, cudaMemset(h->scal, 0, sizeof(double) * 64));
   h->L.push_back(make_level(ex, ey, ez, 0));
   RSO_TRY(build_topology(h, em, fa, la, ln));
+  {
+    // restriction scratch, sized once the hierarchy exists: z-filtered fine
+    // columns of the largest restriction, 3 * nx * ny * nz_coarse values
+    size_t xf = 1;
+    for (size_t li = 1; li < h->L.size(); li++)
+      xf = std::max(xf, (size_t)3 * h->L[li - 1].nx * h->L[li - 1].ny * h->L[li].nz);
+    ALLOC(h->xfer, sizeof(double) * xf);
+    h->xfer_n = xf;
+  }
+  {
+    // one partial per CTA of the fine operator kernel (32 x 8 threads,
+    // 31 x 7 nodes per z-chunk of 32 planes)
+    const Level& f0 = h->L[0];
+    h->fpart_n = (long long)cdiv(f0.nx, 31) * cdiv(f0.ny, 7) * cdiv(f0.nz, 32);
+    ALLOC(h->fpart, sizeof(double) * h->fpart_n);
+  }
   // per-level buffers
   for (size_t li = 0; li < h->L.size(); li++) {
     Level& l = h->L[li];

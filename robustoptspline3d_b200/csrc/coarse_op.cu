@@ -41,7 +41,9 @@ __device__ __forceinline__ void stencil_apply(const Level& L, const T* __restric
   }
 }
 
-// MODE 0 residual, MODE 2 damped block Jacobi (out of place)
+// Per-node variant for the large coarse levels, which are bandwidth-bound:
+// one thread reads a node's 243 stencil entries and 27 neighbours once.
+// MODE 0 residual, MODE 2 damped block Jacobi (out of place).
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) k_coarse(const Level L, const T* __restrict__ st, const T* __restrict__ u,
                                                 const T* __restrict__ f, T* __restrict__ out, T omega) {
@@ -73,6 +75,61 @@ __global__ void __launch_bounds__(256) k_coarse(const Level L, const T* __restri
   }
 }
 
+// Row-split variant for the small, latency-bound levels (MODE as above).
+// Thread (x, y, r) owns
+// output component r of node (x, y, z), so each node's 243 stencil entries
+// are read by three threads (81 each) and the small, latency-bound coarse
+// levels get three times the independent loads in flight.  The damped
+// Jacobi update exchanges the three residual components through shared
+// memory.
+constexpr int CTY = 4;
+template <typename T, int MODE>
+__global__ void __launch_bounds__(32 * CTY * 3) k_coarse_r(const Level L, const T* __restrict__ st,
+                                                           const T* __restrict__ u, const T* __restrict__ f,
+                                                           T* __restrict__ out, T omega) {
+  __shared__ T sres[3][CTY][32];
+  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * CTY + threadIdx.y, z = blockIdx.z;
+  const int r = threadIdx.z;
+  const bool in = x < L.nx && y < L.ny;
+  const long long NP = L.NP, px = L.px, pxy = (long long)L.px * L.py;
+  const long long n = in ? L.nidx(x, y, z) : 0;
+  const bool act = in && (L.vclass[n] & NC_ACTIVE) != 0;
+  T acc = 0;
+  if (act) {
+    const T* sr = st + (long long)(r * 3) * NP + n;
+#pragma unroll
+    for (int d = 0; d < 27; d++) {
+      const long long nb = n + (d % 3 - 1) + (d / 3 % 3 - 1) * px + (d / 9 - 1) * pxy;
+      const T* sd = sr + (long long)(d * 9) * NP;
+      acc = fma(sd[0], u[nb], acc);
+      acc = fma(sd[NP], u[nb + NP], acc);
+      acc = fma(sd[2 * NP], u[nb + 2 * NP], acc);
+    }
+  }
+  if (MODE == 0) {
+    if (in) out[n + r * NP] = f[n + r * NP] - acc;
+    return;
+  }
+  const T res = act ? f[n + r * NP] - acc : T(0);
+  sres[r][threadIdx.y][threadIdx.x] = res;
+  __syncthreads();
+  if (!in) return;
+  if (!act) { out[n + r * NP] = 0; return; }
+  T S[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) S[i] = st[(13 * 9 + i) * NP + n];
+  // row r of the adjugate of the 3x3 diagonal block
+  const T c00 = S[4] * S[8] - S[5] * S[7], c01 = -(S[3] * S[8] - S[5] * S[6]), c02 = S[3] * S[7] - S[4] * S[6];
+  const T det = S[0] * c00 + S[1] * c01 + S[2] * c02;
+  T a0, a1, a2;
+  if (r == 0) { a0 = c00; a1 = -(S[1] * S[8] - S[2] * S[7]); a2 = S[1] * S[5] - S[2] * S[4]; }
+  else if (r == 1) { a0 = c01; a1 = S[0] * S[8] - S[2] * S[6]; a2 = -(S[0] * S[5] - S[2] * S[3]); }
+  else { a0 = c02; a1 = -(S[0] * S[7] - S[1] * S[6]); a2 = S[0] * S[4] - S[1] * S[3]; }
+  const T r0 = sres[0][threadIdx.y][threadIdx.x], r1 = sres[1][threadIdx.y][threadIdx.x],
+          r2 = sres[2][threadIdx.y][threadIdx.x];
+  out[n + r * NP] = u[n + r * NP] + (omega / det) * (a0 * r0 + a1 * r1 + a2 * r2);
+}
+
 // one colour of the point Gauss-Seidel sweep on stored stencils (gs_relax_kernel grid/Grid.cu:1497-1609)
 template <typename T>
 __global__ void __launch_bounds__(256) k_coarse_gs(const Level L, const T* __restrict__ st, T* __restrict__ u,
@@ -101,56 +158,95 @@ __global__ void __launch_bounds__(256) k_coarse_gs(const Level L, const T* __res
 
 // ---------------------------------------------------------------- transfers
 // f_c(X) = sum_x w(x - F X) r_f(x), w = prod (F-|d|)/F  (R = P^T)
-template <typename T>
-__global__ void k_restrict(const Level Fl, const Level C, int F, const T* __restrict__ rf, T* __restrict__ fc) {
+// Restriction in two separable passes.  Pass 1 (one thread per fine column
+// (x, y) and coarse plane Z) filters along z into the scratch array
+// t[c][Z][y][x]; pass 2 (one thread per coarse node) filters along y and x.
+// Weights (F - |d|) / F per axis, d in (-F, F).
+template <typename T, int F>
+__global__ void k_restrict_z(const Level Fl, int nZ, const T* __restrict__ rf, T* __restrict__ t) {
+  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, Z = blockIdx.z;
+  if (x >= Fl.nx || y >= Fl.ny) return;
+  T s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll
+  for (int dz = -F + 1; dz < F; dz++) {
+    const int z = F * Z + dz;
+    if (z < 0 || z >= Fl.nz) continue;
+    const long long n = Fl.nidx(x, y, z);
+    const T w = (T)(F - (dz < 0 ? -dz : dz)) / (T)F;
+    s0 += w * rf[n]; s1 += w * rf[n + Fl.NP]; s2 += w * rf[n + 2 * Fl.NP];
+  }
+  const long long plane = (long long)Fl.nx * Fl.ny, comp = plane * nZ;
+  const long long i = (long long)Z * plane + (long long)y * Fl.nx + x;
+  t[i] = s0; t[i + comp] = s1; t[i + 2 * comp] = s2;
+}
+
+template <typename T, int F>
+__global__ void k_restrict_xy(const Level Fl, const Level C, const T* __restrict__ t, T* __restrict__ fc) {
   const int X = blockIdx.x * 32 + threadIdx.x, Y = blockIdx.y * 8 + threadIdx.y, Z = blockIdx.z;
   if (X >= C.nx || Y >= C.ny) return;
   const long long nC = C.nidx(X, Y, Z);
   T s0 = 0, s1 = 0, s2 = 0;
   if (C.vclass[nC] & NC_ACTIVE) {
-    const T inv = T(1) / (T)(F * F * F);
-    for (int dz = -F + 1; dz < F; dz++) {
-      const int z = F * Z + dz;
-      if (z < 0 || z >= Fl.nz) continue;
-      for (int dy = -F + 1; dy < F; dy++) {
-        const int y = F * Y + dy;
-        if (y < 0 || y >= Fl.ny) continue;
-        const T wyz = (T)((F - abs(dy)) * (F - abs(dz)));
-        for (int dx = -F + 1; dx < F; dx++) {
-          const int x = F * X + dx;
-          if (x < 0 || x >= Fl.nx) continue;
-          const long long n = Fl.nidx(x, y, z);
-          const T w = wyz * (T)(F - abs(dx)) * inv;
-          s0 += w * rf[n]; s1 += w * rf[n + Fl.NP]; s2 += w * rf[n + 2 * Fl.NP];
-        }
+    const long long plane = (long long)Fl.nx * Fl.ny, comp = plane * C.nz;
+    const T* tz = t + (long long)Z * plane;
+#pragma unroll
+    for (int dy = -F + 1; dy < F; dy++) {
+      const int y = F * Y + dy;
+      if (y < 0 || y >= Fl.ny) continue;
+      const T wy = (T)(F - (dy < 0 ? -dy : dy)) / (T)F;
+#pragma unroll
+      for (int dx = -F + 1; dx < F; dx++) {
+        const int x = F * X + dx;
+        if (x < 0 || x >= Fl.nx) continue;
+        const T w = wy * ((T)(F - (dx < 0 ? -dx : dx)) / (T)F);
+        const long long i = (long long)y * Fl.nx + x;
+        s0 += w * tz[i]; s1 += w * tz[i + comp]; s2 += w * tz[i + 2 * comp];
       }
     }
   }
   fc[nC] = s0; fc[nC + C.NP] = s1; fc[nC + 2 * C.NP] = s2;
 }
 
-// u_f += P u_c at active, non-support fine nodes
-template <typename T>
-__global__ void k_prolong(const Level Fl, const Level C, int F, const T* __restrict__ uc, T* __restrict__ uf) {
-  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
-  if (x >= Fl.nx || y >= Fl.ny) return;
-  const long long n = Fl.nidx(x, y, z);
-  const uint8_t cls = Fl.vclass[n];
-  if (!(cls & NC_ACTIVE) || (cls & NC_SUPPORT)) return;
-  const int X0 = x / F, Y0 = y / F, Z0 = z / F;
-  const int ox = x - F * X0, oy = y - F * Y0, oz = z - F * Z0;
-  const T inv = T(1) / (T)(F * F * F);
-  T s0 = 0, s1 = 0, s2 = 0;
+// u_f += P u_c at active, non-support fine nodes (trilinear, F = 2 or 4).
+// A thread owns the F fine nodes x = F X0 + o (o < F) of one row segment,
+// so the 8 coarse corners are read once for F nodes; every load is issued
+// before the node classes are tested.  The +1 corner lies in the padded halo
+// where its weight is 0.
+template <typename T, int F>
+__global__ void k_prolong(const Level Fl, const Level C, const T* __restrict__ uc, T* __restrict__ uf) {
+  const int X0 = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+  if (F * X0 >= Fl.nx || y >= Fl.ny) return;
+  const int Y0 = y / F, Z0 = z / F, oy = y - F * Y0, oz = z - F * Z0;
+  const T wy[2] = {(T)(F - oy) / (T)F, (T)oy / (T)F};
+  const T wz[2] = {(T)(F - oz) / (T)F, (T)oz / (T)F};
+  const long long c0 = C.nidx(X0, Y0, Z0), cpx = C.px, cpxy = (long long)C.px * C.py;
+  // corner values folded along y and z: e[ax][comp]
+  T e[2][3];
 #pragma unroll
-  for (int A = 0; A < 8; A++) {
-    const int ax = A & 1, ay = (A >> 1) & 1, az = A >> 2;
-    const int wx = ax ? ox : F - ox, wy = ay ? oy : F - oy, wz = az ? oz : F - oz;
-    if (wx == 0 || wy == 0 || wz == 0) continue;
-    const long long nC = C.nidx(X0 + ax, Y0 + ay, Z0 + az);
-    const T w = (T)(wx * wy * wz) * inv;
-    s0 += w * uc[nC]; s1 += w * uc[nC + C.NP]; s2 += w * uc[nC + 2 * C.NP];
+  for (int ax = 0; ax < 2; ax++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      T s = 0;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int ay = k & 1, az = k >> 1;
+        s += wy[ay] * wz[az] * uc[c0 + ax + ay * cpx + az * cpxy + c * C.NP];
+      }
+      e[ax][c] = s;
+    }
+  const long long n0 = Fl.nidx(F * X0, y, z);
+#pragma unroll
+  for (int o = 0; o < F; o++) {
+    if (F * X0 + o >= Fl.nx) break;
+    const long long n = n0 + o;
+    const uint8_t cls = Fl.vclass[n];
+    const T u0 = uf[n], u1 = uf[n + Fl.NP], u2 = uf[n + 2 * Fl.NP];
+    if (!(cls & NC_ACTIVE) || (cls & NC_SUPPORT)) continue;
+    const T w1 = (T)o / (T)F, w0 = (T)(F - o) / (T)F;
+    uf[n] = u0 + (w0 * e[0][0] + w1 * e[1][0]);
+    uf[n + Fl.NP] = u1 + (w0 * e[0][1] + w1 * e[1][1]);
+    uf[n + 2 * Fl.NP] = u2 + (w0 * e[0][2] + w1 * e[1][2]);
   }
-  uf[n] += s0; uf[n + Fl.NP] += s1; uf[n + 2 * Fl.NP] += s2;
 }
 
 // ---------------------------------------------------------------- Galerkin
@@ -389,6 +485,8 @@ __global__ void k_gemv_scatter(const Level C, const double* __restrict__ Kinv, c
 
 // ---------------------------------------------------------------- host wrappers
 static inline dim3 node_grid(const Level& l) { return dim3(cdiv(l.nx, 32), cdiv(l.ny, 8), l.nz); }
+// levels above this many nodes use the per-node stencil kernel
+static const long long kRowSplitMaxNodes = 100000;
 
 template <typename T>
 static const T* stencil_of(const Level& l);
@@ -401,7 +499,11 @@ template <typename T>
 rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* r) {
   const Level& l = h->L[level];
   if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
-  k_coarse<T, 0><<<node_grid(l), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0)); rso::note_launch();
+  if (l.nn > kRowSplitMaxNodes) {
+    k_coarse<T, 0><<<node_grid(l), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0)); rso::note_launch();
+  } else {
+    k_coarse_r<T, 0><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0)); rso::note_launch();
+  }
   if (h->prof_on) prof_end(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64));
   return launch_check(h, "coarse_residual");
 }
@@ -409,7 +511,11 @@ template <typename T>
 rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T* u_out, double omega) {
   const Level& l = h->L[level];
   if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
-  k_coarse<T, 2><<<node_grid(l), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega); rso::note_launch();
+  if (l.nn > kRowSplitMaxNodes) {
+    k_coarse<T, 2><<<node_grid(l), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega); rso::note_launch();
+  } else {
+    k_coarse_r<T, 2><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega); rso::note_launch();
+  }
   if (h->prof_on) prof_end(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64));
   return launch_check(h, "coarse_jacobi");
 }
@@ -427,13 +533,37 @@ rso_status coarse_gs(rso_handle* h, int level, T* u, const T* f, int colour, int
 template <typename T>
 rso_status restrict_(rso_handle* h, int cl, const T* rf, T* fc) {
   const Level& c = h->L[cl];
-  k_restrict<T><<<node_grid(c), dim3(32, 8), 0, h->stream>>>(h->L[cl - 1], c, c.factor, rf, fc); rso::note_launch();
+  const Level& f = h->L[cl - 1];
+  if ((size_t)3 * f.nx * f.ny * c.nz > h->xfer_n) {
+    h->err = "restriction scratch smaller than the level pair needs";
+    return RSO_ERR_STATE;
+  }
+  T* t = reinterpret_cast<T*>(h->xfer);
+  const dim3 gz(cdiv(f.nx, 32), cdiv(f.ny, 8), c.nz);
+  if (c.factor == 4) {
+    k_restrict_z<T, 4><<<gz, dim3(32, 8), 0, h->stream>>>(f, c.nz, rf, t); rso::note_launch();
+    k_restrict_xy<T, 4><<<node_grid(c), dim3(32, 8), 0, h->stream>>>(f, c, t, fc); rso::note_launch();
+  } else if (c.factor == 2) {
+    k_restrict_z<T, 2><<<gz, dim3(32, 8), 0, h->stream>>>(f, c.nz, rf, t); rso::note_launch();
+    k_restrict_xy<T, 2><<<node_grid(c), dim3(32, 8), 0, h->stream>>>(f, c, t, fc); rso::note_launch();
+  } else {
+    h->err = "coarsening factor must be 2 or 4";
+    return RSO_ERR_UNSUPPORTED;
+  }
   return launch_check(h, "restrict");
 }
 template <typename T>
 rso_status prolong(rso_handle* h, int cl, const T* uc, T* uf) {
   const Level& f = h->L[cl - 1];
-  k_prolong<T><<<node_grid(f), dim3(32, 8), 0, h->stream>>>(f, h->L[cl], h->L[cl].factor, uc, uf); rso::note_launch();
+  const Level& c = h->L[cl];
+  if (c.factor == 4) {
+    k_prolong<T, 4><<<dim3(cdiv(cdiv(f.nx, 4), 32), cdiv(f.ny, 8), f.nz), dim3(32, 8), 0, h->stream>>>(f, c, uc, uf); rso::note_launch();
+  } else if (c.factor == 2) {
+    k_prolong<T, 2><<<dim3(cdiv(cdiv(f.nx, 2), 32), cdiv(f.ny, 8), f.nz), dim3(32, 8), 0, h->stream>>>(f, c, uc, uf); rso::note_launch();
+  } else {
+    h->err = "coarsening factor must be 2 or 4";
+    return RSO_ERR_UNSUPPORTED;
+  }
   return launch_check(h, "prolong");
 }
 template <typename T>

@@ -174,7 +174,7 @@ constexpr int walsh_smem_bytes() {
 template <typename T, int MODE, int TY>
 __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
     k_fine_w(const Level L, const T* __restrict__ u, const T* __restrict__ f, T* __restrict__ out,
-             const T* __restrict__ rp, T omega) {
+             const T* __restrict__ rp, T omega, double* __restrict__ dotp) {
   constexpr int NX = WTX + 1, NPL = NX * (TY + 1), NE = WTX * TY, SLOT = 3 * NPL + NE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* ss = reinterpret_cast<T*>(smem_raw);  // [WNSLOT][SLOT]: u plane (3 comps) + rho layer
@@ -245,6 +245,7 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
   // layers around it
   T F[4][3], Gt[4][3], uc[3], uo[3], own[3], fo[3], ra[4], rb[4];
   uint8_t clo = 0;
+  double pq = 0;  // MODE 1 with dotp: this thread's share of u . (K u)
   face(ss + ((z0 - 1 + WNSLOT) % WNSLOT) * SLOT, F, uc);
 #pragma unroll
   for (int q = 0; q < 4; q++) {
@@ -270,7 +271,11 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
     } else if (MODE == 1) {
       const bool pass = (clo & NC_SUPPORT) != 0;
 #pragma unroll
-      for (int c = 0; c < 3; c++) out[n + c * NP] = pass ? uo[c] : (work ? acc[c] : T(0));
+      for (int c = 0; c < 3; c++) {
+        const T q = pass ? uo[c] : (work ? acc[c] : T(0));
+        out[n + c * NP] = q;
+        pq += (double)uo[c] * (double)q;
+      }
     } else {
       if (!work) {
 #pragma unroll
@@ -384,6 +389,20 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
   }
   __syncthreads();
   emit(z1 - 1, sx + ((z1 - 1) & 1) * 9 * NE);
+  if (MODE == 1 && dotp != nullptr) {
+    // per-CTA partial of u . (K u), summed by a second pass on the host side
+    __shared__ double sred[TY];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pq += __shfl_down_sync(0xffffffffu, pq, o);
+    if (tx == 0) sred[ty] = pq;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0;
+#pragma unroll
+      for (int w = 0; w < TY; w++) t += sred[w];
+      dotp[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = t;
+    }
+  }
   __pipeline_wait_prior(0);
 }
 
@@ -507,7 +526,7 @@ static inline int pcls(int c32, int c64) { return sizeof(T) == 4 ? c32 : c64; }
 
 template <typename T, int MODE>
 static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, const T* rp, double omega, int cls,
-                              const char* what) {
+                              const char* what, double* dotp = nullptr) {
   const Level& l = h->L[0];
   if (3 * l.NP >= (1LL << 31)) {
     h->err = "fine level too large for 32-bit in-plane offsets";
@@ -520,7 +539,7 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
     attr = true;
   }
   if (h->prof_on) prof_begin(h, cls, (double)l.nn);
-  k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega);
+  k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega, dotp);
   rso::note_launch();
   if (h->prof_on) prof_end(h, cls);
   return launch_check(h, what);
@@ -533,6 +552,18 @@ rso_status fine_residual(rso_handle* h, const T* u, const T* f, T* r, const T* r
 template <typename T>
 rso_status fine_applyK(rso_handle* h, const T* u, T* f, const T* rp) {
   return launch_fine<T, 1>(h, u, u, f, rp, 0.0, pcls<T>(PC_FINE_RES32, PC_FINE_APPLYK64), "fine_applyK");
+}
+// f = K u and dot_dev = u . f in one pass (the CG step's p . q)
+rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const double* rp, double* dot_dev) {
+  const dim3 g = march_grid(h->L[0]);
+  const long long nb = (long long)g.x * g.y * g.z;
+  if (nb > h->fpart_n) {
+    h->err = "fine partial-sum buffer smaller than the grid";
+    return RSO_ERR_STATE;
+  }
+  const rso_status st = launch_fine<double, 1>(h, u, u, f, rp, 0.0, PC_FINE_APPLYK64, "fine_applyK_dot", h->fpart);
+  if (st != RSO_OK) return st;
+  return reduce_partials(h, h->fpart, (int)nb, dot_dev);
 }
 template <typename T>
 rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega) {

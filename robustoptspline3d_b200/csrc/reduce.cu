@@ -66,17 +66,15 @@ rso_status dot(rso_handle* h, const double* a, const double* b, long long n, dou
   return launch_check(h, "dot");
 }
 
-// CG step fused with the norm of the new residual: x += a p, r -= a q,
-// sum r.r, and (mixed precision) the FP32 copy of r that the V-cycle smooths
-__global__ void __launch_bounds__(RED_THREADS) k_cg_update_rr(long long n, const double* __restrict__ alpha,
-                                                              const double* __restrict__ p,
-                                                              const double* __restrict__ q, double* __restrict__ x,
-                                                              double* __restrict__ r, float* __restrict__ r32,
-                                                              double* __restrict__ part) {
+// CG residual step fused with its norm: r -= a q, sum r.r, and (mixed
+// precision) the FP32 copy of r that the V-cycle smooths.  The matching
+// x += a p is deferred to the direction update, which reads p anyway.
+__global__ void __launch_bounds__(RED_THREADS) k_cg_resid_rr(long long n, const double* __restrict__ alpha,
+                                                             const double* __restrict__ q, double* __restrict__ r,
+                                                             float* __restrict__ r32, double* __restrict__ part) {
   const double a = *alpha;
   double s = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    x[i] += a * p[i];
     const double ri = r[i] - a * q[i];
     r[i] = ri;
     if (r32) r32[i] = (float)ri;
@@ -97,11 +95,16 @@ __global__ void __launch_bounds__(RED_THREADS) k_dot_df_partial(const double* __
   if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
-rso_status cg_update_rr(rso_handle* h, long long n, const double* alpha, const double* p, const double* q, double* x,
-                        double* r, float* r32, double* rr_dev) {
-  k_cg_update_rr<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, alpha, p, q, x, r, r32, h->red); rso::note_launch();
+rso_status cg_resid_rr(rso_handle* h, long long n, const double* alpha, const double* q, double* r, float* r32,
+                       double* rr_dev) {
+  k_cg_resid_rr<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, alpha, q, r, r32, h->red); rso::note_launch();
   k_final<<<1, RED_THREADS, 0, h->stream>>>(h->red, RED_BLOCKS, rr_dev); rso::note_launch();
-  return launch_check(h, "cg_update_rr");
+  return launch_check(h, "cg_resid_rr");
+}
+
+rso_status reduce_partials(rso_handle* h, const double* part, int n, double* dev_out) {
+  k_final<<<1, RED_THREADS, 0, h->stream>>>(part, n, dev_out); rso::note_launch();
+  return launch_check(h, "reduce_partials");
 }
 
 rso_status dot_df(rso_handle* h, const double* a, const float* b, long long n, double* dev_out) {

@@ -97,6 +97,10 @@ struct rso_handle {
   int* c_flag = nullptr;              // factorisation status
   // reductions
   double* red = nullptr;              // partials
+  double* xfer = nullptr;             // restriction scratch: z-filtered fine columns
+  size_t xfer_n = 0;                  // its capacity in doubles
+  double* fpart = nullptr;            // per-CTA partial sums of the fine operator kernel
+  long long fpart_n = 0;
   double* scal = nullptr;             // device scalars
   double* h_scal = nullptr;           // pinned host mirror
   // PCG / solver vectors (fine, FP64, padded)
@@ -155,8 +159,9 @@ rso_status launch_check(rso_handle* h, const char* what);
 // reductions (reduce.cu)
 rso_status dot(rso_handle* h, const double* a, const double* b, long long n, double* dev_out);
 rso_status dot_host(rso_handle* h, const double* a, const double* b, long long n, double* out);
-rso_status cg_update_rr(rso_handle* h, long long n, const double* alpha, const double* p, const double* q, double* x,
-                        double* r, float* r32, double* rr_dev);
+rso_status cg_resid_rr(rso_handle* h, long long n, const double* alpha, const double* q, double* r, float* r32,
+                       double* rr_dev);
+rso_status reduce_partials(rso_handle* h, const double* part, int n, double* dev_out);
 rso_status dot_df(rso_handle* h, const double* a, const float* b, long long n, double* dev_out);
 rso_status sum_float(rso_handle* h, const float* a, long long n, double* dev_out);
 
@@ -177,6 +182,7 @@ template <typename T>
 rso_status fine_residual(rso_handle* h, const T* u, const T* f, T* r, const T* rp);
 template <typename T>
 rso_status fine_applyK(rso_handle* h, const T* u, T* f, const T* rp);
+rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const double* rp, double* dot_dev);
 template <typename T>
 rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega);
 template <typename T>

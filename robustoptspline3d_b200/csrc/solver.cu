@@ -122,20 +122,6 @@ rso_status precondition(rso_handle* h, const double* r, double* z) {
   return launch_check(h, "precondition");
 }
 
-// x += a p; r -= a q; partial sums of r.r
-__global__ void k_cg_update(long long n, const double* __restrict__ alpha, const double* __restrict__ p,
-                            const double* __restrict__ q, double* __restrict__ x, double* __restrict__ r) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double a = *alpha;
-  x[i] += a * p[i];
-  r[i] -= a * q[i];
-}
-__global__ void k_cg_dir(long long n, const double* __restrict__ beta, const double* __restrict__ z,
-                         double* __restrict__ p) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < n) p[i] = z[i] + (*beta) * p[i];
-}
 // scalar updates on the device: s[0]=rz, s[1]=pq, s[2]=alpha, s[3]=rz_new, s[4]=beta
 __global__ void k_cg_alpha(double* s) { s[2] = s[0] / s[1]; }
 __global__ void k_cg_beta(double* s) {
@@ -143,10 +129,20 @@ __global__ void k_cg_beta(double* s) {
   s[0] = s[3];
 }
 
-__global__ void k_cg_dir_f(long long n, const double* __restrict__ beta, const float* __restrict__ z,
-                           double* __restrict__ p) {
+// x += alpha p (the step of the previous iteration); p = z + beta p
+template <typename Z>
+__global__ void k_cg_step_dir(long long n, const double* __restrict__ alpha, const double* __restrict__ beta,
+                              const Z* __restrict__ z, double* __restrict__ p, double* __restrict__ x) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < n) p[i] = (double)z[i] + (*beta) * p[i];
+  if (i >= n) return;
+  const double pi = p[i];
+  x[i] += (*alpha) * pi;
+  p[i] = (double)z[i] + (*beta) * pi;
+}
+__global__ void k_cg_step(long long n, const double* __restrict__ alpha, const double* __restrict__ p,
+                          double* __restrict__ x) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) x[i] += (*alpha) * p[i];
 }
 
 // mixed precision: one FP32 V-cycle from a zero iterate on L[0].f32 (already
@@ -191,27 +187,29 @@ rso_status solve_pcg(rso_handle* h, const double* f, double* x, double tol, int 
       RSO_TRY(dot(h, h->r, h->z, n3, s + 0));
     }
     while (it < max_iter) {
-      RSO_TRY(fine_applyK<double>(h, h->p, h->q, h->rp64));
-      RSO_TRY(dot(h, h->p, h->q, n3, s + 1));
+      RSO_TRY(fine_applyK_dot(h, h->p, h->q, h->rp64, s + 1));
       k_cg_alpha<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
-      RSO_TRY(cg_update_rr(h, n3, s + 2, h->p, h->q, x, h->r, mixed ? h->L[0].f32 : nullptr, s + 5));
+      RSO_TRY(cg_resid_rr(h, n3, s + 2, h->q, h->r, mixed ? h->L[0].f32 : nullptr, s + 5));
       RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->h_scal + 5, s + 5, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
       RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
       rn2 = h->h_scal[5];
       it++;
       rel = std::sqrt(rn2) / fn;
       if (!std::isfinite(rel)) { h->err = "non-finite residual in PCG"; return RSO_ERR_NONFINITE; }
-      if (rel < tol) break;
+      if (rel < tol || it >= max_iter) {
+        k_cg_step<<<cdiv(n3, 256), 256, 0, h->stream>>>(n3, s + 2, h->p, x); rso::note_launch();
+        break;
+      }
       if (mixed) {
         RSO_TRY(vcycle_mixed(h));
         RSO_TRY(dot_df(h, h->r, h->L[0].u32, n3, s + 3));
         k_cg_beta<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
-        k_cg_dir_f<<<cdiv(n3, 256), 256, 0, h->stream>>>(n3, s + 4, h->L[0].u32, h->p); rso::note_launch();
+        k_cg_step_dir<float><<<cdiv(n3, 256), 256, 0, h->stream>>>(n3, s + 2, s + 4, h->L[0].u32, h->p, x); rso::note_launch();
       } else {
         RSO_TRY(precondition(h, h->r, h->z));
         RSO_TRY(dot(h, h->r, h->z, n3, s + 3));
         k_cg_beta<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
-        k_cg_dir<<<cdiv(n3, 256), 256, 0, h->stream>>>(n3, s + 4, h->z, h->p); rso::note_launch();
+        k_cg_step_dir<double><<<cdiv(n3, 256), 256, 0, h->stream>>>(n3, s + 2, s + 4, h->z, h->p, x); rso::note_launch();
       }
       RSO_TRY(launch_check(h, "pcg"));
     }

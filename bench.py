@@ -11,6 +11,12 @@ measured beside it.  Data are synthetic and seeded.  Inputs (17M nodes)
 exceed the 126 MB L2, so no flush is inserted between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--size S]
+  python bench.py --mode solve [--precision mixed|fp64] [--size S]
+
+`--mode solve` times single multigrid-preconditioned CG solves (to relative
+residual 1e-6) on the density of the seeded initial design, with a seeded
+load on the top-face nodes, and reports per-iteration time and the live
+per-kernel-class CUDA-event profile (the kernel mix of one Lanczos step).
 
 With torchrun each rank runs an independent replica (the path does not
 shard: one design problem per GPU), timing is max over ranks.
@@ -174,6 +180,52 @@ def oracle_design_iteration(O, n, em, fa, la, order, parts, coeff, beta=8.0):
     return lam
 
 
+def run_solves(args):
+    """Multigrid-preconditioned CG solves on the initial design's density."""
+    import ctypes
+    import torch
+    import robustoptspline3d_b200 as R
+    n = args.size
+    em, fa, la, order, parts, coeff = problem(n)
+    prec = R.rso.MIXED if args.precision == "mixed" else R.rso.FP64
+    g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=prec, smoother=R.rso.SMOOTH_JACOBI, omega=0.6,
+                                                    pre=2, post=2, poisson_ratio=0.3))
+    nc = g.set_spline_partition(parts, parts, parts, order)
+    rho = g.projectDensities(g.coeff2density(np.asarray(coeff, np.float32)[:nc]), 8.0)
+    g.set_density(rho)
+    g.update_stencil()
+    f = torch.zeros(3 * g.nn, dtype=torch.float64, device="cuda")
+    ln = torch.as_tensor(g.load_nodes(), device="cuda").long()
+    f[2 * g.nn + ln] = torch.as_tensor(np.random.default_rng(1).standard_normal(len(ln)), device="cuda")
+    for _ in range(args.warmup):
+        g.solve(f, tol=1e-6, max_iter=500)
+    lib = g.lib
+    lib.rso_profile_reset(g.h)
+    lib.rso_set_profiling(g.h, 1)
+    its, ms = 0, 0.0
+    for _ in range(args.steps):
+        _, it, rr, t = g.solve(f, tol=1e-6, max_iter=500)
+        its += it
+        ms += t
+    lib.rso_set_profiling(g.h, 0)
+    name = ctypes.create_string_buffer(64)
+    cnt, tot, b, fl = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    classes = {}
+    for cls in range(16):
+        if lib.rso_profile_class(g.h, cls, name, 64, ctypes.byref(cnt), ctypes.byref(tot), ctypes.byref(b),
+                                 ctypes.byref(fl)) != 0:
+            break
+        if cnt.value:
+            avg = tot.value / cnt.value / 1e3
+            classes[name.value.decode()] = {"launches": cnt.value, "avg_us": avg * 1e6,
+                                            "algorithmic_GBps": b.value / avg / 1e9}
+    print(json.dumps({"metric": f"multigrid PCG solve @{n}^3 to rel.resid 1e-6 ({args.precision})",
+                      "value": ms / args.steps, "unit": "ms/solve", "higher_is_better": False,
+                      "iterations_per_solve": its / args.steps, "ms_per_iteration": ms / its,
+                      "levels": g_levels(n), "kernel_classes": classes}), flush=True)
+    g.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -184,7 +236,12 @@ def main():
     ap.add_argument("--ref-size", type=int, default=24)
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="design", choices=["design", "solve"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
+    if args.mode == "solve":
+        run_solves(args)
+        return
     if args.impl == "reference":
         # host-only arm: rank 0 times the CPU path, other ranks exit at once
         # (no process group is needed for that)
@@ -269,8 +326,14 @@ def main():
     hbm = peaks.get("hbm_gbs", 6650.0)
     avg_ms = tot.value / max(cnt.value, 1)
     achieved = bytes_per.value / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
-    roofline = {"kernel": kname.value.decode(), "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None, "launches": cnt.value, "avg_ms": avg_ms,
+    # DRAM bytes per fine node of one launch, measured by ncu
+    # (dram__bytes_read.sum + dram__bytes_write.sum) on a 193^3 case whose
+    # working set exceeds L2, where traffic grows with the node count
+    traffic_per_node = {"fine_jacobi_fp32": 289.9e6 / 193 ** 3}
+    kn = kname.value.decode()
+    traffic = traffic_per_node[kn] * (n + 1) ** 3 if kn in traffic_per_node else None
+    roofline = {"kernel": kn, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": traffic, "launches": cnt.value, "avg_ms": avg_ms,
                 "algorithmic_bytes_per_launch": bytes_per.value,
                 "fp_flops_per_launch": flops_per.value,
                 "fp_tflops": flops_per.value / (avg_ms / 1e3) / 1e12 if avg_ms > 0 else 0.0,

@@ -15,6 +15,9 @@
 #include "rso_internal.cuh"
 #include <cmath>
 #include <cstdio>
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
 
 namespace rso {
 
@@ -208,45 +211,47 @@ __global__ void k_restrict_xy(const Level Fl, const Level C, const T* __restrict
 }
 
 // u_f += P u_c at active, non-support fine nodes (trilinear, F = 2 or 4).
-// A thread owns the F fine nodes x = F X0 + o (o < F) of one row segment,
-// so the 8 coarse corners are read once for F nodes; every load is issued
-// before the node classes are tested.  The +1 corner lies in the padded halo
-// where its weight is 0.
+// One thread per fine node, so fine loads and stores are coalesced.  The
+// warp's 32 nodes span 32/F + 1 coarse x positions: lane l folds the coarse
+// column X = xb + l along y and z (12 loads), and each node takes its two
+// x-corners from the lanes that hold them by shuffle.
 template <typename T, int F>
 __global__ void k_prolong(const Level Fl, const Level C, const T* __restrict__ uc, T* __restrict__ uf) {
-  const int X0 = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
-  if (F * X0 >= Fl.nx || y >= Fl.ny) return;
+  const int lane = threadIdx.x;
+  const int x = blockIdx.x * 32 + lane, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+  const bool yok = y < Fl.ny;
+  const int xb = blockIdx.x * (32 / F);
   const int Y0 = y / F, Z0 = z / F, oy = y - F * Y0, oz = z - F * Z0;
   const T wy[2] = {(T)(F - oy) / (T)F, (T)oy / (T)F};
   const T wz[2] = {(T)(F - oz) / (T)F, (T)oz / (T)F};
-  const long long c0 = C.nidx(X0, Y0, Z0), cpx = C.px, cpxy = (long long)C.px * C.py;
-  // corner values folded along y and z: e[ax][comp]
-  T e[2][3];
-#pragma unroll
-  for (int ax = 0; ax < 2; ax++)
+  T E[3] = {T(0), T(0), T(0)};
+  const int X = xb + lane;
+  if (yok && X <= C.nx) {  // index C.nx is the padded halo (zero)
+    const long long c0 = C.nidx(X, Y0, Z0), cpx = C.px, cpxy = (long long)C.px * C.py;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       T s = 0;
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const int ay = k & 1, az = k >> 1;
-        s += wy[ay] * wz[az] * uc[c0 + ax + ay * cpx + az * cpxy + c * C.NP];
-      }
-      e[ax][c] = s;
+      for (int k = 0; k < 4; k++) s += wy[k & 1] * wz[k >> 1] * uc[c0 + (k & 1) * cpx + (k >> 1) * cpxy + c * C.NP];
+      E[c] = s;
     }
-  const long long n0 = Fl.nidx(F * X0, y, z);
-#pragma unroll
-  for (int o = 0; o < F; o++) {
-    if (F * X0 + o >= Fl.nx) break;
-    const long long n = n0 + o;
-    const uint8_t cls = Fl.vclass[n];
-    const T u0 = uf[n], u1 = uf[n + Fl.NP], u2 = uf[n + 2 * Fl.NP];
-    if (!(cls & NC_ACTIVE) || (cls & NC_SUPPORT)) continue;
-    const T w1 = (T)o / (T)F, w0 = (T)(F - o) / (T)F;
-    uf[n] = u0 + (w0 * e[0][0] + w1 * e[1][0]);
-    uf[n + Fl.NP] = u1 + (w0 * e[0][1] + w1 * e[1][1]);
-    uf[n + 2 * Fl.NP] = u2 + (w0 * e[0][2] + w1 * e[1][2]);
   }
+  const int X0 = x / F - xb, ox = x - F * (x / F);
+  T e0[3], e1[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    e0[c] = __shfl_sync(0xffffffffu, E[c], X0);
+    e1[c] = __shfl_sync(0xffffffffu, E[c], X0 + 1);
+  }
+  if (x >= Fl.nx || !yok) return;
+  const long long n = Fl.nidx(x, y, z);
+  const uint8_t cls = Fl.vclass[n];
+  const T u0 = uf[n], u1 = uf[n + Fl.NP], u2 = uf[n + 2 * Fl.NP];
+  if (!(cls & NC_ACTIVE) || (cls & NC_SUPPORT)) return;
+  const T w1 = (T)ox / (T)F, w0 = (T)(F - ox) / (T)F;
+  uf[n] = u0 + (w0 * e0[0] + w1 * e1[0]);
+  uf[n + Fl.NP] = u1 + (w0 * e0[1] + w1 * e1[1]);
+  uf[n + 2 * Fl.NP] = u2 + (w0 * e0[2] + w1 * e1[2]);
 }
 
 // ---------------------------------------------------------------- Galerkin
@@ -483,6 +488,212 @@ __global__ void k_gemv_scatter(const Level C, const double* __restrict__ Kinv, c
   if (lane == 0) u[cnodes[row / 3] + (row % 3) * C.NP] = (T)s;
 }
 
+// ---------------------------------------------------------------- bottom of the V-cycle
+// The small levels (at most kBottomMaxNodes nodes each) and the coarsest
+// solve run as one kernel on an 8-CTA thread-block cluster: a sweep on a
+// 17^3-node level is a few microseconds of work, less than a launch, so
+// every phase (Jacobi sweeps, residual, restriction, dense coarsest solve,
+// prolongation) is separated by a cluster barrier instead of a launch.  A
+// cluster rather than one CTA because a single SM cannot pull the level's
+// stencils from L2 fast enough.  Damped Jacobi only; results are left in the
+// levels' u vectors exactly as the per-level launches leave them.
+constexpr int BOT_CTAS = 8, BOT_THREADS = 1024, BOT_MAX_LEVELS = 12;
+static const long long kBottomMaxNodes = 6000;
+
+template <typename T>
+struct BottomArgs {
+  Level L[BOT_MAX_LEVELS];
+  T omega[BOT_MAX_LEVELS];
+  int lb, nl, pre, post;
+  const double* kinv;  // coarsest inverse, N x N, N = 3 nc
+  const int* cnodes;
+  int nc;
+  double* cf;          // coarsest right-hand side (N doubles)
+};
+
+template <typename T>
+__device__ __forceinline__ T* bv_u(const Level& L) { if constexpr (sizeof(T) == 4) return (T*)L.u32; else return (T*)L.u64; }
+template <typename T>
+__device__ __forceinline__ T* bv_f(const Level& L) { if constexpr (sizeof(T) == 4) return (T*)L.f32; else return (T*)L.f64; }
+template <typename T>
+__device__ __forceinline__ T* bv_r(const Level& L) { if constexpr (sizeof(T) == 4) return (T*)L.r32; else return (T*)L.r64; }
+template <typename T>
+__device__ __forceinline__ T* bv_t(const Level& L) { if constexpr (sizeof(T) == 4) return (T*)L.t32; else return (T*)L.t64; }
+template <typename T>
+__device__ __forceinline__ const T* bv_st(const Level& L) {
+  if constexpr (sizeof(T) == 4) return (const T*)L.st32; else return (const T*)L.st64;
+}
+
+__device__ __forceinline__ long long bot_node(const Level& L, long long i) {
+  const int x = (int)(i % L.nx), y = (int)((i / L.nx) % L.ny), z = (int)(i / ((long long)L.nx * L.ny));
+  return L.nidx(x, y, z);
+}
+
+// out = (zero ? 0 : u) + omega D^-1 (f - K u); inactive nodes 0
+template <typename T>
+__device__ void bot_jacobi(const Level& L, const T* st, const T* u, const T* f, T* out, T om, bool zero, int g0,
+                           int gs) {
+  const long long NP = L.NP;
+  for (long long i = g0; i < L.nn; i += gs) {
+    const long long n = bot_node(L, i);
+    if (!(L.vclass[n] & NC_ACTIVE)) { out[n] = 0; out[n + NP] = 0; out[n + 2 * NP] = 0; continue; }
+    T acc[3] = {0, 0, 0};
+    if (!zero) stencil_apply<T>(L, st, u, n, false, acc);
+    T S[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) S[k] = st[(13 * 9 + k) * NP + n];
+    const T r0 = f[n] - acc[0], r1 = f[n + NP] - acc[1], r2 = f[n + 2 * NP] - acc[2];
+    const T A = S[4] * S[8] - S[5] * S[7], B = -(S[3] * S[8] - S[5] * S[6]), C = S[3] * S[7] - S[4] * S[6];
+    const T det = S[0] * A + S[1] * B + S[2] * C;
+    const T id = om / det;
+    const T i01 = -(S[1] * S[8] - S[2] * S[7]), i02 = S[1] * S[5] - S[2] * S[4];
+    const T i11 = S[0] * S[8] - S[2] * S[6], i12 = -(S[0] * S[5] - S[2] * S[3]);
+    const T i21 = -(S[0] * S[7] - S[1] * S[6]), i22 = S[0] * S[4] - S[1] * S[3];
+    const T u0 = zero ? T(0) : u[n], u1 = zero ? T(0) : u[n + NP], u2 = zero ? T(0) : u[n + 2 * NP];
+    out[n] = u0 + id * (A * r0 + i01 * r1 + i02 * r2);
+    out[n + NP] = u1 + id * (B * r0 + i11 * r1 + i12 * r2);
+    out[n + 2 * NP] = u2 + id * (C * r0 + i21 * r1 + i22 * r2);
+  }
+}
+
+template <typename T>
+__device__ void bot_residual(const Level& L, const T* st, const T* u, const T* f, T* r, int g0, int gs) {
+  const long long NP = L.NP;
+  for (long long i = g0; i < L.nn; i += gs) {
+    const long long n = bot_node(L, i);
+    T acc[3] = {0, 0, 0};
+    if (L.vclass[n] & NC_ACTIVE) stencil_apply<T>(L, st, u, n, false, acc);
+    r[n] = f[n] - acc[0]; r[n + NP] = f[n + NP] - acc[1]; r[n + 2 * NP] = f[n + 2 * NP] - acc[2];
+  }
+}
+
+template <typename T>
+__device__ void bot_restrict(const Level& Fl, const Level& C, const T* rf, T* fc, int g0, int gs) {
+  const int F = C.factor;
+  for (long long i = g0; i < C.nn; i += gs) {
+    const int X = (int)(i % C.nx), Y = (int)((i / C.nx) % C.ny), Z = (int)(i / ((long long)C.nx * C.ny));
+    const long long nC = C.nidx(X, Y, Z);
+    T s0 = 0, s1 = 0, s2 = 0;
+    if (C.vclass[nC] & NC_ACTIVE) {
+      for (int dz = -F + 1; dz < F; dz++) {
+        const int z = F * Z + dz;
+        if (z < 0 || z >= Fl.nz) continue;
+        for (int dy = -F + 1; dy < F; dy++) {
+          const int y = F * Y + dy;
+          if (y < 0 || y >= Fl.ny) continue;
+          const T wyz = (T)(F - abs(dy)) / (T)F * ((T)(F - abs(dz)) / (T)F);
+          for (int dx = -F + 1; dx < F; dx++) {
+            const int x = F * X + dx;
+            if (x < 0 || x >= Fl.nx) continue;
+            const long long n = Fl.nidx(x, y, z);
+            const T w = wyz * ((T)(F - abs(dx)) / (T)F);
+            s0 += w * rf[n]; s1 += w * rf[n + Fl.NP]; s2 += w * rf[n + 2 * Fl.NP];
+          }
+        }
+      }
+    }
+    fc[nC] = s0; fc[nC + C.NP] = s1; fc[nC + 2 * C.NP] = s2;
+  }
+}
+
+template <typename T>
+__device__ void bot_prolong(const Level& Fl, const Level& C, const T* uc, T* uf, int g0, int gs) {
+  const int F = C.factor;
+  for (long long i = g0; i < Fl.nn; i += gs) {
+    const int x = (int)(i % Fl.nx), y = (int)((i / Fl.nx) % Fl.ny), z = (int)(i / ((long long)Fl.nx * Fl.ny));
+    const long long n = Fl.nidx(x, y, z);
+    const uint8_t cls = Fl.vclass[n];
+    if (!(cls & NC_ACTIVE) || (cls & NC_SUPPORT)) continue;
+    const int X0 = x / F, Y0 = y / F, Z0 = z / F;
+    const int ox = x - F * X0, oy = y - F * Y0, oz = z - F * Z0;
+    T s0 = 0, s1 = 0, s2 = 0;
+    for (int A = 0; A < 8; A++) {
+      const int ax = A & 1, ay = (A >> 1) & 1, az = A >> 2;
+      const T w = (ax ? (T)ox : (T)(F - ox)) / (T)F * ((ay ? (T)oy : (T)(F - oy)) / (T)F) *
+                  ((az ? (T)oz : (T)(F - oz)) / (T)F);
+      const long long nC = C.nidx(X0 + ax, Y0 + ay, Z0 + az);
+      s0 += w * uc[nC]; s1 += w * uc[nC + C.NP]; s2 += w * uc[nC + 2 * C.NP];
+    }
+    uf[n] += s0; uf[n + Fl.NP] += s1; uf[n + 2 * Fl.NP] += s2;
+  }
+}
+
+template <typename T>
+__device__ void bot_copy(const Level& L, const T* a, T* b, int g0, int gs) {
+  for (long long i = g0; i < 3 * L.NP; i += gs) b[i] = a[i];
+}
+
+template <typename T>
+__global__ void __cluster_dims__(BOT_CTAS, 1, 1) __launch_bounds__(BOT_THREADS, 1)
+    k_bottom(const __grid_constant__ BottomArgs<T> A) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int g0 = (int)cl.block_rank() * BOT_THREADS + threadIdx.x, gs = BOT_CTAS * BOT_THREADS;
+  // down: pre-smoothing from a zero iterate, residual, restriction
+  for (int li = A.lb; li < A.nl - 1; li++) {
+    const Level& L = A.L[li];
+    const T* st = bv_st<T>(L);
+    T* u = bv_u<T>(L);
+    T* t = bv_t<T>(L);
+    T *cur = u, *oth = t;
+    for (int s = 0; s < A.pre; s++) {
+      bot_jacobi<T>(L, st, cur, bv_f<T>(L), oth, A.omega[li], s == 0, g0, gs);
+      cl.sync();
+      T* w = cur; cur = oth; oth = w;
+    }
+    if (A.pre == 0) {
+      for (long long i = g0; i < 3 * L.NP; i += gs) u[i] = T(0);
+      cl.sync();
+    } else if (cur != u) {
+      bot_copy<T>(L, cur, u, g0, gs);
+      cl.sync();
+    }
+    bot_residual<T>(L, st, u, bv_f<T>(L), bv_r<T>(L), g0, gs);
+    cl.sync();
+    bot_restrict<T>(L, A.L[li + 1], bv_r<T>(L), bv_f<T>(A.L[li + 1]), g0, gs);
+    cl.sync();
+  }
+  // coarsest: u = Kinv f at the listed nodes, zero elsewhere
+  {
+    const Level& C = A.L[A.nl - 1];
+    T* u = bv_u<T>(C);
+    const T* f = bv_f<T>(C);
+    for (long long i = g0; i < 3 * C.NP; i += gs) u[i] = T(0);
+    for (int i = g0; i < A.nc; i += gs) {
+      const long long n = A.cnodes[i];
+      A.cf[3 * i + 0] = (double)f[n];
+      A.cf[3 * i + 1] = (double)f[n + C.NP];
+      A.cf[3 * i + 2] = (double)f[n + 2 * C.NP];
+    }
+    cl.sync();
+    const int N = 3 * A.nc;
+    for (int row = g0; row < N; row += gs) {
+      double s = 0;
+      const double* k = A.kinv + (long long)row * N;
+      for (int j = 0; j < N; j++) s += k[j] * A.cf[j];
+      u[A.cnodes[row / 3] + (row % 3) * C.NP] = (T)s;
+    }
+    cl.sync();
+  }
+  // up: prolongation and post-smoothing
+  for (int li = A.nl - 2; li >= A.lb; li--) {
+    const Level& L = A.L[li];
+    const T* st = bv_st<T>(L);
+    T* u = bv_u<T>(L);
+    bot_prolong<T>(L, A.L[li + 1], bv_u<T>(A.L[li + 1]), u, g0, gs);
+    cl.sync();
+    T *cur = u, *oth = bv_t<T>(L);
+    for (int s = 0; s < A.post; s++) {
+      bot_jacobi<T>(L, st, cur, bv_f<T>(L), oth, A.omega[li], false, g0, gs);
+      cl.sync();
+      T* w = cur; cur = oth; oth = w;
+    }
+    if (cur != u) {
+      bot_copy<T>(L, cur, u, g0, gs);
+      cl.sync();
+    }
+  }
+}
+
 // ---------------------------------------------------------------- host wrappers
 static inline dim3 node_grid(const Level& l) { return dim3(cdiv(l.nx, 32), cdiv(l.ny, 8), l.nz); }
 // levels above this many nodes use the per-node stencil kernel
@@ -557,9 +768,9 @@ rso_status prolong(rso_handle* h, int cl, const T* uc, T* uf) {
   const Level& f = h->L[cl - 1];
   const Level& c = h->L[cl];
   if (c.factor == 4) {
-    k_prolong<T, 4><<<dim3(cdiv(cdiv(f.nx, 4), 32), cdiv(f.ny, 8), f.nz), dim3(32, 8), 0, h->stream>>>(f, c, uc, uf); rso::note_launch();
+    k_prolong<T, 4><<<node_grid(f), dim3(32, 8), 0, h->stream>>>(f, c, uc, uf); rso::note_launch();
   } else if (c.factor == 2) {
-    k_prolong<T, 2><<<dim3(cdiv(cdiv(f.nx, 2), 32), cdiv(f.ny, 8), f.nz), dim3(32, 8), 0, h->stream>>>(f, c, uc, uf); rso::note_launch();
+    k_prolong<T, 2><<<node_grid(f), dim3(32, 8), 0, h->stream>>>(f, c, uc, uf); rso::note_launch();
   } else {
     h->err = "coarsening factor must be 2 or 4";
     return RSO_ERR_UNSUPPORTED;
@@ -575,6 +786,37 @@ rso_status coarsest_solve(rso_handle* h, const T* f, T* u) {
   k_gemv_scatter<T><<<cdiv(N, 8), 256, 0, h->stream>>>(c, h->c_K + (size_t)N * N, h->c_f, h->nc, h->c_nodes, u); rso::note_launch();
   return launch_check(h, "coarsest_solve");
 }
+
+// index of the first level handled by k_bottom (-1: none).  It needs damped
+// Jacobi, at least one smoothed level above the coarsest, and every level from
+// it down small enough.
+int bottom_level(const rso_handle* h) {
+  const int nl = (int)h->L.size();
+  if (h->cfg.smoother != RSO_SMOOTH_JACOBI || nl < 3 || nl > BOT_MAX_LEVELS || h->nc == 0) return -1;
+  int lb = nl - 1;
+  while (lb - 1 >= 1 && h->L[lb - 1].nn <= kBottomMaxNodes) lb--;
+  return lb <= nl - 2 ? lb : -1;
+}
+
+template <typename T>
+rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post) {
+  BottomArgs<T> A;
+  const int nl = (int)h->L.size();
+  for (int li = 0; li < nl; li++) {
+    A.L[li] = h->L[li];
+    A.omega[li] = (T)(h->cfg.omega * 2.0 / h->L[li].lam);
+  }
+  A.lb = lb; A.nl = nl; A.pre = pre; A.post = post;
+  const int N = 3 * h->nc;
+  A.kinv = h->c_K + (size_t)N * N;
+  A.cnodes = h->c_nodes;
+  A.nc = h->nc;
+  A.cf = h->c_f;
+  k_bottom<T><<<BOT_CTAS, BOT_THREADS, 0, h->stream>>>(A); rso::note_launch();
+  return launch_check(h, "bottom_vcycle");
+}
+template rso_status bottom_vcycle<double>(rso_handle*, int, int, int);
+template rso_status bottom_vcycle<float>(rso_handle*, int, int, int);
 
 rso_status galerkin(rso_handle* h) {
   for (size_t li = 1; li < h->L.size(); li++) {

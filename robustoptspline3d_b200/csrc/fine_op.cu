@@ -166,7 +166,7 @@ constexpr int WTX = 32, FZC = 32, WPD = 2, WNSLOT = 4;
 
 template <typename T, int TY>
 constexpr int walsh_smem_bytes() {
-  return (int)sizeof(T) * (WNSLOT * (3 * (WTX + 1) * (TY + 1) + WTX * TY) + 2 * 9 * WTX * TY);
+  return (int)sizeof(T) * (WNSLOT * (3 * 36 * (TY + 1) + 36 * TY) + 2 * 9 * WTX * TY);
 }
 
 // MODE 0: out = f - K u;  MODE 1: out = K u (support rows pass u);
@@ -175,48 +175,60 @@ template <typename T, int MODE, int TY>
 __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
     k_fine_w(const Level L, const T* __restrict__ u, const T* __restrict__ f, T* __restrict__ out,
              const T* __restrict__ rp, T omega, double* __restrict__ dotp) {
-  constexpr int NX = WTX + 1, NPL = NX * (TY + 1), NE = WTX * TY, SLOT = 3 * NPL + NE;
+  // Staged rows are 16-byte aligned windows of RX entries starting at the
+  // tile's first padded x index rounded down to a multiple of 4 (ox = offset
+  // of the tile inside the window), copied in 16-byte chunks.
+  constexpr int RX = 36, NPL = RX * (TY + 1), NE = WTX * TY, SLOT = 3 * NPL + RX * TY;
+  constexpr int EPC = 16 / (int)sizeof(T), CPR = RX / EPC;  // entries per chunk, chunks per row
+  constexpr int NCH = (3 * (TY + 1) + TY) * CPR, KC = (NCH + NE - 1) / NE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* ss = reinterpret_cast<T*>(smem_raw);  // [WNSLOT][SLOT]: u plane (3 comps) + rho layer
+  T* ss = reinterpret_cast<T*>(smem_raw);  // [WNSLOT][SLOT]: u plane (3 comps x (TY+1) rows) + rho layer (TY rows)
   T* sx = ss + WNSLOT * SLOT;              // [2][9][NE]: corners (0,0), (1,0), (0,1), by plane parity
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * WTX + tx;
   const int x0 = blockIdx.x * (WTX - 1), y0 = blockIdx.y * (TY - 1);
   const int z0 = blockIdx.z * FZC, z1 = min(z0 + FZC, L.nz);
   const int ex = x0 - 1 + tx, ey = y0 - 1 + ty;
   const long long NP = L.NP;
+  const int xs = x0 & ~3, ox = x0 - xs;
 
-  // per-thread staging slots: entry i = tid + k*NE of the plane tile, as an
-  // in-plane offset (component plane included; -1 outside the padded box)
-  constexpr int KU = (3 * NPL + NE - 1) / NE;
-  int ioff[KU];
+  // this thread's chunks: in-plane global offset (-1: zero fill), shared
+  // offset, and whether the chunk belongs to the rho layer
+  int goff[KC], soff[KC];
+  bool isr[KC];
 #pragma unroll
-  for (int k = 0; k < KU; k++) {
-    const int i = tid + k * NE;
-    const int c = i / NPL, r = i - c * NPL, sy = r / NX, sxx = r - sy * NX;
-    const int gx = x0 - 1 + sxx, gy = y0 - 1 + sy;
-    ioff[k] = (i < 3 * NPL && gx <= L.nx && gy <= L.ny) ? (int)(c * NP + (gx + 1) + (long long)L.px * (gy + 1)) : -1;
+  for (int kk = 0; kk < KC; kk++) {
+    const int k = tid + kk * NE;
+    const int row = k / CPR, j = k - row * CPR, xg = xs + j * EPC;
+    goff[kk] = -1;
+    soff[kk] = -1;
+    isr[kk] = false;
+    if (k < NCH) {
+      if (row < 3 * (TY + 1)) {
+        const int c = row / (TY + 1), yr = row - c * (TY + 1), gyp = y0 + yr;  // padded y index
+        soff[kk] = c * NPL + yr * RX + j * EPC;
+        if (gyp <= L.py - 1 && xg + EPC <= L.px) goff[kk] = (int)(c * NP + (long long)gyp * L.px + xg);
+      } else {
+        const int yr = row - 3 * (TY + 1), gyp = y0 + yr;
+        isr[kk] = true;
+        soff[kk] = 3 * NPL + yr * RX + j * EPC;
+        if (gyp <= L.qy - 1 && xg + EPC <= L.qx) goff[kk] = (int)((long long)gyp * L.qx + xg);
+      }
+    }
   }
-  const bool rvalid = ex <= L.ex && ey <= L.ey;
-  const long long roff = rvalid ? L.eidx(ex, ey, -1) : 0;
   const long long pxy = (long long)L.px * L.py, qxy = (long long)L.qx * L.qy;
   // stage s: node plane s of u and element layer s of rho^p (zero outside)
   auto issue = [&](int s) {
     T* dst = ss + ((s + WNSLOT) % WNSLOT) * SLOT;
-    const long long po = pxy * (s + 1);
+    const long long po = pxy * (s + 1), qo = qxy * (s + 1);
 #pragma unroll
-    for (int k = 0; k < KU; k++) {
-      const int i = tid + k * NE;
-      if (i < 3 * NPL) {
-        if (ioff[k] >= 0 && s <= L.nz)
-          __pipeline_memcpy_async(dst + i, u + po + ioff[k], sizeof(T));
-        else
-          dst[i] = T(0);
-      }
+    for (int kk = 0; kk < KC; kk++) {
+      if (soff[kk] < 0) continue;
+      const bool ok = goff[kk] >= 0 && (isr[kk] ? s <= L.ez : s <= L.nz);
+      if (ok)
+        __pipeline_memcpy_async(dst + soff[kk], isr[kk] ? rp + qo + goff[kk] : u + po + goff[kk], 16);
+      else
+        *reinterpret_cast<float4*>(dst + soff[kk]) = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    if (rvalid && s <= L.ez)
-      __pipeline_memcpy_async(dst + 3 * NPL + tid, rp + roff + qxy * (s + 1), sizeof(T));
-    else
-      dst[3 * NPL + tid] = T(0);
     __pipeline_commit();
   };
   // xy modes of the 4 face nodes of this column on a staged plane; also the
@@ -224,8 +236,8 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
   auto face = [&](const T* pl, T (&F)[4][3], T (&own)[3]) {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      const T* p = pl + c * NPL + ty * NX + tx;
-      const T a00 = p[0], a10 = p[1], a01 = p[NX], a11 = p[NX + 1];
+      const T* p = pl + c * NPL + ty * RX + tx + ox;
+      const T a00 = p[0], a10 = p[1], a01 = p[RX], a11 = p[RX + 1];
       const T s0 = a00 + a10, d0 = a10 - a00, s1 = a01 + a11, d1 = a11 - a01;
       F[0][c] = s0 + s1;  // (mx, my) = (0, 0)
       F[1][c] = d0 + d1;  // (1, 0)
@@ -334,7 +346,8 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
         }
     }
     // blocks of B, in place (block c maps its three entries onto themselves), times rho^p
-    const T re = sr[tid];
+    const int ri = ty * RX + tx + ox;
+    const T re = sr[ri];
 #pragma unroll
     for (int c = 0; c < 8; c++) {
       T in[3], o[3];
@@ -355,9 +368,9 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
 #pragma unroll
       for (int q = 0; q < 4; q++) ra[q] = rb[q];
       rb[0] = re;
-      rb[1] = writer ? sr[tid + 1] : T(0);
-      rb[2] = writer ? sr[tid + WTX] : T(0);
-      rb[3] = writer ? sr[tid + WTX + 1] : T(0);
+      rb[1] = writer ? sr[ri + 1] : T(0);
+      rb[2] = writer ? sr[ri + RX] : T(0);
+      rb[3] = writer ? sr[ri + RX + 1] : T(0);
     }
     // bottom face (plane z) = S - D, top face (plane z+1) = S + D
     T tot[4][3];
@@ -531,6 +544,11 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
   if (3 * l.NP >= (1LL << 31)) {
     h->err = "fine level too large for 32-bit in-plane offsets";
     return RSO_ERR_UNSUPPORTED;
+  }
+  // the kernel stages 16-byte chunks: both arrays must start on 16 bytes
+  if ((reinterpret_cast<uintptr_t>(u) | reinterpret_cast<uintptr_t>(rp)) & 15) {
+    h->err = "fine operator inputs must be 16-byte aligned";
+    return RSO_ERR_INVALID_ARG;
   }
   constexpr int smem = walsh_smem_bytes<T, WTY>();
   static bool attr = false;

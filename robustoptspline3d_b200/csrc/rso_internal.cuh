@@ -182,6 +182,9 @@ template <typename T>
 rso_status fine_residual(rso_handle* h, const T* u, const T* f, T* r, const T* rp);
 template <typename T>
 rso_status fine_applyK(rso_handle* h, const T* u, T* f, const T* rp);
+int bottom_level(const rso_handle* h);
+template <typename T>
+rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post);
 rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const double* rp, double* dot_dev);
 template <typename T>
 rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega);

@@ -69,7 +69,10 @@ static rso_status level_residual(rso_handle* h, int li) {
 template <typename T>
 rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric, bool u0_zero) {
   const int nl = (int)h->L.size();
-  for (int li = 0; li < nl; li++) {
+  // levels from lb down run inside one cluster kernel (bottom_vcycle)
+  const int lb = bottom_level(h);
+  const int top = lb > 0 ? lb : nl;
+  for (int li = 0; li < top; li++) {
     Level& l = h->L[li];
     if (li > 0) {
       RSO_TRY(level_residual<T>(h, li - 1));
@@ -84,7 +87,13 @@ rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric, bool u
       RSO_TRY(smooth<T>(h, li, post, symmetric ? 1 : 0));
     }
   }
-  for (int li = nl - 2; li >= 0; li--) {
+  if (lb > 0) {
+    RSO_TRY(level_residual<T>(h, lb - 1));
+    RSO_TRY(restrict_<T>(h, lb, LV<T>::r(h->L[lb - 1]), LV<T>::f(h->L[lb])));
+    RSO_TRY(bottom_vcycle<T>(h, lb, pre, post));
+  }
+  // up-sweep from the level above the coarsest (or above the cluster kernel's levels)
+  for (int li = lb > 0 ? lb - 1 : nl - 2; li >= 0; li--) {
     RSO_TRY(prolong<T>(h, li + 1, LV<T>::u(h->L[li + 1]), LV<T>::u(h->L[li])));
     RSO_TRY(smooth<T>(h, li, post, symmetric ? 1 : 0));
   }

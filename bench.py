@@ -37,6 +37,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "worst-case TO design iterations/s @256^3 (mixed FP32 V-cycle + FP64 CG, rel.resid 1e-6)"
 UNIT = "iter/s"
+# damped-Jacobi factor relative to 2 / lambda_max(D^-1 K); 0.8 needs fewer PCG
+# iterations than 0.6 on this workload at the same cost per iteration
+OMEGA = 0.8
 
 
 def problem(n, seed=2026):
@@ -188,7 +191,7 @@ def run_solves(args):
     n = args.size
     em, fa, la, order, parts, coeff = problem(n)
     prec = R.rso.MIXED if args.precision == "mixed" else R.rso.FP64
-    g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=prec, smoother=R.rso.SMOOTH_JACOBI, omega=0.6,
+    g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=prec, smoother=R.rso.SMOOTH_JACOBI, omega=OMEGA,
                                                     pre=2, post=2, poisson_ratio=0.3))
     nc = g.set_spline_partition(parts, parts, parts, order)
     rho = g.projectDensities(g.coeff2density(np.asarray(coeff, np.float32)[:nc]), 8.0)
@@ -257,7 +260,7 @@ def main():
     prm = R.IterParams(lanczos_steps=20, solve_tol=1e-6, ss_mode=4)
 
     def make(precision):
-        g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=precision, smoother=R.rso.SMOOTH_JACOBI, omega=0.6,
+        g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=precision, smoother=R.rso.SMOOTH_JACOBI, omega=OMEGA,
                                                         pre=2, post=2, poisson_ratio=0.3))
         nc = g.set_spline_partition(parts, parts, parts, order)
         mma = R.MMA(nc, 2, 0.0, 1.0)

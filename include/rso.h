@@ -41,7 +41,11 @@ typedef enum {
 } rso_status;
 
 /* smoothers */
-enum { RSO_SMOOTH_GS = 0, RSO_SMOOTH_JACOBI = 1 };
+enum { RSO_SMOOTH_GS = 0, RSO_SMOOTH_JACOBI = 1, RSO_SMOOTH_CHEBYSHEV = 2 };
+/* RSO_SMOOTH_CHEBYSHEV (no counterpart in the reference, which smooths with
+ * damped Jacobi or coloured Gauss-Seidel): `pre`/`post` Chebyshev steps for
+ * D^-1 K on [lambda_max/4, lambda_max], D the 3x3 diagonal blocks; omega is
+ * not used.  A polynomial in D^-1 K, so the V-cycle stays symmetric. */
 /* V-cycle arithmetic */
 enum { RSO_FP64 = 0, RSO_MIXED = 1 };
 /* solve methods */
@@ -66,7 +70,7 @@ typedef struct {
   double rho_min;          /* density floor */
   int n_levels;            /* 0: reference policy, coarsen while > 400 active elements */
   int first_factor;        /* 4: non-dyadic first coarsening (skip layer 1, reference); 2: dyadic */
-  int smoother;            /* RSO_SMOOTH_* */
+  int smoother;            /* RSO_SMOOTH_GS, _JACOBI or _CHEBYSHEV */
   double omega;            /* damped Jacobi factor relative to the bound 2/lambda_max(D^-1 K) */
   int pre, post;           /* smoothing sweeps */
   int precision;           /* RSO_FP64 or RSO_MIXED (FP32 V-cycle inside FP64 outer iteration) */

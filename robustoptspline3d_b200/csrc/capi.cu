@@ -247,7 +247,11 @@ extern "C" rso_status rso_create(const rso_config* cfg, int ex, int ey, int ez, 
   if (cfg) h->cfg = *cfg;
   else rso_default_config(&h->cfg);
   if (h->cfg.first_factor != 2 && h->cfg.first_factor != 4) { delete h; return RSO_ERR_INVALID_ARG; }
-  if (h->cfg.pre < 0 || h->cfg.post < 0 || h->cfg.penal <= 0) { delete h; return RSO_ERR_INVALID_ARG; }
+  if (h->cfg.pre < 0 || h->cfg.post < 0 || h->cfg.penal <= 0 || h->cfg.pre > 16 || h->cfg.post > 16) {
+    delete h;
+    return RSO_ERR_INVALID_ARG;
+  }
+  if (h->cfg.smoother < RSO_SMOOTH_GS || h->cfg.smoother > RSO_SMOOTH_CHEBYSHEV) { delete h; return RSO_ERR_INVALID_ARG; }
   if (h->cfg.mode == RSO_NO_SUPPORT_CONSTRAIN_FORCE_DIRECTION || h->cfg.mode == RSO_NO_SUPPORT_FREE_FORCE) {
     // the dense coarsest solve needs supports (a support-free operator is singular)
     g_create_err = "support-free modes are not supported";
@@ -311,7 +315,7 @@ extern "C" rso_status rso_update_operators(rso_handle* h) {
   if (!h) return RSO_ERR_INVALID_ARG;
   RSO_TRY(galerkin(h));
   RSO_TRY(coarsest_factor(h));
-  if (h->cfg.smoother == RSO_SMOOTH_JACOBI) RSO_TRY(estimate_lambda(h));
+  if (h->cfg.smoother != RSO_SMOOTH_GS) RSO_TRY(estimate_lambda(h));
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   h->operators_ready = true;
   return RSO_OK;

@@ -49,7 +49,8 @@ __device__ __forceinline__ void stencil_apply(const Level& L, const T* __restric
 // MODE 0 residual, MODE 2 damped block Jacobi (out of place).
 template <typename T, int MODE>
 __global__ void __launch_bounds__(256) k_coarse(const Level L, const T* __restrict__ st, const T* __restrict__ u,
-                                                const T* __restrict__ f, T* __restrict__ out, T omega) {
+                                                const T* __restrict__ f, T* __restrict__ out, T omega,
+                                                const T* __restrict__ uprev, T c1) {
   const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
   if (x >= L.nx || y >= L.ny) return;
   const long long NP = L.NP;
@@ -72,9 +73,10 @@ __global__ void __launch_bounds__(256) k_coarse(const Level L, const T* __restri
     const T i01 = -(S[1] * S[8] - S[2] * S[7]), i02 = S[1] * S[5] - S[2] * S[4];
     const T i11 = S[0] * S[8] - S[2] * S[6], i12 = -(S[0] * S[5] - S[2] * S[3]);
     const T i21 = -(S[0] * S[7] - S[1] * S[6]), i22 = S[0] * S[4] - S[1] * S[3];
-    out[n] = u[n] + id * (A * r0 + i01 * r1 + i02 * r2);
-    out[n + NP] = u[n + NP] + id * (B * r0 + i11 * r1 + i12 * r2);
-    out[n + 2 * NP] = u[n + 2 * NP] + id * (C * r0 + i21 * r1 + i22 * r2);
+    const T p0 = uprev ? uprev[n] : T(0), p1 = uprev ? uprev[n + NP] : T(0), p2 = uprev ? uprev[n + 2 * NP] : T(0);
+    out[n] = u[n] + c1 * (u[n] - p0) + id * (A * r0 + i01 * r1 + i02 * r2);
+    out[n + NP] = u[n + NP] + c1 * (u[n + NP] - p1) + id * (B * r0 + i11 * r1 + i12 * r2);
+    out[n + 2 * NP] = u[n + 2 * NP] + c1 * (u[n + 2 * NP] - p2) + id * (C * r0 + i21 * r1 + i22 * r2);
   }
 }
 
@@ -89,7 +91,8 @@ constexpr int CTY = 4;
 template <typename T, int MODE>
 __global__ void __launch_bounds__(32 * CTY * 3) k_coarse_r(const Level L, const T* __restrict__ st,
                                                            const T* __restrict__ u, const T* __restrict__ f,
-                                                           T* __restrict__ out, T omega) {
+                                                           T* __restrict__ out, T omega,
+                                                           const T* __restrict__ uprev, T c1) {
   __shared__ T sres[3][CTY][32];
   const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * CTY + threadIdx.y, z = blockIdx.z;
   const int r = threadIdx.z;
@@ -130,7 +133,8 @@ __global__ void __launch_bounds__(32 * CTY * 3) k_coarse_r(const Level L, const 
   else { a0 = c02; a1 = -(S[0] * S[7] - S[1] * S[6]); a2 = S[0] * S[4] - S[1] * S[3]; }
   const T r0 = sres[0][threadIdx.y][threadIdx.x], r1 = sres[1][threadIdx.y][threadIdx.x],
           r2 = sres[2][threadIdx.y][threadIdx.x];
-  out[n + r * NP] = u[n + r * NP] + (omega / det) * (a0 * r0 + a1 * r1 + a2 * r2);
+  const T ur = u[n + r * NP], pr = uprev ? uprev[n + r * NP] : T(0);
+  out[n + r * NP] = ur + c1 * (ur - pr) + (omega / det) * (a0 * r0 + a1 * r1 + a2 * r2);
 }
 
 // one colour of the point Gauss-Seidel sweep on stored stencils (gs_relax_kernel grid/Grid.cu:1497-1609)
@@ -500,10 +504,12 @@ __global__ void k_gemv_scatter(const Level C, const double* __restrict__ Kinv, c
 constexpr int BOT_CTAS = 8, BOT_THREADS = 1024, BOT_MAX_LEVELS = 12;
 static const long long kBottomMaxNodes = 6000;
 
+constexpr int BOT_MAX_SWEEPS = 8;
 template <typename T>
 struct BottomArgs {
   Level L[BOT_MAX_LEVELS];
-  T omega[BOT_MAX_LEVELS];
+  T om[BOT_MAX_LEVELS][BOT_MAX_SWEEPS];  // smoother step coefficients per level and step
+  T c1[BOT_MAX_LEVELS][BOT_MAX_SWEEPS];
   int lb, nl, pre, post;
   const double* kinv;  // coarsest inverse, N x N, N = 3 nc
   const int* cnodes;
@@ -529,10 +535,11 @@ __device__ __forceinline__ long long bot_node(const Level& L, long long i) {
   return L.nidx(x, y, z);
 }
 
-// out = (zero ? 0 : u) + omega D^-1 (f - K u); inactive nodes 0
+// out = u + c1 (u - up) + om D^-1 (f - K u), u read as 0 when zero and up as
+// 0 when NULL; inactive nodes 0
 template <typename T>
-__device__ void bot_jacobi(const Level& L, const T* st, const T* u, const T* f, T* out, T om, bool zero, int g0,
-                           int gs) {
+__device__ void bot_jacobi(const Level& L, const T* st, const T* u, const T* f, T* out, T om, bool zero, const T* up,
+                           T c1, int g0, int gs) {
   const long long NP = L.NP;
   for (long long i = g0; i < L.nn; i += gs) {
     const long long n = bot_node(L, i);
@@ -550,9 +557,10 @@ __device__ void bot_jacobi(const Level& L, const T* st, const T* u, const T* f, 
     const T i11 = S[0] * S[8] - S[2] * S[6], i12 = -(S[0] * S[5] - S[2] * S[3]);
     const T i21 = -(S[0] * S[7] - S[1] * S[6]), i22 = S[0] * S[4] - S[1] * S[3];
     const T u0 = zero ? T(0) : u[n], u1 = zero ? T(0) : u[n + NP], u2 = zero ? T(0) : u[n + 2 * NP];
-    out[n] = u0 + id * (A * r0 + i01 * r1 + i02 * r2);
-    out[n + NP] = u1 + id * (B * r0 + i11 * r1 + i12 * r2);
-    out[n + 2 * NP] = u2 + id * (C * r0 + i21 * r1 + i22 * r2);
+    const T p0 = up ? up[n] : T(0), p1 = up ? up[n + NP] : T(0), p2 = up ? up[n + 2 * NP] : T(0);
+    out[n] = u0 + c1 * (u0 - p0) + id * (A * r0 + i01 * r1 + i02 * r2);
+    out[n + NP] = u1 + c1 * (u1 - p1) + id * (B * r0 + i11 * r1 + i12 * r2);
+    out[n + 2 * NP] = u2 + c1 * (u2 - p2) + id * (C * r0 + i21 * r1 + i22 * r2);
   }
 }
 
@@ -633,12 +641,13 @@ __global__ void __cluster_dims__(BOT_CTAS, 1, 1) __launch_bounds__(BOT_THREADS, 
     const Level& L = A.L[li];
     const T* st = bv_st<T>(L);
     T* u = bv_u<T>(L);
-    T* t = bv_t<T>(L);
-    T *cur = u, *oth = t;
+    // current / next / previous iterate rotate over u, t and the (free) r
+    T *cur = u, *oth = bv_t<T>(L), *prv = bv_r<T>(L);
     for (int s = 0; s < A.pre; s++) {
-      bot_jacobi<T>(L, st, cur, bv_f<T>(L), oth, A.omega[li], s == 0, g0, gs);
+      bot_jacobi<T>(L, st, cur, bv_f<T>(L), oth, A.om[li][s], s == 0, s <= 1 ? (const T*)nullptr : prv, A.c1[li][s],
+                    g0, gs);
       cl.sync();
-      T* w = cur; cur = oth; oth = w;
+      T* w = prv; prv = cur; cur = oth; oth = w;
     }
     if (A.pre == 0) {
       for (long long i = g0; i < 3 * L.NP; i += gs) u[i] = T(0);
@@ -681,11 +690,12 @@ __global__ void __cluster_dims__(BOT_CTAS, 1, 1) __launch_bounds__(BOT_THREADS, 
     T* u = bv_u<T>(L);
     bot_prolong<T>(L, A.L[li + 1], bv_u<T>(A.L[li + 1]), u, g0, gs);
     cl.sync();
-    T *cur = u, *oth = bv_t<T>(L);
+    T *cur = u, *oth = bv_t<T>(L), *prv = bv_r<T>(L);
     for (int s = 0; s < A.post; s++) {
-      bot_jacobi<T>(L, st, cur, bv_f<T>(L), oth, A.omega[li], false, g0, gs);
+      bot_jacobi<T>(L, st, cur, bv_f<T>(L), oth, A.om[li][s], false, s == 0 ? (const T*)nullptr : prv, A.c1[li][s],
+                    g0, gs);
       cl.sync();
-      T* w = cur; cur = oth; oth = w;
+      T* w = prv; prv = cur; cur = oth; oth = w;
     }
     if (cur != u) {
       bot_copy<T>(L, cur, u, g0, gs);
@@ -711,21 +721,22 @@ rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* 
   const Level& l = h->L[level];
   if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
   if (l.nn > kRowSplitMaxNodes) {
-    k_coarse<T, 0><<<node_grid(l), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0)); rso::note_launch();
+    k_coarse<T, 0><<<node_grid(l), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0)); rso::note_launch();
   } else {
-    k_coarse_r<T, 0><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0)); rso::note_launch();
+    k_coarse_r<T, 0><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0)); rso::note_launch();
   }
   if (h->prof_on) prof_end(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64));
   return launch_check(h, "coarse_residual");
 }
 template <typename T>
-rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T* u_out, double omega) {
+rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T* u_out, double omega,
+                         const T* u_prev, double c1) {
   const Level& l = h->L[level];
   if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
   if (l.nn > kRowSplitMaxNodes) {
-    k_coarse<T, 2><<<node_grid(l), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega); rso::note_launch();
+    k_coarse<T, 2><<<node_grid(l), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1); rso::note_launch();
   } else {
-    k_coarse_r<T, 2><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega); rso::note_launch();
+    k_coarse_r<T, 2><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1); rso::note_launch();
   }
   if (h->prof_on) prof_end(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64));
   return launch_check(h, "coarse_jacobi");
@@ -792,7 +803,8 @@ rso_status coarsest_solve(rso_handle* h, const T* f, T* u) {
 // it down small enough.
 int bottom_level(const rso_handle* h) {
   const int nl = (int)h->L.size();
-  if (h->cfg.smoother != RSO_SMOOTH_JACOBI || nl < 3 || nl > BOT_MAX_LEVELS || h->nc == 0) return -1;
+  if (h->cfg.smoother == RSO_SMOOTH_GS || nl < 3 || nl > BOT_MAX_LEVELS || h->nc == 0) return -1;
+  if (h->cfg.pre > BOT_MAX_SWEEPS || h->cfg.post > BOT_MAX_SWEEPS) return -1;
   int lb = nl - 1;
   while (lb - 1 >= 1 && h->L[lb - 1].nn <= kBottomMaxNodes) lb--;
   return lb <= nl - 2 ? lb : -1;
@@ -804,7 +816,12 @@ rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post) {
   const int nl = (int)h->L.size();
   for (int li = 0; li < nl; li++) {
     A.L[li] = h->L[li];
-    A.omega[li] = (T)(h->cfg.omega * 2.0 / h->L[li].lam);
+    double om[BOT_MAX_SWEEPS], c1[BOT_MAX_SWEEPS];
+    smoother_steps(h, h->L[li].lam, BOT_MAX_SWEEPS, om, c1);
+    for (int k = 0; k < BOT_MAX_SWEEPS; k++) {
+      A.om[li][k] = (T)om[k];
+      A.c1[li][k] = (T)c1[k];
+    }
   }
   A.lb = lb; A.nl = nl; A.pre = pre; A.post = post;
   const int N = 3 * h->nc;
@@ -894,8 +911,10 @@ rso_status estimate_lambda(rso_handle* h) {
 
 template rso_status coarse_residual<double>(rso_handle*, int, const double*, const double*, double*);
 template rso_status coarse_residual<float>(rso_handle*, int, const float*, const float*, float*);
-template rso_status coarse_jacobi<double>(rso_handle*, int, const double*, const double*, double*, double);
-template rso_status coarse_jacobi<float>(rso_handle*, int, const float*, const float*, float*, double);
+template rso_status coarse_jacobi<double>(rso_handle*, int, const double*, const double*, double*, double,
+                                          const double*, double);
+template rso_status coarse_jacobi<float>(rso_handle*, int, const float*, const float*, float*, double, const float*,
+                                         double);
 template rso_status coarse_gs<double>(rso_handle*, int, double*, const double*, int, int);
 template rso_status coarse_gs<float>(rso_handle*, int, float*, const float*, int, int);
 template rso_status restrict_<double>(rso_handle*, int, const double*, double*);

@@ -48,7 +48,7 @@ static rso_status evaluate_design(rso_handle* h, const double* c, const rso_iter
   // operators (update_stencil)
   RSO_TRY(galerkin(h));
   RSO_TRY(coarsest_factor(h));
-  if (h->cfg.smoother == RSO_SMOOTH_JACOBI) RSO_TRY(estimate_lambda(h));
+  if (h->cfg.smoother != RSO_SMOOTH_GS) RSO_TRY(estimate_lambda(h));
   h->operators_ready = true;
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   const double t1 = now_ms();

@@ -170,11 +170,14 @@ constexpr int walsh_smem_bytes() {
 }
 
 // MODE 0: out = f - K u;  MODE 1: out = K u (support rows pass u);
-// MODE 2: out = u + omega D^-1 (f - K u)  (damped block Jacobi, D = 3x3 diagonal block)
+// MODE 2: out = u + c1 (u - uprev) + omega D^-1 (f - K u), D = 3x3 diagonal
+//         block: damped block Jacobi for c1 = 0, a Chebyshev step otherwise
+//         (uprev NULL reads as zero)
 template <typename T, int MODE, int TY>
 __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
     k_fine_w(const Level L, const T* __restrict__ u, const T* __restrict__ f, T* __restrict__ out,
-             const T* __restrict__ rp, T omega, double* __restrict__ dotp) {
+             const T* __restrict__ rp, T omega, double* __restrict__ dotp, const T* __restrict__ uprev,
+             T c1) {
   // Staged rows are 16-byte aligned windows of RX entries starting at the
   // tile's first padded x index rounded down to a multiple of 4 (ox = offset
   // of the tile inside the window), copied in 16-byte chunks.
@@ -255,7 +258,7 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
   // z-1; uc/uo u at the own node on planes z / z-1; own corner, f and class
   // of the plane being emitted; ra/rb rho^p of the 4 columns in the two
   // layers around it
-  T F[4][3], Gt[4][3], uc[3], uo[3], own[3], fo[3], ra[4], rb[4];
+  T F[4][3], Gt[4][3], uc[3], uo[3], own[3], fo[3], po[3], ra[4], rb[4];
   uint8_t clo = 0;
   double pq = 0;  // MODE 1 with dotp: this thread's share of u . (K u)
   face(ss + ((z0 - 1 + WNSLOT) % WNSLOT) * SLOT, F, uc);
@@ -265,7 +268,7 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
     ra[q] = rb[q] = T(0);
   }
 #pragma unroll
-  for (int c = 0; c < 3; c++) uo[c] = own[c] = fo[c] = T(0);
+  for (int c = 0; c < 3; c++) uo[c] = own[c] = fo[c] = po[c] = T(0);
 
   // node plane zo from the corners its 4 columns left in exchange buffer xb
   auto emit = [&](int zo, const T* xb) {
@@ -307,9 +310,9 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
         const T det = a * A + b * B + cc * C;
         const T id = omega / det;
         const T E = a * g - cc * cc, Fm = b * cc - a * e, I = a * d - b * b;
-        out[n] = uo[0] + id * (A * r0 + B * r1 + C * r2);
-        out[n + NP] = uo[1] + id * (B * r0 + E * r1 + Fm * r2);
-        out[n + 2 * NP] = uo[2] + id * (C * r0 + Fm * r1 + I * r2);
+        out[n] = uo[0] + c1 * (uo[0] - po[0]) + id * (A * r0 + B * r1 + C * r2);
+        out[n + NP] = uo[1] + c1 * (uo[1] - po[1]) + id * (B * r0 + E * r1 + Fm * r2);
+        out[n + 2 * NP] = uo[2] + c1 * (uo[2] - po[2]) + id * (C * r0 + Fm * r1 + I * r2);
       }
     }
   };
@@ -328,6 +331,10 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
       if (MODE != 1) {
 #pragma unroll
         for (int c = 0; c < 3; c++) fo[c] = f[n + c * NP];
+        if (MODE == 2 && uprev != nullptr) {
+#pragma unroll
+          for (int c = 0; c < 3; c++) po[c] = uprev[n + c * NP];
+        }
       }
     }
     const T* su = ss + ((z + 1 + WNSLOT) % WNSLOT) * SLOT;
@@ -539,7 +546,7 @@ static inline int pcls(int c32, int c64) { return sizeof(T) == 4 ? c32 : c64; }
 
 template <typename T, int MODE>
 static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, const T* rp, double omega, int cls,
-                              const char* what, double* dotp = nullptr) {
+                              const char* what, double* dotp = nullptr, const T* uprev = nullptr, double c1 = 0.0) {
   const Level& l = h->L[0];
   if (3 * l.NP >= (1LL << 31)) {
     h->err = "fine level too large for 32-bit in-plane offsets";
@@ -557,7 +564,7 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
     attr = true;
   }
   if (h->prof_on) prof_begin(h, cls, (double)l.nn);
-  k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega, dotp);
+  k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega, dotp, uprev, (T)c1);
   rso::note_launch();
   if (h->prof_on) prof_end(h, cls);
   return launch_check(h, what);
@@ -584,8 +591,10 @@ rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const doub
   return reduce_partials(h, h->fpart, (int)nb, dot_dev);
 }
 template <typename T>
-rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega) {
-  return launch_fine<T, 2>(h, u_in, f, u_out, rp, omega, pcls<T>(PC_FINE_JAC32, PC_FINE_JAC64), "fine_jacobi");
+rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega,
+                       const T* u_prev, double c1) {
+  return launch_fine<T, 2>(h, u_in, f, u_out, rp, omega, pcls<T>(PC_FINE_JAC32, PC_FINE_JAC64), "fine_jacobi", nullptr,
+                           u_prev, c1);
 }
 template <typename T>
 rso_status fine_jacobi0(rso_handle* h, const T* f, T* u_out, const T* rp, double omega) {
@@ -612,8 +621,10 @@ template rso_status fine_residual<double>(rso_handle*, const double*, const doub
 template rso_status fine_residual<float>(rso_handle*, const float*, const float*, float*, const float*);
 template rso_status fine_applyK<double>(rso_handle*, const double*, double*, const double*);
 template rso_status fine_applyK<float>(rso_handle*, const float*, float*, const float*);
-template rso_status fine_jacobi<double>(rso_handle*, const double*, const double*, double*, const double*, double);
-template rso_status fine_jacobi<float>(rso_handle*, const float*, const float*, float*, const float*, double);
+template rso_status fine_jacobi<double>(rso_handle*, const double*, const double*, double*, const double*, double,
+                                        const double*, double);
+template rso_status fine_jacobi<float>(rso_handle*, const float*, const float*, float*, const float*, double,
+                                       const float*, double);
 template rso_status fine_jacobi0<double>(rso_handle*, const double*, double*, const double*, double);
 template rso_status fine_jacobi0<float>(rso_handle*, const float*, float*, const float*, double);
 template rso_status fine_gs<double>(rso_handle*, double*, const double*, const double*, int, int);

@@ -182,12 +182,15 @@ template <typename T>
 rso_status fine_residual(rso_handle* h, const T* u, const T* f, T* r, const T* rp);
 template <typename T>
 rso_status fine_applyK(rso_handle* h, const T* u, T* f, const T* rp);
+constexpr int kMaxSweeps = 16;
+void smoother_steps(const rso_handle* h, double lam, int m, double* om, double* c1);
 int bottom_level(const rso_handle* h);
 template <typename T>
 rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post);
 rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const double* rp, double* dot_dev);
 template <typename T>
-rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega);
+rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega,
+                       const T* u_prev = nullptr, double c1 = 0.0);
 template <typename T>
 rso_status fine_jacobi0(rso_handle* h, const T* f, T* u_out, const T* rp, double omega);
 template <typename T>
@@ -199,7 +202,8 @@ rso_status penalise(rso_handle* h);
 template <typename T>
 rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* r);
 template <typename T>
-rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T* u_out, double omega);
+rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T* u_out, double omega,
+                         const T* u_prev = nullptr, double c1 = 0.0);
 template <typename T>
 rso_status coarse_gs(rso_handle* h, int level, T* u, const T* f, int colour, int reverse);
 template <typename T>

@@ -33,8 +33,32 @@ struct LV<float> {
   static const float* rp(rso_handle* h) { return h->rp32; }
 };
 
+// Step coefficients of the stationary smoothers, out = u + c1 (u - u_prev) +
+// om D^-1 (f - K u): damped Jacobi (om = omega * 2 / lambda_max, c1 = 0), or
+// Chebyshev iteration for D^-1 K on [lambda_max / 4, lambda_max] (three-term
+// recurrence: theta = (b + a) / 2, delta = (b - a) / 2, sigma = theta / delta,
+// rho_0 = 1 / sigma, rho_k = 1 / (2 sigma - rho_{k-1}); step 0 has om = 1 / theta,
+// step k has c1 = rho_k rho_{k-1} and om = 2 rho_k / delta).
+void smoother_steps(const rso_handle* h, double lam, int m, double* om, double* c1) {
+  if (h->cfg.smoother == RSO_SMOOTH_CHEBYSHEV) {
+    const double b = lam, a = lam / 4.0, theta = 0.5 * (b + a), delta = 0.5 * (b - a), sigma = theta / delta;
+    double rho_prev = 1.0 / sigma;
+    for (int k = 0; k < m; k++) {
+      if (k == 0) { om[0] = 1.0 / theta; c1[0] = 0.0; continue; }
+      const double rho = 1.0 / (2.0 * sigma - rho_prev);
+      c1[k] = rho * rho_prev;
+      om[k] = 2.0 * rho / delta;
+      rho_prev = rho;
+    }
+  } else {
+    for (int k = 0; k < m; k++) { om[k] = h->cfg.omega * 2.0 / lam; c1[k] = 0.0; }
+  }
+}
+
 // zero: the iterate is known to be zero before the first sweep (the first
-// damped-Jacobi sweep on the fine level then needs no operator application)
+// sweep on the fine level then needs no operator application).  Jacobi and
+// Chebyshev steps rotate three level vectors: u (current), t (next) and r
+// (previous iterate; free while the level is being smoothed).
 template <typename T>
 static rso_status smooth(rso_handle* h, int li, int sweeps, int reverse, bool zero = false) {
   Level& l = h->L[li];
@@ -45,12 +69,24 @@ static rso_status smooth(rso_handle* h, int li, int sweeps, int reverse, bool ze
         if (li == 0) RSO_TRY(fine_gs<T>(h, LV<T>::u(l), LV<T>::f(l), LV<T>::rp(h), c, reverse));
         else RSO_TRY(coarse_gs<T>(h, li, LV<T>::u(l), LV<T>::f(l), c, reverse));
       }
-  } else {
-    const double om = h->cfg.omega * 2.0 / l.lam;
-    for (int s = 0; s < sweeps; s++) {
-      if (li == 0 && zero && s == 0) RSO_TRY(fine_jacobi0<T>(h, LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om));
-      else if (li == 0) RSO_TRY(fine_jacobi<T>(h, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om));
-      else RSO_TRY(coarse_jacobi<T>(h, li, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), om));
+    return RSO_OK;
+  }
+  double om[kMaxSweeps], c1[kMaxSweeps];
+  if (sweeps > kMaxSweeps) { h->err = "too many smoothing sweeps"; return RSO_ERR_INVALID_ARG; }
+  smoother_steps(h, l.lam, sweeps, om, c1);
+  const bool cheb = h->cfg.smoother == RSO_SMOOTH_CHEBYSHEV;
+  for (int s = 0; s < sweeps; s++) {
+    // previous iterate: none before the second step; zero when the smoothing started from zero
+    const T* prev = (!cheb || s == 0 || (zero && s == 1)) ? nullptr : LV<T>::r(l);
+    if (li == 0 && zero && s == 0) RSO_TRY(fine_jacobi0<T>(h, LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om[0]));
+    else if (li == 0) RSO_TRY(fine_jacobi<T>(h, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om[s], prev, c1[s]));
+    else RSO_TRY(coarse_jacobi<T>(h, li, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), om[s], prev, c1[s]));
+    if (cheb) {  // previous <- current <- next
+      T* old_prev = LV<T>::r(l);
+      LV<T>::r(l) = LV<T>::u(l);
+      LV<T>::u(l) = LV<T>::t(l);
+      LV<T>::t(l) = old_prev;
+    } else {
       std::swap(LV<T>::u(l), LV<T>::t(l));
     }
   }

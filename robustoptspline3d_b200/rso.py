@@ -162,7 +162,7 @@ def load_library():
 _STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA", 4: "DIVERGED", 5: "NONFINITE", 6: "BUDGET_EXCEEDED",
            7: "UNSUPPORTED", 8: "STATE"}
 
-SMOOTH_GS, SMOOTH_JACOBI = 0, 1
+SMOOTH_GS, SMOOTH_JACOBI, SMOOTH_CHEBYSHEV = 0, 1, 2
 FP64, MIXED = 0, 1
 SOLVE_VCYCLE, SOLVE_PCG = 0, 1
 NO_SUPPORT_CF, NO_SUPPORT_FF, WITH_SUPPORT_CF, WITH_SUPPORT_FF = 0, 1, 2, 3

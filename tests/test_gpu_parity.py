@@ -166,8 +166,10 @@ def test_vcycle_reference_sequence(oracle, cuda):
     assert rel(ug.cpu().numpy(), u) < 1e-10
 
 
-@pytest.mark.parametrize("precision,smoother", [(0, 0), (0, 1), (1, 1), (1, 0)])
+@pytest.mark.parametrize("precision,smoother", [(0, 0), (0, 1), (1, 1), (1, 0), (0, 2), (1, 2)])
 def test_solve_cantilever(oracle, cuda, precision, smoother):
+    """smoother 0 Gauss-Seidel, 1 damped Jacobi, 2 Chebyshev (the solution does
+    not depend on the preconditioner; the oracle solves with its own)"""
     prob = P.cantilever(32, 16, 16)
     g, o = make(oracle, prob, n_levels=3, first_factor=2, smoother=smoother, precision=precision, nu=0.4, pre=2,
                 post=2)

@@ -189,9 +189,10 @@ rso_status rso_filter(rso_handle* h, double radius, const float* in_dev, float* 
 rso_status rso_density_filter(rso_handle* h, double radius, const float* in_dev, float* out_dev);
 rso_status rso_density_filter_adjoint(rso_handle* h, double radius, const float* in_dev, float* out_dev);
 /* The sensitivity filter of rso_filter, computed without any device memory
- * allocation; it has no counterpart in the reference.  rso_filter copies its
- * tap table into a stream-ordered allocation made on every call; this entry
- * point keeps the table in a fixed array of the library instead (52,728 bytes
+ * allocation; it has no counterpart in the reference.  rso_filter keeps its
+ * tap table in a device allocation of the handle, made on its first call and
+ * again whenever the radius grows; this entry point never allocates, not
+ * even on first use: it keeps the table in a fixed array of the library (52,728 bytes
  * per device), for callers that cannot allocate device memory inside their
  * loop: all free memory already handed to their own pool, a fixed device
  * footprint, or no room for the pool growth and synchronisation an allocation

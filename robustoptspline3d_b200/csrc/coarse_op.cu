@@ -16,6 +16,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cooperative_groups.h>
+#include <cublas_v2.h>
+#include <vector>
 
 namespace cg = cooperative_groups;
 
@@ -261,58 +263,82 @@ __global__ void k_prolong(const Level Fl, const Level C, const T* __restrict__ u
 // ---------------------------------------------------------------- Galerkin
 __device__ __forceinline__ double pw(int F, int o, int A) { return A ? (double)o / F : (double)(F - o) / F; }
 
-// first coarsening: one block per coarse element, 288 threads x 2 entries
-__global__ void __launch_bounds__(288) k_galerkin_first(const Level Fl, const Level C, int F,
-                                                        const double* __restrict__ rp, const double* __restrict__ T1,
-                                                        const double* __restrict__ K0g, double* __restrict__ KE) {
-  const long long E = blockIdx.x;
+// Support-free children enter the first-level coarse element matrices as a
+// plain GEMM, KE[E] = sum_pos w[E][pos] T1[pos] (w = rho^p of child pos, 0
+// for inactive or support-touching children), done by cuBLAS; the
+// support-touching children are added by k_galerkin_fix on the few coarse
+// elements that have them.
+__global__ void k_elem_fixmask(const Level Fl, uint8_t* __restrict__ efix) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= Fl.ne) return;
+  const int x = i % Fl.ex, y = (i / Fl.ex) % Fl.ey, z = i / ((long long)Fl.ex * Fl.ey);
+  unsigned m = 0;
+#pragma unroll
+  for (int a = 0; a < 8; a++)
+    if (Fl.vclass[Fl.nidx(x + (a & 1), y + ((a >> 1) & 1), z + (a >> 2))] & NC_SUPPORT) m |= 1u << a;
+  efix[Fl.eidx(x, y, z)] = (uint8_t)m;
+}
+
+__global__ void k_gal_weights(const Level Fl, const Level C, int F, const double* __restrict__ rp,
+                              const uint8_t* __restrict__ efix, double* __restrict__ w) {
+  const long long E = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (E >= C.ne) return;
+  const int X = E % C.ex, Y = (E / C.ex) % C.ey, Z = E / ((long long)C.ex * C.ey);
+  const int F3 = F * F * F;
+  for (int pos = 0; pos < F3; pos++) {
+    const int px = pos % F, py = (pos / F) % F, pz = pos / (F * F);
+    const int x = X * F + px, y = Y * F + py, z = Z * F + pz;
+    double r = 0.0;
+    if (x < Fl.ex && y < Fl.ey && z < Fl.ez) {
+      const long long e = Fl.eidx(x, y, z);
+      if (Fl.emask[e] && !efix[e]) r = rp[e];
+    }
+    w[E * F3 + pos] = r;
+  }
+}
+
+// support-touching children of listed coarse elements, added to KE
+__global__ void __launch_bounds__(288) k_galerkin_fix(const Level Fl, const Level C, int F,
+                                                      const double* __restrict__ rp, const double* __restrict__ K0g,
+                                                      const uint8_t* __restrict__ efix, const int* __restrict__ list,
+                                                      double* __restrict__ KE) {
+  const long long E = list[blockIdx.x];
   const int X = E % C.ex, Y = (E / C.ex) % C.ey, Z = E / ((long long)C.ex * C.ey);
   const int t = threadIdx.x;
   double acc[2] = {0, 0};
-  if (C.emask[C.eidx(X, Y, Z)]) {
-    for (int pz = 0; pz < F; pz++)
-      for (int py = 0; py < F; py++)
-        for (int px = 0; px < F; px++) {
-          const int x = X * F + px, y = Y * F + py, z = Z * F + pz;
-          if (x >= Fl.ex || y >= Fl.ey || z >= Fl.ez) continue;
-          const long long e = Fl.eidx(x, y, z);
-          if (!Fl.emask[e]) continue;
-          const double r = rp[e];
-          unsigned fixmask = 0;
-#pragma unroll
-          for (int a = 0; a < 8; a++)
-            if (Fl.vclass[Fl.nidx(x + (a & 1), y + ((a >> 1) & 1), z + (a >> 2))] & NC_SUPPORT) fixmask |= 1u << a;
-          const int pos = px + F * (py + F * pz);
-          if (!fixmask) {
-            acc[0] += r * T1[(long long)pos * 576 + t];
-            acc[1] += r * T1[(long long)pos * 576 + t + 288];
-          } else {
-            for (int h2 = 0; h2 < 2; h2++) {
-              const int ent = t + 288 * h2;
-              const int row = ent / 24, col = ent % 24;
-              const int A = row / 3, i = row % 3, B = col / 3, j = col % 3;
-              double s = 0;
-              for (int a = 0; a < 8; a++) {
-                const double wa = pw(F, px + (a & 1), A & 1) * pw(F, py + ((a >> 1) & 1), (A >> 1) & 1) *
-                                  pw(F, pz + (a >> 2), A >> 2);
-                if (wa == 0) continue;
-                for (int b = 0; b < 8; b++) {
-                  const double wb = pw(F, px + (b & 1), B & 1) * pw(F, py + ((b >> 1) & 1), (B >> 1) & 1) *
-                                    pw(F, pz + (b >> 2), B >> 2);
-                  if (wb == 0) continue;
-                  double kv;
-                  if ((fixmask >> a & 1u) || (fixmask >> b & 1u)) kv = (a == b && i == j) ? DIRICHLET_W : 0.0;
-                  else kv = r * K0g[(a * 3 + i) * 24 + b * 3 + j];
-                  s += wa * wb * kv;
-                }
-              }
-              acc[h2] += s;
+  for (int pz = 0; pz < F; pz++)
+    for (int py = 0; py < F; py++)
+      for (int px = 0; px < F; px++) {
+        const int x = X * F + px, y = Y * F + py, z = Z * F + pz;
+        if (x >= Fl.ex || y >= Fl.ey || z >= Fl.ez) continue;
+        const long long e = Fl.eidx(x, y, z);
+        const unsigned fixmask = efix[e];
+        if (!Fl.emask[e] || !fixmask) continue;
+        const double r = rp[e];
+        for (int h2 = 0; h2 < 2; h2++) {
+          const int ent = t + 288 * h2;
+          const int row = ent / 24, col = ent % 24;
+          const int A = row / 3, i = row % 3, B = col / 3, j = col % 3;
+          double s = 0;
+          for (int a = 0; a < 8; a++) {
+            const double wa = pw(F, px + (a & 1), A & 1) * pw(F, py + ((a >> 1) & 1), (A >> 1) & 1) *
+                              pw(F, pz + (a >> 2), A >> 2);
+            if (wa == 0) continue;
+            for (int b = 0; b < 8; b++) {
+              const double wb = pw(F, px + (b & 1), B & 1) * pw(F, py + ((b >> 1) & 1), (B >> 1) & 1) *
+                                pw(F, pz + (b >> 2), B >> 2);
+              if (wb == 0) continue;
+              double kv;
+              if ((fixmask >> a & 1u) || (fixmask >> b & 1u)) kv = (a == b && i == j) ? DIRICHLET_W : 0.0;
+              else kv = r * K0g[(a * 3 + i) * 24 + b * 3 + j];
+              s += wa * wb * kv;
             }
           }
+          acc[h2] += s;
         }
-  }
-  KE[E * 576 + t] = acc[0];
-  KE[E * 576 + t + 288] = acc[1];
+      }
+  KE[E * 576 + t] += acc[0];
+  KE[E * 576 + t + 288] += acc[1];
 }
 
 // dyadic recursion on element matrices
@@ -835,12 +861,71 @@ rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post) {
 template rso_status bottom_vcycle<double>(rso_handle*, int, int, int);
 template rso_status bottom_vcycle<float>(rso_handle*, int, int, int);
 
+// once per handle: the support mask of every fine element, the list of
+// coarse elements that have support-touching children, and the cuBLAS handle
+rso_status galerkin_setup(rso_handle* h) {
+  if (h->L.size() < 2) return RSO_OK;
+  const Level& f = h->L[0];
+  const Level& c = h->L[1];
+  const int F = c.factor, F3 = F * F * F;
+  RSO_CHECK_CUDA(h, cudaMalloc(&h->efix, f.NQ));
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(h->efix, 0, f.NQ, h->stream));
+  k_elem_fixmask<<<cdiv(f.ne, 256), 256, 0, h->stream>>>(f, h->efix); rso::note_launch();
+  RSO_TRY(launch_check(h, "element support mask"));
+  std::vector<uint8_t> ef(f.NQ);
+  RSO_CHECK_CUDA(h, cudaMemcpyAsync(ef.data(), h->efix, f.NQ, cudaMemcpyDeviceToHost, h->stream));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::vector<uint8_t> mark(c.ne, 0);
+  for (int z = 0; z < f.ez; z++)
+    for (int y = 0; y < f.ey; y++)
+      for (int x = 0; x < f.ex; x++)
+        if (ef[f.eidx(x, y, z)]) mark[x / F + (long long)c.ex * (y / F + (long long)c.ey * (z / F))] = 1;
+  std::vector<int> list;
+  for (long long E = 0; E < c.ne; E++)
+    if (mark[E]) list.push_back((int)E);
+  h->n_gfix = (int)list.size();
+  if (h->n_gfix) {
+    RSO_CHECK_CUDA(h, cudaMalloc(&h->gfix, sizeof(int) * list.size()));
+    RSO_CHECK_CUDA(h, cudaMemcpy(h->gfix, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice));
+  }
+  RSO_CHECK_CUDA(h, cudaMalloc(&h->gal_w, sizeof(double) * (size_t)c.ne * F3));
+  cublasHandle_t cb = nullptr;
+  if (cublasCreate(&cb) != CUBLAS_STATUS_SUCCESS) {
+    h->err = "cublasCreate failed";
+    return RSO_ERR_CUDA;
+  }
+  h->cublas = cb;
+  // a fixed workspace and the handle's stream, set once (rso_set_stream re-binds the stream)
+  const size_t ws = 32u << 20;
+  RSO_CHECK_CUDA(h, cudaMalloc(&h->cublas_ws, ws));
+  if (cublasSetWorkspace(cb, h->cublas_ws, ws) != CUBLAS_STATUS_SUCCESS ||
+      cublasSetStream(cb, h->stream) != CUBLAS_STATUS_SUCCESS) {
+    h->err = "cuBLAS workspace/stream set-up failed";
+    return RSO_ERR_CUDA;
+  }
+  return RSO_OK;
+}
+
 rso_status galerkin(rso_handle* h) {
   for (size_t li = 1; li < h->L.size(); li++) {
     Level& c = h->L[li];
     const Level& f = h->L[li - 1];
     if (li == 1)
-      k_galerkin_first<<<(unsigned)c.ne, 288, 0, h->stream>>>(f, c, c.factor, h->rp64, h->T1, h->K0_dev, c.KE);
+    {
+      const int F = c.factor, F3 = F * F * F;
+      k_gal_weights<<<cdiv(c.ne, 256), 256, 0, h->stream>>>(f, c, F, h->rp64, h->efix, h->gal_w); rso::note_launch();
+      RSO_TRY(launch_check(h, "galerkin weights"));
+      cublasHandle_t cb = (cublasHandle_t)h->cublas;
+      const double one = 1.0, zero = 0.0;
+      if (cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, 576, (int)c.ne, F3, &one, h->T1, 576, h->gal_w, F3, &zero, c.KE,
+                      576) != CUBLAS_STATUS_SUCCESS) {
+        h->err = "cublasDgemm of the first-level Galerkin product failed";
+        return RSO_ERR_CUDA;
+      }
+      if (h->n_gfix > 0) {
+        k_galerkin_fix<<<h->n_gfix, 288, 0, h->stream>>>(f, c, F, h->rp64, h->K0_dev, h->efix, h->gfix, c.KE);
+      }
+    }
     else
       k_galerkin_next<<<(unsigned)c.ne, 288, 0, h->stream>>>(f, c, f.KE, c.KE);
     rso::note_launch();
@@ -874,34 +959,35 @@ rso_status coarsest_factor(rso_handle* h) {
 }
 
 // lambda_max(D^-1 K) per level: power iteration on the Jacobi operator
-__global__ void k_seed_vec(double* v, long long n, uint64_t seed) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < n) v[i] = rso_urand(seed, (uint64_t)i);
-}
-__global__ void k_sub_scale(const double* u, const double* v, double* w, long long n, const double* nrm) {
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < n) w[i] = (u[i] - v[i]);
+// random start vector, zero at inactive nodes, halo and (fine level) support nodes
+__global__ void k_seed_vec(const Level L, float* v, uint64_t seed, int zero_support) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= L.NP) return;
+  const uint8_t c = L.vclass[i];
+  const bool z = !(c & NC_ACTIVE) || (zero_support && (c & NC_SUPPORT));
+#pragma unroll
+  for (int k = 0; k < 3; k++) v[i + k * L.NP] = z ? 0.f : (float)rso_urand(seed, (uint64_t)(i + k * L.NP));
 }
 
+// lambda_max(D^-1 K) of every smoothed level: 12 power iterations in FP32
+// (the estimate only sets the smoother's step sizes and gets a 5 % margin)
 rso_status estimate_lambda(rso_handle* h) {
   const int iters = 12;
   for (size_t li = 0; li + 1 < h->L.size() || (li == 0 && h->L.size() == 1); li++) {
     Level& l = h->L[li];
     const long long n3 = 3 * l.NP;
-    k_seed_vec<<<cdiv(n3, 256), 256, 0, h->stream>>>(l.u64, n3, 777 + li); rso::note_launch();
-    if (li == 0) RSO_TRY(zero_support(h, l.u64));
-    RSO_CHECK_CUDA(h, cudaMemsetAsync(l.f64, 0, sizeof(double) * n3, h->stream));
+    k_seed_vec<<<cdiv(l.NP, 256), 256, 0, h->stream>>>(l, l.u32, 777 + li, li == 0); rso::note_launch();
+    RSO_CHECK_CUDA(h, cudaMemsetAsync(l.f32, 0, sizeof(float) * n3, h->stream));
     double lam = 1.0;
     for (int it = 0; it < iters; it++) {
-      // t = u - D^-1 K u  ->  r = D^-1 K u
-      if (li == 0) RSO_TRY(fine_jacobi<double>(h, l.u64, l.f64, l.t64, h->rp64, 1.0));
-      else RSO_TRY(coarse_jacobi<double>(h, (int)li, l.u64, l.f64, l.t64, 1.0));
-      k_sub_scale<<<cdiv(n3, 256), 256, 0, h->stream>>>(l.u64, l.t64, l.r64, n3, nullptr); rso::note_launch();
-      double nu = 0, nw = 0;
-      RSO_TRY(dot_host(h, l.u64, l.u64, n3, &nu));
-      RSO_TRY(dot_host(h, l.r64, l.r64, n3, &nw));
-      lam = std::sqrt(nw / nu);
-      RSO_CHECK_CUDA(h, cudaMemcpyAsync(l.u64, l.r64, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
+      // t = u - D^-1 K u, r = D^-1 K u
+      if (li == 0) RSO_TRY(fine_jacobi<float>(h, l.u32, l.f32, l.t32, h->rp32, 1.0));
+      else RSO_TRY(coarse_jacobi<float>(h, (int)li, l.u32, l.f32, l.t32, 1.0));
+      double uu = 0, rr = 0;
+      RSO_TRY(pow_step(h, n3, l.u32, l.t32, l.r32, &uu, &rr));
+      if (!(uu > 0)) break;
+      lam = std::sqrt(rr / uu);
+      std::swap(l.u32, l.r32);
     }
     l.lam = 1.05 * lam;
     if (h->L.size() == 1) break;

@@ -122,9 +122,21 @@ rso_status filter(rso_handle* h, double R, const float* in_pad, float* out_pad, 
         const double r = std::sqrt(r2 / R2), rr = r * r;
         off.push_back({dx, dy, dz, 1 - 6 * rr + 8 * rr * r - 3 * rr * rr});
       }
-  FOff* d_off = nullptr;
-  RSO_CHECK_CUDA(h, cudaMallocAsync(&d_off, sizeof(FOff) * off.size(), h->stream));
-  RSO_CHECK_CUDA(h, cudaMemcpyAsync(d_off, off.data(), sizeof(FOff) * off.size(), cudaMemcpyHostToDevice, h->stream));
+  // the tap table is kept on the handle and rebuilt only when the radius changes
+  if (!h->filt_taps || h->filt_radius != R) {
+    if ((long long)off.size() > h->filt_cap) {
+      if (h->filt_taps) RSO_CHECK_CUDA(h, cudaFree(h->filt_taps));
+      h->filt_taps = nullptr;
+      RSO_CHECK_CUDA(h, cudaMalloc(&h->filt_taps, sizeof(FOff) * off.size()));
+      h->filt_cap = (long long)off.size();
+    }
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->filt_taps, off.data(), sizeof(FOff) * off.size(), cudaMemcpyHostToDevice,
+                                      h->stream));
+    // the host table is a local vector: finish the copy before it goes away
+    RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->filt_radius = R;
+  }
+  const FOff* d_off = static_cast<const FOff*>(h->filt_taps);
   if (!adjoint) {
     k_filter<<<cdiv(l.ne, 256), 256, 0, h->stream>>>(l, d_off, (int)off.size(), in_pad, out_pad, 0, nullptr); rso::note_launch();
   } else {
@@ -132,9 +144,7 @@ rso_status filter(rso_handle* h, double R, const float* in_pad, float* out_pad, 
     k_filter<<<cdiv(l.ne, 256), 256, 0, h->stream>>>(l, d_off, (int)off.size(), in_pad, W, 1, nullptr); rso::note_launch();
     k_filter<<<cdiv(l.ne, 256), 256, 0, h->stream>>>(l, d_off, (int)off.size(), in_pad, out_pad, 2, W); rso::note_launch();
   }
-  RSO_TRY(launch_check(h, "filter"));
-  RSO_CHECK_CUDA(h, cudaFreeAsync(d_off, h->stream));
-  return RSO_OK;
+  return launch_check(h, "filter");
 }
 
 // ---------------------------------------------------------------- volume

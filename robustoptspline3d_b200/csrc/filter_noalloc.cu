@@ -1,14 +1,15 @@
 // Sensitivity filter that allocates no device memory.
 //
 // rso_filter builds its table of filter taps (offset + weight) on the host
-// and copies it into a stream-ordered allocation made for each call.  Some
+// and copies it into a device allocation owned by the handle, made on the
+// first call and again whenever the radius grows.  Some
 // callers cannot allow a device allocation inside their loop: an application
 // that has handed all free device memory to its own pool up front (so any
 // allocation outside that pool fails), one that must keep a fixed, known
 // device footprint, or one that cannot accept the pool growth or the
 // synchronisation an allocation may cause.  rso_filter_noalloc gives them
 // the same filter with the tap table held in a fixed device array of this
-// library, so the call itself makes no allocation.
+// library, so no call makes an allocation, the first one included.
 //
 // The table holds the full cube of offsets |dx|,|dy|,|dz| <= reach, with a
 // flag for the offsets inside the filter ball; reach = int(radius + 0.5) is

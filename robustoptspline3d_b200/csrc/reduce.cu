@@ -107,6 +107,34 @@ rso_status reduce_partials(rso_handle* h, const double* part, int n, double* dev
   return launch_check(h, "reduce_partials");
 }
 
+// power-iteration step in FP32: r = u - t (t = u - D^-1 K u), with the sums
+// u.u and r.r accumulated in FP64 and returned to the host
+__global__ void __launch_bounds__(RED_THREADS) k_pow_step(long long n, const float* __restrict__ u,
+                                                          const float* __restrict__ t, float* __restrict__ r,
+                                                          double* __restrict__ part) {
+  double su = 0, sr = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float ui = u[i], ri = ui - t[i];
+    r[i] = ri;
+    su += (double)ui * ui;
+    sr += (double)ri * ri;
+  }
+  su = block_sum(su);
+  sr = block_sum(sr);
+  if (threadIdx.x == 0) { part[blockIdx.x] = su; part[RED_BLOCKS + blockIdx.x] = sr; }
+}
+
+rso_status pow_step(rso_handle* h, long long n, const float* u, const float* t, float* r, double* uu, double* rr) {
+  k_pow_step<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n, u, t, r, h->red); rso::note_launch();
+  k_final<<<1, RED_THREADS, 0, h->stream>>>(h->red, RED_BLOCKS, h->scal + 6); rso::note_launch();
+  k_final<<<1, RED_THREADS, 0, h->stream>>>(h->red + RED_BLOCKS, RED_BLOCKS, h->scal + 7); rso::note_launch();
+  RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->h_scal + 6, h->scal + 6, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  *uu = h->h_scal[6];
+  *rr = h->h_scal[7];
+  return RSO_OK;
+}
+
 rso_status dot_df(rso_handle* h, const double* a, const float* b, long long n, double* dev_out) {
   k_dot_df_partial<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(a, b, n, h->red); rso::note_launch();
   k_final<<<1, RED_THREADS, 0, h->stream>>>(h->red, RED_BLOCKS, dev_out); rso::note_launch();

@@ -89,6 +89,15 @@ struct rso_handle {
   double* load_normals = nullptr;     // 3 per load node
   // Galerkin tables
   double* T1 = nullptr;               // F^3 x 576 table for the first coarsening
+  void* cublas = nullptr;             // cublasHandle_t of the first-level Galerkin product
+  double* gal_w = nullptr;            // [coarse element][F^3] rho^p of the support-free children
+  uint8_t* efix = nullptr;            // per padded fine element: bit a set if local node a is a support node
+  int* gfix = nullptr;                // coarse elements with a child that touches a support node
+  int n_gfix = 0;
+  void* cublas_ws = nullptr;          // fixed cuBLAS workspace (no allocation inside calls)
+  void* filt_taps = nullptr;          // sensitivity-filter tap table of the last radius used
+  long long filt_cap = 0;
+  double filt_radius = -1.0;
   // coarsest dense solve
   int nc = 0;                         // active coarsest nodes
   int* c_nodes = nullptr;             // padded node ids of active coarsest nodes
@@ -162,6 +171,7 @@ rso_status dot_host(rso_handle* h, const double* a, const double* b, long long n
 rso_status cg_resid_rr(rso_handle* h, long long n, const double* alpha, const double* q, double* r, float* r32,
                        double* rr_dev);
 rso_status reduce_partials(rso_handle* h, const double* part, int n, double* dev_out);
+rso_status pow_step(rso_handle* h, long long n, const float* u, const float* t, float* r, double* uu, double* rr);
 rso_status dot_df(rso_handle* h, const double* a, const float* b, long long n, double* dev_out);
 rso_status sum_float(rso_handle* h, const float* a, long long n, double* dev_out);
 
@@ -212,6 +222,7 @@ template <typename T>
 rso_status prolong(rso_handle* h, int coarse_level, const T* uc, T* uf);
 template <typename T>
 rso_status coarsest_solve(rso_handle* h, const T* f, T* u);
+rso_status galerkin_setup(rso_handle* h);
 rso_status galerkin(rso_handle* h);
 rso_status coarsest_factor(rso_handle* h);
 rso_status estimate_lambda(rso_handle* h);

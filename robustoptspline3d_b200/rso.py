@@ -560,16 +560,26 @@ class HierarchyGrid:
                   "rso_design_iteration")
         return {f[0]: getattr(info, f[0]) for f in _IterInfo._fields_}
 
-    def design_iteration_host(self, mma, coeff_in, params=None):
+    def design_iteration_host(self, mma, coeff_in, params=None, coeff_out=None, density=True):
+        """One design iteration from host coefficients.  coeff_in / coeff_out may be
+        numpy arrays or (pinned) CPU torch tensors of float64; density=False skips
+        the download of the density field (returned as None)."""
         p = (params or IterParams())._c()
         info = _IterInfo()
-        cin = np.ascontiguousarray(coeff_in, np.float64)
-        cout = np.zeros(self.n_coeff)
-        rho = np.zeros(self.ne, np.float32)
-        self._chk(self.lib.rso_design_iteration_host(self.h, mma.s, ctypes.byref(p), _np_ptr(cin, _pd),
-                                                     _np_ptr(cout, _pd), rho.ctypes.data_as(
-                                                         ctypes.POINTER(ctypes.c_float)), ctypes.byref(info)),
-                  "rso_design_iteration_host")
+
+        def host_ptr(a):
+            if hasattr(a, "data_ptr"):
+                if a.is_cuda or a.dtype.itemsize != 8 or not a.is_contiguous():
+                    raise RSOError("expected a contiguous float64 CPU tensor")
+                return ctypes.cast(ctypes.c_void_p(a.data_ptr()), _pd)
+            return _np_ptr(a, _pd)
+
+        cin = coeff_in if hasattr(coeff_in, "data_ptr") else np.ascontiguousarray(coeff_in, np.float64)
+        cout = coeff_out if coeff_out is not None else np.zeros(self.n_coeff)
+        rho = np.zeros(self.ne, np.float32) if density else None
+        rptr = rho.ctypes.data_as(ctypes.POINTER(ctypes.c_float)) if density else None
+        self._chk(self.lib.rso_design_iteration_host(self.h, mma.s, ctypes.byref(p), host_ptr(cin), host_ptr(cout),
+                                                     rptr, ctypes.byref(info)), "rso_design_iteration_host")
         return cout, rho, {f[0]: getattr(info, f[0]) for f in _IterInfo._fields_}
 
     def design_gradient(self, coeff, params=None):

@@ -44,8 +44,8 @@ typedef enum {
 enum { RSO_SMOOTH_GS = 0, RSO_SMOOTH_JACOBI = 1, RSO_SMOOTH_CHEBYSHEV = 2 };
 /* RSO_SMOOTH_CHEBYSHEV (no counterpart in the reference, which smooths with
  * damped Jacobi or coloured Gauss-Seidel): `pre`/`post` Chebyshev steps for
- * D^-1 K on [lambda_max/4, lambda_max], D the 3x3 diagonal blocks; omega is
- * not used.  A polynomial in D^-1 K, so the V-cycle stays symmetric. */
+ * D^-1 K on [cheb_lower * lambda_max, lambda_max] (cheb_lower defaults to
+ * 0.25), D the 3x3 diagonal blocks; omega is not used.  A polynomial in D^-1 K, so the V-cycle stays symmetric. */
 /* V-cycle arithmetic */
 enum { RSO_FP64 = 0, RSO_MIXED = 1 };
 /* solve methods */
@@ -75,6 +75,7 @@ typedef struct {
   int pre, post;           /* smoothing sweeps */
   int precision;           /* RSO_FP64 or RSO_MIXED (FP32 V-cycle inside FP64 outer iteration) */
   int mode;                /* RSO_WITH_SUPPORT_* / RSO_NO_SUPPORT_* */
+  double cheb_lower;       /* Chebyshev smoother: lower end of the damped interval, as a fraction of lambda_max */
 } rso_config;
 
 typedef struct {

@@ -98,6 +98,7 @@ extern "C" void rso_default_config(rso_config* c) {
   c->post = 2;
   c->precision = RSO_MIXED;
   c->mode = RSO_WITH_SUPPORT_FREE_FORCE;
+  c->cheb_lower = 0.25;
 }
 
 static void free_handle(rso_handle* h) {
@@ -257,6 +258,10 @@ extern "C" rso_status rso_create(const rso_config* cfg, int ex, int ey, int ez, 
     return RSO_ERR_INVALID_ARG;
   }
   if (h->cfg.smoother < RSO_SMOOTH_GS || h->cfg.smoother > RSO_SMOOTH_CHEBYSHEV) { delete h; return RSO_ERR_INVALID_ARG; }
+  if (h->cfg.smoother == RSO_SMOOTH_CHEBYSHEV && !(h->cfg.cheb_lower > 0 && h->cfg.cheb_lower < 1)) {
+    delete h;
+    return RSO_ERR_INVALID_ARG;
+  }
   if (h->cfg.mode == RSO_NO_SUPPORT_CONSTRAIN_FORCE_DIRECTION || h->cfg.mode == RSO_NO_SUPPORT_FREE_FORCE) {
     // the dense coarsest solve needs supports (a support-free operator is singular)
     g_create_err = "support-free modes are not supported";

@@ -35,13 +35,15 @@ struct LV<float> {
 
 // Step coefficients of the stationary smoothers, out = u + c1 (u - u_prev) +
 // om D^-1 (f - K u): damped Jacobi (om = omega * 2 / lambda_max, c1 = 0), or
-// Chebyshev iteration for D^-1 K on [lambda_max / 4, lambda_max] (three-term
-// recurrence: theta = (b + a) / 2, delta = (b - a) / 2, sigma = theta / delta,
-// rho_0 = 1 / sigma, rho_k = 1 / (2 sigma - rho_{k-1}); step 0 has om = 1 / theta,
-// step k has c1 = rho_k rho_{k-1} and om = 2 rho_k / delta).
+// Chebyshev iteration for D^-1 K on [a, b] = [cheb_lower lambda_max,
+// lambda_max] by the three-term recurrence: theta = (b + a) / 2,
+// delta = (b - a) / 2, sigma = theta / delta, rho_0 = 1 / sigma,
+// rho_k = 1 / (2 sigma - rho_{k-1}); step 0 has om = 1 / theta, step k has
+// c1 = rho_k rho_{k-1} and om = 2 rho_k / delta.
 void smoother_steps(const rso_handle* h, double lam, int m, double* om, double* c1) {
   if (h->cfg.smoother == RSO_SMOOTH_CHEBYSHEV) {
-    const double b = lam, a = lam / 4.0, theta = 0.5 * (b + a), delta = 0.5 * (b - a), sigma = theta / delta;
+    const double b = lam, a = lam * h->cfg.cheb_lower, theta = 0.5 * (b + a), delta = 0.5 * (b - a),
+                 sigma = theta / delta;
     double rho_prev = 1.0 / sigma;
     for (int k = 0; k < m; k++) {
       if (k == 0) { om[0] = 1.0 / theta; c1[0] = 0.0; continue; }

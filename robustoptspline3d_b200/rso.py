@@ -40,7 +40,8 @@ class _Config(ctypes.Structure):
     _fields_ = [("youngs_modulus", ctypes.c_double), ("poisson_ratio", ctypes.c_double),
                 ("penal", ctypes.c_double), ("rho_min", ctypes.c_double), ("n_levels", ctypes.c_int),
                 ("first_factor", ctypes.c_int), ("smoother", ctypes.c_int), ("omega", ctypes.c_double),
-                ("pre", ctypes.c_int), ("post", ctypes.c_int), ("precision", ctypes.c_int), ("mode", ctypes.c_int)]
+                ("pre", ctypes.c_int), ("post", ctypes.c_int), ("precision", ctypes.c_int), ("mode", ctypes.c_int),
+                ("cheb_lower", ctypes.c_double)]
 
 
 class _SolveInfo(ctypes.Structure):
@@ -207,6 +208,7 @@ class Config:
     post: int = 2
     precision: int = MIXED
     mode: int = WITH_SUPPORT_FF
+    cheb_lower: float = 0.25
 
     def _c(self):
         c = _Config()

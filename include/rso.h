@@ -169,6 +169,16 @@ rso_status rso_vcycle(rso_handle* h, double* u_dev, const double* f_dev, int pre
  * RSO_SOLVE_PCG runs FP64 CG preconditioned by one V-cycle (FP32 in mixed mode). */
 rso_status rso_solve(rso_handle* h, const double* f_dev, double* u_dev, double tol, int max_iter,
                      int method, rso_solve_info* info);
+/* k systems K u_i = f_i on the same operator solved together (load cases of
+ * one design; no counterpart in the reference, which solves them one after
+ * the other): one PCG recurrence per system with per-system scalars, every
+ * V-cycle kernel launch carrying all k systems.  F_dev, U_dev: k * 3*Nn
+ * doubles, system-major (U holds the initial guesses and returns the
+ * solutions); infos: k entries or NULL.  1 <= k <= 64; damped Jacobi or
+ * Chebyshev smoother (Gauss-Seidel returns RSO_ERR_UNSUPPORTED).  Device
+ * buffers for k systems are allocated on the first call with that k and kept. */
+rso_status rso_solve_batch(rso_handle* h, int k, const double* F_dev, double* U_dev, double tol, int max_iter,
+                           rso_solve_info* infos);
 /* Grid::compliance (grid/Grid.cpp:4118-4121): c = f . u */
 rso_status rso_dot(rso_handle* h, const double* a_dev, const double* b_dev, double* out);
 

@@ -1,0 +1,337 @@
+// Batched solves: k systems K u_i = f_i on one operator (the load cases of a
+// worst-case or multi-load study).  Every level vector becomes a slab of k
+// consecutive vectors and the levels carry nb = k, so each V-cycle kernel
+// launch works on all k systems (the fine operator, transfers and row-split
+// stencil kernels over a system index in the grid, the large-level stencil
+// kernel reading each stencil entry once for up to four systems, the cluster
+// kernel of the small levels over system x node pairs).  CG runs one
+// recurrence per system with per-system scalars; a converged system keeps
+// alpha = beta = 0 while the others continue.
+#include "rso_internal.cuh"
+#include <chrono>
+#include <cmath>
+#include <utility>
+
+namespace rso {
+
+constexpr int BR_BLOCKS = 296, BR_THREADS = 512, KS = 8;  // KS doubles of scalars per system
+
+__device__ __forceinline__ double b_block_sum(double v) {
+  __shared__ double ws[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  v = (threadIdx.x < blockDim.x / 32) ? ws[lane] : 0.0;
+  if (w == 0)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  return v;
+}
+
+// partial sums of a_b . b_b for every system b = blockIdx.y
+template <typename B>
+__global__ void __launch_bounds__(BR_THREADS) k_bdot(long long n, const double* __restrict__ a,
+                                                     const B* __restrict__ b, double* __restrict__ part) {
+  const long long o = (long long)blockIdx.y * n;
+  double s = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s += a[o + i] * (double)b[o + i];
+  s = b_block_sum(s);
+  if (threadIdx.x == 0) part[blockIdx.y * BR_BLOCKS + blockIdx.x] = s;
+}
+
+// r -= alpha_b q, FP32 copy of r, partial sums of r.r per system
+__global__ void __launch_bounds__(BR_THREADS) k_bresid(long long n, const double* __restrict__ s,
+                                                       const double* __restrict__ q, double* __restrict__ r,
+                                                       float* __restrict__ r32, double* __restrict__ part) {
+  const long long o = (long long)blockIdx.y * n;
+  const double a = s[blockIdx.y * KS + 2];
+  double acc = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double ri = r[o + i] - a * q[o + i];
+    r[o + i] = ri;
+    if (r32) r32[o + i] = (float)ri;
+    acc += ri * ri;
+  }
+  acc = b_block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.y * BR_BLOCKS + blockIdx.x] = acc;
+}
+
+__global__ void k_bsum(const double* __restrict__ part, double* __restrict__ s, int slot) {
+  double v = 0;
+  for (int i = threadIdx.x; i < BR_BLOCKS; i += blockDim.x) v += part[blockIdx.x * BR_BLOCKS + i];
+  v = b_block_sum(v);
+  if (threadIdx.x == 0) s[blockIdx.x * KS + slot] = v;
+}
+
+// s: 0 rz, 1 pq, 2 alpha, 3 rz_new, 4 beta, 5 rr, 6 ff
+__global__ void k_balpha(int k, double* s, const int* __restrict__ done) {
+  const int b = threadIdx.x;
+  if (b >= k) return;
+  const double pq = s[b * KS + 1];
+  s[b * KS + 2] = (done[b] || pq == 0.0) ? 0.0 : s[b * KS + 0] / pq;
+}
+__global__ void k_bbeta(int k, double* s, const int* __restrict__ done) {
+  const int b = threadIdx.x;
+  if (b >= k) return;
+  const double rz = s[b * KS + 0];
+  s[b * KS + 4] = (done[b] || rz == 0.0) ? 0.0 : s[b * KS + 3] / rz;
+  s[b * KS + 0] = s[b * KS + 3];
+}
+
+// x += alpha_b p; p = z + beta_b p
+template <typename Z>
+__global__ void k_bstep_dir(long long n, long long total, const double* __restrict__ s, const Z* __restrict__ z,
+                            double* __restrict__ p, double* __restrict__ x) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const long long b = i / n;
+  const double pi = p[i];
+  x[i] += s[b * KS + 2] * pi;
+  p[i] = (double)z[i] + s[b * KS + 4] * pi;
+}
+__global__ void k_bstep(long long n, long long total, const double* __restrict__ s, const double* __restrict__ p,
+                        double* __restrict__ x) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  x[i] += s[(i / n) * KS + 2] * p[i];
+}
+__global__ void k_bd2f(long long total, const double* __restrict__ a, float* __restrict__ b) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < total) b[i] = (float)a[i];
+}
+__global__ void k_bf2d(long long total, const float* __restrict__ a, double* __restrict__ b) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < total) b[i] = (double)a[i];
+}
+
+static void batch_free(rso_handle* h) {
+  auto& B = h->batch;
+  for (auto* v : {&B.u32, &B.f32, &B.r32, &B.t32})
+    for (float* p : *v) cudaFree(p);
+  for (auto* v : {&B.u64, &B.f64, &B.r64, &B.t64})
+    for (double* p : *v) cudaFree(p);
+  B.u32.clear(); B.f32.clear(); B.r32.clear(); B.t32.clear();
+  B.u64.clear(); B.f64.clear(); B.r64.clear(); B.t64.clear();
+  for (double* p : {B.x, B.r, B.p, B.q, B.z, B.cf, B.red, B.fpart, B.xfer, B.scal}) cudaFree(p);
+  if (B.h_scal) cudaFreeHost(B.h_scal);
+  cudaFree(B.done);
+  B = rso_handle::Batch();  // c_fb aliases B.cf, freed above
+  h->c_fb = nullptr;
+}
+
+void batch_release(rso_handle* h) { batch_free(h); }
+
+static rso_status batch_alloc(rso_handle* h, int k) {
+  auto& B = h->batch;
+  if (B.cap >= k) return RSO_OK;
+  batch_free(h);
+  const bool mixed = h->cfg.precision == RSO_MIXED;
+  const size_t nl = h->L.size();
+#define BALLOC(ptr, bytes)                                                   \
+  do {                                                                       \
+    if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess) {                \
+      cudaGetLastError();                                                    \
+      batch_free(h);                                                         \
+      h->err = "out of device memory for the batch of systems";              \
+      return RSO_ERR_OOM;                                                    \
+    }                                                                        \
+  } while (0)
+  for (size_t li = 0; li < nl; li++) {
+    const size_t n = (size_t)k * 3 * h->L[li].NP;
+    if (mixed) {
+      float *a, *b, *c, *d;
+      BALLOC(a, 4 * n); B.u32.push_back(a);
+      BALLOC(b, 4 * n); B.f32.push_back(b);
+      BALLOC(c, 4 * n); B.r32.push_back(c);
+      BALLOC(d, 4 * n); B.t32.push_back(d);
+    } else {
+      double *a, *b, *c, *d;
+      BALLOC(a, 8 * n); B.u64.push_back(a);
+      BALLOC(b, 8 * n); B.f64.push_back(b);
+      BALLOC(c, 8 * n); B.r64.push_back(c);
+      BALLOC(d, 8 * n); B.t64.push_back(d);
+    }
+  }
+  const size_t n0 = (size_t)k * 3 * h->L[0].NP;
+  BALLOC(B.x, 8 * n0); BALLOC(B.r, 8 * n0); BALLOC(B.p, 8 * n0); BALLOC(B.q, 8 * n0);
+  if (!mixed) BALLOC(B.z, 8 * n0);
+  BALLOC(B.cf, sizeof(double) * std::max(1, 3 * h->nc) * k);
+  BALLOC(B.red, sizeof(double) * BR_BLOCKS * k);
+  BALLOC(B.fpart, sizeof(double) * h->fpart_n * k);
+  BALLOC(B.xfer, sizeof(double) * h->xfer_n * k);
+  BALLOC(B.scal, sizeof(double) * KS * k);
+  BALLOC(B.done, sizeof(int) * k);
+#undef BALLOC
+  if (cudaMallocHost((void**)&B.h_scal, sizeof(double) * KS * k) != cudaSuccess) {
+    cudaGetLastError();
+    batch_free(h);
+    h->err = "out of pinned host memory for the batch";
+    return RSO_ERR_OOM;
+  }
+  h->c_fb = B.cf;
+  B.cap = k;
+  return RSO_OK;
+}
+
+// swaps the batch slabs into the levels (nb = k) for the lifetime of the guard
+struct BatchScope {
+  rso_handle* h;
+  std::vector<Level> saved;
+  double* xfer;
+  size_t xfer_n;
+  double* fpart;
+  long long fpart_n;
+  BatchScope(rso_handle* hh, int k) : h(hh), saved(hh->L), xfer(hh->xfer), xfer_n(hh->xfer_n), fpart(hh->fpart),
+                                      fpart_n(hh->fpart_n) {
+    auto& B = h->batch;
+    const bool mixed = h->cfg.precision == RSO_MIXED;
+    for (size_t li = 0; li < h->L.size(); li++) {
+      Level& l = h->L[li];
+      l.nb = k;
+      if (mixed) { l.u32 = B.u32[li]; l.f32 = B.f32[li]; l.r32 = B.r32[li]; l.t32 = B.t32[li]; }
+      else { l.u64 = B.u64[li]; l.f64 = B.f64[li]; l.r64 = B.r64[li]; l.t64 = B.t64[li]; }
+    }
+    h->xfer = B.xfer;
+    h->xfer_n = xfer_n * k;
+    h->fpart = B.fpart;
+    h->fpart_n = fpart_n * k;
+  }
+  ~BatchScope() {
+    h->L = saved;
+    h->xfer = xfer;
+    h->xfer_n = xfer_n;
+    h->fpart = fpart;
+    h->fpart_n = fpart_n;
+  }
+};
+
+static double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, double tol, int max_iter,
+                           rso_solve_info* infos) {
+  if (h->cfg.smoother == RSO_SMOOTH_GS) {
+    h->err = "batched solves need the damped Jacobi or Chebyshev smoother";
+    return RSO_ERR_UNSUPPORTED;
+  }
+  RSO_TRY(batch_alloc(h, k));
+  auto& B = h->batch;
+  const double t0 = now_ms();
+  const long long n3 = 3 * h->L[0].NP, tot = (long long)k * n3, nn3 = 3 * h->L[0].nn;
+  // dense -> padded slabs (x holds the initial guesses, p the right-hand sides for now)
+  for (int b = 0; b < k; b++) {
+    RSO_TRY(pad_nodes(h, 0, U + b * nn3, B.x + b * n3));
+    RSO_TRY(pad_nodes(h, 0, F + b * nn3, B.q + b * n3));
+    RSO_TRY(zero_support(h, B.x + b * n3));
+    RSO_TRY(zero_support(h, B.q + b * n3));
+  }
+  const bool mixed = h->cfg.precision == RSO_MIXED;
+  std::vector<int> it(k, 0), done(k, 0);
+  std::vector<double> fn(k, 0), rel(k, 0);
+  rso_status status = RSO_OK;
+  {
+    BatchScope scope(h, k);
+    Level& l0 = h->L[0];
+    const dim3 rg(BR_BLOCKS, k);
+    double* s = B.scal;
+    // r = f - K x; |f|^2 and |r|^2 per system
+    RSO_TRY(fine_residual<double>(h, B.x, B.q, B.r, h->rp64));
+    k_bdot<double><<<rg, BR_THREADS, 0, h->stream>>>(n3, B.q, B.q, B.red); rso::note_launch();
+    k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 6); rso::note_launch();
+    k_bdot<double><<<rg, BR_THREADS, 0, h->stream>>>(n3, B.r, B.r, B.red); rso::note_launch();
+    k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 5); rso::note_launch();
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.h_scal, s, sizeof(double) * KS * k, cudaMemcpyDeviceToHost, h->stream));
+    RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+    int left = 0;
+    for (int b = 0; b < k; b++) {
+      fn[b] = std::sqrt(B.h_scal[b * KS + 6]);
+      rel[b] = fn[b] > 0 ? std::sqrt(B.h_scal[b * KS + 5]) / fn[b] : 0.0;
+      done[b] = rel[b] < tol ? 1 : 0;
+      left += !done[b];
+    }
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.done, done.data(), sizeof(int) * k, cudaMemcpyHostToDevice, h->stream));
+    auto precondition_z = [&]() -> rso_status {
+      if (mixed) {
+        k_bd2f<<<cdiv(tot, 256), 256, 0, h->stream>>>(tot, B.r, l0.f32); rso::note_launch();
+        return vcycle_mixed(h);
+      }
+      RSO_CHECK_CUDA(h, cudaMemcpyAsync(l0.f64, B.r, sizeof(double) * tot, cudaMemcpyDeviceToDevice, h->stream));
+      RSO_TRY(vcycle_levels<double>(h, h->cfg.pre, h->cfg.post, 1, true));
+      RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.z, h->L[0].u64, sizeof(double) * tot, cudaMemcpyDeviceToDevice, h->stream));
+      return RSO_OK;
+    };
+    if (left > 0) {
+      RSO_TRY(precondition_z());
+      if (mixed) {
+        k_bf2d<<<cdiv(tot, 256), 256, 0, h->stream>>>(tot, h->L[0].u32, B.p); rso::note_launch();
+        k_bdot<float><<<rg, BR_THREADS, 0, h->stream>>>(n3, B.r, h->L[0].u32, B.red); rso::note_launch();
+      } else {
+        RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.p, B.z, sizeof(double) * tot, cudaMemcpyDeviceToDevice, h->stream));
+        k_bdot<double><<<rg, BR_THREADS, 0, h->stream>>>(n3, B.r, B.z, B.red); rso::note_launch();
+      }
+      k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 0); rso::note_launch();
+      int iter = 0;
+      while (true) {
+        RSO_TRY(fine_applyK_dot(h, B.p, B.q, h->rp64, s + 1, KS));
+        k_balpha<<<1, 64, 0, h->stream>>>(k, s, B.done); rso::note_launch();
+        k_bresid<<<rg, BR_THREADS, 0, h->stream>>>(n3, s, B.q, B.r, mixed ? h->L[0].f32 : nullptr, B.red); rso::note_launch();
+        k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 5); rso::note_launch();
+        RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.h_scal, s, sizeof(double) * KS * k, cudaMemcpyDeviceToHost, h->stream));
+        RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+        iter++;
+        left = 0;
+        for (int b = 0; b < k; b++) {
+          if (done[b]) continue;
+          it[b] = iter;
+          rel[b] = std::sqrt(B.h_scal[b * KS + 5]) / fn[b];
+          if (!std::isfinite(rel[b])) { h->err = "non-finite residual in batched PCG"; return RSO_ERR_NONFINITE; }
+          if (rel[b] < tol) done[b] = 2;  // converged in this iteration: x still takes this step
+          else left++;
+        }
+        if (left == 0 || iter >= max_iter) {
+          k_bstep<<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, s, B.p, B.x); rso::note_launch();
+          break;
+        }
+        // systems that converged now take their last step with the direction update, then freeze
+        RSO_TRY(precondition_z());
+        if (mixed) { k_bdot<float><<<rg, BR_THREADS, 0, h->stream>>>(n3, B.r, h->L[0].u32, B.red); rso::note_launch(); }
+        else { k_bdot<double><<<rg, BR_THREADS, 0, h->stream>>>(n3, B.r, B.z, B.red); rso::note_launch(); }
+        k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 3); rso::note_launch();
+        k_bbeta<<<1, 64, 0, h->stream>>>(k, s, B.done); rso::note_launch();
+        if (mixed) { k_bstep_dir<float><<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, s, h->L[0].u32, B.p, B.x); }
+        else { k_bstep_dir<double><<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, s, B.z, B.p, B.x); }
+        rso::note_launch();
+        for (int b = 0; b < k; b++)
+          if (done[b] == 2) done[b] = 1;
+        RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.done, done.data(), sizeof(int) * k, cudaMemcpyHostToDevice, h->stream));
+        RSO_TRY(launch_check(h, "batched pcg"));
+      }
+    }
+  }
+  for (int b = 0; b < k; b++) {
+    RSO_TRY(unpad_nodes(h, 0, B.x + b * n3, U + b * nn3));
+    if (rel[b] >= tol && fn[b] > 0) status = RSO_ERR_BUDGET_EXCEEDED;
+  }
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  const double ms = now_ms() - t0;
+  if (infos)
+    for (int b = 0; b < k; b++) { infos[b].iterations = it[b]; infos[b].rel_res = rel[b]; infos[b].ms = ms; }
+  if (status != RSO_OK) h->err = "batched PCG: a system did not reach the tolerance within max_iter";
+  return status;
+}
+
+}  // namespace rso
+
+using namespace rso;
+
+extern "C" rso_status rso_solve_batch(rso_handle* h, int k, const double* F, double* U, double tol, int max_iter,
+                                      rso_solve_info* infos) {
+  if (!h || !F || !U || k < 1 || k > 64 || !(tol > 0) || max_iter < 0) return RSO_ERR_INVALID_ARG;
+  if (!h->operators_ready) { h->err = "call rso_update_operators after rso_set_density"; return RSO_ERR_STATE; }
+  return solve_pcg_batch(h, k, F, U, tol, max_iter, infos);
+}

@@ -113,6 +113,7 @@ static void free_handle(rso_handle* h) {
   cudaFree(h->gal_w); cudaFree(h->efix); cudaFree(h->gfix);
   if (h->cublas) cublasDestroy((cublasHandle_t)h->cublas);
   cudaFree(h->cublas_ws); cudaFree(h->filt_taps);
+  batch_release(h);
   cudaFree(h->c_nodes); cudaFree(h->c_K); cudaFree(h->c_f); cudaFree(h->c_flag);
   cudaFree(h->red); cudaFree(h->scal); cudaFree(h->xfer); cudaFree(h->fpart);
   if (h->h_scal) cudaFreeHost(h->h_scal);

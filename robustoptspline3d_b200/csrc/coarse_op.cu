@@ -49,36 +49,63 @@ __device__ __forceinline__ void stencil_apply(const Level& L, const T* __restric
 // Per-node variant for the large coarse levels, which are bandwidth-bound:
 // one thread reads a node's 243 stencil entries and 27 neighbours once.
 // MODE 0 residual, MODE 2 damped block Jacobi (out of place).
-template <typename T, int MODE>
+template <typename T, int MODE, int KB>
 __global__ void __launch_bounds__(256) k_coarse(const Level L, const T* __restrict__ st, const T* __restrict__ u,
                                                 const T* __restrict__ f, T* __restrict__ out, T omega,
                                                 const T* __restrict__ uprev, T c1) {
-  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+  // blockIdx.z = z + nz * (chunk of KB systems): each stencil entry is read
+  // once and applied to the chunk's systems
+  const int chunk = blockIdx.z / L.nz;
+  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z - chunk * L.nz;
   if (x >= L.nx || y >= L.ny) return;
-  const long long NP = L.NP;
+  const long long NP = L.NP, px = L.px, pxy = (long long)L.px * L.py, VS = 3 * NP;
+  const int b0 = chunk * KB, nv = min(KB, L.nb - b0);
   const long long n = L.nidx(x, y, z);
   const bool act = (L.vclass[n] & NC_ACTIVE) != 0;
-  T acc[3] = {0, 0, 0};
-  if (act) stencil_apply<T>(L, st, u, n, false, acc);
-  if (MODE == 0) {
+  T acc[KB][3];
 #pragma unroll
-    for (int r = 0; r < 3; r++) out[n + r * NP] = f[n + r * NP] - acc[r];
-  } else {
-    if (!act) { out[n] = 0; out[n + NP] = 0; out[n + 2 * NP] = 0; return; }
-    T S[9];
+  for (int j = 0; j < KB; j++) acc[j][0] = acc[j][1] = acc[j][2] = T(0);
+  if (act) {
+#pragma unroll
+    for (int d = 0; d < 27; d++) {
+      const long long nbr = n + (d % 3 - 1) + (d / 3 % 3 - 1) * px + (d / 9 - 1) * pxy;
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const T sv = st[(d * 9 + r * 3 + c) * NP + n];
+#pragma unroll
+          for (int j = 0; j < KB; j++)
+            if (j < nv) acc[j][r] = fma(sv, u[(b0 + j) * VS + nbr + c * NP], acc[j][r]);
+        }
+    }
+  }
+  T S[9];
+  if (MODE == 2 && act) {
 #pragma unroll
     for (int i = 0; i < 9; i++) S[i] = st[(13 * 9 + i) * NP + n];
-    const T r0 = f[n] - acc[0], r1 = f[n + NP] - acc[1], r2 = f[n + 2 * NP] - acc[2];
-    const T A = S[4] * S[8] - S[5] * S[7], B = -(S[3] * S[8] - S[5] * S[6]), C = S[3] * S[7] - S[4] * S[6];
-    const T det = S[0] * A + S[1] * B + S[2] * C;
-    const T id = omega / det;
-    const T i01 = -(S[1] * S[8] - S[2] * S[7]), i02 = S[1] * S[5] - S[2] * S[4];
-    const T i11 = S[0] * S[8] - S[2] * S[6], i12 = -(S[0] * S[5] - S[2] * S[3]);
-    const T i21 = -(S[0] * S[7] - S[1] * S[6]), i22 = S[0] * S[4] - S[1] * S[3];
-    const T p0 = uprev ? uprev[n] : T(0), p1 = uprev ? uprev[n + NP] : T(0), p2 = uprev ? uprev[n + 2 * NP] : T(0);
-    out[n] = u[n] + c1 * (u[n] - p0) + id * (A * r0 + i01 * r1 + i02 * r2);
-    out[n + NP] = u[n + NP] + c1 * (u[n + NP] - p1) + id * (B * r0 + i11 * r1 + i12 * r2);
-    out[n + 2 * NP] = u[n + 2 * NP] + c1 * (u[n + 2 * NP] - p2) + id * (C * r0 + i21 * r1 + i22 * r2);
+  }
+#pragma unroll
+  for (int j = 0; j < KB; j++) {
+    if (j >= nv) break;
+    const long long o = (b0 + j) * VS + n;
+    if (MODE == 0) {
+#pragma unroll
+      for (int r = 0; r < 3; r++) out[o + r * NP] = f[o + r * NP] - acc[j][r];
+    } else {
+      if (!act) { out[o] = 0; out[o + NP] = 0; out[o + 2 * NP] = 0; continue; }
+      const T r0 = f[o] - acc[j][0], r1 = f[o + NP] - acc[j][1], r2 = f[o + 2 * NP] - acc[j][2];
+      const T A = S[4] * S[8] - S[5] * S[7], B = -(S[3] * S[8] - S[5] * S[6]), C = S[3] * S[7] - S[4] * S[6];
+      const T det = S[0] * A + S[1] * B + S[2] * C;
+      const T id = omega / det;
+      const T i01 = -(S[1] * S[8] - S[2] * S[7]), i02 = S[1] * S[5] - S[2] * S[4];
+      const T i11 = S[0] * S[8] - S[2] * S[6], i12 = -(S[0] * S[5] - S[2] * S[3]);
+      const T i21 = -(S[0] * S[7] - S[1] * S[6]), i22 = S[0] * S[4] - S[1] * S[3];
+      const T p0 = uprev ? uprev[o] : T(0), p1 = uprev ? uprev[o + NP] : T(0), p2 = uprev ? uprev[o + 2 * NP] : T(0);
+      out[o] = u[o] + c1 * (u[o] - p0) + id * (A * r0 + i01 * r1 + i02 * r2);
+      out[o + NP] = u[o + NP] + c1 * (u[o + NP] - p1) + id * (B * r0 + i11 * r1 + i12 * r2);
+      out[o + 2 * NP] = u[o + 2 * NP] + c1 * (u[o + 2 * NP] - p2) + id * (C * r0 + i21 * r1 + i22 * r2);
+    }
   }
 }
 
@@ -96,7 +123,15 @@ __global__ void __launch_bounds__(32 * CTY * 3) k_coarse_r(const Level L, const 
                                                            T* __restrict__ out, T omega,
                                                            const T* __restrict__ uprev, T c1) {
   __shared__ T sres[3][CTY][32];
-  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * CTY + threadIdx.y, z = blockIdx.z;
+  const int bsys = blockIdx.z / L.nz;
+  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * CTY + threadIdx.y, z = blockIdx.z - bsys * L.nz;
+  {
+    const long long off = (long long)bsys * 3 * L.NP;
+    u += off;
+    f += off;
+    out += off;
+    if (uprev != nullptr) uprev += off;
+  }
   const int r = threadIdx.z;
   const bool in = x < L.nx && y < L.ny;
   const long long NP = L.NP, px = L.px, pxy = (long long)L.px * L.py;
@@ -173,8 +208,11 @@ __global__ void __launch_bounds__(256) k_coarse_gs(const Level L, const T* __res
 // Weights (F - |d|) / F per axis, d in (-F, F).
 template <typename T, int F>
 __global__ void k_restrict_z(const Level Fl, int nZ, const T* __restrict__ rf, T* __restrict__ t) {
-  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, Z = blockIdx.z;
+  const int bsys = blockIdx.z / nZ;
+  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, Z = blockIdx.z - bsys * nZ;
   if (x >= Fl.nx || y >= Fl.ny) return;
+  rf += (long long)bsys * 3 * Fl.NP;
+  t += (long long)bsys * 3 * Fl.nx * Fl.ny * nZ;
   T s0 = 0, s1 = 0, s2 = 0;
 #pragma unroll
   for (int dz = -F + 1; dz < F; dz++) {
@@ -191,8 +229,11 @@ __global__ void k_restrict_z(const Level Fl, int nZ, const T* __restrict__ rf, T
 
 template <typename T, int F>
 __global__ void k_restrict_xy(const Level Fl, const Level C, const T* __restrict__ t, T* __restrict__ fc) {
-  const int X = blockIdx.x * 32 + threadIdx.x, Y = blockIdx.y * 8 + threadIdx.y, Z = blockIdx.z;
+  const int bsys = blockIdx.z / C.nz;
+  const int X = blockIdx.x * 32 + threadIdx.x, Y = blockIdx.y * 8 + threadIdx.y, Z = blockIdx.z - bsys * C.nz;
   if (X >= C.nx || Y >= C.ny) return;
+  t += (long long)bsys * 3 * Fl.nx * Fl.ny * C.nz;
+  fc += (long long)bsys * 3 * C.NP;
   const long long nC = C.nidx(X, Y, Z);
   T s0 = 0, s1 = 0, s2 = 0;
   if (C.vclass[nC] & NC_ACTIVE) {
@@ -224,7 +265,10 @@ __global__ void k_restrict_xy(const Level Fl, const Level C, const T* __restrict
 template <typename T, int F>
 __global__ void k_prolong(const Level Fl, const Level C, const T* __restrict__ uc, T* __restrict__ uf) {
   const int lane = threadIdx.x;
-  const int x = blockIdx.x * 32 + lane, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+  const int bsys = blockIdx.z / Fl.nz;
+  const int x = blockIdx.x * 32 + lane, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z - bsys * Fl.nz;
+  uc += (long long)bsys * 3 * C.NP;
+  uf += (long long)bsys * 3 * Fl.NP;
   const bool yok = y < Fl.ny;
   const int xb = blockIdx.x * (32 / F);
   const int Y0 = y / F, Z0 = z / F, oy = y - F * Y0, oz = z - F * Z0;
@@ -564,10 +608,15 @@ __device__ __forceinline__ long long bot_node(const Level& L, long long i) {
 // out = u + c1 (u - up) + om D^-1 (f - K u), u read as 0 when zero and up as
 // 0 when NULL; inactive nodes 0
 template <typename T>
-__device__ void bot_jacobi(const Level& L, const T* st, const T* u, const T* f, T* out, T om, bool zero, const T* up,
-                           T c1, int g0, int gs) {
+__device__ void bot_jacobi(const Level& L, const T* st, const T* u0v, const T* f0v, T* out0v, T om, bool zero,
+                           const T* up0v, T c1, int g0, int gs) {
   const long long NP = L.NP;
-  for (long long i = g0; i < L.nn; i += gs) {
+  for (long long ib = g0; ib < L.nn * L.nb; ib += gs) {
+    const long long b = ib / L.nn, i = ib - b * L.nn, vo = b * 3 * NP;
+    const T* u = u0v + vo;
+    const T* f = f0v + vo;
+    T* out = out0v + vo;
+    const T* up = up0v ? up0v + vo : nullptr;
     const long long n = bot_node(L, i);
     if (!(L.vclass[n] & NC_ACTIVE)) { out[n] = 0; out[n + NP] = 0; out[n + 2 * NP] = 0; continue; }
     T acc[3] = {0, 0, 0};
@@ -591,9 +640,13 @@ __device__ void bot_jacobi(const Level& L, const T* st, const T* u, const T* f, 
 }
 
 template <typename T>
-__device__ void bot_residual(const Level& L, const T* st, const T* u, const T* f, T* r, int g0, int gs) {
+__device__ void bot_residual(const Level& L, const T* st, const T* u0v, const T* f0v, T* r0v, int g0, int gs) {
   const long long NP = L.NP;
-  for (long long i = g0; i < L.nn; i += gs) {
+  for (long long ib = g0; ib < L.nn * L.nb; ib += gs) {
+    const long long b = ib / L.nn, i = ib - b * L.nn, vo = b * 3 * NP;
+    const T* u = u0v + vo;
+    const T* f = f0v + vo;
+    T* r = r0v + vo;
     const long long n = bot_node(L, i);
     T acc[3] = {0, 0, 0};
     if (L.vclass[n] & NC_ACTIVE) stencil_apply<T>(L, st, u, n, false, acc);
@@ -602,9 +655,12 @@ __device__ void bot_residual(const Level& L, const T* st, const T* u, const T* f
 }
 
 template <typename T>
-__device__ void bot_restrict(const Level& Fl, const Level& C, const T* rf, T* fc, int g0, int gs) {
+__device__ void bot_restrict(const Level& Fl, const Level& C, const T* rf0, T* fc0, int g0, int gs) {
   const int F = C.factor;
-  for (long long i = g0; i < C.nn; i += gs) {
+  for (long long ib = g0; ib < C.nn * C.nb; ib += gs) {
+    const long long b = ib / C.nn, i = ib - b * C.nn;
+    const T* rf = rf0 + b * 3 * Fl.NP;
+    T* fc = fc0 + b * 3 * C.NP;
     const int X = (int)(i % C.nx), Y = (int)((i / C.nx) % C.ny), Z = (int)(i / ((long long)C.nx * C.ny));
     const long long nC = C.nidx(X, Y, Z);
     T s0 = 0, s1 = 0, s2 = 0;
@@ -631,9 +687,12 @@ __device__ void bot_restrict(const Level& Fl, const Level& C, const T* rf, T* fc
 }
 
 template <typename T>
-__device__ void bot_prolong(const Level& Fl, const Level& C, const T* uc, T* uf, int g0, int gs) {
+__device__ void bot_prolong(const Level& Fl, const Level& C, const T* uc0, T* uf0, int g0, int gs) {
   const int F = C.factor;
-  for (long long i = g0; i < Fl.nn; i += gs) {
+  for (long long ib = g0; ib < Fl.nn * Fl.nb; ib += gs) {
+    const long long b = ib / Fl.nn, i = ib - b * Fl.nn;
+    const T* uc = uc0 + b * 3 * C.NP;
+    T* uf = uf0 + b * 3 * Fl.NP;
     const int x = (int)(i % Fl.nx), y = (int)((i / Fl.nx) % Fl.ny), z = (int)(i / ((long long)Fl.nx * Fl.ny));
     const long long n = Fl.nidx(x, y, z);
     const uint8_t cls = Fl.vclass[n];
@@ -654,7 +713,7 @@ __device__ void bot_prolong(const Level& Fl, const Level& C, const T* uc, T* uf,
 
 template <typename T>
 __device__ void bot_copy(const Level& L, const T* a, T* b, int g0, int gs) {
-  for (long long i = g0; i < 3 * L.NP; i += gs) b[i] = a[i];
+  for (long long i = g0; i < 3 * L.NP * L.nb; i += gs) b[i] = a[i];
 }
 
 template <typename T>
@@ -676,7 +735,7 @@ __global__ void __cluster_dims__(BOT_CTAS, 1, 1) __launch_bounds__(BOT_THREADS, 
       T* w = prv; prv = cur; cur = oth; oth = w;
     }
     if (A.pre == 0) {
-      for (long long i = g0; i < 3 * L.NP; i += gs) u[i] = T(0);
+      for (long long i = g0; i < 3 * L.NP * L.nb; i += gs) u[i] = T(0);
       cl.sync();
     } else if (cur != u) {
       bot_copy<T>(L, cur, u, g0, gs);
@@ -692,20 +751,26 @@ __global__ void __cluster_dims__(BOT_CTAS, 1, 1) __launch_bounds__(BOT_THREADS, 
     const Level& C = A.L[A.nl - 1];
     T* u = bv_u<T>(C);
     const T* f = bv_f<T>(C);
-    for (long long i = g0; i < 3 * C.NP; i += gs) u[i] = T(0);
-    for (int i = g0; i < A.nc; i += gs) {
-      const long long n = A.cnodes[i];
-      A.cf[3 * i + 0] = (double)f[n];
-      A.cf[3 * i + 1] = (double)f[n + C.NP];
-      A.cf[3 * i + 2] = (double)f[n + 2 * C.NP];
+    const long long VS = 3 * C.NP;
+    const int N = 3 * A.nc;
+    for (long long i = g0; i < VS * C.nb; i += gs) u[i] = T(0);
+    for (long long ib = g0; ib < (long long)A.nc * C.nb; ib += gs) {
+      const long long b = ib / A.nc, i = ib - b * A.nc;
+      const long long n = A.cnodes[i] + b * VS;
+      double* cf = A.cf + b * N;
+      cf[3 * i + 0] = (double)f[n];
+      cf[3 * i + 1] = (double)f[n + C.NP];
+      cf[3 * i + 2] = (double)f[n + 2 * C.NP];
     }
     cl.sync();
-    const int N = 3 * A.nc;
-    for (int row = g0; row < N; row += gs) {
+    for (long long rb = g0; rb < (long long)N * C.nb; rb += gs) {
+      const long long b = rb / N;
+      const int row = (int)(rb - b * N);
+      const double* cf = A.cf + b * N;
       double s = 0;
       const double* k = A.kinv + (long long)row * N;
-      for (int j = 0; j < N; j++) s += k[j] * A.cf[j];
-      u[A.cnodes[row / 3] + (row % 3) * C.NP] = (T)s;
+      for (int j = 0; j < N; j++) s += k[j] * cf[j];
+      u[b * VS + A.cnodes[row / 3] + (row % 3) * C.NP] = (T)s;
     }
     cl.sync();
   }
@@ -731,7 +796,9 @@ __global__ void __cluster_dims__(BOT_CTAS, 1, 1) __launch_bounds__(BOT_THREADS, 
 }
 
 // ---------------------------------------------------------------- host wrappers
-static inline dim3 node_grid(const Level& l) { return dim3(cdiv(l.nx, 32), cdiv(l.ny, 8), l.nz); }
+// grids over the nodes of a level for every system it carries
+static inline dim3 node_grid(const Level& l) { return dim3(cdiv(l.nx, 32), cdiv(l.ny, 8), l.nz * l.nb); }
+static inline dim3 chunk_grid(const Level& l, int kb) { return dim3(cdiv(l.nx, 32), cdiv(l.ny, 8), l.nz * cdiv(l.nb, kb)); }
 // levels above this many nodes use the per-node stencil kernel
 static const long long kRowSplitMaxNodes = 100000;
 
@@ -747,9 +814,14 @@ rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* 
   const Level& l = h->L[level];
   if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
   if (l.nn > kRowSplitMaxNodes) {
-    k_coarse<T, 0><<<node_grid(l), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0)); rso::note_launch();
+    if (l.nb == 1) {
+      k_coarse<T, 0, 1><<<chunk_grid(l, 1), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0));
+    } else {
+      k_coarse<T, 0, 4><<<chunk_grid(l, 4), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0));
+    }
+    rso::note_launch();
   } else {
-    k_coarse_r<T, 0><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0)); rso::note_launch();
+    k_coarse_r<T, 0><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz * l.nb), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0)); rso::note_launch();
   }
   if (h->prof_on) prof_end(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64));
   return launch_check(h, "coarse_residual");
@@ -760,9 +832,14 @@ rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T*
   const Level& l = h->L[level];
   if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
   if (l.nn > kRowSplitMaxNodes) {
-    k_coarse<T, 2><<<node_grid(l), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1); rso::note_launch();
+    if (l.nb == 1) {
+      k_coarse<T, 2, 1><<<chunk_grid(l, 1), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1);
+    } else {
+      k_coarse<T, 2, 4><<<chunk_grid(l, 4), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1);
+    }
+    rso::note_launch();
   } else {
-    k_coarse_r<T, 2><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1); rso::note_launch();
+    k_coarse_r<T, 2><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz * l.nb), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1); rso::note_launch();
   }
   if (h->prof_on) prof_end(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64));
   return launch_check(h, "coarse_jacobi");
@@ -782,12 +859,12 @@ template <typename T>
 rso_status restrict_(rso_handle* h, int cl, const T* rf, T* fc) {
   const Level& c = h->L[cl];
   const Level& f = h->L[cl - 1];
-  if ((size_t)3 * f.nx * f.ny * c.nz > h->xfer_n) {
+  if ((size_t)3 * f.nx * f.ny * c.nz * c.nb > h->xfer_n) {
     h->err = "restriction scratch smaller than the level pair needs";
     return RSO_ERR_STATE;
   }
   T* t = reinterpret_cast<T*>(h->xfer);
-  const dim3 gz(cdiv(f.nx, 32), cdiv(f.ny, 8), c.nz);
+  const dim3 gz(cdiv(f.nx, 32), cdiv(f.ny, 8), c.nz * c.nb);
   if (c.factor == 4) {
     k_restrict_z<T, 4><<<gz, dim3(32, 8), 0, h->stream>>>(f, c.nz, rf, t); rso::note_launch();
     k_restrict_xy<T, 4><<<node_grid(c), dim3(32, 8), 0, h->stream>>>(f, c, t, fc); rso::note_launch();
@@ -818,9 +895,13 @@ template <typename T>
 rso_status coarsest_solve(rso_handle* h, const T* f, T* u) {
   const Level& c = h->L.back();
   if (h->nc == 0) return RSO_OK;
-  k_gather_coarse<T><<<cdiv(h->nc, 128), 128, 0, h->stream>>>(c, f, h->c_nodes, h->nc, h->c_f); rso::note_launch();
   const int N = 3 * h->nc;
-  k_gemv_scatter<T><<<cdiv(N, 8), 256, 0, h->stream>>>(c, h->c_K + (size_t)N * N, h->c_f, h->nc, h->c_nodes, u); rso::note_launch();
+  for (int b = 0; b < c.nb; b++) {  // one system after the other through the shared right-hand side buffer
+    const long long vo = (long long)b * 3 * c.NP;
+    k_gather_coarse<T><<<cdiv(h->nc, 128), 128, 0, h->stream>>>(c, f + vo, h->c_nodes, h->nc, h->c_f); rso::note_launch();
+    k_gemv_scatter<T><<<cdiv(N, 8), 256, 0, h->stream>>>(c, h->c_K + (size_t)N * N, h->c_f, h->nc, h->c_nodes, u + vo);
+    rso::note_launch();
+  }
   return launch_check(h, "coarsest_solve");
 }
 
@@ -854,7 +935,7 @@ rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post) {
   A.kinv = h->c_K + (size_t)N * N;
   A.cnodes = h->c_nodes;
   A.nc = h->nc;
-  A.cf = h->c_f;
+  A.cf = h->L[0].nb > 1 ? h->c_fb : h->c_f;
   k_bottom<T><<<BOT_CTAS, BOT_THREADS, 0, h->stream>>>(A); rso::note_launch();
   return launch_check(h, "bottom_vcycle");
 }

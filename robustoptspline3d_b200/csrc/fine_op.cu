@@ -189,7 +189,16 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
   T* sx = ss + WNSLOT * SLOT;              // [2][9][NE]: corners (0,0), (1,0), (0,1), by plane parity
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * WTX + tx;
   const int x0 = blockIdx.x * (WTX - 1), y0 = blockIdx.y * (TY - 1);
-  const int z0 = blockIdx.z * FZC, z1 = min(z0 + FZC, L.nz);
+  // blockIdx.z = z chunk + (number of chunks) * system; systems share rho^p
+  const int nzc = (L.nz + FZC - 1) / FZC, bsys = blockIdx.z / nzc;
+  const int z0 = (blockIdx.z - bsys * nzc) * FZC, z1 = min(z0 + FZC, L.nz);
+  {
+    const long long off = (long long)bsys * 3 * L.NP;
+    u += off;
+    f += off;
+    out += off;
+    if (uprev != nullptr) uprev += off;
+  }
   const int ex = x0 - 1 + tx, ey = y0 - 1 + ty;
   const long long NP = L.NP;
   const int xs = x0 & ~3, ox = x0 - xs;
@@ -420,7 +429,8 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
       double t = 0;
 #pragma unroll
       for (int w = 0; w < TY; w++) t += sred[w];
-      dotp[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = t;
+      dotp[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * (blockIdx.z - bsys * nzc)) +
+           (long long)bsys * gridDim.x * gridDim.y * nzc] = t;
     }
   }
   __pipeline_wait_prior(0);
@@ -430,9 +440,12 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
 template <typename T>
 __global__ void __launch_bounds__(256) k_fine_jacobi0(const Level L, const T* __restrict__ f, T* __restrict__ out,
                                                       const T* __restrict__ rp, T omega) {
-  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z;
+  const int bsys = blockIdx.z / L.nz;
+  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y, z = blockIdx.z - bsys * L.nz;
   if (x >= L.nx || y >= L.ny) return;
   const long long NP = L.NP, qx = L.qx, qxy = (long long)L.qx * L.qy;
+  f += (long long)bsys * 3 * NP;
+  out += (long long)bsys * 3 * NP;
   const long long n = L.nidx(x, y, z);
   const uint8_t cls = L.vclass[n];
   if (!(cls & NC_ACTIVE) || (cls & NC_SUPPORT)) {
@@ -537,9 +550,11 @@ __global__ void __launch_bounds__(256) k_fine_gs(const Level L, T* __restrict__ 
   u[n] = v[0]; u[n + NP] = v[1]; u[n + 2 * NP] = v[2];
 }
 
-static inline dim3 plane_grid(const Level& l) { return dim3(cdiv(l.nx, 32), cdiv(l.ny, 8), l.nz); }
+static inline dim3 plane_grid(const Level& l) { return dim3(cdiv(l.nx, 32), cdiv(l.ny, 8), l.nz * l.nb); }
 constexpr int WTY = 8;
-static inline dim3 march_grid(const Level& l) { return dim3(cdiv(l.nx, WTX - 1), cdiv(l.ny, WTY - 1), cdiv(l.nz, FZC)); }
+static inline dim3 march_grid(const Level& l) {
+  return dim3(cdiv(l.nx, WTX - 1), cdiv(l.ny, WTY - 1), cdiv(l.nz, FZC) * l.nb);
+}
 
 template <typename T>
 static inline int pcls(int c32, int c64) { return sizeof(T) == 4 ? c32 : c64; }
@@ -579,16 +594,17 @@ rso_status fine_applyK(rso_handle* h, const T* u, T* f, const T* rp) {
   return launch_fine<T, 1>(h, u, u, f, rp, 0.0, pcls<T>(PC_FINE_RES32, PC_FINE_APPLYK64), "fine_applyK");
 }
 // f = K u and dot_dev = u . f in one pass (the CG step's p . q)
-rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const double* rp, double* dot_dev) {
+rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const double* rp, double* dot_dev, int stride) {
   const dim3 g = march_grid(h->L[0]);
-  const long long nb = (long long)g.x * g.y * g.z;
+  const long long nb = (long long)g.x * g.y * g.z;  // all systems
   if (nb > h->fpart_n) {
     h->err = "fine partial-sum buffer smaller than the grid";
     return RSO_ERR_STATE;
   }
   const rso_status st = launch_fine<double, 1>(h, u, u, f, rp, 0.0, PC_FINE_APPLYK64, "fine_applyK_dot", h->fpart);
   if (st != RSO_OK) return st;
-  return reduce_partials(h, h->fpart, (int)nb, dot_dev);
+  // one sum per system: dot_dev[b] over the b-th block of partials
+  return reduce_partials_batch(h, h->fpart, (int)(nb / h->L[0].nb), h->L[0].nb, dot_dev, stride);
 }
 template <typename T>
 rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega,

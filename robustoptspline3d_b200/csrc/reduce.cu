@@ -102,6 +102,21 @@ rso_status cg_resid_rr(rso_handle* h, long long n, const double* alpha, const do
   return launch_check(h, "cg_resid_rr");
 }
 
+// one sum per system: out[b * stride] = sum of part[b * nper .. (b + 1) * nper)
+__global__ void __launch_bounds__(RED_THREADS) k_final_batch(const double* __restrict__ part, int nper,
+                                                             double* __restrict__ out, int stride) {
+  const double* p = part + (long long)blockIdx.x * nper;
+  double s = 0;
+  for (int i = threadIdx.x; i < nper; i += blockDim.x) s += p[i];
+  s = block_sum(s);
+  if (threadIdx.x == 0) out[(long long)blockIdx.x * stride] = s;
+}
+
+rso_status reduce_partials_batch(rso_handle* h, const double* part, int nper, int nb, double* dev_out, int stride) {
+  k_final_batch<<<nb, RED_THREADS, 0, h->stream>>>(part, nper, dev_out, stride); rso::note_launch();
+  return launch_check(h, "reduce_partials_batch");
+}
+
 rso_status reduce_partials(rso_handle* h, const double* part, int n, double* dev_out) {
   k_final<<<1, RED_THREADS, 0, h->stream>>>(part, n, dev_out); rso::note_launch();
   return launch_check(h, "reduce_partials");

@@ -28,6 +28,8 @@ struct Level {
   long long NP = 0, NQ = 0;       // padded node / element counts
   long long nn = 0, ne = 0;       // unpadded counts
   int factor = 0;                 // coarsening factor from the finer level
+  int nb = 1;                     // systems carried by the level vectors (batched solves): each of
+                                  // u/f/r/t then holds nb consecutive vectors of 3 NP entries
   long long n_active_e = 0, n_active_v = 0;
   uint8_t* emask = nullptr;       // padded element mask
   uint8_t* vclass = nullptr;      // padded node class
@@ -98,6 +100,18 @@ struct rso_handle {
   void* filt_taps = nullptr;          // sensitivity-filter tap table of the last radius used
   long long filt_cap = 0;
   double filt_radius = -1.0;
+  // batched solves (rso_solve_batch): system-major slabs, allocated on first use
+  struct Batch {
+    int cap = 0;                                      // systems the slabs hold
+    std::vector<float*> u32, f32, r32, t32;           // per level, cap * 3 NP each
+    std::vector<double*> u64, f64, r64, t64;
+    double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr;  // fine FP64, cap * 3 NP
+    double *cf = nullptr, *red = nullptr, *fpart = nullptr, *xfer = nullptr;
+    double *scal = nullptr, *h_scal = nullptr;
+    int* done = nullptr;
+  } batch;
+  double* c_fb = nullptr;             // coarsest right-hand sides of a batch (cap x 3 nc)
+
   // coarsest dense solve
   int nc = 0;                         // active coarsest nodes
   int* c_nodes = nullptr;             // padded node ids of active coarsest nodes
@@ -171,6 +185,8 @@ rso_status dot_host(rso_handle* h, const double* a, const double* b, long long n
 rso_status cg_resid_rr(rso_handle* h, long long n, const double* alpha, const double* q, double* r, float* r32,
                        double* rr_dev);
 rso_status reduce_partials(rso_handle* h, const double* part, int n, double* dev_out);
+rso_status reduce_partials_batch(rso_handle* h, const double* part, int nper, int nb, double* dev_out,
+                                 int stride = 1);
 rso_status pow_step(rso_handle* h, long long n, const float* u, const float* t, float* r, double* uu, double* rr);
 rso_status dot_df(rso_handle* h, const double* a, const float* b, long long n, double* dev_out);
 rso_status sum_float(rso_handle* h, const float* a, long long n, double* dev_out);
@@ -197,7 +213,8 @@ void smoother_steps(const rso_handle* h, double lam, int m, double* om, double* 
 int bottom_level(const rso_handle* h);
 template <typename T>
 rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post);
-rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const double* rp, double* dot_dev);
+rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const double* rp, double* dot_dev,
+                           int stride = 1);
 template <typename T>
 rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega,
                        const T* u_prev = nullptr, double c1 = 0.0);
@@ -231,6 +248,10 @@ rso_status estimate_lambda(rso_handle* h);
 template <typename T>
 rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric, bool u0_zero);
 rso_status precondition(rso_handle* h, const double* r, double* z);
+rso_status vcycle_mixed(rso_handle* h);
+void batch_release(rso_handle* h);
+rso_status solve_pcg_batch(rso_handle* h, int k, const double* F_dense, double* U_dense, double tol, int max_iter,
+                           rso_solve_info* infos);
 rso_status solve_pcg(rso_handle* h, const double* f, double* u, double tol, int max_iter, rso_solve_info* info);
 rso_status solve_vcycles(rso_handle* h, const double* f, double* u, double tol, int max_iter,
                          rso_solve_info* info);

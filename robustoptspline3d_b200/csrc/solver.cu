@@ -115,7 +115,7 @@ rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric, bool u
     if (li > 0) {
       RSO_TRY(level_residual<T>(h, li - 1));
       RSO_TRY(restrict_<T>(h, li, LV<T>::r(h->L[li - 1]), LV<T>::f(l)));
-      RSO_CHECK_CUDA(h, cudaMemsetAsync(LV<T>::u(l), 0, sizeof(T) * 3 * l.NP, h->stream));
+      RSO_CHECK_CUDA(h, cudaMemsetAsync(LV<T>::u(l), 0, sizeof(T) * 3 * l.NP * l.nb, h->stream));
     }
     const bool zero = li > 0 || u0_zero;
     if (li < nl - 1) RSO_TRY(smooth<T>(h, li, pre, 0, zero));
@@ -194,11 +194,11 @@ __global__ void k_cg_step(long long n, const double* __restrict__ alpha, const d
 
 // mixed precision: one FP32 V-cycle from a zero iterate on L[0].f32 (already
 // holding the FP32 residual); the result is left in L[0].u32
-static rso_status vcycle_mixed(rso_handle* h) {
+rso_status vcycle_mixed(rso_handle* h) {
   Level& l0 = h->L[0];
   // the first damped-Jacobi sweep from zero reads no iterate; Gauss-Seidel does
   if (h->cfg.smoother == RSO_SMOOTH_GS || h->cfg.pre == 0)
-    RSO_CHECK_CUDA(h, cudaMemsetAsync(l0.u32, 0, sizeof(float) * 3 * l0.NP, h->stream));
+    RSO_CHECK_CUDA(h, cudaMemsetAsync(l0.u32, 0, sizeof(float) * 3 * l0.NP * l0.nb, h->stream));
   return vcycle_levels<float>(h, h->cfg.pre, h->cfg.post, 1, true);
 }
 

@@ -101,6 +101,7 @@ SIGNATURES = {
     "rso_level_lambda": (_ci, [_vp, _ci, _pd]),
     "rso_vcycle": (_ci, [_vp, _vp, _vp, _ci, _ci, _ci, _pd]),
     "rso_solve": (_ci, [_vp, _vp, _vp, _cd, _ci, _ci, ctypes.POINTER(_SolveInfo)]),
+    "rso_solve_batch": (_ci, [_vp, _ci, _vp, _vp, _cd, _ci, ctypes.POINTER(_SolveInfo)]),
     "rso_dot": (_ci, [_vp, _vp, _vp, _pd]),
     "rso_sensitivity": (_ci, [_vp, _vp, _vp]),
     "rso_element_energy": (_ci, [_vp, _vp, _vp]),
@@ -422,6 +423,18 @@ class HierarchyGrid:
         self._chk(self.lib.rso_solve(self.h, _dev(f, torch.float64), _dev(u), tol, max_iter, method, ctypes.byref(info)),
                   "rso_solve")
         return u, info.iterations, info.rel_res, info.ms
+
+    def solve_batch(self, F, U0=None, tol=1e-10, max_iter=200):
+        """k systems at once: F (k, 3*Nn) float64 CUDA tensor; returns U (k, 3*Nn)
+        and per-system (iterations, rel_res)."""
+        import torch
+        F = F.reshape(F.shape[0], -1).contiguous()
+        k = F.shape[0]
+        U = torch.zeros_like(F) if U0 is None else U0.reshape(k, -1).clone().contiguous()
+        infos = (_SolveInfo * k)()
+        self._chk(self.lib.rso_solve_batch(self.h, k, _dev(F, torch.float64), _dev(U, torch.float64), tol, max_iter,
+                                           infos), "rso_solve_batch")
+        return U, [(infos[b].iterations, infos[b].rel_res) for b in range(k)]
 
     def compliance(self, f, u):
         v = ctypes.c_double(0)

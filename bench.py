@@ -307,6 +307,72 @@ def run_batch(args):
     g.close()
 
 
+def cube_problem(n, seed):
+    """Config-0 style cube: all voxels active, x = 0 nodes clamped, a unit total
+    -z load spread over the nodes of the x = n face's mid-height line, density
+    i.i.d. U[0.2, 1] followed by one 3x3x3 mean over the in-box neighbours."""
+    from scipy.ndimage import uniform_filter
+    rng = np.random.default_rng(seed)
+    em = np.ones((n, n, n), np.uint8)
+    fa = np.zeros((n + 1,) * 3, np.uint8)
+    fa[:, :, 0] = 1
+    la = np.zeros((n + 1,) * 3, np.uint8)
+    rho = rng.uniform(0.2, 1.0, (n, n, n))
+    rho = (uniform_filter(rho, 3, mode="constant") / uniform_filter(np.ones_like(rho), 3, mode="constant"))
+    nn = (n + 1) ** 3
+    f = np.zeros(3 * nn)
+    ids = n + (n + 1) * (np.arange(n + 1) + (n + 1) * (n // 2))
+    f[2 * nn + ids] = -1.0 / (n + 1)
+    return em, fa, la, rho.astype(np.float32), f
+
+
+def run_problems(args):
+    """Config 3b: 32 independent cubes of uneven size (edges drawn from
+    {32, 48, 64, 96, 128}), one handle and CUDA stream each, solved one after
+    another and then concurrently from host threads (ctypes releases the GIL,
+    so the problems' kernels overlap on the GPU)."""
+    import concurrent.futures
+    import torch
+    import robustoptspline3d_b200 as R
+    rng = np.random.default_rng(2026)
+    sizes = rng.choice([32, 48, 64, 96, 128], size=32)
+    grids, loads = [], []
+    for i, n in enumerate(sizes):
+        em, fa, la, rho, f = cube_problem(int(n), 100 + i)
+        g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=R.rso.MIXED, smoother=smoother_id(R), omega=OMEGA,
+                                                        cheb_lower=CHEB_LOWER, pre=2, post=2, poisson_ratio=0.4,
+                                                        youngs_modulus=1e6))
+        g.set_density(rho.ravel())
+        g.update_stencil()
+        grids.append(g)
+        loads.append(torch.as_tensor(f, device="cuda"))
+
+    def solve(i):
+        return grids[i].solve(loads[i], tol=1e-6, max_iter=500)[1]
+
+    for i in range(len(grids)):
+        solve(i)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    its = [solve(i) for i in range(len(grids))]
+    t_seq = time.perf_counter() - t0
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(grids)) as ex:
+        list(ex.map(solve, range(len(grids))))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        its_c = list(ex.map(solve, range(len(grids))))
+        torch.cuda.synchronize()
+        t_con = time.perf_counter() - t0
+    print(json.dumps({"metric": "32 uneven cubes (edges 32-128) to rel.resid 1e-6 (mixed), concurrent handles",
+                      "value": len(grids) / t_con, "unit": "solves/s", "higher_is_better": True,
+                      "sequential_solves_per_s": len(grids) / t_seq, "concurrent_vs_sequential": t_seq / t_con,
+                      "sizes": [int(n) for n in sizes], "iterations": its, "iterations_concurrent": its_c,
+                      "data": "synthetic", "config": {"workload": "config 3b", "smoother": f"{SMOOTHER} 2+2"}}),
+          flush=True)
+    for g in grids:
+        g.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -317,7 +383,7 @@ def main():
     ap.add_argument("--ref-size", type=int, default=24)
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="design", choices=["design", "solve", "batch"])
+    ap.add_argument("--mode", default="design", choices=["design", "solve", "batch", "problems"])
     ap.add_argument("--systems", type=int, default=16)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
@@ -326,6 +392,9 @@ def main():
         return
     if args.mode == "batch":
         run_batch(args)
+        return
+    if args.mode == "problems":
+        run_problems(args)
         return
     if args.impl == "reference":
         # host-only arm: rank 0 times the CPU path, other ranks exit at once

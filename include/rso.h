@@ -11,8 +11,13 @@
  *  - Pointers named *_dev are CUDA device pointers owned by the caller and
  *    borrowed for the duration of the call; *_host are host pointers.
  *  - Every call returns rso_status and never aborts; rso_last_error() gives a
- *    message.  Calls on one handle are ordered on the handle's stream; handles
- *    are not thread-safe, distinct handles are independent.
+ *    message.  Calls on one handle are ordered on the handle's stream (its
+ *    own non-blocking stream unless rso_set_stream binds another): device
+ *    inputs written on a different stream must be complete (synchronised, or
+ *    ordered by an event) before the call.  Handles are not thread-safe;
+ *    distinct handles are independent and may be used from different host
+ *    threads at once, provided the live handles on one device share the
+ *    same Young's modulus and Poisson ratio (rso_create refuses otherwise).
  *  - Dirichlet (support) DOFs are homogeneous: entries of f and u at support
  *    nodes are ignored on input and returned as zero.
  *

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <mutex>
 
 using namespace rso;
 
@@ -245,6 +246,39 @@ static rso_status setup(rso_handle* h, int ex, int ey, int ez, const uint8_t* em
 
 static thread_local std::string g_create_err;
 
+// K0 and its sum/difference blocks live in per-device constant memory, shared
+// by every handle on the device: live handles on one device must agree on
+// (E, nu).  Registry of the material of the live handles per device.
+namespace {
+std::mutex g_mat_mu;
+struct DevMaterial { double E = 0, nu = 0; int live = 0; };
+DevMaterial g_mat[64];
+}  // namespace
+
+static rso_status claim_material(rso_handle* h) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { g_create_err = "no CUDA device"; return RSO_ERR_CUDA; }
+  std::lock_guard<std::mutex> lock(g_mat_mu);
+  DevMaterial& m = g_mat[dev];
+  if (m.live > 0 && (m.E != h->cfg.youngs_modulus || m.nu != h->cfg.poisson_ratio)) {
+    g_create_err = "another live handle on this device uses a different Young's modulus or Poisson ratio "
+                   "(the element matrix is held in per-device constant memory)";
+    return RSO_ERR_UNSUPPORTED;
+  }
+  m.E = h->cfg.youngs_modulus;
+  m.nu = h->cfg.poisson_ratio;
+  m.live++;
+  h->material_dev = dev;
+  return RSO_OK;
+}
+
+static void release_material(rso_handle* h) {
+  if (h->material_dev < 0) return;
+  std::lock_guard<std::mutex> lock(g_mat_mu);
+  g_mat[h->material_dev].live--;
+  h->material_dev = -1;
+}
+
 extern "C" rso_status rso_create(const rso_config* cfg, int ex, int ey, int ez, const uint8_t* em,
                                  const uint8_t* fa, const uint8_t* la, const double* ln, rso_handle** out) {
   if (!out || !em || ex <= 0 || ey <= 0 || ez <= 0) return RSO_ERR_INVALID_ARG;
@@ -269,9 +303,14 @@ extern "C" rso_status rso_create(const rso_config* cfg, int ex, int ey, int ez, 
     delete h;
     return RSO_ERR_UNSUPPORTED;
   }
+  if (rso_status sm = claim_material(h); sm != RSO_OK) {
+    delete h;
+    return sm;
+  }
   rso_status s = setup(h, ex, ey, ez, em, fa, la, ln);
   if (s != RSO_OK) {
     g_create_err = h->err;
+    release_material(h);
     free_handle(h);
     return s;
   }
@@ -282,6 +321,7 @@ extern "C" rso_status rso_create(const rso_config* cfg, int ex, int ey, int ez, 
 extern "C" void rso_destroy(rso_handle* h) {
   if (!h) return;
   cudaStreamSynchronize(h->stream);
+  release_material(h);
   free_handle(h);
 }
 

@@ -16,6 +16,7 @@
 #include "rso_internal.cuh"
 #include <cmath>
 #include <cuda_pipeline.h>
+#include <atomic>
 
 namespace rso {
 
@@ -573,10 +574,12 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
     return RSO_ERR_INVALID_ARG;
   }
   constexpr int smem = walsh_smem_bytes<T, WTY>();
-  static bool attr = false;
-  if (!attr) {
+  // the shared-memory opt-in is per device; setting it twice from racing
+  // threads is harmless, so an atomic flag per device suffices
+  static std::atomic<bool> attr[64];
+  if (h->device < 0 || h->device >= 64 || !attr[h->device].load(std::memory_order_acquire)) {
     RSO_CHECK_CUDA(h, cudaFuncSetAttribute(k_fine_w<T, MODE, WTY>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr = true;
+    if (h->device >= 0 && h->device < 64) attr[h->device].store(true, std::memory_order_release);
   }
   if (h->prof_on) prof_begin(h, cls, (double)l.nn);
   k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega, dotp, uprev, (T)c1);

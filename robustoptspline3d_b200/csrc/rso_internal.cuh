@@ -75,6 +75,7 @@ struct rso_handle {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int device = 0;
+  int material_dev = -1;            // device whose constant-memory element matrix this handle holds
   std::vector<rso::Level> L;
   std::vector<std::vector<uint8_t>> h_emask, h_vmask;  // per level, unpadded host copies (set-up only)
   double K0[576];

@@ -143,6 +143,27 @@ SIGNATURES = {
 _lib = None
 
 
+class _StreamOrderedLib:
+    """The library seen through the torch binding: before every call, torch's
+    current CUDA stream is synchronised, so tensors produced there (fresh
+    allocations, fills, copies) are complete when the library reads them on
+    its own stream."""
+
+    def __init__(self, lib):
+        self._lib = lib
+
+    def __getattr__(self, name):
+        fn = getattr(self._lib, name)
+
+        def call(*args):
+            import torch
+            if torch.cuda.is_initialized():
+                torch.cuda.current_stream().synchronize()
+            return fn(*args)
+
+        return call
+
+
 def load_library():
     """Load librso.so; raises if it has not been built (no CPU fallback exists)."""
     global _lib
@@ -251,7 +272,7 @@ class HierarchyGrid:
 
     def __init__(self, emask, fixed_area, load_area, load_normals=None, config=None):
         import torch  # noqa: F401  (CUDA context / allocator)
-        self.lib = load_library()
+        self.lib = _StreamOrderedLib(load_library())
         self.cfg = config or Config()
         emask = np.ascontiguousarray(emask, dtype=np.uint8)
         self.ez, self.ey, self.ex = emask.shape
@@ -615,7 +636,7 @@ class MMA:
     """MMA::mma_t (optimization/mma_t.h:159) on the device in FP64."""
 
     def __init__(self, n, m, xmin, xmax):
-        self.lib = load_library()
+        self.lib = _StreamOrderedLib(load_library())
         self.n, self.m = n, m
         lo = np.broadcast_to(np.asarray(xmin, np.float64), (n,)).copy()
         hi = np.broadcast_to(np.asarray(xmax, np.float64), (n,)).copy()

@@ -149,6 +149,15 @@ rso_status rso_update_operators(rso_handle* h);
 rso_status rso_apply_K(rso_handle* h, const double* u_dev, double* f_dev);
 /* r = f - K u; Grid::update_residual (grid/Grid.cu:2463-2497) */
 rso_status rso_residual(rso_handle* h, const double* u_dev, const double* f_dev, double* r_dev);
+/* One sweep of the FP32 fine-level kernel that the mixed-precision V-cycle
+ * runs (no counterpart in the reference, whose V-cycle is FP64 only; the
+ * operator is update_residual_OTFA_WS_kernel grid/Grid.cu:2320-2376): the
+ * FP64 inputs are rounded to FP32, op 0 gives r = f - K u, op 1 K u (support
+ * rows pass u; f may be NULL), op 2 the damped block-Jacobi / Chebyshev step
+ * u + c1 (u - uprev) + omega D^-1 (f - K u) (uprev NULL reads as zero); the
+ * FP32 result comes back widened to FP64. */
+rso_status rso_fine_sweep_fp32(rso_handle* h, int op, const double* u_dev, const double* f_dev,
+                               const double* uprev_dev, double omega, double c1, double* out_dev);
 /* coarse-level stencil (243 x Nn_level doubles, [d][row][col][node]); rxStencil */
 rso_status rso_get_stencil(rso_handle* h, int level, double* out_dev);
 /* coarse residual on stored stencils; update_residual_kernel_1 (grid/Grid.cu:2169-2267) */

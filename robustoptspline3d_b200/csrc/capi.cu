@@ -406,6 +406,35 @@ extern "C" rso_status rso_residual(rso_handle* h, const double* u, const double*
   return RSO_OK;
 }
 
+extern "C" rso_status rso_fine_sweep_fp32(rso_handle* h, int op, const double* u, const double* f,
+                                          const double* uprev, double omega, double c1, double* out) {
+  if (!h || !u || !out || op < 0 || op > 2 || (op != 1 && !f)) return RSO_ERR_INVALID_ARG;
+  Level& l0 = h->L[0];
+  const long long n3 = 3 * l0.NP;
+  RSO_TRY(pad_nodes(h, 0, u, l0.u64));
+  RSO_TRY(zero_support(h, l0.u64));
+  RSO_TRY(to_f32(h, l0.u64, l0.u32, n3));
+  if (f) {
+    RSO_TRY(pad_nodes(h, 0, f, l0.f64));
+    RSO_TRY(zero_support(h, l0.f64));
+    RSO_TRY(to_f32(h, l0.f64, l0.f32, n3));
+  }
+  const float* up = nullptr;
+  if (uprev && op == 2) {
+    RSO_TRY(pad_nodes(h, 0, uprev, l0.t64));
+    RSO_TRY(zero_support(h, l0.t64));
+    RSO_TRY(to_f32(h, l0.t64, l0.t32, n3));
+    up = l0.t32;
+  }
+  if (op == 0) RSO_TRY(fine_residual<float>(h, l0.u32, l0.f32, l0.r32, h->rp32));
+  else if (op == 1) RSO_TRY(fine_applyK<float>(h, l0.u32, l0.r32, h->rp32));
+  else RSO_TRY(fine_jacobi<float>(h, l0.u32, l0.f32, l0.r32, h->rp32, omega, up, c1));
+  RSO_TRY(to_f64(h, l0.r32, l0.r64, n3));
+  RSO_TRY(unpad_nodes(h, 0, l0.r64, out));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  return RSO_OK;
+}
+
 __global__ void k_unpad_planes(Level L, const double* __restrict__ pad, double* __restrict__ dense, int planes) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= L.nn) return;

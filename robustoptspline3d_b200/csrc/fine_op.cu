@@ -72,6 +72,8 @@ __constant__ double cBd[72];  // [c][i][j]
 __constant__ float cBf[72];
 __constant__ double cD0d[9];  // diagonal 3x3 block of local node 0
 __constant__ float cD0f[9];
+__constant__ float2 cBp[72];  // cBf entries duplicated into both lanes (packed FP32 kernel)
+__constant__ float2 cD0p[9];
 
 template <typename T>
 __device__ __forceinline__ T bw(int i);
@@ -142,6 +144,11 @@ rso_status upload_walsh(rso_handle* h) {
   RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cBf, Bf, sizeof(Bf), 0, cudaMemcpyHostToDevice, h->stream));
   RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cD0d, D0, sizeof(D0), 0, cudaMemcpyHostToDevice, h->stream));
   RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cD0f, Df, sizeof(Df), 0, cudaMemcpyHostToDevice, h->stream));
+  float2 Bp[72], Dp[9];
+  for (int i = 0; i < 72; i++) Bp[i] = make_float2(Bf[i], Bf[i]);
+  for (int i = 0; i < 9; i++) Dp[i] = make_float2(Df[i], Df[i]);
+  RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cBp, Bp, sizeof(Bp), 0, cudaMemcpyHostToDevice, h->stream));
+  RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cD0p, Dp, sizeof(Dp), 0, cudaMemcpyHostToDevice, h->stream));
   // the host copies are stack arrays: finish the copies before returning
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   return RSO_OK;
@@ -437,6 +444,301 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
   __pipeline_wait_prior(0);
 }
 
+// ---------------------------------------------------------------- FP32 kernel on packed pairs
+//
+// The same operator as k_fine_w for FP32, with two element columns per
+// thread: column A = (ex, ey) and column B = (ex, ey + 1).  Every addition and
+// multiplication of the two columns is the same, so they run as one packed
+// FP32x2 instruction on B200 (add/sub/mul/fma .f32x2), which halves the
+// issue slots of the arithmetic; the staging, indexing and loop overhead is
+// shared by both columns.  A thread emits the nodes (ex + 1, ey + 1) and
+// (ex + 1, ey + 2).
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 p_sub(float2 a, float2 b) {
+  unsigned long long r;
+  const unsigned long long x = *reinterpret_cast<const unsigned long long*>(&a);
+  const unsigned long long y = *reinterpret_cast<const unsigned long long*>(&b);
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(x), "l"(y));
+  return *reinterpret_cast<const float2*>(&r);
+}
+
+template <int TYP>
+constexpr int pair_smem_bytes() {
+  // slots: u plane (3 comps x (2 TYP + 1) rows) + rho layer (2 TYP rows);
+  // exchange: [2][4 values][3 comps][32 TYP]
+  return 4 * (WNSLOT * (3 * 36 * (2 * TYP + 1) + 36 * 2 * TYP) + 2 * 12 * 32 * TYP);
+}
+
+template <int MODE, int TYP>
+__global__ void __launch_bounds__(32 * TYP, 3)
+    k_fine_p(const Level L, const float* __restrict__ u, const float* __restrict__ f, float* __restrict__ out,
+             const float* __restrict__ rp, float omega, double* __restrict__ dotp, const float* __restrict__ uprev,
+             float c1) {
+  constexpr int RX = 36, ROWS = 2 * TYP, NPL = RX * (ROWS + 1), NT = WTX * TYP, SLOT = 3 * NPL + RX * ROWS;
+  constexpr int CPR = RX / 4;  // 16-byte chunks per staged row
+  constexpr int NCH = (3 * (ROWS + 1) + ROWS) * CPR, KC = (NCH + NT - 1) / NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* ss = reinterpret_cast<float*>(smem_raw);  // [WNSLOT][SLOT]
+  float* sx = ss + WNSLOT * SLOT;                  // [2][4][3][NT] corner exchange, by plane parity
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * WTX + tx;
+  const int x0 = blockIdx.x * (WTX - 1), y0 = blockIdx.y * (ROWS - 1);
+  const int nzc = (L.nz + FZC - 1) / FZC, bsys = blockIdx.z / nzc;
+  const int z0 = (blockIdx.z - bsys * nzc) * FZC, z1 = min(z0 + FZC, L.nz);
+  {
+    const long long off = (long long)bsys * 3 * L.NP;
+    u += off;
+    f += off;
+    out += off;
+    if (uprev != nullptr) uprev += off;
+  }
+  const int ex = x0 - 1 + tx, ey = y0 - 1 + 2 * ty;
+  const int NP = (int)L.NP, px = L.px;  // 3 NP < 2^31 (checked by the launcher)
+  const int xs = x0 & ~3, ox = x0 - xs;
+
+  int goff[KC], soff[KC];
+  bool isr[KC];
+#pragma unroll
+  for (int kk = 0; kk < KC; kk++) {
+    const int k = tid + kk * NT;
+    const int row = k / CPR, j = k - row * CPR, xg = xs + j * 4;
+    goff[kk] = -1;
+    soff[kk] = -1;
+    isr[kk] = false;
+    if (k < NCH) {
+      if (row < 3 * (ROWS + 1)) {
+        const int c = row / (ROWS + 1), yr = row - c * (ROWS + 1), gyp = y0 + yr;
+        soff[kk] = c * NPL + yr * RX + j * 4;
+        if (gyp <= L.py - 1 && xg + 4 <= L.px) goff[kk] = c * NP + gyp * L.px + xg;
+      } else {
+        const int yr = row - 3 * (ROWS + 1), gyp = y0 + yr;
+        isr[kk] = true;
+        soff[kk] = 3 * NPL + yr * RX + j * 4;
+        if (gyp <= L.qy - 1 && xg + 4 <= L.qx) goff[kk] = gyp * L.qx + xg;
+      }
+    }
+  }
+  const long long pxy = (long long)L.px * L.py, qxy = (long long)L.qx * L.qy;
+  auto issue = [&](int s) {
+    float* dst = ss + ((s + WNSLOT) % WNSLOT) * SLOT;
+    const long long po = pxy * (s + 1), qo = qxy * (s + 1);
+#pragma unroll
+    for (int kk = 0; kk < KC; kk++) {
+      if (soff[kk] < 0) continue;
+      const bool ok = goff[kk] >= 0 && (isr[kk] ? s <= L.ez : s <= L.nz);
+      if (ok)
+        __pipeline_memcpy_async(dst + soff[kk], isr[kk] ? rp + qo + goff[kk] : u + po + goff[kk], 16);
+      else
+        *reinterpret_cast<float4*>(dst + soff[kk]) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __pipeline_commit();
+  };
+  // xy modes of the face nodes of both columns on a staged plane (lane 0:
+  // column A, lane 1: column B), and u at the two emitted nodes
+  auto face = [&](const float* pl, float2 (&F)[4][3], float2 (&own)[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float* p = pl + c * NPL + 2 * ty * RX + tx + ox;
+      const float2 q00 = make_float2(p[0], p[RX]), q10 = make_float2(p[1], p[RX + 1]);
+      const float2 q01 = make_float2(p[RX], p[2 * RX]), q11 = make_float2(p[RX + 1], p[2 * RX + 1]);
+      const float2 s0 = p_add(q00, q10), d0 = p_sub(q10, q00), s1 = p_add(q01, q11), d1 = p_sub(q11, q01);
+      F[0][c] = p_add(s0, s1);
+      F[1][c] = p_add(d0, d1);
+      F[2][c] = p_sub(s1, s0);
+      F[3][c] = p_sub(d1, d0);
+      own[c] = q11;
+    }
+  };
+
+  for (int s = z0 - 1; s <= z0 - 1 + WPD; s++) issue(s);
+  __pipeline_wait_prior(WPD);
+  __syncthreads();
+  const bool wA = tx < WTX - 1 && ex + 1 < L.nx && ey + 1 < L.ny;
+  const bool wB = wA && ty < TYP - 1 && ey + 2 < L.ny;
+  const float2 zero2 = make_float2(0.f, 0.f);
+  float2 F[4][3], Gt[4][3], uc[3], uo[3], own[3], fo[3], po[3], ra[4], rb[4];
+  uint8_t clA = 0, clB = 0;
+  double pq = 0;
+  face(ss + ((z0 - 1 + WNSLOT) % WNSLOT) * SLOT, F, uc);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    Gt[q][0] = Gt[q][1] = Gt[q][2] = zero2;
+    ra[q] = rb[q] = zero2;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) uo[c] = own[c] = fo[c] = po[c] = zero2;
+
+  auto emit = [&](int zo, const float* xb) {
+    if (!wA) return;
+    float2 acc[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      acc[c] = p_add(own[c], make_float2(xb[(0 * 3 + c) * NT + tid + 1], xb[(1 * 3 + c) * NT + tid + 1]));
+      if (wB) acc[c].y += xb[(2 * 3 + c) * NT + tid + WTX] + xb[(3 * 3 + c) * NT + tid + WTX + 1];
+    }
+    const int n = (int)L.nidx(ex + 1, ey + 1, zo);
+    const bool workA = (clA & NC_ACTIVE) && !(clA & NC_SUPPORT);
+    const bool workB = (clB & NC_ACTIVE) && !(clB & NC_SUPPORT);
+    float2 res[3];
+    if (MODE == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+        res[c] = make_float2(fo[c].x - (workA ? acc[c].x : 0.f), fo[c].y - (workB ? acc[c].y : 0.f));
+    } else if (MODE == 1) {
+      const bool passA = (clA & NC_SUPPORT) != 0, passB = (clB & NC_SUPPORT) != 0;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        res[c] = make_float2(passA ? uo[c].x : (workA ? acc[c].x : 0.f), passB ? uo[c].y : (workB ? acc[c].y : 0.f));
+        pq += (double)uo[c].x * (double)res[c].x;
+        if (wB) pq += (double)uo[c].y * (double)res[c].y;
+      }
+    } else {
+      // diagonal block from rho^p of the 4 columns around each node in the
+      // layers below (ra) and above (rb), as in k_fine_w
+      const float2 R = p_add(p_add(p_add(ra[0], ra[1]), p_add(ra[2], ra[3])), p_add(p_add(rb[0], rb[1]), p_add(rb[2], rb[3])));
+      const float2 pxy_ = p_add(p_sub(p_add(ra[0], ra[3]), p_add(ra[1], ra[2])), p_sub(p_add(rb[0], rb[3]), p_add(rb[1], rb[2])));
+      const float2 xlo = p_sub(p_add(ra[1], ra[3]), p_add(ra[0], ra[2])), xhi = p_sub(p_add(rb[1], rb[3]), p_add(rb[0], rb[2]));
+      const float2 ylo = p_sub(p_add(ra[2], ra[3]), p_add(ra[0], ra[1])), yhi = p_sub(p_add(rb[2], rb[3]), p_add(rb[0], rb[1]));
+      const float2 pxz = p_sub(xhi, xlo), pyz = p_sub(yhi, ylo);
+      const float2 a = p_mul(cD0p[0], R), b = p_mul(cD0p[1], pxy_), cc = p_mul(cD0p[2], pxz);
+      const float2 d = p_mul(cD0p[4], R), e = p_mul(cD0p[5], pyz), g = p_mul(cD0p[8], R);
+      const float2 r0 = p_sub(fo[0], acc[0]), r1 = p_sub(fo[1], acc[1]), r2 = p_sub(fo[2], acc[2]);
+      const float2 A = p_sub(p_mul(d, g), p_mul(e, e)), B = p_sub(p_mul(cc, e), p_mul(b, g));
+      const float2 C = p_sub(p_mul(b, e), p_mul(cc, d));
+      const float2 det = p_fma(a, A, p_fma(b, B, p_mul(cc, C)));
+      const float2 id = make_float2(__fdividef(omega, det.x), __fdividef(omega, det.y));
+      const float2 E = p_sub(p_mul(a, g), p_mul(cc, cc)), Fm = p_sub(p_mul(b, cc), p_mul(a, e));
+      const float2 I = p_sub(p_mul(a, d), p_mul(b, b));
+      const float2 cc1 = make_float2(c1, c1);
+      float2 dl[3];
+      dl[0] = p_fma(A, r0, p_fma(B, r1, p_mul(C, r2)));
+      dl[1] = p_fma(B, r0, p_fma(E, r1, p_mul(Fm, r2)));
+      dl[2] = p_fma(C, r0, p_fma(Fm, r1, p_mul(I, r2)));
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const float2 v = p_fma(id, dl[c], p_fma(cc1, p_sub(uo[c], po[c]), uo[c]));
+        res[c] = make_float2(workA ? v.x : 0.f, workB ? v.y : 0.f);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      out[n + c * NP] = res[c].x;
+      if (wB) out[n + px + c * NP] = res[c].y;
+    }
+  };
+
+  for (int z = z0 - 1; z < z1; z++) {
+    __pipeline_wait_prior(WPD - 1);
+    __syncthreads();
+    issue(z + 1 + WPD);
+    if (z - 1 >= z0) emit(z - 1, sx + ((z - 1) & 1) * 12 * NT);
+    if (wA && z >= z0) {
+      const int n = (int)L.nidx(ex + 1, ey + 1, z);
+      clA = L.vclass[n];
+      if (wB) clB = L.vclass[n + px];
+      if (MODE != 1) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) fo[c] = make_float2(f[n + c * NP], wB ? f[n + px + c * NP] : 0.f);
+        if (MODE == 2 && uprev != nullptr) {
+#pragma unroll
+          for (int c = 0; c < 3; c++) po[c] = make_float2(uprev[n + c * NP], wB ? uprev[n + px + c * NP] : 0.f);
+        }
+      }
+    }
+    const float* su = ss + ((z + 1 + WNSLOT) % WNSLOT) * SLOT;
+    const float* sr = ss + ((z + WNSLOT) % WNSLOT) * SLOT + 3 * NPL;
+    float2 v[8][3], un[3];
+    {
+      float2 Fn[4][3];
+      face(su, Fn, un);
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          v[q][c] = p_add(F[q][c], Fn[q][c]);
+          v[q + 4][c] = p_sub(Fn[q][c], F[q][c]);
+          F[q][c] = Fn[q][c];
+        }
+    }
+    const int ri = 2 * ty * RX + tx + ox;
+    const float2 re = make_float2(sr[ri], sr[ri + RX]);
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      float2 in[3], o[3];
+#pragma unroll
+      for (int j = 0; j < 3; j++) in[j] = v[c ^ (1 << j)][j];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        float2 s = zero2;
+        bool first = true;
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+          if (!b_zero(c, i, j)) {
+            s = first ? p_mul(cBp[c * 9 + i * 3 + j], in[j]) : p_fma(cBp[c * 9 + i * 3 + j], in[j], s);
+            first = false;
+          }
+        o[i] = p_mul(s, re);
+      }
+#pragma unroll
+      for (int i = 0; i < 3; i++) v[c ^ (1 << i)][i] = o[i];
+    }
+    if (MODE == 2) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) ra[q] = rb[q];
+      rb[0] = re;
+      // lane 1 reads row 2 ty + 2, which exists for ty < TYP - 1 only
+      rb[1] = make_float2(sr[ri + 1], sr[ri + RX + 1]);
+      rb[2] = make_float2(sr[ri + RX], wB ? sr[ri + 2 * RX] : 0.f);
+      rb[3] = make_float2(sr[ri + RX + 1], wB ? sr[ri + 2 * RX + 1] : 0.f);
+    }
+    float2 tot[4][3];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        tot[q][c] = p_add(Gt[q][c], p_sub(v[q][c], v[q + 4][c]));
+        Gt[q][c] = p_add(v[q][c], v[q + 4][c]);
+      }
+    if (z >= z0) {
+      float* xb = sx + (z & 1) * 12 * NT;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const float2 e0 = p_sub(tot[0][c], tot[1][c]), e1 = p_add(tot[0][c], tot[1][c]);
+        const float2 g0 = p_sub(tot[2][c], tot[3][c]), g1 = p_add(tot[2][c], tot[3][c]);
+        const float2 c00 = p_sub(e0, g0), c10 = p_sub(e1, g1), c01 = p_add(e0, g0), c11 = p_add(e1, g1);
+        xb[(0 * 3 + c) * NT + tid] = c01.x + c00.y;  // A (0,1) + B (0,0): node (ex, ey + 1)
+        xb[(1 * 3 + c) * NT + tid] = c01.y;          // B (0,1): node (ex, ey + 2)
+        xb[(2 * 3 + c) * NT + tid] = c10.x;          // A (1,0): node (ex + 1, ey)
+        xb[(3 * 3 + c) * NT + tid] = c00.x;          // A (0,0): node (ex, ey)
+        own[c] = make_float2(c11.x + c10.y, c11.y);  // nodes (ex + 1, ey + 1), (ex + 1, ey + 2)
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      uo[c] = uc[c];
+      uc[c] = un[c];
+    }
+  }
+  __syncthreads();
+  emit(z1 - 1, sx + ((z1 - 1) & 1) * 12 * NT);
+  if (MODE == 1 && dotp != nullptr) {
+    __shared__ double sred[TYP];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pq += __shfl_down_sync(0xffffffffu, pq, o);
+    if (tx == 0) sred[ty] = pq;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0;
+#pragma unroll
+      for (int w = 0; w < TYP; w++) t += sred[w];
+      dotp[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * (blockIdx.z - bsys * nzc)) +
+           (long long)bsys * gridDim.x * gridDim.y * nzc] = t;
+    }
+  }
+  __pipeline_wait_prior(0);
+}
+
 // damped Jacobi from a zero iterate: out = omega D^-1 f (no neighbour reads)
 template <typename T>
 __global__ void __launch_bounds__(256) k_fine_jacobi0(const Level L, const T* __restrict__ f, T* __restrict__ out,
@@ -556,6 +858,10 @@ constexpr int WTY = 8;
 static inline dim3 march_grid(const Level& l) {
   return dim3(cdiv(l.nx, WTX - 1), cdiv(l.ny, WTY - 1), cdiv(l.nz, FZC) * l.nb);
 }
+constexpr int PTY = 4;  // thread rows of the packed FP32 kernel (2 PTY element rows)
+static inline dim3 pair_grid(const Level& l) {
+  return dim3(cdiv(l.nx, WTX - 1), cdiv(l.ny, 2 * PTY - 1), cdiv(l.nz, FZC) * l.nb);
+}
 
 template <typename T>
 static inline int pcls(int c32, int c64) { return sizeof(T) == 4 ? c32 : c64; }
@@ -573,16 +879,25 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
     h->err = "fine operator inputs must be 16-byte aligned";
     return RSO_ERR_INVALID_ARG;
   }
-  constexpr int smem = walsh_smem_bytes<T, WTY>();
+  // FP32: two columns per thread on packed pairs; FP64: one column per thread
+  constexpr bool packed = sizeof(T) == 4;
+  constexpr int smem = packed ? pair_smem_bytes<PTY>() : walsh_smem_bytes<T, WTY>();
+  void (*kern)(const Level, const T*, const T*, T*, const T*, T, double*, const T*, T);
+  if constexpr (packed)
+    kern = k_fine_p<MODE, PTY>;
+  else
+    kern = k_fine_w<T, MODE, WTY>;
   // the shared-memory opt-in is per device; setting it twice from racing
   // threads is harmless, so an atomic flag per device suffices
   static std::atomic<bool> attr[64];
   if (h->device < 0 || h->device >= 64 || !attr[h->device].load(std::memory_order_acquire)) {
-    RSO_CHECK_CUDA(h, cudaFuncSetAttribute(k_fine_w<T, MODE, WTY>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    RSO_CHECK_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     if (h->device >= 0 && h->device < 64) attr[h->device].store(true, std::memory_order_release);
   }
+  const dim3 grid = packed ? pair_grid(l) : march_grid(l);
+  const dim3 block = packed ? dim3(WTX, PTY) : dim3(WTX, WTY);
   if (h->prof_on) prof_begin(h, cls, (double)l.nn);
-  k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega, dotp, uprev, (T)c1);
+  kern<<<grid, block, smem, h->stream>>>(l, u, f, out, rp, (T)omega, dotp, uprev, (T)c1);
   rso::note_launch();
   if (h->prof_on) prof_end(h, cls);
   return launch_check(h, what);

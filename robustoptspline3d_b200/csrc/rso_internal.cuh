@@ -198,6 +198,8 @@ rso_status unpad_nodes(rso_handle* h, int level, const double* padded, double* d
 rso_status pad_elems_f(rso_handle* h, const float* dense, float* padded);
 rso_status unpad_elems_f(rso_handle* h, const float* padded, float* dense);
 rso_status zero_support(rso_handle* h, double* padded);
+rso_status to_f32(rso_handle* h, const double* a, float* b, long long n);
+rso_status to_f64(rso_handle* h, const float* a, double* b, long long n);
 
 // topology (topology.cu)
 Level make_level(int ex, int ey, int ez, int factor);

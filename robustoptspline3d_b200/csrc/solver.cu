@@ -150,6 +150,15 @@ __global__ void k_f2d(const float* __restrict__ a, double* __restrict__ b, long 
   if (i < n) b[i] = (double)a[i];
 }
 
+rso_status to_f32(rso_handle* h, const double* a, float* b, long long n) {
+  k_d2f<<<cdiv(n, 256), 256, 0, h->stream>>>(a, b, n); rso::note_launch();
+  return launch_check(h, "to_f32");
+}
+rso_status to_f64(rso_handle* h, const float* a, double* b, long long n) {
+  k_f2d<<<cdiv(n, 256), 256, 0, h->stream>>>(a, b, n); rso::note_launch();
+  return launch_check(h, "to_f64");
+}
+
 // z = M r: one V-cycle from a zero iterate (FP32 in mixed precision)
 rso_status precondition(rso_handle* h, const double* r, double* z) {
   Level& l0 = h->L[0];

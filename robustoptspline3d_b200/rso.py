@@ -92,6 +92,7 @@ SIGNATURES = {
     "rso_update_operators": (_ci, [_vp]),
     "rso_apply_K": (_ci, [_vp, _vp, _vp]),
     "rso_residual": (_ci, [_vp, _vp, _vp, _vp]),
+    "rso_fine_sweep_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
     "rso_get_stencil": (_ci, [_vp, _ci, _vp]),
     "rso_coarse_residual": (_ci, [_vp, _ci, _vp, _vp, _vp]),
     "rso_smooth": (_ci, [_vp, _ci, _vp, _vp, _ci, _cd, _ci, _ci]),
@@ -383,6 +384,16 @@ class HierarchyGrid:
         r = torch.empty_like(u)
         self._chk(self.lib.rso_residual(self.h, _dev(u, torch.float64), _dev(f, torch.float64), _dev(r)), "rso_residual")
         return r
+
+    def fine_sweep_fp32(self, op, u, f=None, uprev=None, omega=1.0, c1=0.0):
+        """One FP32 fine-level sweep (op 0 residual, 1 K u, 2 Jacobi/Chebyshev step), FP64 in and out."""
+        import torch
+        out = torch.empty_like(u)
+        self._chk(self.lib.rso_fine_sweep_fp32(self.h, op, _dev(u, torch.float64),
+                                               None if f is None else _dev(f, torch.float64),
+                                               None if uprev is None else _dev(uprev, torch.float64),
+                                               omega, c1, _dev(out)), "rso_fine_sweep_fp32")
+        return out
 
     def stencil(self, level):
         import torch

@@ -85,6 +85,32 @@ def test_operator_fp64(oracle, cuda, gen):
     assert rel(r_g, r_o) < 1e-13
 
 
+@pytest.mark.parametrize("gen", [lambda: P.ellipsoid(24, 16, 12), lambda: P.voids_box(20, 12, 12, 3),
+                                 lambda: P.cantilever(40, 30, 36)])
+def test_operator_fp32(oracle, cuda, gen):
+    """FP32 fine kernels of the mixed V-cycle (residual, K u, Jacobi and Chebyshev steps) against the
+    FP64 oracle.  Tolerance 2e-5 relative in norm: the inputs are rounded to FP32 and the element
+    products accumulate in FP32.  The 41 x 31 x 37-node cantilever spans two tiles in x, a ragged
+    last tile in y and two z chunks."""
+    prob = gen()
+    g, o = make(oracle, prob)
+    rng = np.random.default_rng(15)
+    cls = o.node_class()
+    fix = np.tile((cls & 4) > 0, 3) | np.tile((cls & 1) == 0, 3)
+    u, f, up = (rng.standard_normal(3 * o.nn) for _ in range(3))
+    u[fix] = 0
+    f[fix] = 0
+    up[fix] = 0
+    tol = 2e-5
+    assert rel(g.fine_sweep_fp32(1, t(u, cuda)).cpu().numpy(), o.apply_K(u)) < tol
+    assert rel(g.fine_sweep_fp32(0, t(u, cuda), t(f, cuda)).cpu().numpy(), o.residual(u, f)) < tol
+    om, c1 = 0.3, 0.7
+    jac = o.smooth(0, u, f, kind=1, omega=om, sweeps=1)
+    assert rel(g.fine_sweep_fp32(2, t(u, cuda), t(f, cuda), omega=om).cpu().numpy(), jac) < tol
+    cheb = g.fine_sweep_fp32(2, t(u, cuda), t(f, cuda), t(up, cuda), omega=om, c1=c1).cpu().numpy()
+    assert rel(cheb, jac + c1 * (u - up)) < tol
+
+
 @pytest.mark.parametrize("gen,nl,ff", [(lambda: P.ellipsoid(40, 24, 24), 0, 4),
                                        (lambda: P.ellipsoid(24, 16, 12), 0, 4),
                                        (lambda: P.cantilever(16, 8, 8), 3, 2)])

@@ -318,6 +318,7 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
     if (rel[b] >= tol && fn[b] > 0) status = RSO_ERR_BUDGET_EXCEEDED;
   }
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  RSO_TRY(fine_stage_check(h));
   const double ms = now_ms() - t0;
   if (infos)
     for (int b = 0; b < k; b++) { infos[b].iterations = it[b]; infos[b].rel_res = rel[b]; infos[b].ms = ms; }

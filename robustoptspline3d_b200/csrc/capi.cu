@@ -432,7 +432,7 @@ extern "C" rso_status rso_fine_sweep_fp32(rso_handle* h, int op, const double* u
   RSO_TRY(to_f64(h, l0.r32, l0.r64, n3));
   RSO_TRY(unpad_nodes(h, 0, l0.r64, out));
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
-  return RSO_OK;
+  return fine_stage_check(h);
 }
 
 __global__ void k_unpad_planes(Level L, const double* __restrict__ pad, double* __restrict__ dense, int planes) {

@@ -1073,7 +1073,7 @@ rso_status estimate_lambda(rso_handle* h) {
     l.lam = 1.05 * lam;
     if (h->L.size() == 1) break;
   }
-  return RSO_OK;
+  return fine_stage_check(h);
 }
 
 template rso_status coarse_residual<double>(rso_handle*, int, const double*, const double*, double*);

@@ -15,8 +15,11 @@
 // the first Jacobi sweep from a zero iterate use K0 directly.
 #include "rso_internal.cuh"
 #include <cmath>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_pipeline.h>
 #include <atomic>
+#include <mutex>
 
 namespace rso {
 
@@ -464,23 +467,86 @@ __device__ __forceinline__ float2 p_sub(float2 a, float2 b) {
   return *reinterpret_cast<const float2*>(&r);
 }
 
-template <int TYP>
-constexpr int pair_smem_bytes() {
-  // slots: u plane (3 comps x (2 TYP + 1) rows) + rho layer (2 TYP rows);
-  // exchange: [2][4 values][3 comps][32 TYP]
-  return 4 * (WNSLOT * (3 * 36 * (2 * TYP + 1) + 36 * 2 * TYP) + 2 * 12 * 32 * TYP);
+constexpr int kPairMinBlocksRes = 4, kPairMinBlocksJac = 3;
+
+// Bulk-tensor staging (TMA): one thread issues the copies of a stage, their
+// completion is tracked by an mbarrier per slot.  Every wait is bounded: after
+// kStageTries polls it gives up, counts the event in g_stage_timeouts (read and
+// reported as an error by the host after the solve) and lets the kernel run
+// on, all of its accesses staying in bounds.
+__device__ unsigned int g_stage_timeouts;
+constexpr int kStageTries = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+  for (int i = 0; i < kStageTries; i++)
+    if (mbar_test(b, parity)) return true;
+  atomicAdd(&g_stage_timeouts, 1u);
+  return false;
+}
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* m, int x, int y, int z, int w, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(m)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* m, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(m)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
 }
 
-template <int MODE, int TYP>
-__global__ void __launch_bounds__(32 * TYP, 3)
+// Slot layout of the packed kernel (floats): the u plane (3 comps x (2 TYP + 1)
+// rows of 36) at 0, the rho^p layer (2 TYP rows of 36) at pair_rho_off, each
+// part starting on 128 bytes as bulk-tensor copies require.
+template <int TYP>
+constexpr int pair_rho_off() { return (3 * 36 * (2 * TYP + 1) + 31) / 32 * 32; }
+template <int TYP>
+constexpr int pair_slot() { return pair_rho_off<TYP>() + (36 * 2 * TYP + 31) / 32 * 32; }
+template <int TYP>
+constexpr int pair_smem_bytes() {
+  // slots + corner exchange [2][4 values][3 comps][32 TYP] + 128 bytes to
+  // round the base up to a 128-byte boundary
+  return 4 * (WNSLOT * pair_slot<TYP>() + 2 * 12 * 32 * TYP) + 128;
+}
+
+// resident CTAs per SM the register budget is cut for: the residual fits 128
+// registers without spills, the Jacobi / Chebyshev step does not
+constexpr int pair_min_blocks(int mode) { return mode == 0 ? kPairMinBlocksRes : kPairMinBlocksJac; }
+
+// TMA: stage u planes and rho^p layers with bulk-tensor copies (tmu: 4-D map
+// (px, py, pz, 3 nb) of u, box 36 x (2 TYP + 1) x 1 x 3; tmr: 3-D map
+// (qx, qy, qz) of rho^p, box 36 x 2 TYP x 1; out-of-range boxes read zero);
+// otherwise every thread stages 16-byte chunks with cp.async.
+template <int MODE, int TYP, bool TMA>
+__global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE))
     k_fine_p(const Level L, const float* __restrict__ u, const float* __restrict__ f, float* __restrict__ out,
              const float* __restrict__ rp, float omega, double* __restrict__ dotp, const float* __restrict__ uprev,
-             float c1) {
-  constexpr int RX = 36, ROWS = 2 * TYP, NPL = RX * (ROWS + 1), NT = WTX * TYP, SLOT = 3 * NPL + RX * ROWS;
+             float c1, const __grid_constant__ CUtensorMap tmu, const __grid_constant__ CUtensorMap tmr) {
+  constexpr int RX = 36, ROWS = 2 * TYP, NPL = RX * (ROWS + 1), NT = WTX * TYP;
+  constexpr int RHO = pair_rho_off<TYP>(), SLOT = pair_slot<TYP>();
+  constexpr uint32_t STAGE_BYTES = sizeof(float) * (3 * NPL + RX * ROWS);  // both boxes of a stage
   constexpr int CPR = RX / 4;  // 16-byte chunks per staged row
   constexpr int NCH = (3 * (ROWS + 1) + ROWS) * CPR, KC = (NCH + NT - 1) / NT;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float* ss = reinterpret_cast<float*>(smem_raw);  // [WNSLOT][SLOT]
+  extern __shared__ __align__(128) unsigned char smem_pair[];
+  // slots start on a 128-byte shared-memory address whatever the base
+  float* ss = reinterpret_cast<float*>(smem_pair + ((128u - (smem_u32(smem_pair) & 127u)) & 127u));  // [WNSLOT][SLOT]
   float* sx = ss + WNSLOT * SLOT;                  // [2][4][3][NT] corner exchange, by plane parity
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * WTX + tx;
   const int x0 = blockIdx.x * (WTX - 1), y0 = blockIdx.y * (ROWS - 1);
@@ -497,10 +563,10 @@ __global__ void __launch_bounds__(32 * TYP, 3)
   const int NP = (int)L.NP, px = L.px;  // 3 NP < 2^31 (checked by the launcher)
   const int xs = x0 & ~3, ox = x0 - xs;
 
-  int goff[KC], soff[KC];
-  bool isr[KC];
+  int goff[TMA ? 1 : KC], soff[TMA ? 1 : KC];
+  bool isr[TMA ? 1 : KC];
 #pragma unroll
-  for (int kk = 0; kk < KC; kk++) {
+  for (int kk = 0; kk < (TMA ? 0 : KC); kk++) {
     const int k = tid + kk * NT;
     const int row = k / CPR, j = k - row * CPR, xg = xs + j * 4;
     goff[kk] = -1;
@@ -514,25 +580,42 @@ __global__ void __launch_bounds__(32 * TYP, 3)
       } else {
         const int yr = row - 3 * (ROWS + 1), gyp = y0 + yr;
         isr[kk] = true;
-        soff[kk] = 3 * NPL + yr * RX + j * 4;
+        soff[kk] = RHO + yr * RX + j * 4;
         if (gyp <= L.qy - 1 && xg + 4 <= L.qx) goff[kk] = gyp * L.qx + xg;
       }
     }
   }
   const long long pxy = (long long)L.px * L.py, qxy = (long long)L.qx * L.qy;
+  __shared__ __align__(8) uint64_t bars[WNSLOT];
+  bool gave_up = false;
+  // stage s (node plane s, element layer s) into slot (s + WNSLOT) % WNSLOT
   auto issue = [&](int s) {
     float* dst = ss + ((s + WNSLOT) % WNSLOT) * SLOT;
-    const long long po = pxy * (s + 1), qo = qxy * (s + 1);
+    if constexpr (TMA) {
+      // thread 0 only; stages past z1 are never read and not issued
+      if (s > z1) return;
+      uint64_t* bar = &bars[(s + WNSLOT) % WNSLOT];
+      mbar_expect_tx(bar, STAGE_BYTES);
+      tma_load_4d(dst, &tmu, xs, y0, s + 1, 3 * bsys, bar);
+      tma_load_3d(dst + RHO, &tmr, xs, y0, s + 1, bar);
+    } else {
+      const long long po = pxy * (s + 1), qo = qxy * (s + 1);
 #pragma unroll
-    for (int kk = 0; kk < KC; kk++) {
-      if (soff[kk] < 0) continue;
-      const bool ok = goff[kk] >= 0 && (isr[kk] ? s <= L.ez : s <= L.nz);
-      if (ok)
-        __pipeline_memcpy_async(dst + soff[kk], isr[kk] ? rp + qo + goff[kk] : u + po + goff[kk], 16);
-      else
-        *reinterpret_cast<float4*>(dst + soff[kk]) = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int kk = 0; kk < KC; kk++) {
+        if (soff[kk] < 0) continue;
+        const bool ok = goff[kk] >= 0 && (isr[kk] ? s <= L.ez : s <= L.nz);
+        if (ok)
+          __pipeline_memcpy_async(dst + soff[kk], isr[kk] ? rp + qo + goff[kk] : u + po + goff[kk], 16);
+        else
+          *reinterpret_cast<float4*>(dst + soff[kk]) = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      __pipeline_commit();
     }
-    __pipeline_commit();
+  };
+  // TMA: wait until stage s has landed (the k-th use of a slot completes phase k)
+  auto wait_stage = [&](int s) {
+    const uint32_t parity = (uint32_t)((s - (z0 - 1)) / WNSLOT) & 1u;
+    if (!mbar_wait(&bars[(s + WNSLOT) % WNSLOT], parity)) gave_up = true;
   };
   // xy modes of the face nodes of both columns on a staged plane (lane 0:
   // column A, lane 1: column B), and u at the two emitted nodes
@@ -551,9 +634,22 @@ __global__ void __launch_bounds__(32 * TYP, 3)
     }
   };
 
-  for (int s = z0 - 1; s <= z0 - 1 + WPD; s++) issue(s);
-  __pipeline_wait_prior(WPD);
-  __syncthreads();
+  if constexpr (TMA) {
+    if (tid == 0) {
+#pragma unroll
+      for (int k = 0; k < WNSLOT; k++) mbar_init(&bars[k], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0)
+      for (int s = z0 - 1; s <= z0 - 1 + WPD; s++) issue(s);
+    wait_stage(z0 - 1);
+  } else {
+    for (int s = z0 - 1; s <= z0 - 1 + WPD; s++) issue(s);
+    __pipeline_wait_prior(WPD);
+    __syncthreads();
+  }
   const bool wA = tx < WTX - 1 && ex + 1 < L.nx && ey + 1 < L.ny;
   const bool wB = wA && ty < TYP - 1 && ey + 2 < L.ny;
   const float2 zero2 = make_float2(0.f, 0.f);
@@ -629,9 +725,17 @@ __global__ void __launch_bounds__(32 * TYP, 3)
   };
 
   for (int z = z0 - 1; z < z1; z++) {
-    __pipeline_wait_prior(WPD - 1);
-    __syncthreads();
-    issue(z + 1 + WPD);
+    // stage z + 1 has landed, the corners of plane z - 1 are visible and the
+    // slot of stage z - 1 is free for refilling
+    if constexpr (TMA) {
+      wait_stage(z + 1);
+      __syncthreads();
+      if (tid == 0) issue(z + 1 + WPD);
+    } else {
+      __pipeline_wait_prior(WPD - 1);
+      __syncthreads();
+      issue(z + 1 + WPD);
+    }
     if (z - 1 >= z0) emit(z - 1, sx + ((z - 1) & 1) * 12 * NT);
     if (wA && z >= z0) {
       const int n = (int)L.nidx(ex + 1, ey + 1, z);
@@ -647,7 +751,7 @@ __global__ void __launch_bounds__(32 * TYP, 3)
       }
     }
     const float* su = ss + ((z + 1 + WNSLOT) % WNSLOT) * SLOT;
-    const float* sr = ss + ((z + WNSLOT) % WNSLOT) * SLOT + 3 * NPL;
+    const float* sr = ss + ((z + WNSLOT) % WNSLOT) * SLOT + RHO;
     float2 v[8][3], un[3];
     {
       float2 Fn[4][3];
@@ -736,7 +840,14 @@ __global__ void __launch_bounds__(32 * TYP, 3)
            (long long)bsys * gridDim.x * gridDim.y * nzc] = t;
     }
   }
-  __pipeline_wait_prior(0);
+  if constexpr (TMA) {
+    // every issued stage was waited for; after a wait that gave up, wait
+    // (bounded) once more for the copies of the last stages still in flight
+    if (gave_up)
+      for (int s = max(z0 - 1, z1 - WNSLOT + 1); s <= z1; s++) wait_stage(s);
+  } else {
+    __pipeline_wait_prior(0);
+  }
 }
 
 // damped Jacobi from a zero iterate: out = omega D^-1 f (no neighbour reads)
@@ -858,13 +969,72 @@ constexpr int WTY = 8;
 static inline dim3 march_grid(const Level& l) {
   return dim3(cdiv(l.nx, WTX - 1), cdiv(l.ny, WTY - 1), cdiv(l.nz, FZC) * l.nb);
 }
-constexpr int PTY = 4;  // thread rows of the packed FP32 kernel (2 PTY element rows)
+constexpr int PTY = 4;          // thread rows of the packed FP32 kernel (2 PTY element rows)
+constexpr bool kPairTMA = true;  // packed kernel stages with TMA (else cp.async)
 static inline dim3 pair_grid(const Level& l) {
   return dim3(cdiv(l.nx, WTX - 1), cdiv(l.ny, 2 * PTY - 1), cdiv(l.nz, FZC) * l.nb);
 }
 
 template <typename T>
 static inline int pcls(int c32, int c64) { return sizeof(T) == 4 ? c32 : c64; }
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// tensor maps of the packed kernel's staged arrays: u as (px, py, pz, 3 nb)
+// with a 36 x (rows + 1) x 1 x 3 box, rho^p as (qx, qy, qz) with 36 x rows x 1
+static rso_status pair_tensor_maps(rso_handle* h, const Level& l, const float* u, const float* rp, int rows,
+                                   CUtensorMap* mu, CUtensorMap* mr) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) {
+    h->err = "cuTensorMapEncodeTiled is not available from the driver";
+    return RSO_ERR_CUDA;
+  }
+  const cuuint64_t F = sizeof(float);
+  const cuuint64_t du[4] = {(cuuint64_t)l.px, (cuuint64_t)l.py, (cuuint64_t)l.pz, (cuuint64_t)(3 * l.nb)};
+  const cuuint64_t su[3] = {F * l.px, F * l.px * l.py, F * (cuuint64_t)l.NP};
+  const cuuint32_t bu[4] = {36, (cuuint32_t)rows + 1, 1, 3}, e4[4] = {1, 1, 1, 1};
+  const cuuint64_t dr[3] = {(cuuint64_t)l.qx, (cuuint64_t)l.qy, (cuuint64_t)l.qz};
+  const cuuint64_t sr[2] = {F * l.qx, F * l.qx * l.qy};
+  const cuuint32_t br[3] = {36, (cuuint32_t)rows, 1};
+  CUresult r1 = enc(mu, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(u), du, su, bu, e4,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r2 = enc(mr, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(rp), dr, sr, br, e4,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r1 != CUDA_SUCCESS || r2 != CUDA_SUCCESS) {
+    h->err = "tensor map encoding of the fine-level arrays failed";
+    return RSO_ERR_CUDA;
+  }
+  return RSO_OK;
+}
+
+// fails if a staged-copy wait of the fine kernels gave up since the last call
+// (never in a healthy run); resets the device-wide count
+rso_status fine_stage_check(rso_handle* h) {
+  unsigned int n = 0, zero = 0;
+  RSO_CHECK_CUDA(h, cudaMemcpyFromSymbolAsync(&n, g_stage_timeouts, sizeof(n), 0, cudaMemcpyDeviceToHost, h->stream));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (n != 0) {
+    RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(g_stage_timeouts, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, h->stream));
+    RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->err = "a staged-copy wait of the fine operator timed out";
+    return RSO_ERR_CUDA;
+  }
+  return RSO_OK;
+}
 
 template <typename T, int MODE>
 static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, const T* rp, double omega, int cls,
@@ -879,14 +1049,15 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
     h->err = "fine operator inputs must be 16-byte aligned";
     return RSO_ERR_INVALID_ARG;
   }
-  // FP32: two columns per thread on packed pairs; FP64: one column per thread
+  // FP32: two columns per thread on packed pairs, staged by TMA; FP64: one
+  // column per thread, staged by cp.async
   constexpr bool packed = sizeof(T) == 4;
   constexpr int smem = packed ? pair_smem_bytes<PTY>() : walsh_smem_bytes<T, WTY>();
-  void (*kern)(const Level, const T*, const T*, T*, const T*, T, double*, const T*, T);
+  const void* kern;
   if constexpr (packed)
-    kern = k_fine_p<MODE, PTY>;
+    kern = reinterpret_cast<const void*>(k_fine_p<MODE, PTY, kPairTMA>);
   else
-    kern = k_fine_w<T, MODE, WTY>;
+    kern = reinterpret_cast<const void*>(k_fine_w<T, MODE, WTY>);
   // the shared-memory opt-in is per device; setting it twice from racing
   // threads is harmless, so an atomic flag per device suffices
   static std::atomic<bool> attr[64];
@@ -894,10 +1065,17 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
     RSO_CHECK_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     if (h->device >= 0 && h->device < 64) attr[h->device].store(true, std::memory_order_release);
   }
-  const dim3 grid = packed ? pair_grid(l) : march_grid(l);
-  const dim3 block = packed ? dim3(WTX, PTY) : dim3(WTX, WTY);
-  if (h->prof_on) prof_begin(h, cls, (double)l.nn);
-  kern<<<grid, block, smem, h->stream>>>(l, u, f, out, rp, (T)omega, dotp, uprev, (T)c1);
+  if constexpr (packed) {
+    CUtensorMap mu{}, mr{};
+    if (kPairTMA) RSO_TRY(pair_tensor_maps(h, l, u, rp, 2 * PTY, &mu, &mr));
+    if (h->prof_on) prof_begin(h, cls, (double)l.nn);
+    k_fine_p<MODE, PTY, kPairTMA><<<pair_grid(l), dim3(WTX, PTY), smem, h->stream>>>(
+        l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, mu, mr);
+  } else {
+    if (h->prof_on) prof_begin(h, cls, (double)l.nn);
+    k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega, dotp,
+                                                                                 uprev, (T)c1);
+  }
   rso::note_launch();
   if (h->prof_on) prof_end(h, cls);
   return launch_check(h, what);

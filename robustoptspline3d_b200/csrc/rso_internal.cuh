@@ -199,6 +199,7 @@ rso_status pad_elems_f(rso_handle* h, const float* dense, float* padded);
 rso_status unpad_elems_f(rso_handle* h, const float* padded, float* dense);
 rso_status zero_support(rso_handle* h, double* padded);
 rso_status to_f32(rso_handle* h, const double* a, float* b, long long n);
+rso_status fine_stage_check(rso_handle* h);
 rso_status to_f64(rso_handle* h, const float* a, double* b, long long n);
 
 // topology (topology.cu)

@@ -467,7 +467,7 @@ __device__ __forceinline__ float2 p_sub(float2 a, float2 b) {
   return *reinterpret_cast<const float2*>(&r);
 }
 
-constexpr int kPairMinBlocksRes = 4, kPairMinBlocksJac = 3;
+constexpr int kPairMinBlocksRes = 4, kPairMinBlocksJac = 4;
 
 // Bulk-tensor staging (TMA): one thread issues the copies of a stage, their
 // completion is tracked by an mbarrier per slot.  Every wait is bounded: after
@@ -519,11 +519,15 @@ template <int TYP>
 constexpr int pair_rho_off() { return (3 * 36 * (2 * TYP + 1) + 31) / 32 * 32; }
 template <int TYP>
 constexpr int pair_slot() { return pair_rho_off<TYP>() + (36 * 2 * TYP + 31) / 32 * 32; }
+// staging slots of the packed kernel: the Jacobi / Chebyshev step keeps two
+// more stages resident, so that it reads rho^p of the layers around the
+// emitted plane and u at the emitted nodes from shared memory, not registers
+constexpr int pair_slots(int mode, bool tma) { return mode == 2 && tma ? WNSLOT + 2 : WNSLOT; }
 template <int TYP>
-constexpr int pair_smem_bytes() {
+constexpr int pair_smem_bytes(int nslot) {
   // slots + corner exchange [2][4 values][3 comps][32 TYP] + 128 bytes to
   // round the base up to a 128-byte boundary
-  return 4 * (WNSLOT * pair_slot<TYP>() + 2 * 12 * 32 * TYP) + 128;
+  return 4 * (nslot * pair_slot<TYP>() + 2 * 12 * 32 * TYP) + 128;
 }
 
 // resident CTAs per SM the register budget is cut for: the residual fits 128
@@ -540,14 +544,16 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE))
              const float* __restrict__ rp, float omega, double* __restrict__ dotp, const float* __restrict__ uprev,
              float c1, const __grid_constant__ CUtensorMap tmu, const __grid_constant__ CUtensorMap tmr) {
   constexpr int RX = 36, ROWS = 2 * TYP, NPL = RX * (ROWS + 1), NT = WTX * TYP;
+  constexpr int NS = pair_slots(MODE, TMA);
+  constexpr bool LEAN = MODE == 2 && TMA;  // operands of the emitted plane re-read from the slots
   constexpr int RHO = pair_rho_off<TYP>(), SLOT = pair_slot<TYP>();
   constexpr uint32_t STAGE_BYTES = sizeof(float) * (3 * NPL + RX * ROWS);  // both boxes of a stage
   constexpr int CPR = RX / 4;  // 16-byte chunks per staged row
   constexpr int NCH = (3 * (ROWS + 1) + ROWS) * CPR, KC = (NCH + NT - 1) / NT;
   extern __shared__ __align__(128) unsigned char smem_pair[];
   // slots start on a 128-byte shared-memory address whatever the base
-  float* ss = reinterpret_cast<float*>(smem_pair + ((128u - (smem_u32(smem_pair) & 127u)) & 127u));  // [WNSLOT][SLOT]
-  float* sx = ss + WNSLOT * SLOT;                  // [2][4][3][NT] corner exchange, by plane parity
+  float* ss = reinterpret_cast<float*>(smem_pair + ((128u - (smem_u32(smem_pair) & 127u)) & 127u));  // [NS][SLOT]
+  float* sx = ss + NS * SLOT;                  // [2][4][3][NT] corner exchange, by plane parity
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * WTX + tx;
   const int x0 = blockIdx.x * (WTX - 1), y0 = blockIdx.y * (ROWS - 1);
   const int nzc = (L.nz + FZC - 1) / FZC, bsys = blockIdx.z / nzc;
@@ -586,15 +592,15 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE))
     }
   }
   const long long pxy = (long long)L.px * L.py, qxy = (long long)L.qx * L.qy;
-  __shared__ __align__(8) uint64_t bars[WNSLOT];
+  __shared__ __align__(8) uint64_t bars[NS];
   bool gave_up = false;
-  // stage s (node plane s, element layer s) into slot (s + WNSLOT) % WNSLOT
+  // stage s (node plane s, element layer s) into slot (s + NS) % NS
   auto issue = [&](int s) {
-    float* dst = ss + ((s + WNSLOT) % WNSLOT) * SLOT;
+    float* dst = ss + ((s + NS) % NS) * SLOT;
     if constexpr (TMA) {
       // thread 0 only; stages past z1 are never read and not issued
       if (s > z1) return;
-      uint64_t* bar = &bars[(s + WNSLOT) % WNSLOT];
+      uint64_t* bar = &bars[(s + NS) % NS];
       mbar_expect_tx(bar, STAGE_BYTES);
       tma_load_4d(dst, &tmu, xs, y0, s + 1, 3 * bsys, bar);
       tma_load_3d(dst + RHO, &tmr, xs, y0, s + 1, bar);
@@ -614,8 +620,8 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE))
   };
   // TMA: wait until stage s has landed (the k-th use of a slot completes phase k)
   auto wait_stage = [&](int s) {
-    const uint32_t parity = (uint32_t)((s - (z0 - 1)) / WNSLOT) & 1u;
-    if (!mbar_wait(&bars[(s + WNSLOT) % WNSLOT], parity)) gave_up = true;
+    const uint32_t parity = (uint32_t)((s - (z0 - 1)) / NS) & 1u;
+    if (!mbar_wait(&bars[(s + NS) % NS], parity)) gave_up = true;
   };
   // xy modes of the face nodes of both columns on a staged plane (lane 0:
   // column A, lane 1: column B), and u at the two emitted nodes
@@ -637,7 +643,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE))
   if constexpr (TMA) {
     if (tid == 0) {
 #pragma unroll
-      for (int k = 0; k < WNSLOT; k++) mbar_init(&bars[k], 1);
+      for (int k = 0; k < NS; k++) mbar_init(&bars[k], 1);
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
@@ -656,7 +662,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE))
   float2 F[4][3], Gt[4][3], uc[3], uo[3], own[3], fo[3], po[3], ra[4], rb[4];
   uint8_t clA = 0, clB = 0;
   double pq = 0;
-  face(ss + ((z0 - 1 + WNSLOT) % WNSLOT) * SLOT, F, uc);
+  face(ss + ((z0 - 1 + NS) % NS) * SLOT, F, uc);
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     Gt[q][0] = Gt[q][1] = Gt[q][2] = zero2;
@@ -692,6 +698,24 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE))
     } else {
       // diagonal block from rho^p of the 4 columns around each node in the
       // layers below (ra) and above (rb), as in k_fine_w
+      if constexpr (LEAN) {
+        // u at the two nodes from plane zo, rho^p from layers zo - 1 and zo
+        // (stages zo - 1 and zo stay resident until stage zo + NS is issued)
+        const int base = 2 * ty * RX + tx + ox;
+        const float* pu = ss + ((zo + NS) % NS) * SLOT + base;
+        const float* pa = ss + ((zo - 1 + NS) % NS) * SLOT + RHO + base;
+        const float* pb = ss + ((zo + NS) % NS) * SLOT + RHO + base;
+#pragma unroll
+        for (int c = 0; c < 3; c++) uo[c] = make_float2(pu[c * NPL + RX + 1], pu[c * NPL + 2 * RX + 1]);
+        ra[0] = make_float2(pa[0], pa[RX]);
+        ra[1] = make_float2(pa[1], pa[RX + 1]);
+        ra[2] = make_float2(pa[RX], wB ? pa[2 * RX] : 0.f);
+        ra[3] = make_float2(pa[RX + 1], wB ? pa[2 * RX + 1] : 0.f);
+        rb[0] = make_float2(pb[0], pb[RX]);
+        rb[1] = make_float2(pb[1], pb[RX + 1]);
+        rb[2] = make_float2(pb[RX], wB ? pb[2 * RX] : 0.f);
+        rb[3] = make_float2(pb[RX + 1], wB ? pb[2 * RX + 1] : 0.f);
+      }
       const float2 R = p_add(p_add(p_add(ra[0], ra[1]), p_add(ra[2], ra[3])), p_add(p_add(rb[0], rb[1]), p_add(rb[2], rb[3])));
       const float2 pxy_ = p_add(p_sub(p_add(ra[0], ra[3]), p_add(ra[1], ra[2])), p_sub(p_add(rb[0], rb[3]), p_add(rb[1], rb[2])));
       const float2 xlo = p_sub(p_add(ra[1], ra[3]), p_add(ra[0], ra[2])), xhi = p_sub(p_add(rb[1], rb[3]), p_add(rb[0], rb[2]));
@@ -750,8 +774,8 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE))
         }
       }
     }
-    const float* su = ss + ((z + 1 + WNSLOT) % WNSLOT) * SLOT;
-    const float* sr = ss + ((z + WNSLOT) % WNSLOT) * SLOT + RHO;
+    const float* su = ss + ((z + 1 + NS) % NS) * SLOT;
+    const float* sr = ss + ((z + NS) % NS) * SLOT + RHO;
     float2 v[8][3], un[3];
     {
       float2 Fn[4][3];
@@ -787,7 +811,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE))
 #pragma unroll
       for (int i = 0; i < 3; i++) v[c ^ (1 << i)][i] = o[i];
     }
-    if (MODE == 2) {
+    if (MODE == 2 && !LEAN) {
 #pragma unroll
       for (int q = 0; q < 4; q++) ra[q] = rb[q];
       rb[0] = re;
@@ -818,10 +842,12 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE))
         own[c] = make_float2(c11.x + c10.y, c11.y);  // nodes (ex + 1, ey + 1), (ex + 1, ey + 2)
       }
     }
+    if constexpr (!LEAN) {
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      uo[c] = uc[c];
-      uc[c] = un[c];
+      for (int c = 0; c < 3; c++) {
+        uo[c] = uc[c];
+        uc[c] = un[c];
+      }
     }
   }
   __syncthreads();
@@ -844,7 +870,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE))
     // every issued stage was waited for; after a wait that gave up, wait
     // (bounded) once more for the copies of the last stages still in flight
     if (gave_up)
-      for (int s = max(z0 - 1, z1 - WNSLOT + 1); s <= z1; s++) wait_stage(s);
+      for (int s = max(z0 - 1, z1 - NS + 1); s <= z1; s++) wait_stage(s);
   } else {
     __pipeline_wait_prior(0);
   }
@@ -1052,7 +1078,7 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
   // FP32: two columns per thread on packed pairs, staged by TMA; FP64: one
   // column per thread, staged by cp.async
   constexpr bool packed = sizeof(T) == 4;
-  constexpr int smem = packed ? pair_smem_bytes<PTY>() : walsh_smem_bytes<T, WTY>();
+  constexpr int smem = packed ? pair_smem_bytes<PTY>(pair_slots(MODE, kPairTMA)) : walsh_smem_bytes<T, WTY>();
   const void* kern;
   if constexpr (packed)
     kern = reinterpret_cast<const void*>(k_fine_p<MODE, PTY, kPairTMA>);

@@ -12,6 +12,7 @@ exceed the 126 MB L2, so no flush is inserted between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--size S]
   python bench.py --mode solve [--precision mixed|fp64] [--size S]
+  python bench.py --mode batch|problems|scale
 
 `--mode solve` times single multigrid-preconditioned CG solves (to relative
 residual 1e-6) on the density of the seeded initial design, with a seeded
@@ -373,6 +374,95 @@ def run_problems(args):
         g.close()
 
 
+def scale_problem(seed=2027, nvoids=200):
+    """Mixed precision at scale: a 511 x 256 x 256 voxel box embedded as 512 x 256
+    x 256 with the last x element plane inactive, with `nvoids` spherical voids
+    (radius ~ U[4, 20], centres ~ U(box), seeded), nodes of x = 0 clamped, load
+    set = the node plane x = 511 with the force along +x (constrained-direction
+    worst case)."""
+    ex, ey, ez = 512, 256, 256
+    rng = np.random.default_rng(seed)
+    em = np.ones((ez, ey, ex), np.uint8)
+    em[:, :, ex - 1] = 0
+    for _ in range(nvoids):
+        r = rng.uniform(4.0, 20.0)
+        cx, cy, cz = rng.uniform(0.0, 511.0), rng.uniform(0.0, ey), rng.uniform(0.0, ez)
+        lo = [max(int(np.floor(c - r - 1)), 0) for c in (cz, cy, cx)]
+        hi = [min(int(np.ceil(c + r + 1)), m) for c, m in zip((cz, cy, cx), (ez, ey, ex))]
+        z, y, x = np.ogrid[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]
+        inside = (x + 0.5 - cx) ** 2 + (y + 0.5 - cy) ** 2 + (z + 0.5 - cz) ** 2 <= r * r
+        em[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]][inside] = 0
+    fa = np.zeros((ez + 1, ey + 1, ex + 1), np.uint8)
+    fa[:, :, 0] = 1
+    la = np.zeros((ez + 1, ey + 1, ex + 1), np.uint8)
+    la[:, :, ex - 1] = 1
+    normals = np.zeros(((ez + 1) * (ey + 1) * (ex + 1), 3))
+    normals[:, 0] = 1.0
+    return em, fa, la, normals
+
+
+def run_scale(args):
+    """One worst-case design iteration on the 512 x 256 x 256 voids box (the
+    FP32-operator-at-scale configuration), mixed and plain FP64; the FP64 path
+    solves to relative residual 1e-10 and serves as the reference the mixed
+    path's worst-case eigenvalue, compliance and coefficient gradients are
+    compared against (the CPU oracle is checked against the GPU at small sizes
+    in the tests)."""
+    import torch
+    import robustoptspline3d_b200 as R
+    em, fa, la, normals = scale_problem()
+    order = 4
+    parts = (60, 28, 28)
+    rng = np.random.default_rng(2026)
+    res = {}
+    for prec, tol in ((R.rso.MIXED, 1e-6), (R.rso.FP64, 1e-10)):
+        t0 = time.perf_counter()
+        g = R.HierarchyGrid(em, fa, la, normals, R.Config(precision=prec, smoother=smoother_id(R), omega=OMEGA,
+                                                          cheb_lower=CHEB_LOWER, pre=2, post=2, poisson_ratio=0.3,
+                                                          mode=R.rso.WITH_SUPPORT_CF))
+        nc = g.set_spline_partition(*parts, order)
+        coeff = np.clip(np.random.default_rng(2026).normal(0.5, 0.15, nc), 0.0, 1.0)
+        setup_s = time.perf_counter() - t0
+        prm = R.IterParams(lanczos_steps=20, solve_tol=tol, ss_mode=4, constrain_direction=1, filter_mode=1)
+        c0 = torch.as_tensor(coeff, dtype=torch.float64, device="cuda")
+        vals, gl, gv, gs = g.design_gradient(c0, prm)
+        mma = R.MMA(nc, 2, 0.0, 1.0)
+        times, info = [], None
+        for _ in range(1 + max(1, min(args.steps, 2))):
+            mma.set_x(c0)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            info = g.design_iteration(mma, prm)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t1)
+        x_new = mma.get()[0]
+        res[prec] = dict(vals=vals, gl=gl.cpu().numpy(), x=x_new, s=min(times[1:]), info=info, setup_s=setup_s,
+                         levels=[g.level_dims(i)[:3].tolist() for i in range(g.n_levels())])
+        mma.close()
+        g.close()
+        del g, gl, gv, gs, c0
+        torch.cuda.empty_cache()
+    m, d = res[R.rso.MIXED], res[R.rso.FP64]
+    rel = lambda a, b: float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
+    out = {"metric": "worst-case design iteration @512x256x256 with 200 voids (mixed vs FP64)",
+           "value": 1.0 / m["s"], "unit": "iter/s", "higher_is_better": True,
+           "fp64_iters_per_s": 1.0 / d["s"], "mixed_vs_fp64": d["s"] / m["s"],
+           "active_elements": int(em.sum()), "levels": m["levels"],
+           "pcg_iterations": {"mixed": m["info"]["solve_iterations"], "fp64": d["info"]["solve_iterations"]},
+           "errors_vs_fp64": {"lambda_max": abs(m["vals"]["lambda"] - d["vals"]["lambda"]) / abs(d["vals"]["lambda"]),
+                              "compliance_worst": abs(m["info"]["c_worst"] - d["info"]["c_worst"]) / abs(d["info"]["c_worst"]),
+                              "dlambda_dcoeff": rel(m["gl"], d["gl"]),
+                              "coefficients_after_mma": rel(m["x"], d["x"])},
+           "setup_s": {"mixed": m["setup_s"], "fp64": d["setup_s"]},
+           "config": {"workload": "511x256x256 voxels (embedded 512x256x256), 200 spherical voids r~U[4,20]",
+                      "load": "x=511 node plane, force along +x (constrained direction)", "support": "x=0 nodes",
+                      "spline": f"order {order}, partition {parts}", "solve_tol": {"mixed": 1e-6, "fp64": 1e-10},
+                      "smoother": f"{SMOOTHER} 2+2 on [{CHEB_LOWER}, 1] x lambda_max",
+                      "smoother_state": "FP32 (BF16/FP16 state not built)", "filter": "none (exact gradients)"},
+           "data": "synthetic"}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -383,7 +473,7 @@ def main():
     ap.add_argument("--ref-size", type=int, default=24)
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="design", choices=["design", "solve", "batch", "problems"])
+    ap.add_argument("--mode", default="design", choices=["design", "solve", "batch", "problems", "scale"])
     ap.add_argument("--systems", type=int, default=16)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
@@ -395,6 +485,9 @@ def main():
         return
     if args.mode == "problems":
         run_problems(args)
+        return
+    if args.mode == "scale":
+        run_scale(args)
         return
     if args.impl == "reference":
         # host-only arm: rank 0 times the CPU path, other ranks exit at once

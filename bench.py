@@ -601,7 +601,7 @@ def main():
     g.close()
     mma.close()
     # plain FP64 GPU path for the mixed-vs-FP64 comparison
-    fp64 = None
+    fp64 = fp64_tight = None
     if args.fp64_steps > 0:
         g64, mma64 = make(R.rso.FP64)
         step(g64, mma64)
@@ -611,6 +611,18 @@ def main():
             step(g64, mma64)
         torch.cuda.synchronize()
         fp64 = barrier_max(world, (time.perf_counter() - t0) / args.fp64_steps)
+        # the FP64 path at the tolerance the FP64 reference method is run to
+        # (relative residual 1e-10), and the mixed result's distance from it
+        prm10 = R.IterParams(lanczos_steps=20, solve_tol=1e-10, ss_mode=4)
+        mma64.set_x(c0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        info10 = g64.design_iteration(mma64, prm10)
+        torch.cuda.synchronize()
+        fp64_tight = {"iters_per_s": world / barrier_max(world, time.perf_counter() - t0), "solve_tol": 1e-10,
+                      "solve_iterations": info10["solve_iterations"],
+                      "mixed_lambda_rel_err": abs(infos[-1]["lam"] - info10["lam"]) / abs(info10["lam"]),
+                      "mixed_c_worst_rel_err": abs(infos[-1]["c_worst"] - info10["c_worst"]) / abs(info10["c_worst"])}
         g64.close()
         mma64.close()
     cpu = None
@@ -636,6 +648,7 @@ def main():
                            "step": "one design iteration from the seeded initial design"},
                 "fp64_iters_per_s": (1.0 / fp64) if fp64 else None,
                 "mixed_vs_fp64": (fp64 / (ms / 1e3 / args.steps)) if fp64 else None,
+                "fp64_rel_resid_1e-10": dict(fp64_tight, mixed_vs_fp64=value / fp64_tight["iters_per_s"]) if fp64_tight else None,
                 "last_iteration": {k: last[k] for k in ("c_worst", "lam", "volume", "ss_value", "solve_iterations",
                                                         "ms_operators", "ms_worst", "ms_selfsupport", "ms_adjoint",
                                                         "ms_mma")},

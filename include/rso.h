@@ -193,6 +193,15 @@ rso_status rso_solve(rso_handle* h, const double* f_dev, double* u_dev, double t
  * buffers for k systems are allocated on the first call with that k and kept. */
 rso_status rso_solve_batch(rso_handle* h, int k, const double* F_dev, double* U_dev, double tol, int max_iter,
                            rso_solve_info* infos);
+/* Replay of the FP32 V-cycle (the mixed-precision preconditioner) from CUDA
+ * graphs (no counterpart in the reference, which launches every kernel):
+ * on by default.  The V-cycle is captured the second time its launch
+ * arguments (level vectors, sizes, smoother step sizes, configuration,
+ * profiling mask) occur and replayed whenever they recur; the results are
+ * the same launches with the same arguments.  A capture needs a stream of the
+ * handle's own or one set by rso_set_stream other than the legacy default
+ * stream; if a capture fails the handle keeps to plain launches. */
+rso_status rso_set_vcycle_graphs(rso_handle* h, int on);
 /* Grid::compliance (grid/Grid.cpp:4118-4121): c = f . u */
 rso_status rso_dot(rso_handle* h, const double* a_dev, const double* b_dev, double* out);
 

@@ -283,6 +283,7 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
         k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 5); rso::note_launch();
         RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.h_scal, s, sizeof(double) * KS * k, cudaMemcpyDeviceToHost, h->stream));
         RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+        vcycle_graphs_harvest(h);
         iter++;
         left = 0;
         for (int b = 0; b < k; b++) {

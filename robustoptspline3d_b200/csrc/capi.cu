@@ -129,6 +129,7 @@ static void free_handle(rso_handle* h) {
   cudaFree(h->e_a); cudaFree(h->e_b); cudaFree(h->e_c); cudaFree(h->e_d); cudaFree(h->e_rhohat);
   cudaFree(h->coef_a); cudaFree(h->coef_b); cudaFree(h->coef_c);
   cudaFree(h->coef_df); cudaFree(h->coef_dg); cudaFree(h->fw); cudaFree(h->uw);
+  vcycle_graphs_free(h);
   prof_free(h);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -403,6 +404,12 @@ extern "C" rso_status rso_residual(rso_handle* h, const double* u, const double*
   RSO_TRY(fine_residual<double>(h, l0.u64, l0.f64, l0.r64, h->rp64));
   RSO_TRY(unpad_nodes(h, 0, l0.r64, r));
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  return RSO_OK;
+}
+
+extern "C" rso_status rso_set_vcycle_graphs(rso_handle* h, int on) {
+  if (!h) return RSO_ERR_INVALID_ARG;
+  h->vc_graphs = on != 0;
   return RSO_OK;
 }
 

@@ -15,6 +15,7 @@ static std::atomic<long long> g_launches{0};
 namespace rso {
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 struct ProfClassInfo {
   const char* name;
@@ -39,10 +40,73 @@ struct Prof {
   std::vector<cudaEvent_t> ev[PC_N];
   std::vector<double> nodes[PC_N];
   size_t used[PC_N] = {};
+  // launches timed inside replayed V-cycle graphs
+  double graph_ms[PC_N] = {}, graph_nodes[PC_N] = {};
+  long long graph_n[PC_N] = {};
 };
+
+// Inside a stream capture the event pair of a launch is recorded as a graph
+// node (cudaEventRecordExternal) from a pool made before the capture began;
+// every replay re-records the same events, so they are read (prof_harvest)
+// before the graph runs again.
+struct ProfPair {
+  int cls = 0;
+  double nodes = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+struct ProfPairs {
+  std::vector<ProfPair> pairs;
+  size_t used = 0;
+};
+
+void* prof_pairs_new(int capacity) {
+  ProfPairs* v = new ProfPairs();
+  v->pairs.resize(capacity);
+  for (auto& p : v->pairs) {
+    cudaEventCreate(&p.e0);
+    cudaEventCreate(&p.e1);
+  }
+  return v;
+}
+
+void prof_pairs_free(void* pairs) {
+  ProfPairs* v = (ProfPairs*)pairs;
+  if (!v) return;
+  for (auto& p : v->pairs) {
+    cudaEventDestroy(p.e0);
+    cudaEventDestroy(p.e1);
+  }
+  delete v;
+}
+
+bool prof_pairs_used(const void* pairs) { return pairs && ((const ProfPairs*)pairs)->used > 0; }
+
+void prof_harvest(rso_handle* h, void* pairs) {
+  ProfPairs* v = (ProfPairs*)pairs;
+  if (!v || v->used == 0) return;
+  Prof* p = (Prof*)h->prof;
+  if (!p) { p = new Prof(); h->prof = p; }
+  for (size_t k = 0; k < v->used; k++) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, v->pairs[k].e0, v->pairs[k].e1) != cudaSuccess) continue;
+    const int c = v->pairs[k].cls;
+    p->graph_ms[c] += ms;
+    p->graph_nodes[c] += v->pairs[k].nodes;
+    p->graph_n[c]++;
+  }
+}
 
 void prof_begin(rso_handle* h, int cls, double nodes) {
   if (!((h->prof_on >> cls) & 1)) return;
+  if (h->cap_prof) {
+    ProfPairs* v = (ProfPairs*)h->cap_prof;
+    if (v->used >= v->pairs.size()) return;  // pool exhausted: launch left untimed
+    ProfPair& pp = v->pairs[v->used];
+    pp.cls = cls;
+    pp.nodes = nodes;
+    cudaEventRecordWithFlags(pp.e0, h->stream, cudaEventRecordExternal);
+    return;
+  }
   Prof* p = (Prof*)h->prof;
   if (!p) { p = new Prof(); h->prof = p; }
   size_t k = p->used[cls];
@@ -58,6 +122,13 @@ void prof_begin(rso_handle* h, int cls, double nodes) {
 
 void prof_end(rso_handle* h, int cls) {
   if (!((h->prof_on >> cls) & 1)) return;
+  if (h->cap_prof) {
+    ProfPairs* v = (ProfPairs*)h->cap_prof;
+    if (v->used >= v->pairs.size()) return;
+    cudaEventRecordWithFlags(v->pairs[v->used].e1, h->stream, cudaEventRecordExternal);
+    v->used++;
+    return;
+  }
   Prof* p = (Prof*)h->prof;
   size_t k = p->used[cls];
   cudaEventRecord(p->ev[cls][k + 1], h->stream);
@@ -93,9 +164,14 @@ extern "C" rso_status rso_set_profiling_classes(rso_handle* h, unsigned mask) {
 
 extern "C" rso_status rso_profile_reset(rso_handle* h) {
   if (!h) return RSO_ERR_INVALID_ARG;
+  vcycle_graphs_harvest(h);  // drop timings of replays still unread
   Prof* p = (Prof*)h->prof;
   if (p)
-    for (int c = 0; c < PC_N; c++) p->used[c] = 0;
+    for (int c = 0; c < PC_N; c++) {
+      p->used[c] = 0;
+      p->graph_ms[c] = p->graph_nodes[c] = 0;
+      p->graph_n[c] = 0;
+    }
   return RSO_OK;
 }
 
@@ -103,10 +179,11 @@ extern "C" rso_status rso_profile_class(rso_handle* h, int cls, char* name, int 
                                         double* total_ms, double* bytes_per_launch, double* flops_per_launch) {
   if (!h || cls < 0 || cls >= PC_N) return RSO_ERR_INVALID_ARG;
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  vcycle_graphs_harvest(h);
   Prof* p = (Prof*)h->prof;
   double tot = 0, nodes = 0;
   long long n = 0;
-  if (p)
+  if (p) {
     for (size_t k = 0; k + 1 < p->used[cls]; k += 2) {
       float ms = 0;
       cudaEventElapsedTime(&ms, p->ev[cls][k], p->ev[cls][k + 1]);
@@ -114,6 +191,10 @@ extern "C" rso_status rso_profile_class(rso_handle* h, int cls, char* name, int 
       nodes += p->nodes[cls][k / 2];
       n++;
     }
+    tot += p->graph_ms[cls];
+    nodes += p->graph_nodes[cls];
+    n += p->graph_n[cls];
+  }
   if (name && name_len > 0) {
     std::strncpy(name, kInfo[cls].name, name_len - 1);
     name[name_len - 1] = 0;

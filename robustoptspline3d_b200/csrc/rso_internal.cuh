@@ -144,6 +144,9 @@ struct rso_handle {
   double *fw = nullptr, *uw = nullptr;             // worst-case force / displacement (padded)
   unsigned prof_on = 0;                            // classes with per-kernel event timing (prof.cu)
   void* prof = nullptr;
+  void* vcg = nullptr;                             // captured FP32 V-cycles (solver.cu)
+  void* cap_prof = nullptr;                        // event pairs of the V-cycle capture in progress (prof.cu)
+  bool vc_graphs = true;                           // replay captured V-cycles (rso_set_vcycle_graphs)
 };
 
 namespace rso {
@@ -153,9 +156,19 @@ enum ProfClass {
   PC_COARSE32, PC_COARSE64, PC_N
 };
 void note_launch();
+void note_launches(long long n);
 void prof_begin(rso_handle* h, int cls, double nodes);
 void prof_end(rso_handle* h, int cls);
 void prof_free(rso_handle* h);
+// event pairs recorded into a captured V-cycle: created before the capture,
+// read after each replay
+void* prof_pairs_new(int capacity);
+void prof_pairs_free(void* pairs);
+bool prof_pairs_used(const void* pairs);
+void prof_harvest(rso_handle* h, void* pairs);
+// captured V-cycles (solver.cu)
+void vcycle_graphs_harvest(rso_handle* h);
+void vcycle_graphs_free(rso_handle* h);
 }  // namespace rso
 
 // ---------------------------------------------------------------- helpers

@@ -10,6 +10,7 @@
 // the coarsest solve stay FP64.
 #include "rso_internal.cuh"
 #include <cmath>
+#include <cstring>
 #include <utility>
 
 namespace rso {
@@ -203,12 +204,183 @@ __global__ void k_cg_step(long long n, const double* __restrict__ alpha, const d
 
 // mixed precision: one FP32 V-cycle from a zero iterate on L[0].f32 (already
 // holding the FP32 residual); the result is left in L[0].u32
-rso_status vcycle_mixed(rso_handle* h) {
+static rso_status vcycle_mixed_launches(rso_handle* h) {
   Level& l0 = h->L[0];
   // the first damped-Jacobi sweep from zero reads no iterate; Gauss-Seidel does
   if (h->cfg.smoother == RSO_SMOOTH_GS || h->cfg.pre == 0)
     RSO_CHECK_CUDA(h, cudaMemsetAsync(l0.u32, 0, sizeof(float) * 3 * l0.NP * l0.nb, h->stream));
   return vcycle_levels<float>(h, h->cfg.pre, h->cfg.post, 1, true);
+}
+
+// ---------------------------------------------------------------- captured V-cycles
+// The FP32 V-cycle of the preconditioner is about forty launches per CG
+// iteration.  It is captured once into a CUDA graph and replayed.  What a
+// capture freezes is the launch arguments: level vectors (the smoothers
+// rotate three per level, so successive V-cycles differ and repeat with a
+// short period), level sizes, smoother step sizes (from lambda_max), scratch
+// and coarsest-solve buffers, the configuration and the profiling mask.  All
+// of them form the key a graph is looked up by; a V-cycle whose key was not
+// seen before runs as plain launches, the second time it is captured.  A
+// graph also records how the rotating vectors end, which the host state takes
+// on after a replay.
+namespace {
+struct VcGraph {
+  std::vector<uint64_t> key, after;
+  cudaGraphExec_t exec = nullptr;
+  long long kernels = 0;
+  void* pairs = nullptr;  // profiling event pairs inside the graph
+  bool unread = false;    // replayed with event pairs not yet read
+};
+struct VcCache {
+  std::vector<VcGraph> graphs;
+  std::vector<std::vector<uint64_t>> seen;
+  bool broken = false;  // a capture failed: plain launches from now on
+};
+constexpr size_t kMaxGraphs = 8, kMaxSeen = 32;
+
+template <typename X>
+void push_bits(std::vector<uint64_t>& k, X v) {
+  uint64_t b = 0;
+  static_assert(sizeof(X) <= 8, "key entries are at most 8 bytes");
+  std::memcpy(&b, &v, sizeof(X));
+  k.push_back(b);
+}
+
+std::vector<uint64_t> vc_key(const rso_handle* h) {
+  std::vector<uint64_t> k;
+  for (const Level& l : h->L) {
+    push_bits(k, l.u32); push_bits(k, l.f32); push_bits(k, l.r32); push_bits(k, l.t32);
+    push_bits(k, l.st32); push_bits(k, l.vclass); push_bits(k, l.emask);
+    push_bits(k, l.NP); push_bits(k, l.nn); push_bits(k, l.nb); push_bits(k, l.lam);
+    push_bits(k, l.nx); push_bits(k, l.ny); push_bits(k, l.nz); push_bits(k, l.px); push_bits(k, l.py);
+    push_bits(k, l.factor);
+  }
+  push_bits(k, h->rp32); push_bits(k, h->xfer); push_bits(k, h->xfer_n);
+  push_bits(k, h->c_K); push_bits(k, h->c_nodes); push_bits(k, h->c_f); push_bits(k, h->c_fb); push_bits(k, h->nc);
+  push_bits(k, h->cfg.smoother); push_bits(k, h->cfg.pre); push_bits(k, h->cfg.post);
+  push_bits(k, h->cfg.omega); push_bits(k, h->cfg.cheb_lower); push_bits(k, h->prof_on);
+  return k;
+}
+
+std::vector<uint64_t> vc_rotating(const rso_handle* h) {
+  std::vector<uint64_t> k;
+  for (const Level& l : h->L) { push_bits(k, l.u32); push_bits(k, l.r32); push_bits(k, l.t32); }
+  return k;
+}
+
+void vc_set_rotating(rso_handle* h, const std::vector<uint64_t>& v) {
+  size_t i = 0;
+  for (Level& l : h->L) {
+    std::memcpy(&l.u32, &v[i++], sizeof(float*));
+    std::memcpy(&l.r32, &v[i++], sizeof(float*));
+    std::memcpy(&l.t32, &v[i++], sizeof(float*));
+  }
+}
+
+void vc_drop(VcGraph& g) {
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  prof_pairs_free(g.pairs);
+  g.exec = nullptr;
+  g.pairs = nullptr;
+}
+}  // namespace
+
+void vcycle_graphs_harvest(rso_handle* h) {
+  VcCache* c = (VcCache*)h->vcg;
+  if (!c) return;
+  for (auto& g : c->graphs)
+    if (g.unread) {
+      prof_harvest(h, g.pairs);
+      g.unread = false;
+    }
+}
+
+void vcycle_graphs_free(rso_handle* h) {
+  VcCache* c = (VcCache*)h->vcg;
+  if (!c) return;
+  for (auto& g : c->graphs) vc_drop(g);
+  delete c;
+  h->vcg = nullptr;
+}
+
+rso_status vcycle_mixed(rso_handle* h) {
+  if (!h->vc_graphs || h->stream == nullptr) return vcycle_mixed_launches(h);
+  if (!h->vcg) h->vcg = new VcCache();
+  VcCache* c = (VcCache*)h->vcg;
+  if (c->broken) return vcycle_mixed_launches(h);
+  const std::vector<uint64_t> key = vc_key(h);
+  for (auto& g : c->graphs)
+    if (g.key == key) {
+      if (g.unread) {  // its events still hold the previous replay's times
+        RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+        vcycle_graphs_harvest(h);
+      }
+      RSO_CHECK_CUDA(h, cudaGraphLaunch(g.exec, h->stream));
+      note_launches(g.kernels);
+      vc_set_rotating(h, g.after);
+      g.unread = prof_pairs_used(g.pairs);
+      return launch_check(h, "vcycle graph");
+    }
+  bool seen = false;
+  for (const auto& k : c->seen) seen = seen || k == key;
+  if (!seen) {
+    if (c->seen.size() >= kMaxSeen) c->seen.erase(c->seen.begin());
+    c->seen.push_back(key);
+    return vcycle_mixed_launches(h);
+  }
+  // capture: the launches are recorded, not run; the graph then runs once
+  const std::vector<uint64_t> before = vc_rotating(h);
+  VcGraph g;
+  g.key = key;
+  if (h->prof_on) g.pairs = prof_pairs_new(128);
+  h->cap_prof = g.pairs;
+  cudaGraph_t graph = nullptr;
+  rso_status st = RSO_OK;
+  if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    st = RSO_ERR_CUDA;
+  } else {
+    st = vcycle_mixed_launches(h);
+    if (cudaStreamEndCapture(h->stream, &graph) != cudaSuccess) st = RSO_ERR_CUDA;
+  }
+  h->cap_prof = nullptr;
+  cudaGetLastError();  // a failed capture leaves its error here; the plain V-cycle below reports its own
+  if (st == RSO_OK && graph && cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess) {
+    g.exec = nullptr;
+    st = RSO_ERR_CUDA;
+  }
+  if (st == RSO_OK) {
+    size_t n = 0;
+    cudaGraphGetNodes(graph, nullptr, &n);
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n) cudaGraphGetNodes(graph, nodes.data(), &n);
+    for (auto nd : nodes) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) g.kernels++;
+    }
+  }
+  if (graph) cudaGraphDestroy(graph);
+  if (st != RSO_OK) {
+    // run this V-cycle (and every later one) as plain launches from the state it started in
+    vc_drop(g);
+    c->broken = true;
+    cudaGetLastError();
+    vc_set_rotating(h, before);
+    return vcycle_mixed_launches(h);
+  }
+  g.after = vc_rotating(h);
+  // the captured launches were counted when they were recorded
+  RSO_CHECK_CUDA(h, cudaGraphLaunch(g.exec, h->stream));
+  g.unread = prof_pairs_used(g.pairs);
+  if (c->graphs.size() >= kMaxGraphs) {
+    if (c->graphs.front().unread) {
+      RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+      vcycle_graphs_harvest(h);
+    }
+    vc_drop(c->graphs.front());
+    c->graphs.erase(c->graphs.begin());
+  }
+  c->graphs.push_back(std::move(g));
+  return launch_check(h, "vcycle graph");
 }
 
 // CG preconditioned by one V-cycle.  In mixed precision the preconditioned
@@ -248,6 +420,7 @@ rso_status solve_pcg(rso_handle* h, const double* f, double* x, double tol, int 
       RSO_TRY(cg_resid_rr(h, n3, s + 2, h->q, h->r, mixed ? h->L[0].f32 : nullptr, s + 5));
       RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->h_scal + 5, s + 5, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
       RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+      vcycle_graphs_harvest(h);
       rn2 = h->h_scal[5];
       it++;
       rel = std::sqrt(rn2) / fn;

@@ -93,6 +93,7 @@ SIGNATURES = {
     "rso_apply_K": (_ci, [_vp, _vp, _vp]),
     "rso_residual": (_ci, [_vp, _vp, _vp, _vp]),
     "rso_fine_sweep_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
+    "rso_set_vcycle_graphs": (_ci, [_vp, _ci]),
     "rso_get_stencil": (_ci, [_vp, _ci, _vp]),
     "rso_coarse_residual": (_ci, [_vp, _ci, _vp, _vp, _vp]),
     "rso_smooth": (_ci, [_vp, _ci, _vp, _vp, _ci, _cd, _ci, _ci]),
@@ -384,6 +385,10 @@ class HierarchyGrid:
         r = torch.empty_like(u)
         self._chk(self.lib.rso_residual(self.h, _dev(u, torch.float64), _dev(f, torch.float64), _dev(r)), "rso_residual")
         return r
+
+    def set_vcycle_graphs(self, on):
+        """Replay captured FP32 V-cycles from CUDA graphs (default) or launch every kernel."""
+        self._chk(self.lib.rso_set_vcycle_graphs(self.h, 1 if on else 0), "rso_set_vcycle_graphs")
 
     def fine_sweep_fp32(self, op, u, f=None, uprev=None, omega=1.0, c1=0.0):
         """One FP32 fine-level sweep (op 0 residual, 1 K u, 2 Jacobi/Chebyshev step), FP64 in and out."""

@@ -721,12 +721,14 @@ __global__ void __cluster_dims__(BOT_CTAS, 1, 1) __launch_bounds__(BOT_THREADS, 
     k_bottom(const __grid_constant__ BottomArgs<T> A) {
   cg::cluster_group cl = cg::this_cluster();
   const int g0 = (int)cl.block_rank() * BOT_THREADS + threadIdx.x, gs = BOT_CTAS * BOT_THREADS;
+  // the smoothers rotate each level's u, t and r; ucur[li] is the one that
+  // holds the level's iterate between the down- and the up-sweep
+  T* ucur[BOT_MAX_LEVELS];
   // down: pre-smoothing from a zero iterate, residual, restriction
   for (int li = A.lb; li < A.nl - 1; li++) {
     const Level& L = A.L[li];
     const T* st = bv_st<T>(L);
     T* u = bv_u<T>(L);
-    // current / next / previous iterate rotate over u, t and the (free) r
     T *cur = u, *oth = bv_t<T>(L), *prv = bv_r<T>(L);
     for (int s = 0; s < A.pre; s++) {
       bot_jacobi<T>(L, st, cur, bv_f<T>(L), oth, A.om[li][s], s == 0, s <= 1 ? (const T*)nullptr : prv, A.c1[li][s],
@@ -737,16 +739,15 @@ __global__ void __cluster_dims__(BOT_CTAS, 1, 1) __launch_bounds__(BOT_THREADS, 
     if (A.pre == 0) {
       for (long long i = g0; i < 3 * L.NP * L.nb; i += gs) u[i] = T(0);
       cl.sync();
-    } else if (cur != u) {
-      bot_copy<T>(L, cur, u, g0, gs);
-      cl.sync();
     }
-    bot_residual<T>(L, st, u, bv_f<T>(L), bv_r<T>(L), g0, gs);
+    ucur[li] = cur;
+    // the residual goes to a vector the iterate is not in
+    bot_residual<T>(L, st, cur, bv_f<T>(L), oth, g0, gs);
     cl.sync();
-    bot_restrict<T>(L, A.L[li + 1], bv_r<T>(L), bv_f<T>(A.L[li + 1]), g0, gs);
+    bot_restrict<T>(L, A.L[li + 1], oth, bv_f<T>(A.L[li + 1]), g0, gs);
     cl.sync();
   }
-  // coarsest: u = Kinv f at the listed nodes, zero elsewhere
+  // coarsest: u = Kinv f at the listed nodes, zero elsewhere; one warp per row
   {
     const Level& C = A.L[A.nl - 1];
     T* u = bv_u<T>(C);
@@ -763,32 +764,46 @@ __global__ void __cluster_dims__(BOT_CTAS, 1, 1) __launch_bounds__(BOT_THREADS, 
       cf[3 * i + 2] = (double)f[n + 2 * C.NP];
     }
     cl.sync();
-    for (long long rb = g0; rb < (long long)N * C.nb; rb += gs) {
+    const int lane = threadIdx.x & 31, warp = g0 >> 5, nwarps = gs >> 5;
+    for (long long rb = warp; rb < (long long)N * C.nb; rb += nwarps) {
       const long long b = rb / N;
       const int row = (int)(rb - b * N);
       const double* cf = A.cf + b * N;
-      double s = 0;
       const double* k = A.kinv + (long long)row * N;
-      for (int j = 0; j < N; j++) s += k[j] * cf[j];
-      u[b * VS + A.cnodes[row / 3] + (row % 3) * C.NP] = (T)s;
+      double s = 0;
+      for (int j = lane; j < N; j += 32) s += k[j] * cf[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (lane == 0) u[b * VS + A.cnodes[row / 3] + (row % 3) * C.NP] = (T)s;
     }
+    ucur[A.nl - 1] = u;
     cl.sync();
   }
-  // up: prolongation and post-smoothing
+  // up: prolongation and post-smoothing; the top level ends in its u
   for (int li = A.nl - 2; li >= A.lb; li--) {
     const Level& L = A.L[li];
     const T* st = bv_st<T>(L);
     T* u = bv_u<T>(L);
-    bot_prolong<T>(L, A.L[li + 1], bv_u<T>(A.L[li + 1]), u, g0, gs);
+    T *cur = ucur[li], *oth, *prv;
+    T* bufs[3] = {u, bv_t<T>(L), bv_r<T>(L)};
+    {
+      int k = 0;
+      T* rest[2];
+      for (int q = 0; q < 3; q++)
+        if (bufs[q] != cur) rest[k++] = bufs[q];
+      oth = rest[0];
+      prv = rest[1];
+    }
+    bot_prolong<T>(L, A.L[li + 1], ucur[li + 1], cur, g0, gs);
     cl.sync();
-    T *cur = u, *oth = bv_t<T>(L), *prv = bv_r<T>(L);
     for (int s = 0; s < A.post; s++) {
       bot_jacobi<T>(L, st, cur, bv_f<T>(L), oth, A.om[li][s], false, s == 0 ? (const T*)nullptr : prv, A.c1[li][s],
                     g0, gs);
       cl.sync();
       T* w = prv; prv = cur; cur = oth; oth = w;
     }
-    if (cur != u) {
+    ucur[li] = cur;
+    if (li == A.lb && cur != u) {
       bot_copy<T>(L, cur, u, g0, gs);
       cl.sync();
     }

@@ -576,7 +576,7 @@ def main():
     # DRAM bytes per fine node of one launch, measured by ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum) on a 193^3 case whose
     # working set exceeds L2, where traffic grows with the node count
-    traffic_per_node = {"fine_jacobi_fp32": 289.9e6 / 193 ** 3}
+    traffic_per_node = {"fine_jacobi_fp32": 284.1e6 / 193 ** 3}
     kn = kname.value.decode()
     traffic = traffic_per_node[kn] * (n + 1) ** 3 if kn in traffic_per_node else None
     roofline = {"kernel": kn, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -207,6 +207,7 @@ def run_solves(args):
     rho = g.projectDensities(g.coeff2density(np.asarray(coeff, np.float32)[:nc]), 8.0)
     g.set_density(rho)
     g.update_stencil()
+    tuned = g.autotune() if prec == R.rso.MIXED and not args.no_autotune else None
     f = torch.zeros(3 * g.nn, dtype=torch.float64, device="cuda")
     ln = torch.as_tensor(g.load_nodes(), device="cuda").long()
     f[2 * g.nn + ln] = torch.as_tensor(np.random.default_rng(1).standard_normal(len(ln)), device="cuda")
@@ -235,7 +236,7 @@ def run_solves(args):
     print(json.dumps({"metric": f"multigrid PCG solve @{n}^3 to rel.resid 1e-6 ({args.precision})",
                       "value": ms / args.steps, "unit": "ms/solve", "higher_is_better": False,
                       "iterations_per_solve": its / args.steps, "ms_per_iteration": ms / its,
-                      "levels": g_levels(n), "kernel_classes": classes}), flush=True)
+                      "levels": g_levels(n), "kernel_classes": classes, "launch_shapes": tuned}), flush=True)
     g.close()
 
 
@@ -281,6 +282,8 @@ def run_batch(args):
                                                     cheb_lower=CHEB_LOWER, pre=2, post=2, poisson_ratio=0.3))
     g.set_density(rho.ravel())
     g.update_stencil()
+    if prec == R.rso.MIXED and not args.no_autotune:
+        g.autotune()
     Ft = torch.as_tensor(F, device="cuda")
     for _ in range(max(1, args.warmup)):
         g.solve_batch(Ft, tol=1e-6, max_iter=500)
@@ -345,6 +348,8 @@ def run_problems(args):
                                                         youngs_modulus=1e6))
         g.set_density(rho.ravel())
         g.update_stencil()
+        if not args.no_autotune:
+            g.autotune()
         grids.append(g)
         loads.append(torch.as_tensor(f, device="cuda"))
 
@@ -473,6 +478,7 @@ def main():
     ap.add_argument("--ref-size", type=int, default=24)
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--mode", default="design", choices=["design", "solve", "batch", "problems", "scale"])
     ap.add_argument("--systems", type=int, default=16)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -528,11 +534,15 @@ def main():
     tot = ctypes.c_double(0)
     bytes_per = ctypes.c_double(0)
     flops_per = ctypes.c_double(0)
+    tuned = None
     for w in range(args.warmup):
         if w == args.warmup - 1:
             lib.rso_profile_reset(g.h)
             lib.rso_set_profiling(g.h, 1)
         step(g, mma)
+        if w == 0 and not args.no_autotune:
+            # launch shapes measured on this hierarchy once its operators exist
+            tuned = g.autotune()
     top_cls, top_ms = 0, -1.0
     for cls in range(16):
         if lib.rso_profile_class(g.h, cls, kname, 64, ctypes.byref(cnt), ctypes.byref(tot), ctypes.byref(bytes_per),
@@ -652,6 +662,7 @@ def main():
                 "last_iteration": {k: last[k] for k in ("c_worst", "lam", "volume", "ss_value", "solve_iterations",
                                                         "ms_operators", "ms_worst", "ms_selfsupport", "ms_adjoint",
                                                         "ms_mma")},
+                "launch_shapes": tuned,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)

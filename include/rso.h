@@ -193,6 +193,22 @@ rso_status rso_solve(rso_handle* h, const double* f_dev, double* u_dev, double t
  * buffers for k systems are allocated on the first call with that k and kept. */
 rso_status rso_solve_batch(rso_handle* h, int k, const double* F_dev, double* U_dev, double tol, int max_iter,
                            rso_solve_info* infos);
+/* Launch-shape autotuner (no counterpart in the reference, whose launch
+ * shapes are fixed): times, on this handle's hierarchy with CUDA events, the
+ * thread rows of the packed FP32 fine kernel (2 or 4), one thread per node or
+ * per (node, row) on every coarse level, and the first level of the bottom
+ * cluster kernel (or none), each timed as mixed-precision solves of a random
+ * load, and keeps the fastest for this handle (a candidate must beat the
+ * built-in rule by 1 %).  The candidates compute the same arithmetic.  Needs
+ * rso_update_operators first, mixed precision and a Jacobi or Chebyshev
+ * smoother; overwrites the solver's work vectors; takes a few dozen solves.  choices_host (NULL or
+ * 2 + number of levels ints): fine rows, bottom level (-1 none), then per
+ * level 0 = node per thread, 1 = row split, -1 not tuned. */
+rso_status rso_autotune(rso_handle* h, int* choices_host);
+/* Sets the launch shapes directly, in rso_autotune's format (n >= 2 ints;
+ * bottom level -2 restores the built-in size rule, a row-split entry of -1
+ * too), e.g. to reuse choices measured once for many handles. */
+rso_status rso_set_launch_shapes(rso_handle* h, const int* choices_host, int n);
 /* Replay of the FP32 V-cycle (the mixed-precision preconditioner) from CUDA
  * graphs (no counterpart in the reference, which launches every kernel):
  * on by default.  The V-cycle is captured the second time its launch

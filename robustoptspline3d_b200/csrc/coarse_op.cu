@@ -824,11 +824,18 @@ const double* stencil_of<double>(const Level& l) { return l.st64; }
 template <>
 const float* stencil_of<float>(const Level& l) { return l.st32; }
 
+// one thread per node on large levels, per (node, row) on small ones, unless
+// rso_autotune measured the level
+static bool node_per_thread(const rso_handle* h, int level) {
+  const int t = level < 16 ? h->tune.rowsplit[level] : -1;
+  return t >= 0 ? t == 0 : h->L[level].nn > kRowSplitMaxNodes;
+}
+
 template <typename T>
 rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* r) {
   const Level& l = h->L[level];
   if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
-  if (l.nn > kRowSplitMaxNodes) {
+  if (node_per_thread(h, level)) {
     if (l.nb == 1) {
       k_coarse<T, 0, 1><<<chunk_grid(l, 1), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0));
     } else {
@@ -846,7 +853,7 @@ rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T*
                          const T* u_prev, double c1) {
   const Level& l = h->L[level];
   if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
-  if (l.nn > kRowSplitMaxNodes) {
+  if (node_per_thread(h, level)) {
     if (l.nb == 1) {
       k_coarse<T, 2, 1><<<chunk_grid(l, 1), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1);
     } else {
@@ -927,6 +934,9 @@ int bottom_level(const rso_handle* h) {
   const int nl = (int)h->L.size();
   if (h->cfg.smoother == RSO_SMOOTH_GS || nl < 3 || nl > BOT_MAX_LEVELS || h->nc == 0) return -1;
   if (h->cfg.pre > BOT_MAX_SWEEPS || h->cfg.post > BOT_MAX_SWEEPS) return -1;
+  // a level chosen by rso_autotune: any level from 1 to nl - 2, or none
+  if (h->tune.bottom == -1) return -1;
+  if (h->tune.bottom >= 1 && h->tune.bottom <= nl - 2) return h->tune.bottom;
   int lb = nl - 1;
   while (lb - 1 >= 1 && h->L[lb - 1].nn <= kBottomMaxNodes) lb--;
   return lb <= nl - 2 ? lb : -1;

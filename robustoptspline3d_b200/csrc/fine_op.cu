@@ -530,16 +530,19 @@ constexpr int pair_smem_bytes(int nslot) {
   return 4 * (nslot * pair_slot<TYP>() + 2 * 12 * 32 * TYP) + 128;
 }
 
-// resident CTAs per SM the register budget is cut for: the residual fits 128
-// registers without spills, the Jacobi / Chebyshev step does not
-constexpr int pair_min_blocks(int mode) { return mode == 0 ? kPairMinBlocksRes : kPairMinBlocksJac; }
+// resident CTAs per SM (for 4 thread rows) the register budget is cut for:
+// the residual and the Jacobi / Chebyshev step fit 128 registers without
+// spills, K u (MODE 1, which carries u at the emitted nodes) 168
+constexpr int pair_min_blocks(int mode, int typ) {
+  return (mode == 0 ? kPairMinBlocksRes : mode == 2 ? kPairMinBlocksJac : 3) * 4 / typ;
+}
 
 // TMA: stage u planes and rho^p layers with bulk-tensor copies (tmu: 4-D map
 // (px, py, pz, 3 nb) of u, box 36 x (2 TYP + 1) x 1 x 3; tmr: 3-D map
 // (qx, qy, qz) of rho^p, box 36 x 2 TYP x 1; out-of-range boxes read zero);
 // otherwise every thread stages 16-byte chunks with cp.async.
 template <int MODE, int TYP, bool TMA>
-__global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE))
+__global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
     k_fine_p(const Level L, const float* __restrict__ u, const float* __restrict__ f, float* __restrict__ out,
              const float* __restrict__ rp, float omega, double* __restrict__ dotp, const float* __restrict__ uprev,
              float c1, const __grid_constant__ CUtensorMap tmu, const __grid_constant__ CUtensorMap tmr) {
@@ -995,10 +998,10 @@ constexpr int WTY = 8;
 static inline dim3 march_grid(const Level& l) {
   return dim3(cdiv(l.nx, WTX - 1), cdiv(l.ny, WTY - 1), cdiv(l.nz, FZC) * l.nb);
 }
-constexpr int PTY = 4;          // thread rows of the packed FP32 kernel (2 PTY element rows)
 constexpr bool kPairTMA = true;  // packed kernel stages with TMA (else cp.async)
-static inline dim3 pair_grid(const Level& l) {
-  return dim3(cdiv(l.nx, WTX - 1), cdiv(l.ny, 2 * PTY - 1), cdiv(l.nz, FZC) * l.nb);
+// thread rows pty of the packed FP32 kernel (2 pty element rows; rso_autotune picks 2 or 4)
+static inline dim3 pair_grid(const Level& l, int pty) {
+  return dim3(cdiv(l.nx, WTX - 1), cdiv(l.ny, 2 * pty - 1), cdiv(l.nz, FZC) * l.nb);
 }
 
 template <typename T>
@@ -1078,25 +1081,34 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
   // FP32: two columns per thread on packed pairs, staged by TMA; FP64: one
   // column per thread, staged by cp.async
   constexpr bool packed = sizeof(T) == 4;
-  constexpr int smem = packed ? pair_smem_bytes<PTY>(pair_slots(MODE, kPairTMA)) : walsh_smem_bytes<T, WTY>();
+  const int pty = h->tune.fine_rows == 2 ? 2 : 4;
+  const int smem = packed ? (pty == 2 ? pair_smem_bytes<2>(pair_slots(MODE, kPairTMA))
+                                      : pair_smem_bytes<4>(pair_slots(MODE, kPairTMA)))
+                          : walsh_smem_bytes<T, WTY>();
   const void* kern;
   if constexpr (packed)
-    kern = reinterpret_cast<const void*>(k_fine_p<MODE, PTY, kPairTMA>);
+    kern = pty == 2 ? reinterpret_cast<const void*>(k_fine_p<MODE, 2, kPairTMA>)
+                    : reinterpret_cast<const void*>(k_fine_p<MODE, 4, kPairTMA>);
   else
     kern = reinterpret_cast<const void*>(k_fine_w<T, MODE, WTY>);
-  // the shared-memory opt-in is per device; setting it twice from racing
-  // threads is harmless, so an atomic flag per device suffices
-  static std::atomic<bool> attr[64];
-  if (h->device < 0 || h->device >= 64 || !attr[h->device].load(std::memory_order_acquire)) {
+  // the shared-memory opt-in is per device and kernel; setting it twice from
+  // racing threads is harmless, so an atomic flag per device suffices
+  static std::atomic<bool> attr[2][64];
+  std::atomic<bool>* done = (h->device >= 0 && h->device < 64) ? &attr[pty == 2][h->device] : nullptr;
+  if (!done || !done->load(std::memory_order_acquire)) {
     RSO_CHECK_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    if (h->device >= 0 && h->device < 64) attr[h->device].store(true, std::memory_order_release);
+    if (done) done->store(true, std::memory_order_release);
   }
   if constexpr (packed) {
     CUtensorMap mu{}, mr{};
-    if (kPairTMA) RSO_TRY(pair_tensor_maps(h, l, u, rp, 2 * PTY, &mu, &mr));
+    if (kPairTMA) RSO_TRY(pair_tensor_maps(h, l, u, rp, 2 * pty, &mu, &mr));
     if (h->prof_on) prof_begin(h, cls, (double)l.nn);
-    k_fine_p<MODE, PTY, kPairTMA><<<pair_grid(l), dim3(WTX, PTY), smem, h->stream>>>(
-        l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, mu, mr);
+    if (pty == 2)
+      k_fine_p<MODE, 2, kPairTMA><<<pair_grid(l, 2), dim3(WTX, 2), smem, h->stream>>>(
+          l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, mu, mr);
+    else
+      k_fine_p<MODE, 4, kPairTMA><<<pair_grid(l, 4), dim3(WTX, 4), smem, h->stream>>>(
+          l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, mu, mr);
   } else {
     if (h->prof_on) prof_begin(h, cls, (double)l.nn);
     k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega, dotp,

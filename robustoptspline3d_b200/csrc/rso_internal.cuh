@@ -144,6 +144,13 @@ struct rso_handle {
   double *fw = nullptr, *uw = nullptr;             // worst-case force / displacement (padded)
   unsigned prof_on = 0;                            // classes with per-kernel event timing (prof.cu)
   void* prof = nullptr;
+  // launch shapes chosen by rso_autotune (autotune.cu); -1 / -2 keep the built-in rules
+  struct Tune {
+    int fine_rows = 4;      // thread rows of a CTA of the packed FP32 fine kernel (2 or 4)
+    int rowsplit[16];       // per level: 1 one thread per (node, row), 0 one per node, -1 by size
+    int bottom = -2;        // first level of the bottom cluster kernel, -1 none, -2 by size
+    Tune() { for (int& r : rowsplit) r = -1; }
+  } tune;
   void* vcg = nullptr;                             // captured FP32 V-cycles (solver.cu)
   void* cap_prof = nullptr;                        // event pairs of the V-cycle capture in progress (prof.cu)
   bool vc_graphs = true;                           // replay captured V-cycles (rso_set_vcycle_graphs)

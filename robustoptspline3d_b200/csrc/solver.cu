@@ -259,6 +259,8 @@ std::vector<uint64_t> vc_key(const rso_handle* h) {
   push_bits(k, h->c_K); push_bits(k, h->c_nodes); push_bits(k, h->c_f); push_bits(k, h->c_fb); push_bits(k, h->nc);
   push_bits(k, h->cfg.smoother); push_bits(k, h->cfg.pre); push_bits(k, h->cfg.post);
   push_bits(k, h->cfg.omega); push_bits(k, h->cfg.cheb_lower); push_bits(k, h->prof_on);
+  push_bits(k, h->tune.fine_rows); push_bits(k, h->tune.bottom);
+  for (int r : h->tune.rowsplit) push_bits(k, r);
   return k;
 }
 

@@ -94,6 +94,8 @@ SIGNATURES = {
     "rso_residual": (_ci, [_vp, _vp, _vp, _vp]),
     "rso_fine_sweep_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
     "rso_set_vcycle_graphs": (_ci, [_vp, _ci]),
+    "rso_autotune": (_ci, [_vp, _pi]),
+    "rso_set_launch_shapes": (_ci, [_vp, _pi, _ci]),
     "rso_get_stencil": (_ci, [_vp, _ci, _vp]),
     "rso_coarse_residual": (_ci, [_vp, _ci, _vp, _vp, _vp]),
     "rso_smooth": (_ci, [_vp, _ci, _vp, _vp, _ci, _cd, _ci, _ci]),
@@ -385,6 +387,19 @@ class HierarchyGrid:
         r = torch.empty_like(u)
         self._chk(self.lib.rso_residual(self.h, _dev(u, torch.float64), _dev(f, torch.float64), _dev(r)), "rso_residual")
         return r
+
+    def autotune(self):
+        """Time the launch-shape alternatives on this hierarchy and keep the fastest
+        (rso_autotune); returns the choices."""
+        c = np.zeros(2 + self.n_levels(), np.int32)
+        self._chk(self.lib.rso_autotune(self.h, _np_ptr(c, _pi)), "rso_autotune")
+        return {"fine_rows": int(c[0]), "bottom_level": int(c[1]), "row_split": [int(x) for x in c[2:]]}
+
+    def set_launch_shapes(self, fine_rows=4, bottom_level=-2, row_split=None):
+        """Launch shapes in rso_autotune's terms (rso_set_launch_shapes)."""
+        rs = list(row_split or [])
+        c = np.array([fine_rows, bottom_level] + rs, np.int32)
+        self._chk(self.lib.rso_set_launch_shapes(self.h, _np_ptr(c, _pi), len(c)), "rso_set_launch_shapes")
 
     def set_vcycle_graphs(self, on):
         """Replay captured FP32 V-cycles from CUDA graphs (default) or launch every kernel."""

@@ -1,0 +1,68 @@
+"""Launch-shape autotuner (rso_autotune / rso_set_launch_shapes) through the C ABI.
+The alternatives compute the same arithmetic in other launch shapes, so every
+forced combination of fine tile height, coarse kernel variant and bottom-kernel
+level must solve to the same answer: the solves run to relative residual 1e-10
+and must agree to 1e-8 relative with iteration counts within one."""
+import numpy as np
+import pytest
+
+import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300)
+
+
+def make(prob):
+    from robustoptspline3d_b200 import Config, HierarchyGrid
+    g = HierarchyGrid(prob["emask"], prob["fixed"], prob["load"], prob["normals"],
+                      Config(precision=1, smoother=2, poisson_ratio=0.4, cheb_lower=0.1))
+    g.set_density(prob["rho"].astype(np.float32).ravel())
+    g.update_stencil()
+    return g
+
+
+def rhs(g, seed=31):
+    rng = np.random.default_rng(seed)
+    f = np.zeros(3 * g.nn)
+    ln = g.load_nodes()
+    for c in range(3):
+        f[c * g.nn + ln] = rng.standard_normal(len(ln))
+    return f
+
+
+@pytest.mark.parametrize("gen", [lambda: P.cantilever(64, 32, 32), lambda: P.ellipsoid(40, 24, 24)])
+def test_autotune_choices_solve_alike(cuda, gen):
+    prob = gen()
+    g = make(prob)
+    nl = g.n_levels()
+    f = cuda.tensor(rhs(g), dtype=cuda.float64, device="cuda")
+    u_ref, it_ref, _, _ = g.solve(f, tol=1e-10, max_iter=300)
+    u_ref = u_ref.cpu().numpy()
+    ch = g.autotune()
+    assert ch["fine_rows"] in (2, 4)
+    assert ch["bottom_level"] == -1 or 1 <= ch["bottom_level"] <= nl - 2
+    assert len(ch["row_split"]) == nl and all(r in (-1, 0, 1) for r in ch["row_split"])
+    u, it, _, _ = g.solve(f, tol=1e-10, max_iter=300)
+    assert abs(it - it_ref) <= 1 and rel(u.cpu().numpy(), u_ref) < 1e-8
+    for rows in (2, 4):
+        for bottom in [-1] + list(range(1, nl - 1)):
+            for split in (0, 1):
+                g.set_launch_shapes(rows, bottom, [-1] + [split] * (nl - 1))
+                u, it, rr, _ = g.solve(f, tol=1e-10, max_iter=300)
+                assert rr < 1e-10
+                assert abs(it - it_ref) <= 1, (rows, bottom, split)
+                assert rel(u.cpu().numpy(), u_ref) < 1e-8, (rows, bottom, split)
+    g.close()
+
+
+def test_launch_shapes_rejected(cuda):
+    from robustoptspline3d_b200 import RSOError
+    g = make(P.cantilever(32, 16, 16))
+    with pytest.raises(RSOError):
+        g.set_launch_shapes(3)
+    with pytest.raises(RSOError):
+        g.set_launch_shapes(4, bottom_level=g.n_levels())
+    g.close()

@@ -109,6 +109,129 @@ __global__ void __launch_bounds__(256) k_coarse(const Level L, const T* __restri
   }
 }
 
+// FP32 variant for large single-system levels: a thread owns four
+// consecutive padded nodes (px is a multiple of 4, so a group never spans two
+// rows and starts on 16 bytes) and streams the 243 stencil rows, f, the
+// iterate and the node classes with 16-byte loads; the neighbour values of a
+// row of the 3 x 3 x 3 neighbourhood come as one 16-byte load and two scalar
+// ones.  Halo rows are skipped, halo and inactive nodes of a group are written
+// as the per-node kernel leaves them (zero, or f for the residual).
+template <int MODE>
+__global__ void __launch_bounds__(256) k_coarse4(const Level L, const float* __restrict__ st,
+                                                 const float* __restrict__ u, const float* __restrict__ f,
+                                                 float* __restrict__ out, float omega,
+                                                 const float* __restrict__ uprev, float c1) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long NP = L.NP, px = L.px, pxy = (long long)L.px * L.py;
+  const long long p0 = 4 * g;
+  if (p0 >= NP) return;
+  const int zp = (int)(p0 / pxy);
+  const long long rem = p0 - zp * pxy;
+  const int yp = (int)(rem / px), xp = (int)(rem - yp * px);
+  if (zp < 1 || zp > L.nz || yp < 1 || yp > L.ny) return;  // halo row: stays zero
+  const uchar4 cl4 = *reinterpret_cast<const uchar4*>(L.vclass + p0);
+  const uint8_t cls[4] = {cl4.x, cl4.y, cl4.z, cl4.w};
+  bool act[4];
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int x = xp + k - 1;  // node x index
+    act[k] = x >= 0 && x < L.nx && (cls[k] & NC_ACTIVE);
+    any = any || act[k];
+  }
+  float acc[3][4];
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) acc[r][k] = 0.f;
+  float S[9][4];
+  if (any) {
+#pragma unroll
+    for (int d = 0; d < 27; d++) {
+      const long long nb = p0 + (d / 3 % 3 - 1) * px + (d / 9 - 1) * pxy;  // same row offset, dx below
+      const int dx = d % 3 - 1;
+      float un[3][4];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const float* uc = u + nb + c * NP;
+        const float4 m = *reinterpret_cast<const float4*>(uc);
+        if (dx == 0) {
+          un[c][0] = m.x; un[c][1] = m.y; un[c][2] = m.z; un[c][3] = m.w;
+        } else if (dx < 0) {
+          // the left neighbour of the group's first node; at xp = 0 that node
+          // is halo (its result is discarded) and the read would leave the row
+          un[c][0] = xp > 0 ? uc[-1] : 0.f; un[c][1] = m.x; un[c][2] = m.y; un[c][3] = m.z;
+        } else {
+          // likewise at the row's end: xp + 3 = px - 1 is halo
+          un[c][0] = m.y; un[c][1] = m.z; un[c][2] = m.w; un[c][3] = xp + 4 < px ? uc[4] : 0.f;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const float4 sv = *reinterpret_cast<const float4*>(st + (d * 9 + r * 3 + c) * NP + p0);
+          acc[r][0] = fmaf(sv.x, un[c][0], acc[r][0]);
+          acc[r][1] = fmaf(sv.y, un[c][1], acc[r][1]);
+          acc[r][2] = fmaf(sv.z, un[c][2], acc[r][2]);
+          acc[r][3] = fmaf(sv.w, un[c][3], acc[r][3]);
+          if (MODE == 2 && d == 13) {
+            S[r * 3 + c][0] = sv.x; S[r * 3 + c][1] = sv.y; S[r * 3 + c][2] = sv.z; S[r * 3 + c][3] = sv.w;
+          }
+        }
+    }
+  }
+  float res[3][4];
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    const float4 fv = *reinterpret_cast<const float4*>(f + p0 + r * NP);
+    // K u is zero at inactive nodes, as in the per-node kernel
+    res[r][0] = fv.x - (act[0] ? acc[r][0] : 0.f); res[r][1] = fv.y - (act[1] ? acc[r][1] : 0.f);
+    res[r][2] = fv.z - (act[2] ? acc[r][2] : 0.f); res[r][3] = fv.w - (act[3] ? acc[r][3] : 0.f);
+  }
+  if (MODE == 0) {
+    // out = f - K u; at the halo nodes of the group f is zero, so they keep their zero
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+      *reinterpret_cast<float4*>(out + p0 + r * NP) = make_float4(res[r][0], res[r][1], res[r][2], res[r][3]);
+    return;
+  }
+  float uo[3][4], up[3][4];
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    const float4 uv = *reinterpret_cast<const float4*>(u + p0 + r * NP);
+    uo[r][0] = uv.x; uo[r][1] = uv.y; uo[r][2] = uv.z; uo[r][3] = uv.w;
+    float4 pv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (uprev) pv = *reinterpret_cast<const float4*>(uprev + p0 + r * NP);
+    up[r][0] = pv.x; up[r][1] = pv.y; up[r][2] = pv.z; up[r][3] = pv.w;
+  }
+  float o[3][4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (!act[k]) {
+      o[0][k] = o[1][k] = o[2][k] = 0.f;
+      continue;
+    }
+    float Sk[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) Sk[i] = S[i][k];
+    const float r0 = res[0][k], r1 = res[1][k], r2 = res[2][k];
+    const float A = Sk[4] * Sk[8] - Sk[5] * Sk[7], B = -(Sk[3] * Sk[8] - Sk[5] * Sk[6]),
+                C = Sk[3] * Sk[7] - Sk[4] * Sk[6];
+    const float det = Sk[0] * A + Sk[1] * B + Sk[2] * C;
+    const float id = omega / det;
+    const float i01 = -(Sk[1] * Sk[8] - Sk[2] * Sk[7]), i02 = Sk[1] * Sk[5] - Sk[2] * Sk[4];
+    const float i11 = Sk[0] * Sk[8] - Sk[2] * Sk[6], i12 = -(Sk[0] * Sk[5] - Sk[2] * Sk[3]);
+    const float i21 = -(Sk[0] * Sk[7] - Sk[1] * Sk[6]), i22 = Sk[0] * Sk[4] - Sk[1] * Sk[3];
+    o[0][k] = uo[0][k] + c1 * (uo[0][k] - up[0][k]) + id * (A * r0 + i01 * r1 + i02 * r2);
+    o[1][k] = uo[1][k] + c1 * (uo[1][k] - up[1][k]) + id * (B * r0 + i11 * r1 + i12 * r2);
+    o[2][k] = uo[2][k] + c1 * (uo[2][k] - up[2][k]) + id * (C * r0 + i21 * r1 + i22 * r2);
+  }
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+    *reinterpret_cast<float4*>(out + p0 + r * NP) = make_float4(o[r][0], o[r][1], o[r][2], o[r][3]);
+}
+
 // Row-split variant for the small, latency-bound levels (MODE as above).
 // Thread (x, y, r) owns
 // output component r of node (x, y, z), so each node's 243 stencil entries
@@ -836,7 +959,10 @@ rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* 
   const Level& l = h->L[level];
   if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
   if (node_per_thread(h, level)) {
-    if (l.nb == 1) {
+    if (l.nb == 1 && sizeof(T) == 4) {
+      k_coarse4<0><<<cdiv(l.NP / 4, 256), 256, 0, h->stream>>>(l, (const float*)stencil_of<T>(l), (const float*)u,
+                                                               (const float*)f, (float*)r, 0.f, nullptr, 0.f);
+    } else if (l.nb == 1) {
       k_coarse<T, 0, 1><<<chunk_grid(l, 1), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0));
     } else {
       k_coarse<T, 0, 4><<<chunk_grid(l, 4), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0));
@@ -854,7 +980,11 @@ rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T*
   const Level& l = h->L[level];
   if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
   if (node_per_thread(h, level)) {
-    if (l.nb == 1) {
+    if (l.nb == 1 && sizeof(T) == 4) {
+      k_coarse4<2><<<cdiv(l.NP / 4, 256), 256, 0, h->stream>>>(l, (const float*)stencil_of<T>(l), (const float*)u_in,
+                                                               (const float*)f, (float*)u_out, (float)omega,
+                                                               (const float*)u_prev, (float)c1);
+    } else if (l.nb == 1) {
       k_coarse<T, 2, 1><<<chunk_grid(l, 1), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1);
     } else {
       k_coarse<T, 2, 4><<<chunk_grid(l, 4), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1);

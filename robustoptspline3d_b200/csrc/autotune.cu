@@ -82,7 +82,7 @@ rso_status solve_ms(rso_handle* h, double* ms) {
 
 // a candidate replaces the incumbent (the first value, the built-in rule's
 // choice) only when it is faster by more than the run-to-run noise
-constexpr double kTuneMargin = 0.99;
+constexpr double kTuneMargin = 0.97;
 
 // tries the values of one choice in turn, keeps the fastest
 template <typename Set>

@@ -129,6 +129,7 @@ static void free_handle(rso_handle* h) {
   cudaFree(h->e_a); cudaFree(h->e_b); cudaFree(h->e_c); cudaFree(h->e_d); cudaFree(h->e_rhohat);
   cudaFree(h->coef_a); cudaFree(h->coef_b); cudaFree(h->coef_c);
   cudaFree(h->coef_df); cudaFree(h->coef_dg); cudaFree(h->fw); cudaFree(h->uw);
+  cudaFree(h->wc_buf);
   vcycle_graphs_free(h);
   prof_free(h);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);

@@ -954,10 +954,17 @@ static bool node_per_thread(const rso_handle* h, int level) {
   return t >= 0 ? t == 0 : h->L[level].nn > kRowSplitMaxNodes;
 }
 
+// profiling class of a coarse sweep: the streamed FP32 kernel has its own
+static int coarse_class(const rso_handle* h, int level, int elem_size) {
+  if (elem_size == 8) return PC_COARSE64;
+  return node_per_thread(h, level) && h->L[level].nb == 1 ? PC_COARSE32_STREAM : PC_COARSE32;
+}
+
 template <typename T>
 rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* r) {
   const Level& l = h->L[level];
-  if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
+  const int cls = coarse_class(h, level, sizeof(T));
+  if (h->prof_on) prof_begin(h, cls, (double)l.nn);
   if (node_per_thread(h, level)) {
     if (l.nb == 1 && sizeof(T) == 4) {
       k_coarse4<0><<<cdiv(l.NP / 4, 256), 256, 0, h->stream>>>(l, (const float*)stencil_of<T>(l), (const float*)u,
@@ -971,14 +978,15 @@ rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* 
   } else {
     k_coarse_r<T, 0><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz * l.nb), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0)); rso::note_launch();
   }
-  if (h->prof_on) prof_end(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64));
+  if (h->prof_on) prof_end(h, cls);
   return launch_check(h, "coarse_residual");
 }
 template <typename T>
 rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T* u_out, double omega,
                          const T* u_prev, double c1) {
   const Level& l = h->L[level];
-  if (h->prof_on) prof_begin(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64), (double)l.nn);
+  const int cls = coarse_class(h, level, sizeof(T));
+  if (h->prof_on) prof_begin(h, cls, (double)l.nn);
   if (node_per_thread(h, level)) {
     if (l.nb == 1 && sizeof(T) == 4) {
       k_coarse4<2><<<cdiv(l.NP / 4, 256), 256, 0, h->stream>>>(l, (const float*)stencil_of<T>(l), (const float*)u_in,
@@ -993,7 +1001,7 @@ rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T*
   } else {
     k_coarse_r<T, 2><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz * l.nb), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1); rso::note_launch();
   }
-  if (h->prof_on) prof_end(h, (sizeof(T) == 4 ? PC_COARSE32 : PC_COARSE64));
+  if (h->prof_on) prof_end(h, cls);
   return launch_check(h, "coarse_jacobi");
 }
 template <typename T>

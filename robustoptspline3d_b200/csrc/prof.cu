@@ -34,6 +34,8 @@ static const ProfClassInfo kInfo[PC_N] = {
     {"fine_gs_fp64", 24 + 24 + 8 + 1 + 24, 1200 + 80},
     {"coarse_stencil_fp32", 243 * 4 + 12 + 12 + 12 + 1, 486},
     {"coarse_stencil_fp64", 243 * 8 + 24 + 24 + 24 + 1, 486},
+    // the same operator, four nodes per thread on 16-byte streams (large FP32 levels)
+    {"coarse_stencil_fp32_streamed", 243 * 4 + 12 + 12 + 12 + 1, 486},
 };
 
 struct Prof {

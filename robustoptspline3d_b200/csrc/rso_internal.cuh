@@ -151,6 +151,10 @@ struct rso_handle {
     int bottom = -2;        // first level of the bottom cluster kernel, -1 none, -2 by size
     Tune() { for (int& r : rowsplit) r = -1; }
   } tune;
+  // worst-case scratch kept between calls (worst.cu): Lanczos load-space
+  // vectors, reorthogonalisation sums, the force-projection vector
+  double* wc_buf = nullptr;
+  size_t wc_cap = 0;
   void* vcg = nullptr;                             // captured FP32 V-cycles (solver.cu)
   void* cap_prof = nullptr;                        // event pairs of the V-cycle capture in progress (prof.cu)
   bool vc_graphs = true;                           // replay captured V-cycles (rso_set_vcycle_graphs)
@@ -160,7 +164,7 @@ namespace rso {
 // launch accounting and profiling (prof.cu)
 enum ProfClass {
   PC_FINE_JAC32, PC_FINE_RES32, PC_FINE_GS32, PC_FINE_APPLYK64, PC_FINE_RES64, PC_FINE_JAC64, PC_FINE_GS64,
-  PC_COARSE32, PC_COARSE64, PC_N
+  PC_COARSE32, PC_COARSE64, PC_COARSE32_STREAM, PC_N
 };
 void note_launch();
 void note_launches(long long n);

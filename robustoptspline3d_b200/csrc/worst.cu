@@ -1,6 +1,7 @@
 // Worst-case load machinery: admissible-load projection on the load nodes,
 // Lanczos for lambda_max of P K^-1 P with full FP64 reorthogonalisation
-// (each step one multigrid solve), and the reference's modified power method.
+// (each step one multigrid solve; classical Gram-Schmidt twice on the
+// device), and the reference's modified power method.
 #include "rso_internal.cuh"
 #include <cmath>
 #include <vector>
@@ -31,6 +32,56 @@ __global__ void k_scatter_load(const double* __restrict__ v, const int* __restri
   f[n] += a * v[3 * k]; f[n + NP] += a * v[3 * k + 1]; f[n + 2 * NP] += a * v[3 * k + 2];
 }
 
+// Reorthogonalisation against all previous Lanczos vectors on the device:
+// classical Gram-Schmidt applied twice ("twice is enough"), so a Lanczos step
+// needs one host synchronisation instead of one per previous vector.
+// s[j] = V_j . w for j < nj, partial sums in a fixed order (reproducible).
+constexpr int MD_PARTS = 32, MD_THREADS = 256, MD_MAX = 128;
+__global__ void __launch_bounds__(MD_THREADS) k_multi_dot_part(const double* __restrict__ V, long long ls,
+                                                               const double* __restrict__ w,
+                                                               double* __restrict__ part) {
+  const int j = blockIdx.y;
+  const double* v = V + ls * j;
+  double s = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ls; i += (long long)gridDim.x * blockDim.x)
+    s += v[i] * w[i];
+  __shared__ double ws[MD_THREADS / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+#pragma unroll
+    for (int k = 0; k < MD_THREADS / 32; k++) t += ws[k];
+    part[j * MD_PARTS + blockIdx.x] = t;
+  }
+}
+__global__ void k_multi_dot_final(const double* __restrict__ part, int nj, double* __restrict__ s) {
+  const int j = threadIdx.x;
+  if (j >= nj) return;
+  double t = 0;
+  for (int p = 0; p < MD_PARTS; p++) t += part[j * MD_PARTS + p];
+  s[j] = t;
+}
+// w -= sum_j s[j] V_j
+__global__ void k_multi_axpy(const double* __restrict__ V, long long ls, int nj, const double* __restrict__ s,
+                             double* __restrict__ w) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= ls) return;
+  double acc = w[i];
+  for (int j = 0; j < nj; j++) acc -= s[j] * V[ls * j + i];
+  w[i] = acc;
+}
+
+static rso_status reorthogonalise(rso_handle* h, const double* V, long long ls, int nj, double* w, double* part,
+                                  double* s) {
+  k_multi_dot_part<<<dim3(MD_PARTS, nj), MD_THREADS, 0, h->stream>>>(V, ls, w, part); note_launch();
+  k_multi_dot_final<<<1, MD_MAX, 0, h->stream>>>(part, nj, s); note_launch();
+  k_multi_axpy<<<cdiv(ls, 256), 256, 0, h->stream>>>(V, ls, nj, s, w); note_launch();
+  return launch_check(h, "reorthogonalise");
+}
+
 __global__ void k_rand_load(double* v, int nl, uint64_t seed) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < 3 * nl) v[i] = rso_urand(seed, (uint64_t)i);
@@ -41,6 +92,21 @@ __global__ void k_project_ls(double* v, const double* __restrict__ nrm, int nl) 
   if (k >= nl) return;
   const double s = v[3 * k] * nrm[3 * k] + v[3 * k + 1] * nrm[3 * k + 1] + v[3 * k + 2] * nrm[3 * k + 2];
   v[3 * k] = s * nrm[3 * k]; v[3 * k + 1] = s * nrm[3 * k + 1]; v[3 * k + 2] = s * nrm[3 * k + 2];
+}
+
+// worst-case scratch of at least n doubles, kept on the handle (grown with a
+// synchronous reallocation, so loops that reuse it allocate nothing)
+static rso_status wc_scratch(rso_handle* h, size_t n, double** out) {
+  if (h->wc_cap < n) {
+    RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+    cudaFree(h->wc_buf);
+    h->wc_buf = nullptr;
+    h->wc_cap = 0;
+    RSO_CHECK_CUDA(h, cudaMalloc(&h->wc_buf, sizeof(double) * n));
+    h->wc_cap = n;
+  }
+  *out = h->wc_buf;
+  return RSO_OK;
 }
 
 rso_status force_project(rso_handle* h, double* f, int cf) {
@@ -105,6 +171,7 @@ rso_status worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t see
   const int nl = h->n_load;
   if (nl == 0) { h->err = "no load nodes"; return RSO_ERR_STATE; }
   if (steps < 1) return RSO_ERR_INVALID_ARG;
+  if (steps >= MD_MAX) { h->err = "at most 127 Lanczos steps"; return RSO_ERR_INVALID_ARG; }
   const long long n3 = 3 * l0.NP;
   const long long ls = 3LL * nl;
   while ((int)h->lanczos_u.size() < steps) {
@@ -112,10 +179,14 @@ rso_status worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t see
     RSO_CHECK_CUDA(h, cudaMalloc(&p, sizeof(double) * n3));
     h->lanczos_u.push_back(p);
   }
-  double* V = nullptr;  // (steps+1) load-space vectors
-  double* wv = nullptr;
-  RSO_CHECK_CUDA(h, cudaMallocAsync(&V, sizeof(double) * ls * (steps + 1), h->stream));
-  RSO_CHECK_CUDA(h, cudaMallocAsync(&wv, sizeof(double) * ls, h->stream));
+  // (steps+1) load-space vectors V, the work vector wv, and the
+  // reorthogonalisation scratch: partials, two coefficient vectors, (alpha, beta^2)
+  double* buf = nullptr;
+  RSO_TRY(wc_scratch(h, (size_t)ls * (steps + 2) + MD_MAX * MD_PARTS + 2 * MD_MAX + 2, &buf));
+  double* V = buf;
+  double* wv = V + (size_t)ls * (steps + 1);
+  double* rw = wv + ls;
+  double *part = rw, *s1 = rw + MD_MAX * MD_PARTS, *s2 = s1 + MD_MAX, *ab = s2 + MD_MAX;
   k_rand_load<<<cdiv(ls, 128), 128, 0, h->stream>>>(V, nl, seed); rso::note_launch();
   if (cf) { k_project_ls<<<cdiv(nl, 128), 128, 0, h->stream>>>(V, h->load_normals, nl); rso::note_launch(); }
   double nv = 0;
@@ -134,17 +205,16 @@ rso_status worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t see
     RSO_TRY(solve_pcg(h, h->w, u, tol, 4000, &si));
     total_it += si.iterations;
     k_gather_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(u, l0.NP, h->load_nodes, h->load_normals, nl, cf, wv); rso::note_launch();
-    double a = 0;
-    RSO_TRY(dot_host(h, v, wv, ls, &a));
+    // alpha = v . w is the first pass's coefficient on v (the newest vector)
+    RSO_TRY(reorthogonalise(h, V, ls, it + 1, wv, part, s1));
+    RSO_TRY(reorthogonalise(h, V, ls, it + 1, wv, part, s2));
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(ab, s1 + it, sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    RSO_TRY(dot(h, wv, wv, ls, ab + 1));
+    double hab[2];
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(hab, ab, sizeof(hab), cudaMemcpyDeviceToHost, h->stream));
+    RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+    const double a = hab[0], b2 = hab[1];
     al.push_back(a);
-    for (int pass = 0; pass < 2; pass++)
-      for (int j = 0; j <= it; j++) {
-        double s = 0;
-        RSO_TRY(dot_host(h, V + ls * j, wv, ls, &s));
-        RSO_TRY(axpby(h, ls, -s, V + ls * j, 1.0, wv));
-      }
-    double b2 = 0;
-    RSO_TRY(dot_host(h, wv, wv, ls, &b2));
     const double b = std::sqrt(b2);
     if (it == steps - 1 || b < 1e-14 * std::fabs(a)) break;
     be.push_back(b);
@@ -165,8 +235,6 @@ rso_status worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t see
     RSO_TRY(axpby(h, n3, y, h->lanczos_u[k], 1.0, u_out));
   }
   RSO_TRY(launch_check(h, "worst_case"));
-  RSO_CHECK_CUDA(h, cudaFreeAsync(V, h->stream));
-  RSO_CHECK_CUDA(h, cudaFreeAsync(wv, h->stream));
   if (iters) *iters = total_it;
   return RSO_OK;
 }

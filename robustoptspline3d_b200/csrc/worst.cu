@@ -109,17 +109,21 @@ static rso_status wc_scratch(rso_handle* h, size_t n, double** out) {
   return RSO_OK;
 }
 
+// the projection vector lives in the last 3 n_load entries of the worst-case
+// scratch (the modified power method keeps its two vectors in front of it)
 rso_status force_project(rso_handle* h, double* f, int cf) {
   const Level& l = h->L[0];
   const int nl = h->n_load;
-  double* v = nullptr;
-  RSO_CHECK_CUDA(h, cudaMallocAsync(&v, sizeof(double) * 3 * (nl > 0 ? nl : 1), h->stream));
+  const size_t ls = (size_t)3 * (nl > 0 ? nl : 1);
+  if (h->wc_cap < 3 * ls) {
+    double* b = nullptr;
+    RSO_TRY(wc_scratch(h, 3 * ls, &b));
+  }
+  double* v = h->wc_buf + 2 * ls;
   if (nl) { k_gather_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(f, l.NP, h->load_nodes, h->load_normals, nl, cf, v); rso::note_launch(); }
   RSO_CHECK_CUDA(h, cudaMemsetAsync(f, 0, sizeof(double) * 3 * l.NP, h->stream));
   if (nl) { k_scatter_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(v, h->load_nodes, nl, l.NP, 1.0, f); rso::note_launch(); }
-  RSO_TRY(launch_check(h, "force_project"));
-  RSO_CHECK_CUDA(h, cudaFreeAsync(v, h->stream));
-  return RSO_OK;
+  return launch_check(h, "force_project");
 }
 
 // symmetric tridiagonal eigenproblem of the Lanczos matrix (tiny, host)
@@ -245,9 +249,10 @@ rso_status modified_pm(rso_handle* h, int cf, uint64_t seed, int max_itn, double
   const int nl = h->n_load;
   if (nl == 0) { h->err = "no load nodes"; return RSO_ERR_STATE; }
   const long long n3 = 3 * l0.NP, ls = 3LL * nl;
-  double *fs = nullptr, *fs_old = nullptr;
-  RSO_CHECK_CUDA(h, cudaMallocAsync(&fs, sizeof(double) * ls, h->stream));
-  RSO_CHECK_CUDA(h, cudaMallocAsync(&fs_old, sizeof(double) * ls, h->stream));
+  // two load-space vectors and the projection vector of force_project, kept on the handle
+  double* buf = nullptr;
+  RSO_TRY(wc_scratch(h, (size_t)3 * ls, &buf));
+  double *fs = buf, *fs_old = buf + ls;
   k_rand_load<<<cdiv(ls, 128), 128, 0, h->stream>>>(fs, nl, seed); rso::note_launch();
   RSO_CHECK_CUDA(h, cudaMemsetAsync(f, 0, sizeof(double) * n3, h->stream));
   k_scatter_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(fs, h->load_nodes, nl, l0.NP, 1.0, f); rso::note_launch();
@@ -277,8 +282,6 @@ rso_status modified_pm(rso_handle* h, int cf, uint64_t seed, int max_itn, double
   }
   if (itn_out) *itn_out = itn;
   if (c_worst) RSO_TRY(dot_host(h, f, u, n3, c_worst));
-  RSO_CHECK_CUDA(h, cudaFreeAsync(fs, h->stream));
-  RSO_CHECK_CUDA(h, cudaFreeAsync(fs_old, h->stream));
   return RSO_OK;
 }
 

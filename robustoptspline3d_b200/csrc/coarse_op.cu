@@ -427,6 +427,81 @@ __global__ void k_prolong(const Level Fl, const Level C, const T* __restrict__ u
   uf[n + 2 * Fl.NP] = u2 + (w0 * e0[2] + w1 * e1[2]);
 }
 
+// FP32, single system: four consecutive padded fine nodes per thread (px is a
+// multiple of 4), the fine vector and node classes as 16-byte vectors, the
+// yz-interpolated coarse values of the (at most four) coarse columns the group
+// touches computed once.  Same arithmetic, in the same order, as k_prolong.
+template <int F>
+__global__ void __launch_bounds__(256) k_prolong_v4(const Level Fl, const Level C, const float* __restrict__ uc,
+                                                    float* __restrict__ uf) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long NP = Fl.NP, px = Fl.px, pxy = (long long)Fl.px * Fl.py;
+  const long long p0 = 4 * g;
+  if (p0 >= NP) return;
+  const int zp = (int)(p0 / pxy);
+  const long long rem = p0 - zp * pxy;
+  const int yp = (int)(rem / px), xp = (int)(rem - yp * px);
+  if (zp < 1 || zp > Fl.nz || yp < 1 || yp > Fl.ny) return;
+  const uchar4 cl4 = *reinterpret_cast<const uchar4*>(Fl.vclass + p0);
+  const uint8_t cls[4] = {cl4.x, cl4.y, cl4.z, cl4.w};
+  bool upd[4];
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int x = xp - 1 + k;
+    upd[k] = x >= 0 && x < Fl.nx && (cls[k] & NC_ACTIVE) && !(cls[k] & NC_SUPPORT);
+    any = any || upd[k];
+  }
+  if (!any) return;
+  const int y = yp - 1, z = zp - 1;
+  const int Y0 = y / F, Z0 = z / F, oy = y - F * Y0, oz = z - F * Z0;
+  const float wy[2] = {(float)(F - oy) / (float)F, (float)oy / (float)F};
+  const float wz[2] = {(float)(F - oz) / (float)F, (float)oz / (float)F};
+  const int x_first = max(xp - 1, 0), x_last = min(xp + 2, Fl.nx - 1);
+  const int Xa = x_first / F, Xb = x_last / F + 1;
+  const long long cpx = C.px, cpxy = (long long)C.px * C.py;
+  float E[4][3];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int X = Xa + j;
+#pragma unroll
+    for (int c = 0; c < 3; c++) E[j][c] = 0.f;
+    if (X <= Xb && X <= C.nx) {  // index C.nx is the padded halo (zero)
+      const long long c0 = C.nidx(X, Y0, Z0);
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        float s = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) s += wy[k & 1] * wz[k >> 1] * uc[c0 + (k & 1) * cpx + (k >> 1) * cpxy + c * C.NP];
+        E[j][c] = s;
+      }
+    }
+  }
+  float u[3][4];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const float4 m = *reinterpret_cast<const float4*>(uf + p0 + c * NP);
+    u[c][0] = m.x; u[c][1] = m.y; u[c][2] = m.z; u[c][3] = m.w;
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (!upd[k]) continue;
+    const int x = xp - 1 + k, X0 = x / F, ox = x - F * X0, j = X0 - Xa;
+    const float w1 = (float)ox / (float)F, w0 = (float)(F - ox) / (float)F;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float e0 = 0.f, e1 = 0.f;
+#pragma unroll
+      for (int q = 0; q < 3; q++)
+        if (q == j) { e0 = E[q][c]; e1 = E[q + 1][c]; }
+      u[c][k] = u[c][k] + (w0 * e0 + w1 * e1);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    *reinterpret_cast<float4*>(uf + p0 + c * NP) = make_float4(u[c][0], u[c][1], u[c][2], u[c][3]);
+}
+
 // ---------------------------------------------------------------- Galerkin
 __device__ __forceinline__ double pw(int F, int o, int A) { return A ? (double)o / F : (double)(F - o) / F; }
 
@@ -1041,7 +1116,14 @@ template <typename T>
 rso_status prolong(rso_handle* h, int cl, const T* uc, T* uf) {
   const Level& f = h->L[cl - 1];
   const Level& c = h->L[cl];
-  if (c.factor == 4) {
+  if (sizeof(T) == 4 && f.nb == 1 && (c.factor == 4 || c.factor == 2)) {
+    const unsigned nblk = (unsigned)cdiv(f.NP / 4, 256);
+    if (c.factor == 4)
+      k_prolong_v4<4><<<nblk, 256, 0, h->stream>>>(f, c, (const float*)uc, (float*)uf);
+    else
+      k_prolong_v4<2><<<nblk, 256, 0, h->stream>>>(f, c, (const float*)uc, (float*)uf);
+    rso::note_launch();
+  } else if (c.factor == 4) {
     k_prolong<T, 4><<<node_grid(f), dim3(32, 8), 0, h->stream>>>(f, c, uc, uf); rso::note_launch();
   } else if (c.factor == 2) {
     k_prolong<T, 2><<<node_grid(f), dim3(32, 8), 0, h->stream>>>(f, c, uc, uf); rso::note_launch();

@@ -919,6 +919,95 @@ __global__ void __launch_bounds__(256) k_fine_jacobi0(const Level L, const T* __
   out[n + 2 * NP] = id * (C * r0 + F * r1 + I * r2);
 }
 
+// FP32 first Jacobi step from zero with four consecutive padded nodes per
+// thread (px is a multiple of 4): f, out and the node classes move as 16-byte
+// vectors, and the 20 rho^p values of the group's elements (5 per row of
+// elements) as one 16-byte and one scalar load per row.  Same arithmetic, in
+// the same order, as k_fine_jacobi0<float>.  Halo rows are skipped; the halo
+// nodes of a group are written as zero.
+__global__ void __launch_bounds__(256) k_fine_jacobi0_v4(const Level L, const float* __restrict__ f,
+                                                         float* __restrict__ out, const float* __restrict__ rp,
+                                                         float omega) {
+  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long NP = L.NP, px = L.px, pxy = (long long)L.px * L.py;
+  const long long p0 = 4 * g;
+  if (p0 >= NP) return;
+  const int zp = (int)(p0 / pxy);
+  const long long rem = p0 - zp * pxy;
+  const int yp = (int)(rem / px), xp = (int)(rem - yp * px);
+  if (zp < 1 || zp > L.nz || yp < 1 || yp > L.ny) return;
+  const uchar4 cl4 = *reinterpret_cast<const uchar4*>(L.vclass + p0);
+  const uint8_t cls[4] = {cl4.x, cl4.y, cl4.z, cl4.w};
+  bool work[4];
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int x = xp + k - 1;
+    work[k] = x >= 0 && x < L.nx && (cls[k] & NC_ACTIVE) && !(cls[k] & NC_SUPPORT);
+    any = any || work[k];
+  }
+  float o[3][4];
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) o[c][k] = 0.f;
+  if (any) {
+    // element rows (y-1+b, z-1+c) of the nodes' 8 elements; element x of node
+    // x + a - 1 ... padded element index xp + j - 1 for j = 0..4
+    const long long qx = L.qx, qxy = (long long)L.qx * L.qy;
+    float rr[4][5];
+#pragma unroll
+    for (int row = 0; row < 4; row++) {
+      const long long e = (long long)(yp - 1 + (row & 1)) * qx + (long long)(zp - 1 + (row >> 1)) * qxy;
+      // padded element x index xp - 1 + j: elements x - 1 + a of node x = xp - 1 + k
+      const float* rowp = rp + e + xp;
+      rr[row][0] = xp > 0 ? rowp[-1] : 0.f;
+      if (xp + 4 <= L.qx) {
+        const float4 m = *reinterpret_cast<const float4*>(rowp);
+        rr[row][1] = m.x; rr[row][2] = m.y; rr[row][3] = m.z; rr[row][4] = m.w;
+      } else {
+#pragma unroll
+        for (int j = 1; j < 5; j++) rr[row][j] = (xp + j - 1 < L.qx) ? rowp[j - 1] : 0.f;
+      }
+    }
+    float fv[3][4];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float4 m = *reinterpret_cast<const float4*>(f + p0 + c * NP);
+      fv[c][0] = m.x; fv[c][1] = m.y; fv[c][2] = m.z; fv[c][3] = m.w;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      if (!work[k]) continue;
+      float D[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        // element q of the node: (a, b, c) = (q & 1, q >> 1 & 1, q >> 2)
+        const float r = rr[((q >> 1) & 1) + 2 * (q >> 2)][k + (q & 1)];
+        const int vi = 7 - q;
+        D[0] += r * k0<float>((vi * 3 + 0) * 24 + vi * 3 + 0);
+        D[1] += r * k0<float>((vi * 3 + 0) * 24 + vi * 3 + 1);
+        D[2] += r * k0<float>((vi * 3 + 0) * 24 + vi * 3 + 2);
+        D[3] += r * k0<float>((vi * 3 + 1) * 24 + vi * 3 + 1);
+        D[4] += r * k0<float>((vi * 3 + 1) * 24 + vi * 3 + 2);
+        D[5] += r * k0<float>((vi * 3 + 2) * 24 + vi * 3 + 2);
+      }
+      const float r0 = fv[0][k], r1 = fv[1][k], r2 = fv[2][k];
+      const float a = D[0], b = D[1], c = D[2], d = D[3], e = D[4], gg = D[5];
+      const float A = d * gg - e * e, B = c * e - b * gg, C = b * e - c * d;
+      const float det = a * A + b * B + c * C;
+      const float id = omega / det;
+      const float E = a * gg - c * c, F = b * c - a * e, I = a * d - b * b;
+      o[0][k] = id * (A * r0 + B * r1 + C * r2);
+      o[1][k] = id * (B * r0 + E * r1 + F * r2);
+      o[2][k] = id * (C * r0 + F * r1 + I * r2);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+    *reinterpret_cast<float4*>(out + p0 + c * NP) = make_float4(o[c][0], o[c][1], o[c][2], o[c][3]);
+}
+
 // one colour of the 8-colour point Gauss-Seidel sweep (in place)
 template <typename T>
 __global__ void __launch_bounds__(256) k_fine_gs(const Level L, T* __restrict__ u, const T* __restrict__ f,
@@ -1149,6 +1238,12 @@ rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const
 template <typename T>
 rso_status fine_jacobi0(rso_handle* h, const T* f, T* u_out, const T* rp, double omega) {
   const Level& l = h->L[0];
+  if (sizeof(T) == 4 && l.nb == 1) {
+    k_fine_jacobi0_v4<<<cdiv(l.NP / 4, 256), 256, 0, h->stream>>>(l, (const float*)f, (float*)u_out,
+                                                                 (const float*)rp, (float)omega);
+    rso::note_launch();
+    return launch_check(h, "fine_jacobi0");
+  }
   k_fine_jacobi0<T><<<plane_grid(l), dim3(32, 8), 0, h->stream>>>(l, f, u_out, rp, (T)omega);
   rso::note_launch();
   return launch_check(h, "fine_jacobi0");

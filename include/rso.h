@@ -154,10 +154,21 @@ rso_status rso_residual(rso_handle* h, const double* u_dev, const double* f_dev,
  * operator is update_residual_OTFA_WS_kernel grid/Grid.cu:2320-2376): the
  * FP64 inputs are rounded to FP32, op 0 gives r = f - K u, op 1 K u (support
  * rows pass u; f may be NULL), op 2 the damped block-Jacobi / Chebyshev step
- * u + c1 (u - uprev) + omega D^-1 (f - K u) (uprev NULL reads as zero); the
- * FP32 result comes back widened to FP64. */
+ * u + c1 (u - uprev) + omega D^-1 (f - K u) (uprev NULL reads as zero), op 3
+ * the first step from a zero iterate, omega D^-1 f (u is ignored); the FP32
+ * result comes back widened to FP64. */
 rso_status rso_fine_sweep_fp32(rso_handle* h, int op, const double* u_dev, const double* f_dev,
                                const double* uprev_dev, double omega, double c1, double* out_dev);
+/* The same for a coarse level's FP32 stencil kernels (no counterpart in the
+ * reference; its coarse levels are FP64, update_residual_kernel_1
+ * grid/Grid.cu:2169-2267): op 0 r = f - K u, op 2 the Jacobi / Chebyshev step;
+ * the kernel variant follows the handle's launch shapes. */
+rso_status rso_coarse_sweep_fp32(rso_handle* h, int level, int op, const double* u_dev, const double* f_dev,
+                                 const double* uprev_dev, double omega, double c1, double* out_dev);
+/* FP32 prolongation out = uf + P uc (Grid::prolongate_correction,
+ * grid/Grid.cu:2717-2734, in the precision of the mixed V-cycle). */
+rso_status rso_prolong_fp32(rso_handle* h, int coarse_level, const double* uc_dev, const double* uf_dev,
+                            double* out_dev);
 /* coarse-level stencil (243 x Nn_level doubles, [d][row][col][node]); rxStencil */
 rso_status rso_get_stencil(rso_handle* h, int level, double* out_dev);
 /* coarse residual on stored stencils; update_residual_kernel_1 (grid/Grid.cu:2169-2267) */

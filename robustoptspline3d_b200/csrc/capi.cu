@@ -408,6 +408,46 @@ extern "C" rso_status rso_residual(rso_handle* h, const double* u, const double*
   return RSO_OK;
 }
 
+extern "C" rso_status rso_coarse_sweep_fp32(rso_handle* h, int level, int op, const double* u, const double* f,
+                                            const double* uprev, double omega, double c1, double* out) {
+  if (!h || !u || !f || !out || level < 1 || level >= (int)h->L.size() || (op != 0 && op != 2))
+    return RSO_ERR_INVALID_ARG;
+  RSO_TRY(need_ops(h));
+  Level& l = h->L[level];
+  const long long n3 = 3 * l.NP;
+  RSO_TRY(pad_nodes(h, level, u, l.u64));
+  RSO_TRY(to_f32(h, l.u64, l.u32, n3));
+  RSO_TRY(pad_nodes(h, level, f, l.f64));
+  RSO_TRY(to_f32(h, l.f64, l.f32, n3));
+  const float* up = nullptr;
+  if (uprev && op == 2) {
+    RSO_TRY(pad_nodes(h, level, uprev, l.t64));
+    RSO_TRY(to_f32(h, l.t64, l.t32, n3));
+    up = l.t32;
+  }
+  if (op == 0) RSO_TRY(coarse_residual<float>(h, level, l.u32, l.f32, l.r32));
+  else RSO_TRY(coarse_jacobi<float>(h, level, l.u32, l.f32, l.r32, omega, up, c1));
+  RSO_TRY(to_f64(h, l.r32, l.r64, n3));
+  RSO_TRY(unpad_nodes(h, level, l.r64, out));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  return RSO_OK;
+}
+
+extern "C" rso_status rso_prolong_fp32(rso_handle* h, int cl, const double* uc, const double* uf, double* out) {
+  if (!h || !uc || !uf || !out || cl < 1 || cl >= (int)h->L.size()) return RSO_ERR_INVALID_ARG;
+  Level& c = h->L[cl];
+  Level& f = h->L[cl - 1];
+  RSO_TRY(pad_nodes(h, cl, uc, c.u64));
+  RSO_TRY(to_f32(h, c.u64, c.u32, 3 * c.NP));
+  RSO_TRY(pad_nodes(h, cl - 1, uf, f.u64));
+  RSO_TRY(to_f32(h, f.u64, f.u32, 3 * f.NP));
+  RSO_TRY(prolong<float>(h, cl, c.u32, f.u32));
+  RSO_TRY(to_f64(h, f.u32, f.u64, 3 * f.NP));
+  RSO_TRY(unpad_nodes(h, cl - 1, f.u64, out));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  return RSO_OK;
+}
+
 extern "C" rso_status rso_set_vcycle_graphs(rso_handle* h, int on) {
   if (!h) return RSO_ERR_INVALID_ARG;
   h->vc_graphs = on != 0;
@@ -416,7 +456,7 @@ extern "C" rso_status rso_set_vcycle_graphs(rso_handle* h, int on) {
 
 extern "C" rso_status rso_fine_sweep_fp32(rso_handle* h, int op, const double* u, const double* f,
                                           const double* uprev, double omega, double c1, double* out) {
-  if (!h || !u || !out || op < 0 || op > 2 || (op != 1 && !f)) return RSO_ERR_INVALID_ARG;
+  if (!h || !u || !out || op < 0 || op > 3 || (op != 1 && !f)) return RSO_ERR_INVALID_ARG;
   Level& l0 = h->L[0];
   const long long n3 = 3 * l0.NP;
   RSO_TRY(pad_nodes(h, 0, u, l0.u64));
@@ -436,7 +476,8 @@ extern "C" rso_status rso_fine_sweep_fp32(rso_handle* h, int op, const double* u
   }
   if (op == 0) RSO_TRY(fine_residual<float>(h, l0.u32, l0.f32, l0.r32, h->rp32));
   else if (op == 1) RSO_TRY(fine_applyK<float>(h, l0.u32, l0.r32, h->rp32));
-  else RSO_TRY(fine_jacobi<float>(h, l0.u32, l0.f32, l0.r32, h->rp32, omega, up, c1));
+  else if (op == 2) RSO_TRY(fine_jacobi<float>(h, l0.u32, l0.f32, l0.r32, h->rp32, omega, up, c1));
+  else RSO_TRY(fine_jacobi0<float>(h, l0.f32, l0.r32, h->rp32, omega));
   RSO_TRY(to_f64(h, l0.r32, l0.r64, n3));
   RSO_TRY(unpad_nodes(h, 0, l0.r64, out));
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));

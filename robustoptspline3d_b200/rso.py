@@ -94,6 +94,8 @@ SIGNATURES = {
     "rso_residual": (_ci, [_vp, _vp, _vp, _vp]),
     "rso_fine_sweep_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
     "rso_set_vcycle_graphs": (_ci, [_vp, _ci]),
+    "rso_coarse_sweep_fp32": (_ci, [_vp, _ci, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
+    "rso_prolong_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp]),
     "rso_autotune": (_ci, [_vp, _pi]),
     "rso_set_launch_shapes": (_ci, [_vp, _pi, _ci]),
     "rso_get_stencil": (_ci, [_vp, _ci, _vp]),
@@ -413,6 +415,23 @@ class HierarchyGrid:
                                                None if f is None else _dev(f, torch.float64),
                                                None if uprev is None else _dev(uprev, torch.float64),
                                                omega, c1, _dev(out)), "rso_fine_sweep_fp32")
+        return out
+
+    def coarse_sweep_fp32(self, level, op, u, f, uprev=None, omega=1.0, c1=0.0):
+        """One FP32 coarse-level sweep (op 0 residual, 2 Jacobi/Chebyshev step), FP64 in and out."""
+        import torch
+        out = torch.empty_like(u)
+        self._chk(self.lib.rso_coarse_sweep_fp32(self.h, level, op, _dev(u, torch.float64), _dev(f, torch.float64),
+                                                 _dev(uprev, torch.float64) if uprev is not None else None,
+                                                 omega, c1, _dev(out)), "rso_coarse_sweep_fp32")
+        return out
+
+    def prolong_fp32(self, coarse_level, uc, uf):
+        """uf + P uc in FP32 (the mixed V-cycle's prolongation), FP64 in and out."""
+        import torch
+        out = torch.empty_like(uf)
+        self._chk(self.lib.rso_prolong_fp32(self.h, coarse_level, _dev(uc, torch.float64), _dev(uf, torch.float64),
+                                            _dev(out)), "rso_prolong_fp32")
         return out
 
     def stencil(self, level):

@@ -78,7 +78,7 @@ def test_graph_profiling_and_batch(cuda):
         g.lib.rso_set_profiling(g.h, 1)
         g.lib.rso_profile_reset(g.h)
         u, it, _, _ = g.solve(cuda.tensor(F[0], dtype=cuda.float64, device="cuda"), tol=1e-8, max_iter=200)
-        prof = [profile(g, c) for c in range(9)]
+        prof = [profile(g, c) for c in range(10)]
         U, infos = g.solve_batch(cuda.tensor(F, dtype=cuda.float64, device="cuda"), tol=1e-8, max_iter=200)
         res[graphs] = (u.cpu().numpy(), it, prof, U.cpu().numpy(), infos)
         g.close()

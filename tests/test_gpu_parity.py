@@ -113,6 +113,54 @@ def test_operator_fp32(oracle, cuda, gen, rows):
     assert rel(cheb, jac + c1 * (u - up)) < tol
 
 
+@pytest.mark.parametrize("split", [0, 1])
+@pytest.mark.parametrize("gen,ff", [(lambda: P.ellipsoid(40, 24, 24), 4), (lambda: P.cantilever(48, 24, 24), 2)])
+def test_coarse_and_transfers_fp32(oracle, cuda, gen, ff, split):
+    """FP32 kernels of the mixed V-cycle below the fine level against the FP64 oracle: coarse
+    residual and Jacobi / Chebyshev steps with both coarse kernel variants (one thread per node
+    with 16-byte streams, split = 0; one per node and row, split = 1), the prolongation, and the
+    fine level's first step from zero.  Tolerance 2e-5 relative in norm (FP32 stencils and
+    vectors)."""
+    prob = gen()
+    g, o = make(oracle, prob, first_factor=ff)
+    g.update_stencil()
+    o.update_stencil()
+    nl = o.n_levels()
+    g.set_launch_shapes(4, -1, [-1] + [split] * (nl - 1))
+    rng = np.random.default_rng(17)
+    tol = 2e-5
+    om, c1 = 0.3, 0.7
+    for lvl in range(1, nl):
+        d = o.level_dims(lvl)
+        nn = int(d[3] * d[4] * d[5])
+        _, vm = o.level_masks(lvl)
+        uc, fc, up = (rng.standard_normal(3 * nn) * np.tile(vm, 3) for _ in range(3))
+        assert rel(g.coarse_sweep_fp32(lvl, 0, t(uc, cuda), t(fc, cuda)).cpu().numpy(),
+                   o.coarse_residual(lvl, uc, fc)) < tol, lvl
+        if lvl < nl - 1:
+            jac = o.smooth(lvl, uc, fc, kind=1, omega=om, sweeps=1)
+            assert rel(g.coarse_sweep_fp32(lvl, 2, t(uc, cuda), t(fc, cuda), omega=om).cpu().numpy(), jac) < tol, lvl
+            cheb = g.coarse_sweep_fp32(lvl, 2, t(uc, cuda), t(fc, cuda), t(up, cuda), omega=om, c1=c1).cpu().numpy()
+            assert rel(cheb, jac + c1 * (uc - up)) < tol, lvl
+        df = o.level_dims(lvl - 1)
+        nnf = int(df[3] * df[4] * df[5])
+        _, vmf = o.level_masks(lvl - 1)
+        uf = rng.standard_normal(3 * nnf) * np.tile(vmf, 3)
+        if lvl == 1:
+            uf[np.tile((o.node_class() & 4) > 0, 3)] = 0
+        po = o.prolong(lvl, uc, uf)
+        if lvl == 1:
+            po[np.tile((o.node_class() & 4) > 0, 3)] = 0
+        assert rel(g.prolong_fp32(lvl, t(uc, cuda), t(uf, cuda)).cpu().numpy(), po) < tol, lvl
+    cls = o.node_class()
+    dead = np.tile(((cls & 4) > 0) | ((cls & 1) == 0), 3)
+    f = rng.standard_normal(3 * o.nn)
+    f[dead] = 0
+    z = np.zeros(3 * o.nn)
+    assert rel(g.fine_sweep_fp32(3, t(z, cuda), t(f, cuda), omega=om).cpu().numpy(),
+               o.smooth(0, z, f, kind=1, omega=om, sweeps=1)) < tol
+
+
 @pytest.mark.parametrize("gen,nl,ff", [(lambda: P.ellipsoid(40, 24, 24), 0, 4),
                                        (lambda: P.ellipsoid(24, 16, 12), 0, 4),
                                        (lambda: P.cantilever(16, 8, 8), 3, 2)])

@@ -543,18 +543,21 @@ def main():
         if w == 0 and not args.no_autotune:
             # launch shapes measured on this hierarchy once its operators exist
             tuned = g.autotune()
-    top_cls, top_ms = 0, -1.0
+    top_cls, top_ms, stencil_cls = 0, -1.0, None
     for cls in range(16):
         if lib.rso_profile_class(g.h, cls, kname, 64, ctypes.byref(cnt), ctypes.byref(tot), ctypes.byref(bytes_per),
                                  ctypes.byref(flops_per)) != 0:
             break
         if tot.value > top_ms:
             top_cls, top_ms = cls, tot.value
+        if kname.value.decode() == "coarse_stencil_fp32_streamed" and cnt.value > 0:
+            stencil_cls = cls
     lib.rso_set_profiling(g.h, 0)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     lib.rso_profile_reset(g.h)
-    lib.rso_set_profiling_classes(g.h, 1 << top_cls)
+    # the dominant kernel and the coarse stencil kernel are timed in the timed steps
+    lib.rso_set_profiling_classes(g.h, (1 << top_cls) | ((1 << stencil_cls) if stencil_cls is not None else 0))
     launches0 = lib.rso_launch_count()
     barrier_max(world, 0.0)
     infos = []
@@ -573,6 +576,14 @@ def main():
     ms = barrier_max(world, max(ms_dev, wall * 1e3))
     value = world * args.steps / (ms / 1e3)
     # dominant-kernel roofline from the live event timings of the timed steps
+    stencil = None
+    if stencil_cls is not None:
+        lib.rso_profile_class(g.h, stencil_cls, kname, 64, ctypes.byref(cnt), ctypes.byref(tot), ctypes.byref(bytes_per),
+                              ctypes.byref(flops_per))
+        s_ms = tot.value / max(cnt.value, 1)
+        stencil = {"kernel": kname.value.decode(), "launches": cnt.value, "avg_ms": s_ms,
+                   "algorithmic_bytes_per_launch": bytes_per.value,
+                   "achieved": bytes_per.value / (s_ms / 1e3) / 1e9 if s_ms > 0 else 0.0}
     lib.rso_profile_top(g.h, kname, 64, ctypes.byref(cnt), ctypes.byref(tot), ctypes.byref(bytes_per),
                         ctypes.byref(flops_per))
     peaks = {}
@@ -651,6 +662,11 @@ def main():
     # cycle at the SM clock sampled during the timed region
     mhz = clocks.get("sm_mhz") or 1965.0
     simt_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    if stencil is not None:
+        # the coarse stencil operator (HBM-bound), the kernel the stencil-bandwidth target is about
+        stencil.update({"bound": "hbm", "peak": hbm, "unit": "GB/s", "frac": stencil["achieved"] / hbm,
+                        "peak_source": roofline["peak_source"]})
+        roofline["coarse_stencil"] = stencil
     roofline["compute"] = {"bound": "fp32_simt", "achieved_tflops": roofline["fp_tflops"], "peak_tflops": simt_peak,
                            "frac": roofline["fp_tflops"] / simt_peak,
                            "note": "algorithmic 1260 flop per node (576 FMA of K0 + smoother); the kernel executes "

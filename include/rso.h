@@ -266,6 +266,31 @@ rso_status rso_density_filter_adjoint(rso_handle* h, double radius, const float*
  * race and must be serialised by the caller.  Synchronises h's stream. */
 #define RSO_FILTER_NOALLOC_MAX_REACH 6
 rso_status rso_filter_noalloc(rso_handle* h, double radius, const float* in_dev, float* out_dev);
+/* Optimality-criteria density update (the reference's alternative to MMA):
+ * variant 0 is updateDensities (optimization/optimization.cu:394-471),
+ * variant 1 updateDensities2 (:473-598, built without ENABLE_HEAVISIDE, as the
+ * reference's build is).  Bisection on the sensitivity threshold g in
+ * [0, max |sens|] of rho' = clamp(clamp(rho (|min(sens, 0)| / g)^damp,
+ * rho - step, rho + step), rho_min, 1) (trySensMultiplier_kernel :366-392),
+ * shell elements 1, until the volume fraction over the active elements is
+ * within 1e-4 of vgoal or after 31 trials (variant 1: also stops when the
+ * bracket's relative width is below 1e-3, at most 51 trials).  rho_out =
+ * the update at the last threshold (may alias rho_src).  Dense element
+ * arrays; info_host (NULL or 5 doubles): g, final volume, trials, max and
+ * mean |rho_out - rho_src|. */
+rso_status rso_oc_update_density(rso_handle* h, int variant, const float* rho_src_dev, const float* sens_dev,
+                                 const uint8_t* shell_dev, double vgoal, double step, double damp, float* rho_out_dev,
+                                 double* info_host);
+/* Optimality-criteria update of the spline coefficients, updateCoeff
+ * (optimization/optimization.cu:600-706, tryCSensMultiplier_kernel :560-598):
+ * the same bisection on the coefficient sensitivities with the coefficients
+ * clamped to [cmin, cmax] and the volume of coeff2density of each trial; as in
+ * the reference the final threshold is applied to the last trial's
+ * coefficients.  coeff_dev (n_coeff floats) is updated in place; rho_out_dev
+ * (NULL or ex*ey*ez floats) receives the final densities; info_host (NULL or 3
+ * doubles): g, final volume, trials. */
+rso_status rso_oc_update_coeff(rso_handle* h, float* coeff_dev, const float* csens_dev, double vgoal, double step,
+                               double damp, double cmin, double cmax, float* rho_out_dev, double* info_host);
 /* volume fraction sum(rho)/n_gs_elements; Grid::volumeRatio (grid/Grid.cu:5642-5650) */
 rso_status rso_volume(rso_handle* h, const float* rho_dev, double* vol);
 

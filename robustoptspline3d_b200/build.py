@@ -19,7 +19,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxe
 
 SOURCES = ["capi.cu", "topology.cu", "fine_op.cu", "coarse_op.cu", "reduce.cu", "solver.cu", "design.cu",
            "design_capi.cu", "worst.cu", "mma.cu", "driver.cu", "prof.cu",
-           "filter_noalloc.cu", "batch.cu", "autotune.cu"]
+           "filter_noalloc.cu", "batch.cu", "autotune.cu", "oc.cu"]
 
 
 def _compile(src, verbose=False):

@@ -94,6 +94,10 @@ SIGNATURES = {
     "rso_residual": (_ci, [_vp, _vp, _vp, _vp]),
     "rso_fine_sweep_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
     "rso_set_vcycle_graphs": (_ci, [_vp, _ci]),
+    "rso_oc_update_density": (_ci, [_vp, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _vp,
+                                    _pd]),
+    "rso_oc_update_coeff": (_ci, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, _vp, _pd]),
     "rso_coarse_sweep_fp32": (_ci, [_vp, _ci, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
     "rso_prolong_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp]),
     "rso_autotune": (_ci, [_vp, _pi]),
@@ -402,6 +406,31 @@ class HierarchyGrid:
         rs = list(row_split or [])
         c = np.array([fine_rows, bottom_level] + rs, np.int32)
         self._chk(self.lib.rso_set_launch_shapes(self.h, _np_ptr(c, _pi), len(c)), "rso_set_launch_shapes")
+
+    def updateDensities(self, rho, sens, vgoal, step=0.1, damp=0.5, shell=None, variant=0):
+        """OC density update (rso_oc_update_density): returns (new rho, info dict)."""
+        import torch
+        src = self._efield(rho)
+        out = torch.empty_like(src)
+        info = np.zeros(5)
+        sh = None if shell is None else torch.as_tensor(np.asarray(shell, np.uint8).ravel(), device="cuda")
+        self._chk(self.lib.rso_oc_update_density(self.h, variant, _dev(src), _dev(self._efield(sens)), _dev(sh), vgoal,
+                                                 step, damp, _dev(out), _np_ptr(info, _pd)), "rso_oc_update_density")
+        return out, {"g": info[0], "volume": info[1], "trials": int(info[2]), "max_change": info[3],
+                     "mean_change": info[4]}
+
+    def updateCoeff(self, coeff, csens, vgoal, step=0.1, damp=0.5, cmin=0.0, cmax=1.0):
+        """OC coefficient update (rso_oc_update_coeff): returns (new coefficients, densities, info dict)."""
+        import torch
+        c = torch.as_tensor(np.asarray(coeff, np.float32) if not isinstance(coeff, torch.Tensor) else coeff,
+                            device="cuda").to(torch.float32).contiguous().clone()
+        cs = torch.as_tensor(np.asarray(csens, np.float32) if not isinstance(csens, torch.Tensor) else csens,
+                             device="cuda").to(torch.float32).contiguous()
+        rho = torch.empty(self.ne, dtype=torch.float32, device="cuda")
+        info = np.zeros(3)
+        self._chk(self.lib.rso_oc_update_coeff(self.h, _dev(c), _dev(cs), vgoal, step, damp, cmin, cmax, _dev(rho),
+                                               _np_ptr(info, _pd)), "rso_oc_update_coeff")
+        return c, rho, {"g": info[0], "volume": info[1], "trials": int(info[2])}
 
     def set_vcycle_graphs(self, on):
         """Replay captured FP32 V-cycles from CUDA graphs (default) or launch every kernel."""

@@ -341,6 +341,15 @@ const double* rso_mma_x_dev(rso_mma* s);
  * info_host[4] = {kkt inf-norm, last step, sub-iterations, overflowed}. */
 rso_status rso_mma_update(rso_mma* s, const double* df_dev, const double* dg_dev, const double* g_host,
                           int* converged, double* info_host);
+/* Checkpoint and resume of the MMA state (no counterpart in the reference,
+ * whose drivers restart MMA from scratch): what one update carries to the
+ * next, x, the asymptotes L and U, the move limits alpha and beta, the
+ * previous step and the stop counter, as 6 n + 1 doubles in that order.
+ * Loading a saved state into an MMA of the same n and bounds continues the
+ * run exactly as if it had not stopped. */
+rso_status rso_mma_state_size(const rso_mma* s, long long* n_doubles);
+rso_status rso_mma_save(rso_mma* s, double* state_host);
+rso_status rso_mma_load(rso_mma* s, const double* state_host);
 void rso_mma_destroy(rso_mma* s);
 
 /* ---------------------------------------------------------------- design iteration */

@@ -369,6 +369,36 @@ extern "C" rso_status rso_mma_get(rso_mma* s, double* x, double* L, double* U, d
 
 extern "C" const double* rso_mma_x_dev(rso_mma* s) { return s ? s->x : nullptr; }
 
+// checkpoint of what an update carries to the next: x, the asymptotes L and
+// U, the move limits alpha and beta, the previous step, the stop counter
+extern "C" rso_status rso_mma_state_size(const rso_mma* s, long long* n_doubles) {
+  if (!s || !n_doubles) return RSO_ERR_INVALID_ARG;
+  *n_doubles = 6LL * s->n + 1;
+  return RSO_OK;
+}
+
+extern "C" rso_status rso_mma_save(rso_mma* s, double* state_host) {
+  if (!s || !state_host) return RSO_ERR_INVALID_ARG;
+  const size_t b = sizeof(double) * s->n;
+  const double* parts[6] = {s->x, s->L, s->U, s->alpha, s->beta, s->lastdx};
+  for (int k = 0; k < 6; k++)
+    MMA_CHECK(s, cudaMemcpyAsync(state_host + (size_t)k * s->n, parts[k], b, cudaMemcpyDeviceToHost, s->stream));
+  MMA_CHECK(s, cudaStreamSynchronize(s->stream));
+  state_host[6LL * s->n] = (double)s->stop_counter;
+  return RSO_OK;
+}
+
+extern "C" rso_status rso_mma_load(rso_mma* s, const double* state_host) {
+  if (!s || !state_host) return RSO_ERR_INVALID_ARG;
+  const size_t b = sizeof(double) * s->n;
+  double* parts[6] = {s->x, s->L, s->U, s->alpha, s->beta, s->lastdx};
+  for (int k = 0; k < 6; k++)
+    MMA_CHECK(s, cudaMemcpyAsync(parts[k], state_host + (size_t)k * s->n, b, cudaMemcpyHostToDevice, s->stream));
+  MMA_CHECK(s, cudaStreamSynchronize(s->stream));
+  s->stop_counter = (int)state_host[6LL * s->n];
+  return RSO_OK;
+}
+
 extern "C" rso_status rso_mma_update(rso_mma* S, const double* df, const double* dg, const double* g, int* converged,
                                      double* info) {
   if (!S || !df || (!dg && S->m > 0) || !g) return RSO_ERR_INVALID_ARG;

@@ -94,6 +94,9 @@ SIGNATURES = {
     "rso_residual": (_ci, [_vp, _vp, _vp, _vp]),
     "rso_fine_sweep_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
     "rso_set_vcycle_graphs": (_ci, [_vp, _ci]),
+    "rso_mma_state_size": (_ci, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "rso_mma_save": (_ci, [_vp, _pd]),
+    "rso_mma_load": (_ci, [_vp, _pd]),
     "rso_oc_update_density": (_ci, [_vp, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _vp,
                                     _pd]),
     "rso_oc_update_coeff": (_ci, [_vp, _vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -741,6 +744,23 @@ class MMA:
             st = self.lib.rso_mma_set_x(self.s, _np_ptr(np.ascontiguousarray(x, np.float64), _pd))
         if st:
             raise RSOError(f"rso_mma_set_x: {_STATUS.get(st, st)}")
+
+    def save(self):
+        """Checkpoint of the MMA state (rso_mma_save): 6 n + 1 doubles."""
+        k = ctypes.c_longlong(0)
+        self.lib.rso_mma_state_size(self.s, ctypes.byref(k))
+        st = np.zeros(k.value)
+        if self.lib.rso_mma_save(self.s, _np_ptr(st, _pd)):
+            raise RSOError("rso_mma_save failed")
+        return st
+
+    def load(self, state):
+        """Resume from a checkpoint made by save() (rso_mma_load)."""
+        st = np.ascontiguousarray(state, np.float64)
+        if st.size != 6 * self.n + 1:
+            raise RSOError("checkpoint size does not match this MMA")
+        if self.lib.rso_mma_load(self.s, _np_ptr(st, _pd)):
+            raise RSOError("rso_mma_load failed")
 
     def get(self):
         x, L, U, a, b = [np.zeros(self.n) for _ in range(5)]

@@ -89,6 +89,21 @@ typedef struct {
   double ms;
 } rso_solve_info;
 
+/* ---------------------------------------------------------------- mesh input */
+/* Solid voxelisation of a closed triangle mesh, the mesh -> voxel-mask step of
+ * the reference's drivers (voxelize_mesh, voxelizer/voxelize_main.cpp:344-399,
+ * with the vendored cuda_voxelizer's solid mode, voxelizer/cpu_voxelizer.cpp:
+ * 206-330): a cubic grid of R^3 voxels, R the smallest power of two above
+ * preferred_resolution, around the mesh's bounding box enlarged to
+ * max_len * R / preferred_resolution per axis and centred; a voxel is solid
+ * when its centre has an odd number of mesh crossings along +x (top-left rule
+ * on projected edges).  vertices: 3 n_vertices floats; faces: 3 n_faces
+ * vertex indices.  solid_host: R^3 bytes, x fastest (NULL with box_out NULL
+ * asks for R only); box_out: NULL or 6 floats (min xyz, max xyz).  Uses the
+ * current device; allocates its own scratch. */
+rso_status rso_voxelize(const float* vertices_host, int n_vertices, const int* faces_host, int n_faces,
+                        int preferred_resolution, uint8_t* solid_host, int* resolution_out, float* box_out);
+
 /* ---------------------------------------------------------------- setup */
 void rso_default_config(rso_config* cfg);
 

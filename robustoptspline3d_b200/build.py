@@ -17,9 +17,13 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xcompiler", "-Wno-unused-function", "-ccbin", "g++"]
 
+# voxelize.cu rounds every operation separately, as the host restatement of
+# the reference's voxeliser does (no fused multiply-add contraction)
+FILE_FLAGS = {"voxelize.cu": ["-fmad=false"]}
+
 SOURCES = ["capi.cu", "topology.cu", "fine_op.cu", "coarse_op.cu", "reduce.cu", "solver.cu", "design.cu",
            "design_capi.cu", "worst.cu", "mma.cu", "driver.cu", "prof.cu",
-           "filter_noalloc.cu", "batch.cu", "autotune.cu", "oc.cu"]
+           "filter_noalloc.cu", "batch.cu", "autotune.cu", "oc.cu", "voxelize.cu"]
 
 
 def _compile(src, verbose=False):
@@ -28,7 +32,7 @@ def _compile(src, verbose=False):
     deps = [path, os.path.join(SRC, "rso_internal.cuh"), os.path.join(HERE, "..", "include", "rso.h")]
     if os.path.exists(obj) and all(os.path.getmtime(obj) >= os.path.getmtime(d) for d in deps):
         return obj, None
-    cmd = [NVCC] + ARCH + FLAGS + ["-c", path, "-o", obj]
+    cmd = [NVCC] + ARCH + FLAGS + FILE_FLAGS.get(src, []) + ["-c", path, "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

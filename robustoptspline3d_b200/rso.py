@@ -94,6 +94,8 @@ SIGNATURES = {
     "rso_residual": (_ci, [_vp, _vp, _vp, _vp]),
     "rso_fine_sweep_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
     "rso_set_vcycle_graphs": (_ci, [_vp, _ci]),
+    "rso_voxelize": (_ci, [ctypes.POINTER(ctypes.c_float), _ci, ctypes.POINTER(ctypes.c_int), _ci, _ci, _pu8, _pi,
+                           ctypes.POINTER(ctypes.c_float)]),
     "rso_mma_state_size": (_ci, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "rso_mma_save": (_ci, [_vp, _pd]),
     "rso_mma_load": (_ci, [_vp, _pd]),

@@ -12,7 +12,7 @@ exceed the 126 MB L2, so no flush is inserted between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--size S]
   python bench.py --mode solve [--precision mixed|fp64] [--size S]
-  python bench.py --mode batch|problems|scale
+  python bench.py --mode batch|problems|scale|mesh
 
 `--mode solve` times single multigrid-preconditioned CG solves (to relative
 residual 1e-6) on the density of the seeded initial design, with a seeded
@@ -406,6 +406,97 @@ def scale_problem(seed=2027, nvoids=200):
     return em, fa, la, normals
 
 
+def torus_mesh(R=2.0, r=0.7, nu=512, nv=256):
+    """Closed torus surface of 2 nu nv triangles, outward winding."""
+    a = 2 * np.pi * np.arange(nu) / nu
+    b = 2 * np.pi * np.arange(nv) / nv
+    A, Bm = np.meshgrid(a, b, indexing="ij")
+    v = np.stack([(R + r * np.cos(Bm)) * np.cos(A), (R + r * np.cos(Bm)) * np.sin(A), r * np.sin(Bm)], axis=-1)
+    i, j = np.meshgrid(np.arange(nu), np.arange(nv), indexing="ij")
+    p, q = i * nv + j, ((i + 1) % nu) * nv + j
+    p1, q1 = i * nv + (j + 1) % nv, ((i + 1) % nu) * nv + (j + 1) % nv
+    f = np.concatenate([np.stack([p, q, q1], -1).reshape(-1, 3), np.stack([p, q1, p1], -1).reshape(-1, 3)])
+    return v.reshape(-1, 3).astype(np.float32), f.astype(np.int32)
+
+
+def run_mesh(args):
+    """The mesh -> HierarchyGrid input chain at 256^3: a 262,144-triangle torus
+    voxelised at preferred resolution 200 (R = 256), shell elements of width 3
+    voxels, fixed and load node masks from two half-spaces on the 257^3 nodes,
+    outward normals and a constant load field at the load nodes.  Each stage is
+    timed through its C-ABI entry point with host buffers (copies included),
+    the median of --steps runs after --warmup; the CPU column is the numpy
+    restatement on a bounded sample of faces / points scaled to the full
+    count (its cost is linear in faces and points)."""
+    import robustoptspline3d_b200 as R
+    from robustoptspline3d_b200 import boundary as B
+    from robustoptspline3d_b200.voxelize import voxelize
+    v, f = torus_mesh()
+    fix = [B.halfspace(0, 0, -1, -0.5, closed=True)]
+    load = [B.halfspace(0, 0, 1, -0.5)]
+    force = [B.Field(load[0], ("constant", 1.0), ("constant", (0.0, 0.0, -1.0)))]
+    stages = {}
+
+    def timed(name, fn):
+        for _ in range(max(args.warmup, 1)):
+            out = fn()
+        ts = []
+        for _ in range(max(args.steps, 1)):
+            t0 = time.perf_counter()
+            out = fn()
+            ts.append(time.perf_counter() - t0)
+        stages[name] = float(np.median(ts)) * 1e3
+        return out
+
+    l0 = R.rso.load_library().rso_launch_count()
+    solid, Rg, bx = timed("voxelize", lambda: voxelize(v, f, 200))
+    origin, h = B.node_grid(bx, Rg)
+    dims = (Rg + 1,) * 3
+    shell = timed("shell_w3", lambda: B.shell_elements(v, f, bx, Rg, 3.0, solid))
+    fixed = timed("region_masks", lambda: (B.region_mask(fix, origin, h, dims), B.region_mask(load, origin, h, dims)))
+    fm, lm = fixed
+    surf = B.surface_nodes(solid)
+    ln = np.flatnonzero(surf & (lm > 0) & (fm == 0))
+    pts = origin[None, :] + np.stack([ln % (Rg + 1), (ln // (Rg + 1)) % (Rg + 1), ln // (Rg + 1) ** 2], 1) * h
+    timed("normals", lambda: B.mesh_normals(v, f, pts))
+    timed("load_field", lambda: B.region_field(force, pts))
+    launches = R.rso.load_library().rso_launch_count() - l0
+    total = sum(stages.values())
+    out = {"metric": "mesh input chain @256^3 (voxelise, shell, region masks, normals, load field)",
+           "value": 1e3 / total, "unit": "chains/s", "higher_is_better": True, "ms_per_chain": total,
+           "stages_ms": stages, "gpu_launches": int(launches),
+           "sizes": {"triangles": int(len(f)), "resolution": int(Rg), "solid": int(solid.sum()),
+                     "shell": int(shell.sum()), "load_nodes": int(len(ln)), "fixed_area_nodes": int(fm.sum())},
+           "data": "synthetic torus (R 2, r 0.7)",
+           "config": {"workload": "torus 262,144 triangles, preferred 200 -> 256^3, shell width 3",
+                      "timing": "host buffers in and out through the C ABI (copies and scratch included)"}}
+    if not args.no_cpu_baseline:
+        from oracle import boundary as OB
+        from oracle import voxel as OV
+        cpu = {}
+        sel = np.random.default_rng(1).choice(len(f), 400, replace=False)
+        t0 = time.perf_counter()
+        OB.shell_elements(v, f[sel], bx, Rg, 3.0, solid)
+        cpu["shell_w3"] = (time.perf_counter() - t0) * 1e3 * len(f) / len(sel)
+        t0 = time.perf_counter()
+        OB.region_mask([(r.kind, r.p, r.closed, r.complement) for r in fix + load], origin, h, dims)
+        cpu["region_masks"] = (time.perf_counter() - t0) * 1e3
+        pk = pts[:64]
+        fk = f[:4096]
+        t0 = time.perf_counter()
+        OB.mesh_normals(v, fk, pk)
+        cpu["normals"] = (time.perf_counter() - t0) * 1e3 * (len(f) / len(fk)) * (len(pts) / len(pk))
+        vs = f[sel]
+        t0 = time.perf_counter()
+        OV.voxelize(v, vs, 200)
+        cpu["voxelize"] = (time.perf_counter() - t0) * 1e3 * len(f) / len(vs)
+        out["cpu_baseline"] = {"value": 1e3 / sum(cpu.values()), "unit": "chains/s", "cores": 1, "kind": "port",
+                               "stages_ms": cpu,
+                               "sample": "400 faces (shell, voxelise), 64 points x 4096 faces (normals), full "
+                                         "region masks; scaled linearly to the full counts"}
+    print(json.dumps(out), flush=True)
+
+
 def run_scale(args):
     """One worst-case design iteration on the 512 x 256 x 256 voids box (the
     FP32-operator-at-scale configuration), mixed and plain FP64; the FP64 path
@@ -479,7 +570,7 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--mode", default="design", choices=["design", "solve", "batch", "problems", "scale"])
+    ap.add_argument("--mode", default="design", choices=["design", "solve", "batch", "problems", "scale", "mesh"])
     ap.add_argument("--systems", type=int, default=16)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
@@ -494,6 +585,9 @@ def main():
         return
     if args.mode == "scale":
         run_scale(args)
+        return
+    if args.mode == "mesh":
+        run_mesh(args)
         return
     if args.impl == "reference":
         # host-only arm: rank 0 times the CPU path, other ranks exit at once

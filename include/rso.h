@@ -104,6 +104,75 @@ typedef struct {
 rso_status rso_voxelize(const float* vertices_host, int n_vertices, const int* faces_host, int n_faces,
                         int preferred_resolution, uint8_t* solid_host, int* resolution_out, float* box_out);
 
+/* Shell elements of a voxelised mesh (HierarchyGrid::setSolidShellElement,
+ * grid/Grid.cpp:253-322): with h = (box max x - box min x) / R (FP32
+ * quotient) and w = shell_width * h, solid element e = (x, y, z) of the R^3
+ * grid is a shell element when some face's index box (its bounding box grown
+ * by 1.3 w, mapped to element indices by truncation, upper end exclusive and
+ * clamped to R - 1) contains e and the squared distance from e's centre to
+ * the mesh is below w^2.  box: 6 floats as rso_voxelize returns them;
+ * solid_host, shell_host: R^3 bytes, x fastest.  Allocates its own scratch. */
+rso_status rso_shell_elements(const float* vertices_host, int n_vertices, const int* faces_host, int n_faces,
+                              const float* box_host, int resolution, double shell_width, const uint8_t* solid_host,
+                              uint8_t* shell_host);
+
+/* Outward unit normals at points (Grid::outwardNormal, grid/Grid.cpp:
+ * 2838-2854): q = closest point of the mesh to p (lowest face index on a
+ * tie), t = (v0 - v2) x (v1 - v2) of that face; the normal is t / |t| when
+ * |q - p| < 1e-6, else (q - p) / |q - p| oriented so that its dot with t is
+ * non-negative.  points, normals: 3 n_points doubles (xyz per point). */
+rso_status rso_mesh_normals(const float* vertices_host, int n_vertices, const int* faces_host, int n_faces,
+                            const double* points_host, int n_points, double* normals_host);
+
+/* Regions of space for boundary conditions (dynamic_range::range_t and its
+ * sphere / box / half-space / cylinder kinds, boundary/BoundaryCondition.h:
+ * 379-538; the static_range kinds :17-175 are the same tests without the
+ * complement flag).  p by kind:
+ *   SPHERE    centre xyz, radius: |p - c|^2 < r^2, closed adds |p - c|^2 - r^2 < 1e-8
+ *   BOX       min xyz, max xyz:  min < p < max on every axis, closed min <= p <= max
+ *   HALFSPACE a b c d:           a x + b y + c z + d > 0, closed adds = 0 (CGAL Plane_3)
+ *   CYLINDER  bottom centre xyz, radius, axis vector xyz: 0 <= axial <= |axis|
+ *             and radial distance < radius (closed and complement are ignored)
+ * complement negates the test (sphere, box, half-space). */
+enum { RSO_REGION_SPHERE = 0, RSO_REGION_BOX = 1, RSO_REGION_HALFSPACE = 2, RSO_REGION_CYLINDER = 3 };
+typedef struct {
+  int kind;
+  int closed;
+  int complement;
+  int reserved;
+  double p[8];
+} rso_region;
+
+/* A vector field restricted to a region (dynamic_range::rangeField_t and
+ * vectorField_t, boundary/BoundaryCondition.h:570-700): inside the region the
+ * value is norm(p) * dir(p), outside zero.
+ *   norm: CONSTANT value | RADIAL centre xyz, amplifier, damp: a exp(-|c - p|^(2 damp))
+ *         | TWIST axis start xyz, axis end xyz, amplifier: a |(p - s) x unit(e - s)|
+ *   dir:  CONSTANT unit(d) | RADIAL unit(c - p) | TWIST unit((p - s) x (e - s))
+ * unit(v) = v / |v| for |v| > 0, else v (Eigen normalized()). */
+enum { RSO_FIELD_CONSTANT = 0, RSO_FIELD_RADIAL = 1, RSO_FIELD_TWIST = 2 };
+typedef struct {
+  rso_region region;
+  int norm_kind;
+  int dir_kind;
+  double norm_p[7];
+  double dir_p[6];
+} rso_field;
+
+/* Node mask of the union of regions (rangeUnion::generate, boundary/
+ * BoundaryCondition.h:342-361 and :540-558) on the node grid
+ * p = origin + (i, j, k) h, i fastest over nx (the node positions of
+ * computeProjectionMatrix, grid/Grid.cpp:2694-2740).  mask_host: nx ny nz
+ * bytes.  The result is the fixed_area / load_area argument of rso_create. */
+rso_status rso_region_mask(const rso_region* regions_host, int n_regions, const double* origin_host, double h,
+                           int nx, int ny, int nz, uint8_t* mask_host);
+
+/* Sum of region fields at points (Field_t::at, boundary/BoundaryCondition.h:
+ * 702-741; the load force of computeProjectionMatrix).  points, vectors:
+ * 3 n_points doubles. */
+rso_status rso_region_field(const rso_field* fields_host, int n_fields, const double* points_host,
+                            int n_points, double* vectors_host);
+
 /* ---------------------------------------------------------------- setup */
 void rso_default_config(rso_config* cfg);
 

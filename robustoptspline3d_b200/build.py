@@ -17,13 +17,14 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xcompiler", "-Wno-unused-function", "-ccbin", "g++"]
 
-# voxelize.cu rounds every operation separately, as the host restatement of
-# the reference's voxeliser does (no fused multiply-add contraction)
-FILE_FLAGS = {"voxelize.cu": ["-fmad=false"]}
+# voxelize.cu and boundary.cu round every operation separately, as their host
+# restatements do (no fused multiply-add contraction)
+FILE_FLAGS = {"voxelize.cu": ["-fmad=false"], "boundary.cu": ["-fmad=false"]}
 
 SOURCES = ["capi.cu", "topology.cu", "fine_op.cu", "coarse_op.cu", "reduce.cu", "solver.cu", "design.cu",
            "design_capi.cu", "worst.cu", "mma.cu", "driver.cu", "prof.cu",
-           "filter_noalloc.cu", "batch.cu", "autotune.cu", "oc.cu", "voxelize.cu"]
+           "filter_noalloc.cu", "batch.cu", "autotune.cu", "oc.cu", "voxelize.cu",
+           "boundary.cu"]
 
 
 def _compile(src, verbose=False):

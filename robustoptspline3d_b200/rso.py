@@ -63,6 +63,16 @@ class _IterInfo(ctypes.Structure):
                 ("ms_mma", ctypes.c_double), ("solve_iterations", ctypes.c_int), ("mma_converged", ctypes.c_int)]
 
 
+class _Region(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("closed", ctypes.c_int), ("complement", ctypes.c_int),
+                ("reserved", ctypes.c_int), ("p", ctypes.c_double * 8)]
+
+
+class _Field(ctypes.Structure):
+    _fields_ = [("region", _Region), ("norm_kind", ctypes.c_int), ("dir_kind", ctypes.c_int),
+                ("norm_p", ctypes.c_double * 7), ("dir_p", ctypes.c_double * 6)]
+
+
 _vp = ctypes.c_void_p
 _ci = ctypes.c_int
 _cd = ctypes.c_double
@@ -96,6 +106,12 @@ SIGNATURES = {
     "rso_set_vcycle_graphs": (_ci, [_vp, _ci]),
     "rso_voxelize": (_ci, [ctypes.POINTER(ctypes.c_float), _ci, ctypes.POINTER(ctypes.c_int), _ci, _ci, _pu8, _pi,
                            ctypes.POINTER(ctypes.c_float)]),
+    "rso_shell_elements": (_ci, [ctypes.POINTER(ctypes.c_float), _ci, ctypes.POINTER(ctypes.c_int), _ci,
+                                 ctypes.POINTER(ctypes.c_float), _ci, _cd, _pu8, _pu8]),
+    "rso_mesh_normals": (_ci, [ctypes.POINTER(ctypes.c_float), _ci, ctypes.POINTER(ctypes.c_int), _ci, _pd, _ci,
+                               _pd]),
+    "rso_region_mask": (_ci, [ctypes.POINTER(_Region), _ci, _pd, _cd, _ci, _ci, _ci, _pu8]),
+    "rso_region_field": (_ci, [ctypes.POINTER(_Field), _ci, _pd, _ci, _pd]),
     "rso_mma_state_size": (_ci, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "rso_mma_save": (_ci, [_vp, _pd]),
     "rso_mma_load": (_ci, [_vp, _pd]),

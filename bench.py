@@ -208,6 +208,8 @@ def run_solves(args):
     g.set_density(rho)
     g.update_stencil()
     tuned = g.autotune() if prec == R.rso.MIXED and not args.no_autotune else None
+    if prec == R.rso.MIXED:
+        g.set_krylov_fp32(args.krylov32)
     f = torch.zeros(3 * g.nn, dtype=torch.float64, device="cuda")
     ln = torch.as_tensor(g.load_nodes(), device="cuda").long()
     f[2 * g.nn + ln] = torch.as_tensor(np.random.default_rng(1).standard_normal(len(ln)), device="cuda")
@@ -216,11 +218,12 @@ def run_solves(args):
     lib = g.lib
     lib.rso_profile_reset(g.h)
     lib.rso_set_profiling(g.h, 1)
-    its, ms = 0, 0.0
+    its, ms, worst = 0, 0.0, 0.0
     for _ in range(args.steps):
         _, it, rr, t = g.solve(f, tol=1e-6, max_iter=500)
         its += it
         ms += t
+        worst = max(worst, rr)
     lib.rso_set_profiling(g.h, 0)
     name = ctypes.create_string_buffer(64)
     cnt, tot, b, fl = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
@@ -236,6 +239,7 @@ def run_solves(args):
     print(json.dumps({"metric": f"multigrid PCG solve @{n}^3 to rel.resid 1e-6 ({args.precision})",
                       "value": ms / args.steps, "unit": "ms/solve", "higher_is_better": False,
                       "iterations_per_solve": its / args.steps, "ms_per_iteration": ms / its,
+                      "max_true_rel_residual": worst, "krylov32_replace_factor": args.krylov32,
                       "levels": g_levels(n), "kernel_classes": classes, "launch_shapes": tuned}), flush=True)
     g.close()
 
@@ -570,6 +574,8 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--krylov32", type=float, default=1e-2,
+                    help="mixed PCG with the FP32 Krylov recurrence, true-residual replacement factor (0: FP64 recurrence)")
     ap.add_argument("--mode", default="design", choices=["design", "solve", "batch", "problems", "scale", "mesh"])
     ap.add_argument("--systems", type=int, default=16)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
@@ -607,6 +613,8 @@ def main():
         g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=precision, smoother=smoother_id(R), omega=OMEGA, cheb_lower=CHEB_LOWER,
                                                         pre=2, post=2, poisson_ratio=0.3))
         nc = g.set_spline_partition(parts, parts, parts, order)
+        if precision == R.rso.MIXED:
+            g.set_krylov_fp32(args.krylov32)
         mma = R.MMA(nc, 2, 0.0, 1.0)
         mma.set_x(coeff)
         return g, mma
@@ -772,7 +780,10 @@ def main():
                 "vs_baseline": None, "dtype": "f32 V-cycle + f64 CG/Lanczos/MMA", "data": "synthetic",
                 "config": {"workload": f"{n}^3 worst-case spline TO iteration (config 4 shape)", "elements": n ** 3,
                            "spline": "order 4, 32^3 coefficients", "lanczos_steps": 20, "solve_tol": 1e-6,
-                           "smoother": f"{SMOOTHER} 2+2 on [{CHEB_LOWER}, 1] x lambda_max", "preconditioner": "one V-cycle per FP64 CG iteration",
+                           "smoother": f"{SMOOTHER} 2+2 on [{CHEB_LOWER}, 1] x lambda_max",
+                           "preconditioner": "one V-cycle per CG iteration",
+                           "krylov": (f"FP32 recurrence, true FP64 residual replacing it every {args.krylov32:g} "
+                                      "reduction and at the end") if args.krylov32 > 0 else "FP64 recurrence",
                            "levels": g_levels(n), "parallelism": f"replicas x{world}",
                            "l2_flush": "inputs larger than L2",
                            "step": "one design iteration from the seeded initial design"},

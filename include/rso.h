@@ -313,6 +313,16 @@ rso_status rso_set_launch_shapes(rso_handle* h, const int* choices_host, int n);
  * handle's own or one set by rso_set_stream other than the legacy default
  * stream; if a capture fails the handle keeps to plain launches. */
 rso_status rso_set_vcycle_graphs(rso_handle* h, int on);
+/* Krylov recurrence of the mixed-precision PCG (no counterpart in the
+ * reference, whose CG is FP64).  0 < replace_factor < 1 (1e-2 by default in
+ * mixed precision): the recurrence runs in FP32 (FP32 operator, FP32
+ * vectors, FP64 sums and FP64 iterate) and the true FP64 residual f - K x
+ * replaces the recursive one whenever that has dropped by replace_factor
+ * since the last replacement and before the solve stops, so the tolerance is
+ * always met by a true FP64 residual.  replace_factor 0: p, q = K p and r are
+ * FP64 and only the V-cycle is FP32.  Batched solves keep the FP64
+ * recurrence. */
+rso_status rso_set_krylov_fp32(rso_handle* h, double replace_factor);
 /* Grid::compliance (grid/Grid.cpp:4118-4121): c = f . u */
 rso_status rso_dot(rso_handle* h, const double* a_dev, const double* b_dev, double* out);
 

@@ -163,10 +163,10 @@ static rso_status setup(rso_handle* h, int ex, int ey, int ez, const uint8_t* em
     h->xfer_n = xf;
   }
   {
-    // one partial per CTA of the fine operator kernel (32 x 8 threads,
-    // 31 x 7 nodes per z-chunk of 32 planes)
+    // one partial per CTA of the fine operator kernels: 31 x 7 nodes per
+    // z-chunk of 32 planes (FP64), 31 x 3 or 31 x 7 (packed FP32, 2 or 4 rows)
     const Level& f0 = h->L[0];
-    h->fpart_n = (long long)cdiv(f0.nx, 31) * cdiv(f0.ny, 7) * cdiv(f0.nz, 32);
+    h->fpart_n = (long long)cdiv(f0.nx, 31) * cdiv(f0.ny, 3) * cdiv(f0.nz, 32);
     ALLOC(h->fpart, sizeof(double) * h->fpart_n);
   }
   // per-level buffers
@@ -289,6 +289,9 @@ extern "C" rso_status rso_create(const rso_config* cfg, int ex, int ey, int ez, 
   if (!h) return RSO_ERR_OOM;
   if (cfg) h->cfg = *cfg;
   else rso_default_config(&h->cfg);
+  // mixed precision runs the PCG recurrence in FP32 with true-residual
+  // replacement every 1e-2 of reduction (rso_set_krylov_fp32)
+  h->krylov32 = h->cfg.precision == RSO_MIXED ? 1e-2 : 0.0;
   if (h->cfg.first_factor != 2 && h->cfg.first_factor != 4) { delete h; return RSO_ERR_INVALID_ARG; }
   if (h->cfg.pre < 0 || h->cfg.post < 0 || h->cfg.penal <= 0 || h->cfg.pre > 16 || h->cfg.post > 16) {
     delete h;
@@ -451,6 +454,12 @@ extern "C" rso_status rso_prolong_fp32(rso_handle* h, int cl, const double* uc, 
 extern "C" rso_status rso_set_vcycle_graphs(rso_handle* h, int on) {
   if (!h) return RSO_ERR_INVALID_ARG;
   h->vc_graphs = on != 0;
+  return RSO_OK;
+}
+
+extern "C" rso_status rso_set_krylov_fp32(rso_handle* h, double replace_factor) {
+  if (!h || !(replace_factor >= 0.0) || !(replace_factor < 1.0)) return RSO_ERR_INVALID_ARG;
+  h->krylov32 = replace_factor;
   return RSO_OK;
 }
 

@@ -1229,6 +1229,19 @@ rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const doub
   // one sum per system: dot_dev[b] over the b-th block of partials
   return reduce_partials_batch(h, h->fpart, (int)(nb / h->L[0].nb), h->L[0].nb, dot_dev, stride);
 }
+// the same in FP32 on the packed kernel (the reliable-update PCG's K p)
+rso_status fine_applyK_dot32(rso_handle* h, const float* u, float* f, double* dot_dev) {
+  const Level& l0 = h->L[0];
+  const dim3 g = pair_grid(l0, h->tune.fine_rows == 2 ? 2 : 4);
+  const long long nb = (long long)g.x * g.y * g.z;
+  if (l0.nb != 1 || nb > h->fpart_n) {
+    h->err = "fine partial-sum buffer smaller than the grid";
+    return RSO_ERR_STATE;
+  }
+  const rso_status st = launch_fine<float, 1>(h, u, u, f, h->rp32, 0.0, PC_FINE_RES32, "fine_applyK_dot32", h->fpart);
+  if (st != RSO_OK) return st;
+  return reduce_partials(h, h->fpart, (int)nb, dot_dev);
+}
 template <typename T>
 rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega,
                        const T* u_prev, double c1) {

@@ -102,6 +102,64 @@ rso_status cg_resid_rr(rso_handle* h, long long n, const double* alpha, const do
   return launch_check(h, "cg_resid_rr");
 }
 
+// FP32 Krylov recurrence (reliable-update PCG): r -= a q in FP32 with the
+// sum r.r in FP64, and a.b of two FP32 vectors summed in FP64; 16-byte
+// vectors (3 NP is a multiple of 4 and the buffers are 256-byte aligned)
+__global__ void __launch_bounds__(RED_THREADS) k_cg32_resid_rr(long long n4, const double* __restrict__ alpha,
+                                                               const float4* __restrict__ q, float4* __restrict__ r,
+                                                               double* __restrict__ part) {
+  const float a = (float)*alpha;
+  double s = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+    const float4 qi = q[i];
+    float4 ri = r[i];
+    ri.x -= a * qi.x;
+    ri.y -= a * qi.y;
+    ri.z -= a * qi.z;
+    ri.w -= a * qi.w;
+    r[i] = ri;
+    s += (double)ri.x * ri.x + (double)ri.y * ri.y + (double)ri.z * ri.z + (double)ri.w * ri.w;
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_dot_ff_partial(const float4* __restrict__ a,
+                                                                const float4* __restrict__ b, long long n4,
+                                                                double* __restrict__ part) {
+  double s = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+    const float4 x = a[i], y = b[i];
+    s += (double)x.x * y.x + (double)x.y * y.y + (double)x.z * y.z + (double)x.w * y.w;
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+rso_status cg32_resid_rr(rso_handle* h, long long n, const double* alpha, const float* q, float* r, double* rr_dev) {
+  if ((n & 3) || ((reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(r)) & 15)) {
+    h->err = "cg32_resid_rr: vectors must be 16-byte aligned multiples of 4 entries";
+    return RSO_ERR_STATE;
+  }
+  k_cg32_resid_rr<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(n / 4, alpha, reinterpret_cast<const float4*>(q),
+                                                              reinterpret_cast<float4*>(r), h->red);
+  rso::note_launch();
+  k_final<<<1, RED_THREADS, 0, h->stream>>>(h->red, RED_BLOCKS, rr_dev); rso::note_launch();
+  return launch_check(h, "cg32_resid_rr");
+}
+
+rso_status dot_ff(rso_handle* h, const float* a, const float* b, long long n, double* dev_out) {
+  if ((n & 3) || ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 15)) {
+    h->err = "dot_ff: vectors must be 16-byte aligned multiples of 4 entries";
+    return RSO_ERR_STATE;
+  }
+  k_dot_ff_partial<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(reinterpret_cast<const float4*>(a),
+                                                               reinterpret_cast<const float4*>(b), n / 4, h->red);
+  rso::note_launch();
+  k_final<<<1, RED_THREADS, 0, h->stream>>>(h->red, RED_BLOCKS, dev_out); rso::note_launch();
+  return launch_check(h, "dot_ff");
+}
+
 // one sum per system: out[b * stride] = sum of part[b * nper .. (b + 1) * nper)
 __global__ void __launch_bounds__(RED_THREADS) k_final_batch(const double* __restrict__ part, int nper,
                                                              double* __restrict__ out, int stride) {

@@ -151,6 +151,11 @@ struct rso_handle {
     int bottom = -2;        // first level of the bottom cluster kernel, -1 none, -2 by size
     Tune() { for (int& r : rowsplit) r = -1; }
   } tune;
+  // reliable-update PCG (mixed precision): the Krylov recurrence in FP32,
+  // the true FP64 residual replacing the recursive one once it has dropped by
+  // this factor since the last replacement (0: FP64 recurrence); rso_create
+  // sets 1e-2 for mixed precision
+  double krylov32 = 0.0;
   // worst-case scratch kept between calls (worst.cu): Lanczos load-space
   // vectors, reorthogonalisation sums, the force-projection vector
   double* wc_buf = nullptr;
@@ -214,6 +219,9 @@ rso_status reduce_partials_batch(rso_handle* h, const double* part, int nper, in
                                  int stride = 1);
 rso_status pow_step(rso_handle* h, long long n, const float* u, const float* t, float* r, double* uu, double* rr);
 rso_status dot_df(rso_handle* h, const double* a, const float* b, long long n, double* dev_out);
+rso_status dot_ff(rso_handle* h, const float* a, const float* b, long long n, double* dev_out);
+rso_status cg32_resid_rr(rso_handle* h, long long n, const double* alpha, const float* q, float* r, double* rr_dev);
+rso_status fine_applyK_dot32(rso_handle* h, const float* u, float* f, double* dot_dev);
 rso_status sum_float(rso_handle* h, const float* a, long long n, double* dev_out);
 
 // conversion between the public dense layout and padded layout

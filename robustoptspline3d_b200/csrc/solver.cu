@@ -385,6 +385,133 @@ rso_status vcycle_mixed(rso_handle* h) {
   return launch_check(h, "vcycle graph");
 }
 
+// reliable-update PCG: x (FP64) += alpha p (FP32), and p = z + beta p in FP32
+// (DIR_ONLY: the direction update alone, x having taken the step already)
+template <bool DIR_ONLY>
+__global__ void k_cg32_step_dir(long long n4, const double* __restrict__ alpha, const double* __restrict__ beta,
+                                const float4* __restrict__ z, float4* __restrict__ p, double2* __restrict__ x) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n4) return;
+  const float4 pi = p[i], zi = z[i];
+  if (!DIR_ONLY) {
+    const double a = *alpha;
+    double2 x0 = x[2 * i], x1 = x[2 * i + 1];
+    x0.x += a * pi.x;
+    x0.y += a * pi.y;
+    x1.x += a * pi.z;
+    x1.y += a * pi.w;
+    x[2 * i] = x0;
+    x[2 * i + 1] = x1;
+  }
+  const float b = (float)*beta;
+  p[i] = make_float4(zi.x + b * pi.x, zi.y + b * pi.y, zi.z + b * pi.z, zi.w + b * pi.w);
+}
+__global__ void k_cg32_step(long long n4, const double* __restrict__ alpha, const float4* __restrict__ p,
+                            double2* __restrict__ x) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n4) return;
+  const float4 pi = p[i];
+  const double a = *alpha;
+  double2 x0 = x[2 * i], x1 = x[2 * i + 1];
+  x0.x += a * pi.x;
+  x0.y += a * pi.y;
+  x1.x += a * pi.z;
+  x1.y += a * pi.w;
+  x[2 * i] = x0;
+  x[2 * i + 1] = x1;
+}
+
+// Mixed-precision PCG with the Krylov recurrence in FP32 (no counterpart in
+// the reference, whose CG is FP64): p, q = K p, r and z are FP32 and the
+// iterate x accumulates alpha p in FP64.  The recursive FP32 residual drifts
+// from the true one by the FP32 operator's rounding, so whenever it has
+// dropped by h->krylov32 since the last replacement, and before stopping, the
+// true residual f - K x is formed in FP64 and replaces it (residual
+// replacement, the search direction kept).  The reported residual is always a
+// true FP64 one.
+static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, double tol, int max_iter,
+                                rso_solve_info* info) {
+  Level& l0 = h->L[0];
+  const long long n3 = 3 * l0.NP, n4 = n3 / 4;
+  double* s = h->scal;  // s[0]=rz, s[1]=pq, s[2]=alpha, s[3]=rz_new, s[4]=beta, s[5]=rr
+  float* r32 = l0.f32;  // the V-cycle's right-hand side (not rotated by the smoothers)
+  // the V-cycle's result is L[0].u32, a pointer the Chebyshev and Jacobi
+  // smoothers rotate: read it after every V-cycle
+  float* p32 = reinterpret_cast<float*>(h->z);  // FP64 buffers unused by the mixed recurrence
+  float* q32 = reinterpret_cast<float*>(h->q);
+  if ((n3 & 3) || (reinterpret_cast<uintptr_t>(x) & 15)) {
+    h->err = "reliable-update PCG: x must be 16-byte aligned";
+    return RSO_ERR_INVALID_ARG;
+  }
+  auto true_residual = [&](double* rn2) -> rso_status {
+    RSO_TRY(fine_residual<double>(h, x, f, h->r, h->rp64));
+    return dot_host(h, h->r, h->r, n3, rn2);
+  };
+  double fn2 = 0, rn2 = 0;
+  RSO_TRY(dot_host(h, f, f, n3, &fn2));
+  RSO_TRY(true_residual(&rn2));
+  const double fn = std::sqrt(fn2);
+  int it = 0;
+  double rel = fn > 0 ? std::sqrt(rn2) / fn : 0.0;
+  if (fn == 0) {
+    RSO_CHECK_CUDA(h, cudaMemsetAsync(x, 0, sizeof(double) * n3, h->stream));
+    rel = 0;
+  }
+  if (rel >= tol && fn > 0) {
+    double rbase = std::sqrt(rn2);  // residual norm at the last replacement
+    // the operator writes interior nodes only: the padding of q (an FP64
+    // buffer seen as FP32, so old doubles split across its entries) must be zero
+    RSO_CHECK_CUDA(h, cudaMemsetAsync(q32, 0, sizeof(float) * n3, h->stream));
+    k_d2f<<<cdiv(n3, 256), 256, 0, h->stream>>>(h->r, r32, n3); rso::note_launch();
+    RSO_TRY(vcycle_mixed(h));
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(p32, l0.u32, sizeof(float) * n3, cudaMemcpyDeviceToDevice, h->stream));
+    RSO_TRY(dot_ff(h, r32, l0.u32, n3, s + 0));
+    while (it < max_iter) {
+      RSO_TRY(fine_applyK_dot32(h, p32, q32, s + 1));
+      k_cg_alpha<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
+      RSO_TRY(cg32_resid_rr(h, n3, s + 2, q32, r32, s + 5));
+      RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->h_scal + 5, s + 5, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+      RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+      vcycle_graphs_harvest(h);
+      it++;
+      const double rnorm = std::sqrt(h->h_scal[5]);
+      if (!std::isfinite(rnorm)) { h->err = "non-finite residual in PCG"; return RSO_ERR_NONFINITE; }
+      const bool replace = rnorm < h->krylov32 * rbase || rnorm < tol * fn || it >= max_iter;
+      if (replace) {
+        k_cg32_step<<<cdiv(n4, 256), 256, 0, h->stream>>>(n4, s + 2, reinterpret_cast<const float4*>(p32),
+                                                          reinterpret_cast<double2*>(x));
+        rso::note_launch();
+        RSO_TRY(true_residual(&rn2));
+        rbase = std::sqrt(rn2);
+        rel = rbase / fn;
+        if (!std::isfinite(rel)) { h->err = "non-finite residual in PCG"; return RSO_ERR_NONFINITE; }
+        if (rel < tol || it >= max_iter) break;
+        k_d2f<<<cdiv(n3, 256), 256, 0, h->stream>>>(h->r, r32, n3); rso::note_launch();
+      } else {
+        rel = rnorm / fn;
+      }
+      RSO_TRY(vcycle_mixed(h));
+      const float* z32 = l0.u32;
+      RSO_TRY(dot_ff(h, r32, z32, n3, s + 3));
+      k_cg_beta<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
+      if (replace)
+        k_cg32_step_dir<true><<<cdiv(n4, 256), 256, 0, h->stream>>>(
+            n4, s + 2, s + 4, reinterpret_cast<const float4*>(z32), reinterpret_cast<float4*>(p32),
+            reinterpret_cast<double2*>(x));
+      else
+        k_cg32_step_dir<false><<<cdiv(n4, 256), 256, 0, h->stream>>>(
+            n4, s + 2, s + 4, reinterpret_cast<const float4*>(z32), reinterpret_cast<float4*>(p32),
+            reinterpret_cast<double2*>(x));
+      rso::note_launch();
+      RSO_TRY(launch_check(h, "pcg32"));
+    }
+  }
+  RSO_TRY(fine_stage_check(h));
+  if (info) { info->iterations = it; info->rel_res = rel; }
+  if (rel >= tol && fn > 0) { h->err = "PCG did not reach the tolerance within max_iter"; return RSO_ERR_BUDGET_EXCEEDED; }
+  return RSO_OK;
+}
+
 // CG preconditioned by one V-cycle.  In mixed precision the preconditioned
 // residual z stays FP32 (it only enters r.z and the direction update), the
 // FP32 copy of r is written by the fused residual update, and the norm of r
@@ -393,6 +520,7 @@ rso_status solve_pcg(rso_handle* h, const double* f, double* x, double tol, int 
   Level& l0 = h->L[0];
   const long long n3 = 3 * l0.NP;
   const bool mixed = h->cfg.precision == RSO_MIXED;
+  if (mixed && h->krylov32 > 0 && l0.nb == 1) return solve_pcg_k32(h, f, x, tol, max_iter, info);
   double* s = h->scal;
   RSO_TRY(fine_residual<double>(h, x, f, h->r, h->rp64));
   double fn2 = 0, rn2 = 0;

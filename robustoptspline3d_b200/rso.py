@@ -104,6 +104,7 @@ SIGNATURES = {
     "rso_residual": (_ci, [_vp, _vp, _vp, _vp]),
     "rso_fine_sweep_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
     "rso_set_vcycle_graphs": (_ci, [_vp, _ci]),
+    "rso_set_krylov_fp32": (_ci, [_vp, _cd]),
     "rso_voxelize": (_ci, [ctypes.POINTER(ctypes.c_float), _ci, ctypes.POINTER(ctypes.c_int), _ci, _ci, _pu8, _pi,
                            ctypes.POINTER(ctypes.c_float)]),
     "rso_shell_elements": (_ci, [ctypes.POINTER(ctypes.c_float), _ci, ctypes.POINTER(ctypes.c_int), _ci,
@@ -452,6 +453,11 @@ class HierarchyGrid:
         self._chk(self.lib.rso_oc_update_coeff(self.h, _dev(c), _dev(cs), vgoal, step, damp, cmin, cmax, _dev(rho),
                                                _np_ptr(info, _pd)), "rso_oc_update_coeff")
         return c, rho, {"g": info[0], "volume": info[1], "trials": int(info[2])}
+
+    def set_krylov_fp32(self, replace_factor=1e-2):
+        """Mixed precision: run the PCG recurrence in FP32 with true-residual replacement
+        whenever the residual has dropped by replace_factor (0 restores the FP64 recurrence)."""
+        self._chk(self.lib.rso_set_krylov_fp32(self.h, float(replace_factor)), "rso_set_krylov_fp32")
 
     def set_vcycle_graphs(self, on):
         """Replay captured FP32 V-cycles from CUDA graphs (default) or launch every kernel."""

@@ -777,7 +777,7 @@ def main():
         last = infos[-1]
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32 V-cycle + f64 CG/Lanczos/MMA", "data": "synthetic",
+                "vs_baseline": None, "dtype": "f32 V-cycle and CG recurrence + f64 iterate, residual replacement, Lanczos, MMA", "data": "synthetic",
                 "config": {"workload": f"{n}^3 worst-case spline TO iteration (config 4 shape)", "elements": n ** 3,
                            "spline": "order 4, 32^3 coefficients", "lanczos_steps": 20, "solve_tol": 1e-6,
                            "smoother": f"{SMOOTHER} 2+2 on [{CHEB_LOWER}, 1] x lambda_max",

@@ -6,8 +6,10 @@
 // finer residual, restricts it, zeroes u and pre-smooths; the coarsest level
 // is solved directly; the up-sweep prolongates and post-smooths.  In mixed
 // precision the V-cycle runs in FP32 on FP32 copies of rho^p and of the
-// coarse stencils, while the outer residual, the CG vectors and scalars and
-// the coarsest solve stay FP64.
+// coarse stencils; the CG recurrence runs in FP32 too unless the handle's
+// replacement factor is 0 (then the outer residual and the CG vectors are
+// FP64), while the iterate, the sums, the residual replacements and the
+// coarsest solve stay FP64.
 #include "rso_internal.cuh"
 #include <cmath>
 #include <cstring>

@@ -6,7 +6,9 @@
 // kernel reading each stencil entry once for up to four systems, the cluster
 // kernel of the small levels over system x node pairs).  CG runs one
 // recurrence per system with per-system scalars; a converged system keeps
-// alpha = beta = 0 while the others continue.
+// alpha = beta = 0 while the others continue.  In mixed precision the
+// recurrence is FP32 with FP64 residual replacement, as for single solves,
+// each system replacing on its own rule.
 #include "rso_internal.cuh"
 #include <chrono>
 #include <cmath>
@@ -108,6 +110,56 @@ __global__ void k_bf2d(long long total, const float* __restrict__ a, double* __r
   if (i < total) b[i] = (double)a[i];
 }
 
+// FP32 Krylov recurrence of the batch (reliable-update PCG, as solve_pcg_k32):
+// r -= alpha_b q in FP32 with per-system sums of r.r, per-system a.b of FP32
+// vectors, x (FP64) += alpha_b p (FP32) and p = z + beta_b p
+__global__ void __launch_bounds__(BR_THREADS) k_bresid32(long long n, const double* __restrict__ s,
+                                                         const float* __restrict__ q, float* __restrict__ r,
+                                                         double* __restrict__ part) {
+  const long long o = (long long)blockIdx.y * n;
+  const float a = (float)s[blockIdx.y * KS + 2];
+  double acc = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float ri = r[o + i] - a * q[o + i];
+    r[o + i] = ri;
+    acc += (double)ri * ri;
+  }
+  acc = b_block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.y * BR_BLOCKS + blockIdx.x] = acc;
+}
+__global__ void __launch_bounds__(BR_THREADS) k_bdot32(long long n, const float* __restrict__ a,
+                                                       const float* __restrict__ b, double* __restrict__ part) {
+  const long long o = (long long)blockIdx.y * n;
+  double acc = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    acc += (double)a[o + i] * b[o + i];
+  acc = b_block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.y * BR_BLOCKS + blockIdx.x] = acc;
+}
+template <bool DIR_ONLY>
+__global__ void k_bstep_dir32(long long n, long long total, const double* __restrict__ s, const float* __restrict__ z,
+                              float* __restrict__ p, double* __restrict__ x) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const long long b = i / n;
+  const float pi = p[i];
+  if (!DIR_ONLY) x[i] += s[b * KS + 2] * pi;
+  p[i] = z[i] + (float)s[b * KS + 4] * pi;
+}
+__global__ void k_bstep32(long long n, long long total, const double* __restrict__ s, const float* __restrict__ p,
+                          double* __restrict__ x) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  x[i] += s[(i / n) * KS + 2] * p[i];
+}
+// r32 = r for the systems whose bit is set in mask (k <= 64)
+__global__ void k_bd2f_sel(long long n, long long total, const double* __restrict__ r, float* __restrict__ r32,
+                           unsigned long long mask) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= total || !((mask >> (i / n)) & 1ULL)) return;
+  r32[i] = (float)r[i];
+}
+
 static void batch_free(rso_handle* h) {
   auto& B = h->batch;
   for (auto* v : {&B.u32, &B.f32, &B.r32, &B.t32})
@@ -158,7 +210,7 @@ static rso_status batch_alloc(rso_handle* h, int k) {
   }
   const size_t n0 = (size_t)k * 3 * h->L[0].NP;
   BALLOC(B.x, 8 * n0); BALLOC(B.r, 8 * n0); BALLOC(B.p, 8 * n0); BALLOC(B.q, 8 * n0);
-  if (!mixed) BALLOC(B.z, 8 * n0);
+  BALLOC(B.z, 8 * n0);  // FP64 z, or the padded right-hand sides of the FP32 recurrence
   BALLOC(B.cf, sizeof(double) * std::max(1, 3 * h->nc) * k);
   BALLOC(B.red, sizeof(double) * BR_BLOCKS * k);
   BALLOC(B.fpart, sizeof(double) * h->fpart_n * k);
@@ -223,14 +275,18 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
   auto& B = h->batch;
   const double t0 = now_ms();
   const long long n3 = 3 * h->L[0].NP, tot = (long long)k * n3, nn3 = 3 * h->L[0].nn;
-  // dense -> padded slabs (x holds the initial guesses, p the right-hand sides for now)
+  const bool mixed = h->cfg.precision == RSO_MIXED;
+  const bool k32 = mixed && h->krylov32 > 0;
+  // dense -> padded slabs: x holds the initial guesses; the right-hand sides
+  // go to q for now (FP64 recurrence) or to z, kept for the residual
+  // replacements (FP32 recurrence, whose p and q are FP32 in p's and q's memory)
+  double* fpad = k32 ? B.z : B.q;
   for (int b = 0; b < k; b++) {
     RSO_TRY(pad_nodes(h, 0, U + b * nn3, B.x + b * n3));
-    RSO_TRY(pad_nodes(h, 0, F + b * nn3, B.q + b * n3));
+    RSO_TRY(pad_nodes(h, 0, F + b * nn3, fpad + b * n3));
     RSO_TRY(zero_support(h, B.x + b * n3));
-    RSO_TRY(zero_support(h, B.q + b * n3));
+    RSO_TRY(zero_support(h, fpad + b * n3));
   }
-  const bool mixed = h->cfg.precision == RSO_MIXED;
   std::vector<int> it(k, 0), done(k, 0);
   std::vector<double> fn(k, 0), rel(k, 0);
   rso_status status = RSO_OK;
@@ -240,8 +296,8 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
     const dim3 rg(BR_BLOCKS, k);
     double* s = B.scal;
     // r = f - K x; |f|^2 and |r|^2 per system
-    RSO_TRY(fine_residual<double>(h, B.x, B.q, B.r, h->rp64));
-    k_bdot<double><<<rg, BR_THREADS, 0, h->stream>>>(n3, B.q, B.q, B.red); rso::note_launch();
+    RSO_TRY(fine_residual<double>(h, B.x, fpad, B.r, h->rp64));
+    k_bdot<double><<<rg, BR_THREADS, 0, h->stream>>>(n3, fpad, fpad, B.red); rso::note_launch();
     k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 6); rso::note_launch();
     k_bdot<double><<<rg, BR_THREADS, 0, h->stream>>>(n3, B.r, B.r, B.red); rso::note_launch();
     k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 5); rso::note_launch();
@@ -265,7 +321,80 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
       RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.z, h->L[0].u64, sizeof(double) * tot, cudaMemcpyDeviceToDevice, h->stream));
       return RSO_OK;
     };
-    if (left > 0) {
+    if (left > 0 && k32) {
+      float* p32 = reinterpret_cast<float*>(B.p);
+      float* q32 = reinterpret_cast<float*>(B.q);
+      float* r32 = l0.f32;  // the batched V-cycle's right-hand sides (the smoothers rotate u, not f)
+      std::vector<double> rbase(k);
+      for (int b = 0; b < k; b++) rbase[b] = rel[b] * fn[b];
+      // the operator writes interior nodes only: q's padding must be zero
+      RSO_CHECK_CUDA(h, cudaMemsetAsync(q32, 0, sizeof(float) * tot, h->stream));
+      k_bd2f<<<cdiv(tot, 256), 256, 0, h->stream>>>(tot, B.r, r32); rso::note_launch();
+      RSO_TRY(vcycle_mixed(h));
+      RSO_CHECK_CUDA(h, cudaMemcpyAsync(p32, l0.u32, sizeof(float) * tot, cudaMemcpyDeviceToDevice, h->stream));
+      k_bdot32<<<rg, BR_THREADS, 0, h->stream>>>(n3, r32, l0.u32, B.red); rso::note_launch();
+      k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 0); rso::note_launch();
+      int iter = 0;
+      while (true) {
+        RSO_TRY(fine_applyK_dot32(h, p32, q32, s + 1, KS));
+        k_balpha<<<1, 64, 0, h->stream>>>(k, s, B.done); rso::note_launch();
+        k_bresid32<<<rg, BR_THREADS, 0, h->stream>>>(n3, s, q32, r32, B.red); rso::note_launch();
+        k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 5); rso::note_launch();
+        RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.h_scal, s, sizeof(double) * KS * k, cudaMemcpyDeviceToHost, h->stream));
+        RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+        vcycle_graphs_harvest(h);
+        iter++;
+        // systems asking for a replacement: their recursive residual dropped
+        // by the factor since their last one, or below the tolerance; all at
+        // the iteration limit
+        unsigned long long ask = 0;
+        for (int b = 0; b < k; b++) {
+          if (done[b]) continue;
+          it[b] = iter;
+          const double rn = std::sqrt(B.h_scal[b * KS + 5]);
+          if (!std::isfinite(rn)) { h->err = "non-finite residual in batched PCG"; return RSO_ERR_NONFINITE; }
+          rel[b] = rn / fn[b];
+          if (rn < tol * fn[b] || rn < h->krylov32 * rbase[b] || iter >= max_iter) ask |= 1ULL << b;
+        }
+        const bool replace = ask != 0;
+        if (replace) {
+          // every system takes its step now (frozen ones have alpha 0; the
+          // direction update below then leaves x alone); the true FP64
+          // residuals replace the recursive ones of the asking systems only,
+          // so each system follows the sequence of its own single solve
+          k_bstep32<<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, s, p32, B.x); rso::note_launch();
+          RSO_TRY(fine_residual<double>(h, B.x, fpad, B.r, h->rp64));
+          k_bdot<double><<<rg, BR_THREADS, 0, h->stream>>>(n3, B.r, B.r, B.red); rso::note_launch();
+          k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 5); rso::note_launch();
+          RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.h_scal, s, sizeof(double) * KS * k, cudaMemcpyDeviceToHost, h->stream));
+          RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+          left = 0;
+          unsigned long long take = 0;
+          for (int b = 0; b < k; b++) {
+            if (done[b]) continue;
+            if (!((ask >> b) & 1ULL)) { left++; continue; }
+            rbase[b] = std::sqrt(B.h_scal[b * KS + 5]);
+            rel[b] = rbase[b] / fn[b];
+            if (!std::isfinite(rel[b])) { h->err = "non-finite residual in batched PCG"; return RSO_ERR_NONFINITE; }
+            if (rel[b] < tol) done[b] = 1;
+            else { left++; take |= 1ULL << b; }
+          }
+          if (left == 0 || iter >= max_iter) break;
+          if (take) { k_bd2f_sel<<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, B.r, r32, take); rso::note_launch(); }
+          RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.done, done.data(), sizeof(int) * k, cudaMemcpyHostToDevice, h->stream));
+        }
+        RSO_TRY(vcycle_mixed(h));
+        k_bdot32<<<rg, BR_THREADS, 0, h->stream>>>(n3, r32, l0.u32, B.red); rso::note_launch();
+        k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 3); rso::note_launch();
+        k_bbeta<<<1, 64, 0, h->stream>>>(k, s, B.done); rso::note_launch();
+        if (replace)
+          k_bstep_dir32<true><<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, s, l0.u32, p32, B.x);
+        else
+          k_bstep_dir32<false><<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, s, l0.u32, p32, B.x);
+        rso::note_launch();
+        RSO_TRY(launch_check(h, "batched pcg32"));
+      }
+    } else if (left > 0) {
       RSO_TRY(precondition_z());
       if (mixed) {
         k_bf2d<<<cdiv(tot, 256), 256, 0, h->stream>>>(tot, h->L[0].u32, B.p); rso::note_launch();

@@ -1229,18 +1229,19 @@ rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const doub
   // one sum per system: dot_dev[b] over the b-th block of partials
   return reduce_partials_batch(h, h->fpart, (int)(nb / h->L[0].nb), h->L[0].nb, dot_dev, stride);
 }
-// the same in FP32 on the packed kernel (the reliable-update PCG's K p)
-rso_status fine_applyK_dot32(rso_handle* h, const float* u, float* f, double* dot_dev) {
+// the same in FP32 on the packed kernel (the reliable-update PCG's K p);
+// dot_dev[b * stride] per system of a batch
+rso_status fine_applyK_dot32(rso_handle* h, const float* u, float* f, double* dot_dev, int stride) {
   const Level& l0 = h->L[0];
   const dim3 g = pair_grid(l0, h->tune.fine_rows == 2 ? 2 : 4);
-  const long long nb = (long long)g.x * g.y * g.z;
-  if (l0.nb != 1 || nb > h->fpart_n) {
+  const long long nb = (long long)g.x * g.y * g.z;  // all systems
+  if (nb > h->fpart_n) {
     h->err = "fine partial-sum buffer smaller than the grid";
     return RSO_ERR_STATE;
   }
   const rso_status st = launch_fine<float, 1>(h, u, u, f, h->rp32, 0.0, PC_FINE_RES32, "fine_applyK_dot32", h->fpart);
   if (st != RSO_OK) return st;
-  return reduce_partials(h, h->fpart, (int)nb, dot_dev);
+  return reduce_partials_batch(h, h->fpart, (int)(nb / l0.nb), l0.nb, dot_dev, stride);
 }
 template <typename T>
 rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega,

@@ -221,7 +221,7 @@ rso_status pow_step(rso_handle* h, long long n, const float* u, const float* t, 
 rso_status dot_df(rso_handle* h, const double* a, const float* b, long long n, double* dev_out);
 rso_status dot_ff(rso_handle* h, const float* a, const float* b, long long n, double* dev_out);
 rso_status cg32_resid_rr(rso_handle* h, long long n, const double* alpha, const float* q, float* r, double* rr_dev);
-rso_status fine_applyK_dot32(rso_handle* h, const float* u, float* f, double* dot_dev);
+rso_status fine_applyK_dot32(rso_handle* h, const float* u, float* f, double* dot_dev, int stride = 1);
 rso_status sum_float(rso_handle* h, const float* a, long long n, double* dev_out);
 
 // conversion between the public dense layout and padded layout

@@ -2,7 +2,8 @@
 
 TEST INFRASTRUCTURE ONLY: the checker of rso_region_mask, rso_region_field,
 rso_shell_elements and rso_mesh_normals; the product library never imports
-it.
+it.  Parity unpinned: the reference ships no fixtures for these and its CGAL /
+Eigen host code cannot be built here.
 
 Follows the reference:
   range and field classes      boundary/BoundaryCondition.h:379-741

@@ -2,7 +2,9 @@
 reference computes in FP32).
 
 TEST INFRASTRUCTURE ONLY: the checker of the library's OC entry points; the
-product library never imports it.
+product library never imports it.  Parity unpinned: the reference ships no OC
+fixtures and cannot be built here, so this restatement of its code is the only
+anchor.
 
 Follows optimization/optimization.cu of the reference:
   trySensMultiplier_kernel  :366-392  (the per-element update)

@@ -1,7 +1,9 @@
 """Solid voxelisation restated in numpy FP32, operation by operation.
 
 TEST INFRASTRUCTURE ONLY: the checker of rso_voxelize; the product library
-never imports it.
+never imports it.  Parity unpinned: the reference ships no voxelisation
+fixtures and its voxeliser cannot be built here; the tests add exact counts on
+a cube and a sphere's volume.
 
 Restates the solid mode of the cuda_voxelizer the reference vendors
 (voxelizer/cpu_voxelizer.cpp:206-330, cpu_voxelize_mesh_solid with

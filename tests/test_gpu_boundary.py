@@ -133,3 +133,37 @@ def test_mesh_problem_chain(cuda):
     assert np.array_equal((cls & 2) > 0, surf)
     assert np.array_equal((cls & 8) > 0, lmask)
     g.close()
+
+
+def test_boundary_edge_cases(cuda):
+    """Empty region and field lists, zero shell width, no points, a degenerate
+    face, points on faces / edges / vertices, and a one-element grid."""
+    from oracle import boundary as OB
+    from robustoptspline3d_b200 import boundary as B
+    from robustoptspline3d_b200.voxelize import voxelize
+    # empty unions: no node selected, zero field
+    assert B.region_mask([], (0, 0, 0), 1.0, (3, 2, 1)).sum() == 0
+    assert np.all(B.region_field([], np.ones((4, 3))) == 0)
+    assert B.region_field([B.Field(B.sphere((0, 0, 0), 1), ("constant", 1.0), ("constant", (0, 0, 1)))],
+                          np.zeros((0, 3))).shape == (0, 3)
+    # a one-node grid
+    m = B.region_mask([B.box((0, 0, 0), (0, 0, 0), closed=True)], (0, 0, 0), 1.0, (1, 1, 1))
+    assert m.shape == (1, 1, 1) and m[0, 0, 0] == 1
+    assert B.region_mask([B.box((0, 0, 0), (0, 0, 0))], (0, 0, 0), 1.0, (1, 1, 1))[0, 0, 0] == 0
+    # zero shell width: no shell element and no launch needed
+    v, f = M.cube(4.0)
+    solid, R, bx = voxelize(v, f, 8)
+    assert B.shell_elements(v, f, bx, R, 0.0, solid).sum() == 0
+    # a degenerate (zero-area) face added to the cube changes neither shell nor normals
+    vd = np.concatenate([np.asarray(v, np.float32), np.array([[4, 4, 4]], np.float32)])
+    fd = np.concatenate([np.asarray(f, np.int32), np.array([[len(v), len(v), len(v)]], np.int32)])
+    s1 = B.shell_elements(v, f, bx, R, 1.5, solid)
+    s2 = B.shell_elements(vd, fd, bx, R, 1.5, solid)
+    assert np.array_equal(s1, s2) and np.array_equal(s2, OB.shell_elements(vd, fd, bx, R, 1.5, solid))
+    # points on a face, on an edge and at a vertex: the face normal of the lowest-index face
+    P = np.array([[0.5, 0.25, 4.0], [4.0, 4.0, 0.0], [4.0, 4.0, 4.0], [0.0, 0.0, 9.0], [1.0, 2.0, 3.0]])
+    n = B.mesh_normals(vd, fd, P)
+    assert np.max(np.abs(n - OB.mesh_normals(vd, fd, P))) <= 1e-12
+    assert np.allclose(n[0], (0, 0, 1)) and np.allclose(n[3], (0, 0, 1))  # top face; above the top face
+    assert np.allclose(np.linalg.norm(n, axis=1), 1.0)
+    assert B.mesh_normals(v, f, np.zeros((0, 3))).shape == (0, 3)

@@ -36,7 +36,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "worst-case TO design iterations/s @256^3 (mixed FP32 V-cycle + FP64 CG, rel.resid 1e-6)"
+METRIC = ("worst-case TO design iterations/s @256^3 (mixed: FP32 V-cycle and CG recurrence, FP64 residual "
+          "replacement; true rel.resid 1e-6)")
 UNIT = "iter/s"
 # V-cycle smoother: 2 + 2 Chebyshev steps for D^-1 K on [0.1 lambda_max,
 # lambda_max].  On this workload a 256^3 solve takes about 11-12 PCG

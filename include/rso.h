@@ -78,7 +78,7 @@ typedef struct {
   int smoother;            /* RSO_SMOOTH_GS, _JACOBI or _CHEBYSHEV */
   double omega;            /* damped Jacobi factor relative to the bound 2/lambda_max(D^-1 K) */
   int pre, post;           /* smoothing sweeps */
-  int precision;           /* RSO_FP64 or RSO_MIXED (FP32 V-cycle inside FP64 outer iteration) */
+  int precision;           /* RSO_FP64 or RSO_MIXED (FP32 V-cycle and CG recurrence, FP64 iterate and residual replacement) */
   int mode;                /* RSO_WITH_SUPPORT_* / RSO_NO_SUPPORT_* */
   double cheb_lower;       /* Chebyshev smoother: lower end of the damped interval, as a fraction of lambda_max */
 } rso_config;
@@ -275,7 +275,9 @@ rso_status rso_vcycle(rso_handle* h, double* u_dev, const double* f_dev, int pre
                       int symmetric, double* rel_res);
 /* solve K u = f to tol; u holds the initial guess.  method RSO_SOLVE_VCYCLE
  * repeats V-cycles (solveFEM, optimization/optimization.cpp:178-184),
- * RSO_SOLVE_PCG runs FP64 CG preconditioned by one V-cycle (FP32 in mixed mode). */
+ * RSO_SOLVE_PCG runs CG preconditioned by one V-cycle: FP64 throughout, or in
+ * mixed mode an FP32 V-cycle and (rso_set_krylov_fp32) an FP32 recurrence with
+ * FP64 iterate and residual replacement. */
 rso_status rso_solve(rso_handle* h, const double* f_dev, double* u_dev, double tol, int max_iter,
                      int method, rso_solve_info* info);
 /* k systems K u_i = f_i on the same operator solved together (load cases of

@@ -120,7 +120,9 @@ rso_status rso_shell_elements(const float* vertices_host, int n_vertices, const 
  * 2838-2854): q = closest point of the mesh to p (lowest face index on a
  * tie), t = (v0 - v2) x (v1 - v2) of that face; the normal is t / |t| when
  * |q - p| < 1e-6, else (q - p) / |q - p| oriented so that its dot with t is
- * non-negative.  points, normals: 3 n_points doubles (xyz per point). */
+ * non-negative.  points, normals: 3 n_points doubles (xyz per point).  Meshes
+ * of 256 faces or more are searched through a uniform face grid, with the
+ * same result as scanning every face. */
 rso_status rso_mesh_normals(const float* vertices_host, int n_vertices, const int* faces_host, int n_faces,
                             const double* points_host, int n_points, double* normals_host);
 

@@ -14,8 +14,9 @@
 // in a face's index box within w of that face is within w of the mesh, and an
 // element within w of the mesh lies in the index box of its nearest face, so
 // the union over faces is the reference's set), a thread per point for the
-// normals (all faces scanned, lowest index kept on a tie), a thread per node
-// or point for the regions and fields.  The file is compiled without
+// normals (the nearest face with the lowest index on a tie, found by a ring
+// search over a uniform face grid, or by scanning all faces of small meshes),
+// a thread per node or point for the regions and fields.  The file is compiled without
 // multiply-add contraction so every product and sum rounds as in the host
 // restatement the tests compare with.
 #include "rso_internal.cuh"
@@ -107,6 +108,27 @@ __global__ void k_shell(const float* __restrict__ vtx, const int* __restrict__ f
 
 constexpr int kNormalTile = 128;
 
+// outwardNormal's rule for the closest point q of face bf to p: the supporting
+// plane's vector (a - c) x (b - c) of CGAL's plane through three points when
+// |q - p| < 1e-6, else (q - p) / |q - p| oriented along it
+__device__ void emit_normal(const float* __restrict__ vtx, const int* __restrict__ faces, int bf, D3 bq, D3 p,
+                            double* __restrict__ out) {
+  const D3 ba = vertex(vtx, faces[3 * bf]), bb = vertex(vtx, faces[3 * bf + 1]), bc = vertex(vtx, faces[3 * bf + 2]);
+  const D3 tn = cross(sub(ba, bc), sub(bb, bc));
+  const D3 pq = sub(bq, p);
+  double len = sqrt(dot(pq, pq));
+  D3 n;
+  if (len < 1e-6) {
+    n = unit(tn);
+  } else {
+    if (dot(pq, tn) < 0.0) len = -len;
+    n = {pq.x / len, pq.y / len, pq.z / len};
+  }
+  out[0] = n.x;
+  out[1] = n.y;
+  out[2] = n.z;
+}
+
 // one thread per point; faces staged through shared memory a tile at a time
 __global__ void __launch_bounds__(kNormalTile) k_normals(const float* __restrict__ vtx, const int* __restrict__ faces,
                                                          int nf, const double* __restrict__ pts, int np,
@@ -144,21 +166,122 @@ __global__ void __launch_bounds__(kNormalTile) k_normals(const float* __restrict
       }
   }
   if (i >= np) return;
-  // supporting plane of (a, b, c): (a - c) x (b - c), CGAL's plane through three points
-  const D3 ba = vertex(vtx, faces[3 * bf]), bb = vertex(vtx, faces[3 * bf + 1]), bc = vertex(vtx, faces[3 * bf + 2]);
-  const D3 tn = cross(sub(ba, bc), sub(bb, bc));
-  const D3 pq = sub(bq, p);
-  double len = sqrt(dot(pq, pq));
-  D3 n;
-  if (len < 1e-6) {
-    n = unit(tn);
-  } else {
-    if (dot(pq, tn) < 0.0) len = -len;
-    n = {pq.x / len, pq.y / len, pq.z / len};
+  emit_normal(vtx, faces, bf, bq, p, nrm + 3 * i);
+}
+
+// A uniform grid over the mesh's bounding box: cell (x, y, z) lists the faces
+// whose bounding box overlaps it (start[cell] .. start[cell + 1] in items).
+struct FaceGrid {
+  double lo[3], cs[3];
+  int g[3];
+  double slack;  // absolute slack on distances to cell boundaries (cell-index rounding)
+  const int* start;
+  const int* items;
+};
+
+__device__ __forceinline__ int cell_of(double x, double lo, double cs, int g) {
+  const double q = floor((x - lo) / cs);
+  return !(q >= 0.0) ? 0 : (q >= (double)g ? g - 1 : (int)q);
+}
+
+__device__ __forceinline__ void face_cells(const FaceGrid& G, D3 a, D3 b, D3 c, int* c0, int* c1) {
+  const double lo[3] = {fmin(fmin(a.x, b.x), c.x), fmin(fmin(a.y, b.y), c.y), fmin(fmin(a.z, b.z), c.z)};
+  const double hi[3] = {fmax(fmax(a.x, b.x), c.x), fmax(fmax(a.y, b.y), c.y), fmax(fmax(a.z, b.z), c.z)};
+  for (int j = 0; j < 3; j++) {
+    c0[j] = cell_of(lo[j], G.lo[j], G.cs[j], G.g[j]);
+    c1[j] = cell_of(hi[j], G.lo[j], G.cs[j], G.g[j]);
   }
-  nrm[3 * i] = n.x;
-  nrm[3 * i + 1] = n.y;
-  nrm[3 * i + 2] = n.z;
+}
+
+// FILL false: count the faces of every cell; true: write them (cursor per cell)
+template <bool FILL>
+__global__ void k_bin_faces(const float* __restrict__ vtx, const int* __restrict__ faces, int nf, FaceGrid G,
+                            int* __restrict__ counts, int* __restrict__ items) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  int c0[3], c1[3];
+  face_cells(G, vertex(vtx, faces[3 * f]), vertex(vtx, faces[3 * f + 1]), vertex(vtx, faces[3 * f + 2]), c0, c1);
+  for (int z = c0[2]; z <= c1[2]; z++)
+    for (int y = c0[1]; y <= c1[1]; y++)
+      for (int x = c0[0]; x <= c1[0]; x++) {
+        const long long cell = x + (long long)G.g[0] * (y + (long long)G.g[1] * z);
+        const int slot = atomicAdd(&counts[cell], 1);
+        if (FILL) items[G.start[cell] + slot] = f;
+      }
+}
+
+// one thread per point: cells in rings of growing Chebyshev radius around the
+// point's cell, until no face outside the visited block can come as close as
+// the best so far (the faces that could still tie or win lie within the
+// bound); the best is the lexicographic minimum of (squared distance, face
+// index), the brute-force scan's answer
+__global__ void k_normals_grid(const float* __restrict__ vtx, const int* __restrict__ faces, FaceGrid G,
+                               const double* __restrict__ pts, int np, double* __restrict__ nrm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  const D3 p = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
+  const double pc[3] = {p.x, p.y, p.z};
+  int c[3];
+  for (int j = 0; j < 3; j++) c[j] = cell_of(pc[j], G.lo[j], G.cs[j], G.g[j]);
+  double best = INFINITY;
+  D3 bq = p;
+  int bf = 0x7fffffff;
+  const int rmax = max(G.g[0], max(G.g[1], G.g[2]));
+  auto visit = [&](int x, int y, int z) {
+    const long long cell = x + (long long)G.g[0] * (y + (long long)G.g[1] * z);
+    for (int k = G.start[cell]; k < G.start[cell + 1]; k++) {
+      const int f = G.items[k];
+      const D3 a = vertex(vtx, faces[3 * f]), b = vertex(vtx, faces[3 * f + 1]), cc = vertex(vtx, faces[3 * f + 2]);
+      const D3 q = closest_on_triangle(p, a, b, cc);
+      const D3 d = sub(q, p);
+      const double d2 = dot(d, d);
+      if (d2 < best || (d2 == best && f < bf)) {
+        best = d2;
+        bq = q;
+        bf = f;
+      }
+    }
+  };
+  for (int r = 0; r <= rmax; r++) {
+    const int z0 = max(c[2] - r, 0), z1 = min(c[2] + r, G.g[2] - 1);
+    const int y0 = max(c[1] - r, 0), y1 = min(c[1] + r, G.g[1] - 1);
+    const int x0 = max(c[0] - r, 0), x1 = min(c[0] + r, G.g[0] - 1);
+    for (int z = z0; z <= z1; z++) {
+      const bool zs = z == c[2] - r || z == c[2] + r;
+      for (int y = y0; y <= y1; y++) {
+        const bool ys = zs || y == c[1] - r || y == c[1] + r;
+        if (ys) {
+          for (int x = x0; x <= x1; x++) visit(x, y, z);
+        } else {
+          if (c[0] - r >= 0) visit(c[0] - r, y, z);
+          if (r > 0 && c[0] + r < G.g[0]) visit(c[0] + r, y, z);
+        }
+      }
+    }
+    // lower bound on the distance from p to cells outside the block: the
+    // nearest of the slabs of the grid beyond each block face
+    const int b0[3] = {x0, y0, z0}, b1[3] = {x1, y1, z1};
+    double bound = INFINITY;
+    for (int a = 0; a < 3; a++)
+      for (int side = 0; side < 2; side++) {
+        if (side == 0 ? b0[a] == 0 : b1[a] == G.g[a] - 1) continue;
+        double d2 = 0;
+        for (int j = 0; j < 3; j++) {
+          double lo = G.lo[j], hi = G.lo[j] + G.g[j] * G.cs[j];
+          if (j == a) {
+            if (side == 0) hi = G.lo[j] + b0[j] * G.cs[j];
+            else lo = G.lo[j] + (b1[j] + 1) * G.cs[j];
+          }
+          const double e = pc[j] < lo ? lo - pc[j] : (pc[j] > hi ? pc[j] - hi : 0.0);
+          d2 += e * e;
+        }
+        bound = fmin(bound, sqrt(d2));
+      }
+    if (bound == INFINITY) break;  // the block covers the grid
+    const double bd = bound - G.slack;
+    if (bd > 0.0 && best < bd * bd * (1.0 - 1e-12)) break;
+  }
+  emit_normal(vtx, faces, bf == 0x7fffffff ? 0 : bf, bq, p, nrm + 3 * i);
 }
 
 __device__ bool region_contains(const rso_region& r, D3 p) {
@@ -340,7 +463,76 @@ extern "C" rso_status rso_mesh_normals(const float* vertices_host, int n_vertice
   const int* df = s.upload(faces_host, 3 * (size_t)n_faces);
   const double* dp = s.upload(points_host, 3 * (size_t)n_points);
   double* dn = s.alloc<double>(3 * (size_t)n_points);
-  if (s.err == cudaSuccess) {
+  // meshes of a few hundred faces or more: bin the faces on a uniform grid
+  // of about two faces per cell and search rings of cells around each point
+  bool grid = false;
+  FaceGrid G{};
+  if (s.err == cudaSuccess && n_faces >= 256) {
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (long long k = 0; k < 3LL * n_faces; k++) {
+      const int v = faces_host[k];
+      for (int a = 0; a < 3; a++) {
+        lo[a] = std::fmin(lo[a], (double)vertices_host[3 * v + a]);
+        hi[a] = std::fmax(hi[a], (double)vertices_host[3 * v + a]);
+      }
+    }
+    double ext[3], emax = 0, mag = 0;
+    for (int a = 0; a < 3; a++) {
+      ext[a] = hi[a] - lo[a];
+      emax = std::fmax(emax, ext[a]);
+      mag = std::fmax(mag, std::fmax(std::fabs(lo[a]), std::fabs(hi[a])));
+    }
+    if (emax > 0 && std::isfinite(emax) && std::isfinite(mag)) {
+      const double target = std::min(std::max(n_faces / 2.0, 1.0), (double)(1 << 21));
+      double vol = 1;
+      for (int a = 0; a < 3; a++) vol *= std::fmax(ext[a], 1e-3 * emax);
+      const double cs = std::cbrt(vol / target);
+      long long ncell = 1;
+      double csmin = INFINITY;
+      for (int a = 0; a < 3; a++) {
+        G.g[a] = (int)std::min(std::max(std::ceil(ext[a] / cs), 1.0), 1024.0);
+        G.cs[a] = ext[a] > 0 ? ext[a] / G.g[a] : cs;
+        G.lo[a] = lo[a];
+        ncell *= G.g[a];
+        csmin = std::fmin(csmin, G.cs[a]);
+      }
+      G.slack = 1e-9 * csmin + 1e-14 * mag;
+      int* counts = s.alloc<int>((size_t)ncell);
+      if (s.err == cudaSuccess) s.err = cudaMemset(counts, 0, sizeof(int) * ncell);
+      if (s.err == cudaSuccess) {
+        k_bin_faces<false><<<cdiv(n_faces, 256), 256>>>(dv, df, n_faces, G, counts, nullptr);
+        note_launch();
+        s.err = cudaGetLastError();
+      }
+      std::vector<int> hc((size_t)ncell);
+      if (s.err == cudaSuccess) s.err = cudaMemcpy(hc.data(), counts, sizeof(int) * ncell, cudaMemcpyDeviceToHost);
+      std::vector<int> hs((size_t)ncell + 1, 0);
+      long long total = 0;
+      for (long long cidx = 0; cidx < ncell; cidx++) {
+        hs[cidx] = (int)std::min(total, (long long)INT32_MAX);
+        total += hc[cidx];
+      }
+      hs[ncell] = (int)std::min(total, (long long)INT32_MAX);
+      if (s.err == cudaSuccess && total <= (1LL << 25)) {
+        int* start = s.upload(hs.data(), hs.size());
+        int* items = s.alloc<int>((size_t)std::max(total, 1LL));
+        if (s.err == cudaSuccess) s.err = cudaMemset(counts, 0, sizeof(int) * ncell);
+        if (s.err == cudaSuccess) {
+          G.start = start;
+          G.items = items;
+          k_bin_faces<true><<<cdiv(n_faces, 256), 256>>>(dv, df, n_faces, G, counts, items);
+          note_launch();
+          s.err = cudaGetLastError();
+          grid = s.err == cudaSuccess;
+        }
+      }
+    }
+  }
+  if (s.err == cudaSuccess && grid) {
+    k_normals_grid<<<cdiv(n_points, 128), 128>>>(dv, df, G, dp, n_points, dn);
+    note_launch();
+    s.err = cudaGetLastError();
+  } else if (s.err == cudaSuccess) {
     k_normals<<<cdiv(n_points, kNormalTile), kNormalTile>>>(dv, df, n_faces, dp, n_points, dn);
     note_launch();
     s.err = cudaGetLastError();

@@ -21,6 +21,8 @@
 // restatement the tests compare with.
 #include "rso_internal.cuh"
 #include <cmath>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 namespace rso {
@@ -387,23 +389,79 @@ __global__ void k_region_field(const rso_field* __restrict__ fields, int nfld, c
 }
 
 // device copies of a host array; frees everything it allocated on destruction
+// Device blocks of these entry points, cached per device in power-of-two
+// size classes between calls: repeated calls reuse them instead of
+// allocating and freeing (a free lets the driver unmap the memory and the
+// next allocation map it again, which made the call times vary by tens of
+// milliseconds).  At most kCacheCap bytes per device stay cached.
+constexpr int kCacheDevices = 64;
+constexpr size_t kCacheCap = size_t(1) << 30;
+struct BlockCache {
+  std::mutex m;
+  std::vector<std::pair<size_t, void*>> blocks[kCacheDevices];
+  size_t held[kCacheDevices] = {};
+};
+BlockCache g_blocks;
+
+cudaError_t block_get(int dev, size_t bytes, void** p, size_t* cls) {
+  size_t c = 256;
+  while (c < bytes) c <<= 1;
+  *cls = c;
+  if (dev >= 0 && dev < kCacheDevices) {
+    std::lock_guard<std::mutex> lk(g_blocks.m);
+    auto& v = g_blocks.blocks[dev];
+    for (size_t i = 0; i < v.size(); i++)
+      if (v[i].first == c) {
+        *p = v[i].second;
+        g_blocks.held[dev] -= c;
+        v.erase(v.begin() + i);
+        return cudaSuccess;
+      }
+  }
+  return cudaMalloc(p, c);
+}
+
+void block_put(int dev, size_t cls, void* p) {
+  if (dev >= 0 && dev < kCacheDevices) {
+    std::lock_guard<std::mutex> lk(g_blocks.m);
+    if (g_blocks.held[dev] + cls <= kCacheCap) {
+      g_blocks.blocks[dev].push_back({cls, p});
+      g_blocks.held[dev] += cls;
+      return;
+    }
+  }
+  cudaFree(p);
+}
+
+// device copies of host arrays and work buffers for one call; the blocks go
+// back to the cache when the call returns (every kernel of the call has
+// finished by then: each entry point ends with a synchronous copy)
 struct Scratch {
-  std::vector<void*> ptrs;
+  struct Block {
+    void* p;
+    size_t cls;
+  };
+  std::vector<Block> blocks;
+  int dev = -1;
   cudaError_t err = cudaSuccess;
+  Scratch() { err = cudaGetDevice(&dev); }
   template <typename T>
   T* upload(const T* host, size_t n) {
     if (err != cudaSuccess) return nullptr;
     void* p = nullptr;
-    err = cudaMalloc(&p, sizeof(T) * (n ? n : 1));
+    size_t cls = 0;
+    err = block_get(dev, sizeof(T) * (n ? n : 1), &p, &cls);
     if (err != cudaSuccess) return nullptr;
-    ptrs.push_back(p);
+    blocks.push_back({p, cls});
     if (host && n) err = cudaMemcpy(p, host, sizeof(T) * n, cudaMemcpyHostToDevice);
     return static_cast<T*>(p);
   }
   template <typename T>
   T* alloc(size_t n) { return upload<T>(nullptr, n); }
   ~Scratch() {
-    for (void* p : ptrs) cudaFree(p);
+    // a failed call may have left work in flight on the device
+    if (err != cudaSuccess) cudaDeviceSynchronize();
+    for (const Block& b : blocks) block_put(dev, b.cls, b.p);
   }
 };
 

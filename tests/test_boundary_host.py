@@ -157,3 +157,51 @@ def test_oracle_normals_on_a_sphere():
         n = OB.mesh_normals(v, f, d * s)
         assert np.allclose(np.linalg.norm(n, axis=1), 1.0)
         assert np.min(np.sum(n * d, axis=1)) > 0.95
+
+
+def test_surface_nodes_against_direct_rule():
+    """surface_nodes: a node touching a solid element is a surface node unless
+    every axis has a solid element pair across it (the library's node class)."""
+    from robustoptspline3d_b200.boundary import surface_nodes
+    rng = np.random.default_rng(8)
+    em = (rng.uniform(size=(5, 6, 7)) < 0.6).astype(np.uint8)
+    got = surface_nodes(em)
+    ez, ey, ex = em.shape
+    want = np.zeros((ez + 1, ey + 1, ex + 1), bool)
+    pad = np.pad(em.astype(bool), 1)
+    for z in range(ez + 1):
+        for y in range(ey + 1):
+            for x in range(ex + 1):
+                s = {(dx, dy, dz): pad[z + dz, y + dy, x + dx] for dx in (0, 1) for dy in (0, 1) for dz in (0, 1)}
+                if not any(s.values()):
+                    continue
+                ax0 = any(s[0, a, b] and s[1, a, b] for a in (0, 1) for b in (0, 1))
+                ax1 = any(s[a, 0, b] and s[a, 1, b] for a in (0, 1) for b in (0, 1))
+                ax2 = any(s[a, b, 0] and s[a, b, 1] for a in (0, 1) for b in (0, 1))
+                want[z, y, x] = not (ax0 and ax1 and ax2)
+    assert np.array_equal(got, want)
+
+
+def test_node_grid_uses_fp32_quotient():
+    from robustoptspline3d_b200.boundary import node_grid
+    box = np.array([-1.1, -2.2, 0.3, 2.9, 1.8, 4.3], np.float32)
+    origin, h = node_grid(box, 7)
+    assert h == float(np.float32(np.float32(box[3] - box[0]) / np.float32(7)))
+    assert np.array_equal(origin, box[:3].astype(np.float64))
+
+
+def test_bench_torus_mesh_is_closed_and_outward():
+    import bench
+    v, f = bench.torus_mesh(nu=24, nv=12)
+    assert v.shape == (24 * 12, 3) and f.shape == (2 * 24 * 12, 3)
+    # every directed edge appears once and its reverse once: closed and consistently wound
+    edges = {}
+    for a, b, c in f:
+        for e in ((a, b), (b, c), (c, a)):
+            edges[e] = edges.get(e, 0) + 1
+    assert all(n == 1 for n in edges.values()) and all((b, a) in edges for a, b in edges)
+    # outward: the signed volume (divergence theorem) is positive
+    A, B, C = v[f[:, 0]].astype(np.float64), v[f[:, 1]].astype(np.float64), v[f[:, 2]].astype(np.float64)
+    vol = np.einsum("ij,ij->i", A, np.cross(B, C)).sum() / 6
+    # an inscribed polygonal torus of 24 x 12 segments holds about 94 % of the smooth volume
+    assert vol > 0 and 0.9 < vol / (2 * np.pi ** 2 * 2.0 * 0.7 ** 2) < 1.0

@@ -7,6 +7,11 @@ The compute lives in ``librso.so`` (hand-written CUDA for sm_100a behind the
 C ABI of ``include/rso.h``).  This package is the host-side mirror of the
 reference's Grid/optimization interface over that C ABI.  Importing it
 without the compiled library raises immediately: there is no CPU fallback.
+
+Submodules beside the solver: ``voxelize`` (OBJ reading, solid
+voxelisation), ``boundary`` (regions, load fields, shell elements, normals,
+``mesh_problem``), ``records`` (run records in the reference's raw layout)
+and ``autograd`` (a torch.autograd.Function over the design gradient).
 """
 from .rso import (  # noqa: F401
     Config,

@@ -324,8 +324,8 @@ rso_status rso_set_vcycle_graphs(rso_handle* h, int on);
  * replaces the recursive one whenever that has dropped by replace_factor
  * since the last replacement and before the solve stops, so the tolerance is
  * always met by a true FP64 residual.  replace_factor 0: p, q = K p and r are
- * FP64 and only the V-cycle is FP32.  Batched solves keep the FP64
- * recurrence. */
+ * FP64 and only the V-cycle is FP32.  rso_solve_batch follows the same
+ * setting, each system replacing its residual on its own rule. */
 rso_status rso_set_krylov_fp32(rso_handle* h, double replace_factor);
 /* Grid::compliance (grid/Grid.cpp:4118-4121): c = f . u */
 rso_status rso_dot(rso_handle* h, const double* a_dev, const double* b_dev, double* out);

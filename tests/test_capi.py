@@ -53,3 +53,17 @@ def test_host_entry_points_without_gpu():
 def test_oracle_header_mentions_pinning():
     txt = open(os.path.join(ROOT, "oracle", "oracle.h")).read()
     assert "TEST INFRASTRUCTURE ONLY" in txt and "parity unpinned" in txt
+
+
+def test_binding_arity_matches_header():
+    """Every prototype in include/rso.h has as many parameters as its ctypes signature."""
+    from robustoptspline3d_b200.rso import SIGNATURES
+    src = open(os.path.join(ROOT, "include", "rso.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    protos = re.findall(r"\b(rso_[a-z0-9_]+)\s*\(([^;{)]*)\)\s*;", src)
+    assert len(protos) > 40
+    for name, params in protos:
+        params = " ".join(params.split())
+        n = 0 if params in ("", "void") else params.count(",") + 1
+        assert name in SIGNATURES, name
+        assert len(SIGNATURES[name][1]) == n, (name, n, len(SIGNATURES[name][1]))

@@ -323,7 +323,10 @@ rso_status rso_set_vcycle_graphs(rso_handle* h, int on);
  * vectors, FP64 sums and FP64 iterate) and the true FP64 residual f - K x
  * replaces the recursive one whenever that has dropped by replace_factor
  * since the last replacement and before the solve stops, so the tolerance is
- * always met by a true FP64 residual.  replace_factor 0: p, q = K p and r are
+ * always met by a true FP64 residual; a cycle between replacements lasts at
+ * most 30 iterations, and one that does not bring the true residual below
+ * max(0.5, sqrt(replace_factor)) of the previous one hands the solve over to
+ * the FP64 recurrence from the current iterate.  replace_factor 0: p, q = K p and r are
  * FP64 and only the V-cycle is FP32.  rso_solve_batch follows the same
  * setting, each system replacing its residual on its own rule. */
 rso_status rso_set_krylov_fp32(rso_handle* h, double replace_factor);

@@ -10,6 +10,7 @@
 // recurrence is FP32 with FP64 residual replacement, as for single solves,
 // each system replacing on its own rule.
 #include "rso_internal.cuh"
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <utility>
@@ -321,7 +322,15 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
       RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.z, h->L[0].u64, sizeof(double) * tot, cudaMemcpyDeviceToDevice, h->stream));
       return RSO_OK;
     };
+    // an FP32 recurrence that stalls hands over to the FP64 one (as for single
+    // solves: a cycle ends after at most kCycleMax iterations, and a true
+    // residual not below max(0.5, sqrt(factor)) of the previous one stalls)
+    bool stalled = false;
+    int used = 0;
     if (left > 0 && k32) {
+      constexpr int kCycleMax = 30;
+      const double stall = std::max(0.5, std::sqrt(h->krylov32));
+      std::vector<int> since(k, 0);
       float* p32 = reinterpret_cast<float*>(B.p);
       float* q32 = reinterpret_cast<float*>(B.q);
       float* r32 = l0.f32;  // the batched V-cycle's right-hand sides (the smoothers rotate u, not f)
@@ -351,10 +360,12 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
         for (int b = 0; b < k; b++) {
           if (done[b]) continue;
           it[b] = iter;
+          since[b]++;
           const double rn = std::sqrt(B.h_scal[b * KS + 5]);
           if (!std::isfinite(rn)) { h->err = "non-finite residual in batched PCG"; return RSO_ERR_NONFINITE; }
           rel[b] = rn / fn[b];
-          if (rn < tol * fn[b] || rn < h->krylov32 * rbase[b] || iter >= max_iter) ask |= 1ULL << b;
+          if (rn < tol * fn[b] || rn < h->krylov32 * rbase[b] || iter >= max_iter || since[b] >= kCycleMax)
+            ask |= 1ULL << b;
         }
         const bool replace = ask != 0;
         if (replace) {
@@ -373,13 +384,22 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
           for (int b = 0; b < k; b++) {
             if (done[b]) continue;
             if (!((ask >> b) & 1ULL)) { left++; continue; }
-            rbase[b] = std::sqrt(B.h_scal[b * KS + 5]);
-            rel[b] = rbase[b] / fn[b];
+            const double rtrue = std::sqrt(B.h_scal[b * KS + 5]);
+            rel[b] = rtrue / fn[b];
             if (!std::isfinite(rel[b])) { h->err = "non-finite residual in batched PCG"; return RSO_ERR_NONFINITE; }
-            if (rel[b] < tol) done[b] = 1;
-            else { left++; take |= 1ULL << b; }
+            if (rel[b] < tol) { done[b] = 1; continue; }
+            if (rtrue > stall * rbase[b]) stalled = true;
+            rbase[b] = rtrue;
+            since[b] = 0;
+            left++;
+            take |= 1ULL << b;
           }
-          if (left == 0 || iter >= max_iter) break;
+          if (left == 0 || iter >= max_iter) { stalled = false; break; }
+          if (stalled) {  // B.r holds every system's true residual of B.x
+            used = iter;
+            RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.done, done.data(), sizeof(int) * k, cudaMemcpyHostToDevice, h->stream));
+            break;
+          }
           if (take) { k_bd2f_sel<<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, B.r, r32, take); rso::note_launch(); }
           RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.done, done.data(), sizeof(int) * k, cudaMemcpyHostToDevice, h->stream));
         }
@@ -394,7 +414,8 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
         rso::note_launch();
         RSO_TRY(launch_check(h, "batched pcg32"));
       }
-    } else if (left > 0) {
+    }
+    if (left > 0 && (!k32 || stalled)) {
       RSO_TRY(precondition_z());
       if (mixed) {
         k_bf2d<<<cdiv(tot, 256), 256, 0, h->stream>>>(tot, h->L[0].u32, B.p); rso::note_launch();
@@ -417,13 +438,13 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
         left = 0;
         for (int b = 0; b < k; b++) {
           if (done[b]) continue;
-          it[b] = iter;
+          it[b] = used + iter;
           rel[b] = std::sqrt(B.h_scal[b * KS + 5]) / fn[b];
           if (!std::isfinite(rel[b])) { h->err = "non-finite residual in batched PCG"; return RSO_ERR_NONFINITE; }
           if (rel[b] < tol) done[b] = 2;  // converged in this iteration: x still takes this step
           else left++;
         }
-        if (left == 0 || iter >= max_iter) {
+        if (left == 0 || used + iter >= max_iter) {
           k_bstep<<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, s, B.p, B.x); rso::note_launch();
           break;
         }

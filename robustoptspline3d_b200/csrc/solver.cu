@@ -431,8 +431,15 @@ __global__ void k_cg32_step(long long n4, const double* __restrict__ alpha, cons
 // true residual f - K x is formed in FP64 and replaces it (residual
 // replacement, the search direction kept).  The reported residual is always a
 // true FP64 one.
+// A cycle (iterations between replacements) ends after at most kCycleMax
+// iterations; a replacement whose true residual is not below
+// max(0.5, sqrt(factor)) times the previous one means the FP32 recurrence
+// stalls (an operator too ill-conditioned for it): the solve then continues
+// from the current iterate with the FP64 recurrence (*stalled, *used = the
+// iterations spent here).
+constexpr int kCycleMax = 30;
 static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, double tol, int max_iter,
-                                rso_solve_info* info) {
+                                rso_solve_info* info, bool* stalled, int* used) {
   Level& l0 = h->L[0];
   const long long n3 = 3 * l0.NP, n4 = n3 / 4;
   double* s = h->scal;  // s[0]=rz, s[1]=pq, s[2]=alpha, s[3]=rz_new, s[4]=beta, s[5]=rr
@@ -459,8 +466,11 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
     RSO_CHECK_CUDA(h, cudaMemsetAsync(x, 0, sizeof(double) * n3, h->stream));
     rel = 0;
   }
+  *stalled = false;
+  const double stall = std::max(0.5, std::sqrt(h->krylov32));
   if (rel >= tol && fn > 0) {
     double rbase = std::sqrt(rn2);  // residual norm at the last replacement
+    int since = 0;                  // iterations since then
     // the operator writes interior nodes only: the padding of q (an FP64
     // buffer seen as FP32, so old doubles split across its entries) must be zero
     RSO_CHECK_CUDA(h, cudaMemsetAsync(q32, 0, sizeof(float) * n3, h->stream));
@@ -476,18 +486,26 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
       RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
       vcycle_graphs_harvest(h);
       it++;
+      since++;
       const double rnorm = std::sqrt(h->h_scal[5]);
       if (!std::isfinite(rnorm)) { h->err = "non-finite residual in PCG"; return RSO_ERR_NONFINITE; }
-      const bool replace = rnorm < h->krylov32 * rbase || rnorm < tol * fn || it >= max_iter;
+      const bool replace =
+          rnorm < h->krylov32 * rbase || rnorm < tol * fn || it >= max_iter || since >= kCycleMax;
       if (replace) {
         k_cg32_step<<<cdiv(n4, 256), 256, 0, h->stream>>>(n4, s + 2, reinterpret_cast<const float4*>(p32),
                                                           reinterpret_cast<double2*>(x));
         rso::note_launch();
         RSO_TRY(true_residual(&rn2));
-        rbase = std::sqrt(rn2);
-        rel = rbase / fn;
+        const double rtrue = std::sqrt(rn2);
+        rel = rtrue / fn;
         if (!std::isfinite(rel)) { h->err = "non-finite residual in PCG"; return RSO_ERR_NONFINITE; }
         if (rel < tol || it >= max_iter) break;
+        if (rtrue > stall * rbase) {  // h->r holds the true residual of x
+          *stalled = true;
+          break;
+        }
+        rbase = rtrue;
+        since = 0;
         k_d2f<<<cdiv(n3, 256), 256, 0, h->stream>>>(h->r, r32, n3); rso::note_launch();
       } else {
         rel = rnorm / fn;
@@ -508,6 +526,8 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
       RSO_TRY(launch_check(h, "pcg32"));
     }
   }
+  *used = it;
+  if (*stalled) return RSO_OK;
   RSO_TRY(fine_stage_check(h));
   if (info) { info->iterations = it; info->rel_res = rel; }
   if (rel >= tol && fn > 0) { h->err = "PCG did not reach the tolerance within max_iter"; return RSO_ERR_BUDGET_EXCEEDED; }
@@ -522,7 +542,13 @@ rso_status solve_pcg(rso_handle* h, const double* f, double* x, double tol, int 
   Level& l0 = h->L[0];
   const long long n3 = 3 * l0.NP;
   const bool mixed = h->cfg.precision == RSO_MIXED;
-  if (mixed && h->krylov32 > 0 && l0.nb == 1) return solve_pcg_k32(h, f, x, tol, max_iter, info);
+  int used = 0;  // iterations of an FP32 recurrence that stalled
+  if (mixed && h->krylov32 > 0 && l0.nb == 1) {
+    bool stalled = false;
+    const rso_status st = solve_pcg_k32(h, f, x, tol, max_iter, info, &stalled, &used);
+    if (st != RSO_OK || !stalled) return st;
+    max_iter -= used;  // the FP64 recurrence from the current iterate for the rest
+  }
   double* s = h->scal;
   RSO_TRY(fine_residual<double>(h, x, f, h->r, h->rp64));
   double fn2 = 0, rn2 = 0;
@@ -576,7 +602,7 @@ rso_status solve_pcg(rso_handle* h, const double* f, double* x, double tol, int 
     }
   }
   RSO_TRY(fine_stage_check(h));
-  if (info) { info->iterations = it; info->rel_res = rel; }
+  if (info) { info->iterations = it + used; info->rel_res = rel; }
   if (rel >= tol && fn > 0) { h->err = "PCG did not reach the tolerance within max_iter"; return RSO_ERR_BUDGET_EXCEEDED; }
   return RSO_OK;
 }

@@ -325,11 +325,21 @@ rso_status rso_set_vcycle_graphs(rso_handle* h, int on);
  * since the last replacement and before the solve stops, so the tolerance is
  * always met by a true FP64 residual; a cycle between replacements lasts at
  * most 30 iterations, and one that does not bring the true residual below
- * max(0.5, sqrt(replace_factor)) of the previous one hands the solve over to
- * the FP64 recurrence from the current iterate.  replace_factor 0: p, q = K p and r are
- * FP64 and only the V-cycle is FP32.  rso_solve_batch follows the same
- * setting, each system replacing its residual on its own rule. */
+ * max(0.5, sqrt(replace_factor), sqrt(claimed)) of the previous one (claimed:
+ * the reduction the recursive residual showed over that cycle) hands the solve
+ * over to the FP64 recurrence from the current iterate, iterations counted on.
+ * replace_factor 0: p, q = K p and r are FP64 and only the V-cycle is FP32.
+ * rso_solve_batch follows the same setting, each system replacing its
+ * residual on its own rule; a hand-over there moves the whole batch to the
+ * FP64 recurrence, so systems still converging in FP32 leave the sequence of
+ * their own single solves from that point (same tolerance, true residuals). */
 rso_status rso_set_krylov_fp32(rso_handle* h, double replace_factor);
+/* Upper bound on the replacement cycles of the FP32 recurrence (no
+ * counterpart in the reference): after max_cycles replacements that did not
+ * end the solve, it continues with the FP64 recurrence from the current
+ * iterate, as after a stall (0, the default: no bound).  Caps the FP32 work a
+ * solve may spend before the FP64 recurrence takes over. */
+rso_status rso_set_krylov_fp32_cycles(rso_handle* h, int max_cycles);
 /* Grid::compliance (grid/Grid.cpp:4118-4121): c = f . u */
 rso_status rso_dot(rso_handle* h, const double* a_dev, const double* b_dev, double* out);
 

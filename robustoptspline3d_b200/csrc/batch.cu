@@ -329,8 +329,8 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
     int used = 0;
     if (left > 0 && k32) {
       constexpr int kCycleMax = 30;
-      const double stall = std::max(0.5, std::sqrt(h->krylov32));
-      std::vector<int> since(k, 0);
+      std::vector<int> since(k, 0), cycles(k, 0);
+      std::vector<double> rrec(k, 0.0);  // recursive residual norms at the last iteration
       float* p32 = reinterpret_cast<float*>(B.p);
       float* q32 = reinterpret_cast<float*>(B.q);
       float* r32 = l0.f32;  // the batched V-cycle's right-hand sides (the smoothers rotate u, not f)
@@ -364,6 +364,7 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
           const double rn = std::sqrt(B.h_scal[b * KS + 5]);
           if (!std::isfinite(rn)) { h->err = "non-finite residual in batched PCG"; return RSO_ERR_NONFINITE; }
           rel[b] = rn / fn[b];
+          rrec[b] = rn;
           if (rn < tol * fn[b] || rn < h->krylov32 * rbase[b] || iter >= max_iter || since[b] >= kCycleMax)
             ask |= 1ULL << b;
         }
@@ -388,7 +389,10 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
             rel[b] = rtrue / fn[b];
             if (!std::isfinite(rel[b])) { h->err = "non-finite residual in batched PCG"; return RSO_ERR_NONFINITE; }
             if (rel[b] < tol) { done[b] = 1; continue; }
-            if (rtrue > stall * rbase[b]) stalled = true;
+            cycles[b]++;
+            if (rtrue > stall_ratio(h->krylov32, rrec[b] / rbase[b]) * rbase[b] ||
+                (h->krylov32_cycles > 0 && cycles[b] >= h->krylov32_cycles))
+              stalled = true;
             rbase[b] = rtrue;
             since[b] = 0;
             left++;
@@ -416,6 +420,9 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
       }
     }
     if (left > 0 && (!k32 || stalled)) {
+      // q held the FP32 recurrence's q (or nothing yet), and the operator
+      // writes interior nodes only while the residual update reads every entry
+      if (stalled) RSO_CHECK_CUDA(h, cudaMemsetAsync(B.q, 0, sizeof(double) * tot, h->stream));
       RSO_TRY(precondition_z());
       if (mixed) {
         k_bf2d<<<cdiv(tot, 256), 256, 0, h->stream>>>(tot, h->L[0].u32, B.p); rso::note_launch();

@@ -463,6 +463,12 @@ extern "C" rso_status rso_set_krylov_fp32(rso_handle* h, double replace_factor) 
   return RSO_OK;
 }
 
+extern "C" rso_status rso_set_krylov_fp32_cycles(rso_handle* h, int max_cycles) {
+  if (!h || max_cycles < 0) return RSO_ERR_INVALID_ARG;
+  h->krylov32_cycles = max_cycles;
+  return RSO_OK;
+}
+
 extern "C" rso_status rso_fine_sweep_fp32(rso_handle* h, int op, const double* u, const double* f,
                                           const double* uprev, double omega, double c1, double* out) {
   if (!h || !u || !out || op < 0 || op > 3 || (op != 1 && !f)) return RSO_ERR_INVALID_ARG;

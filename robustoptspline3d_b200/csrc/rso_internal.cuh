@@ -156,6 +156,9 @@ struct rso_handle {
   // this factor since the last replacement (0: FP64 recurrence); rso_create
   // sets 1e-2 for mixed precision
   double krylov32 = 0.0;
+  // replacement cycles the FP32 recurrence may run before the solve goes on
+  // with the FP64 recurrence (0: no limit; rso_set_krylov_fp32_cycles)
+  int krylov32_cycles = 0;
   // worst-case scratch kept between calls (worst.cu): Lanczos load-space
   // vectors, reorthogonalisation sums, the force-projection vector
   double* wc_buf = nullptr;
@@ -289,6 +292,9 @@ void batch_release(rso_handle* h);
 rso_status solve_pcg_batch(rso_handle* h, int k, const double* F_dense, double* U_dense, double tol, int max_iter,
                            rso_solve_info* infos);
 rso_status solve_pcg(rso_handle* h, const double* f, double* u, double tol, int max_iter, rso_solve_info* info);
+// the FP32 recurrence stalls when a replacement's true residual is not below
+// this fraction of the previous one (claimed: the recursive residual's reduction)
+double stall_ratio(double factor, double claimed);
 rso_status solve_vcycles(rso_handle* h, const double* f, double* u, double tol, int max_iter,
                          rso_solve_info* info);
 rso_status vcycle_fp64(rso_handle* h, double* u, const double* f, int pre, int post, int symmetric,

@@ -432,12 +432,18 @@ __global__ void k_cg32_step(long long n4, const double* __restrict__ alpha, cons
 // replacement, the search direction kept).  The reported residual is always a
 // true FP64 one.
 // A cycle (iterations between replacements) ends after at most kCycleMax
-// iterations; a replacement whose true residual is not below
-// max(0.5, sqrt(factor)) times the previous one means the FP32 recurrence
-// stalls (an operator too ill-conditioned for it): the solve then continues
-// from the current iterate with the FP64 recurrence (*stalled, *used = the
-// iterations spent here).
+// iterations.  A replacement whose true residual is not below
+// max(0.5, sqrt(factor), sqrt(claimed)) times the previous one, claimed being
+// the reduction the recursive residual showed over the cycle, means the FP32
+// recurrence stalls (an operator too ill-conditioned for it): the solve then
+// continues from the current iterate with the FP64 recurrence (*stalled,
+// *used = the iterations spent here).  The claimed term keeps a short last
+// cycle, ended by the tolerance after a small reduction, from counting as a
+// stall.  h->krylov32_cycles > 0 hands over after that many cycles as well.
 constexpr int kCycleMax = 30;
+double stall_ratio(double factor, double claimed) {
+  return std::max(std::max(0.5, std::sqrt(factor)), std::sqrt(std::max(claimed, 0.0)));
+}
 static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, double tol, int max_iter,
                                 rso_solve_info* info, bool* stalled, int* used) {
   Level& l0 = h->L[0];
@@ -467,10 +473,10 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
     rel = 0;
   }
   *stalled = false;
-  const double stall = std::max(0.5, std::sqrt(h->krylov32));
   if (rel >= tol && fn > 0) {
     double rbase = std::sqrt(rn2);  // residual norm at the last replacement
     int since = 0;                  // iterations since then
+    int cycles = 0;                 // replacements so far
     // the operator writes interior nodes only: the padding of q (an FP64
     // buffer seen as FP32, so old doubles split across its entries) must be zero
     RSO_CHECK_CUDA(h, cudaMemsetAsync(q32, 0, sizeof(float) * n3, h->stream));
@@ -500,7 +506,9 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
         rel = rtrue / fn;
         if (!std::isfinite(rel)) { h->err = "non-finite residual in PCG"; return RSO_ERR_NONFINITE; }
         if (rel < tol || it >= max_iter) break;
-        if (rtrue > stall * rbase) {  // h->r holds the true residual of x
+        cycles++;
+        if (rtrue > stall_ratio(h->krylov32, rnorm / rbase) * rbase ||
+            (h->krylov32_cycles > 0 && cycles >= h->krylov32_cycles)) {  // h->r holds the true residual of x
           *stalled = true;
           break;
         }
@@ -549,6 +557,9 @@ rso_status solve_pcg(rso_handle* h, const double* f, double* x, double tol, int 
     if (st != RSO_OK || !stalled) return st;
     max_iter -= used;  // the FP64 recurrence from the current iterate for the rest
   }
+  // q may hold FP32 words of an earlier FP32 recurrence, and the operator
+  // writes interior nodes only while the residual update reads every entry
+  if (mixed) RSO_CHECK_CUDA(h, cudaMemsetAsync(h->q, 0, sizeof(double) * n3, h->stream));
   double* s = h->scal;
   RSO_TRY(fine_residual<double>(h, x, f, h->r, h->rp64));
   double fn2 = 0, rn2 = 0;

@@ -105,6 +105,7 @@ SIGNATURES = {
     "rso_fine_sweep_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
     "rso_set_vcycle_graphs": (_ci, [_vp, _ci]),
     "rso_set_krylov_fp32": (_ci, [_vp, _cd]),
+    "rso_set_krylov_fp32_cycles": (_ci, [_vp, _ci]),
     "rso_voxelize": (_ci, [ctypes.POINTER(ctypes.c_float), _ci, ctypes.POINTER(ctypes.c_int), _ci, _ci, _pu8, _pi,
                            ctypes.POINTER(ctypes.c_float)]),
     "rso_shell_elements": (_ci, [ctypes.POINTER(ctypes.c_float), _ci, ctypes.POINTER(ctypes.c_int), _ci,
@@ -458,6 +459,11 @@ class HierarchyGrid:
         """Mixed precision: run the PCG recurrence in FP32 with true-residual replacement
         whenever the residual has dropped by replace_factor (0 restores the FP64 recurrence)."""
         self._chk(self.lib.rso_set_krylov_fp32(self.h, float(replace_factor)), "rso_set_krylov_fp32")
+
+    def set_krylov_fp32_cycles(self, max_cycles=0):
+        """Mixed precision: hand the solve over to the FP64 recurrence after max_cycles
+        residual replacements of the FP32 recurrence (0: only when it stalls)."""
+        self._chk(self.lib.rso_set_krylov_fp32_cycles(self.h, int(max_cycles)), "rso_set_krylov_fp32_cycles")
 
     def set_vcycle_graphs(self, on):
         """Replay captured FP32 V-cycles from CUDA graphs (default) or launch every kernel."""

@@ -91,3 +91,66 @@ def test_set_krylov_fp32_arguments(cuda):
         with pytest.raises(RSOError):
             g.set_krylov_fp32(bad)
     g.close()
+
+
+def applyk64_launches(g):
+    import ctypes
+    n = ctypes.c_longlong(0)
+    ms, b, fl = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_double(0)
+    name = ctypes.create_string_buffer(64)
+    assert g.lib.rso_profile_class(g.h, 3, name, 64, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(b),
+                                   ctypes.byref(fl)) == 0
+    assert name.value.decode() == "fine_applyK_fp64"
+    return n.value
+
+
+def true_rel(g, fh, u):
+    r = fh - g.applyK(u).cpu().numpy()
+    sup = np.tile((g.node_class() & 4) > 0, 3)
+    r[sup] = 0
+    return np.linalg.norm(r) / np.linalg.norm(fh)
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+def test_forced_handover_to_fp64_recurrence(cuda, graphs):
+    """rso_set_krylov_fp32_cycles(1) hands every solve over to the FP64
+    recurrence after its first residual replacement: the FP64 K p kernel runs
+    (profiled launches), the true residual meets the tolerance, and single and
+    batched solves agree with the FP64 recurrence's solutions.  Covers the
+    q buffer the FP64 recurrence takes over from the FP32 one."""
+    prob = P.cantilever(48, 24, 24)
+    g = make(prob)
+    g.set_vcycle_graphs(graphs)
+    tol = 1e-8
+    F = np.stack([rhs(g, s) for s in (41, 42, 43, 44)])
+    g.set_krylov_fp32(0.0)
+    refs = [g.solve(cuda.tensor(F[b], dtype=cuda.float64, device="cuda"), tol=tol, max_iter=300) for b in range(4)]
+    g.set_krylov_fp32(1e-2)
+    g.set_krylov_fp32_cycles(1)
+    g.lib.rso_set_profiling(g.h, 1)
+    g.lib.rso_profile_reset(g.h)
+    for b in range(4):
+        u, it, rr, _ = g.solve(cuda.tensor(F[b], dtype=cuda.float64, device="cuda"), tol=tol, max_iter=300)
+        assert rr < tol and np.isfinite(rr)
+        assert abs(true_rel(g, F[b], u) - rr) <= 1e-3 * rr + 1e-15
+        assert rel(u.cpu().numpy(), refs[b][0].cpu().numpy()) < 1e3 * tol
+        assert it <= refs[b][1] + 4, (it, refs[b][1])
+    assert applyk64_launches(g) > 0
+    U, infos = g.solve_batch(cuda.tensor(F, dtype=cuda.float64, device="cuda"), tol=tol, max_iter=300)
+    for b in range(4):
+        it, rr = infos[b]
+        assert rr < tol and np.isfinite(rr)
+        assert true_rel(g, F[b], U[b]) < 1.01 * tol
+        assert rel(U[b].cpu().numpy(), refs[b][0].cpu().numpy()) < 1e3 * tol
+        assert it <= refs[b][1] + 4, (it, refs[b][1])
+    # without the bound the FP32 recurrence does not stall on this problem
+    g.set_krylov_fp32_cycles(0)
+    g.lib.rso_profile_reset(g.h)
+    for b in range(2):
+        g.solve(cuda.tensor(F[b], dtype=cuda.float64, device="cuda"), tol=tol, max_iter=300)
+    g.solve_batch(cuda.tensor(F, dtype=cuda.float64, device="cuda"), tol=tol, max_iter=300)
+    assert applyk64_launches(g) == 0
+    g.lib.rso_set_profiling(g.h, 0)
+    with pytest.raises(Exception):
+        g.set_krylov_fp32_cycles(-1)
+    g.close()

@@ -3,8 +3,9 @@
 in FP64, and the true FP64 residual replacing the recursive one whenever it
 has dropped by the replacement factor, after at most 30 iterations, and
 before stopping; a replacement whose true residual is not below
-max(0.5, sqrt(factor)) of the previous one hands the solve over to the FP64
-recurrence from the current iterate.  On a well-conditioned system the FP32
+max(0.5, sqrt(factor), sqrt(claimed)) of the previous one (claimed: the
+reduction the recursive residual showed over the cycle) hands the solve over
+to the FP64 recurrence from the current iterate.  On a well-conditioned system the FP32
 recurrence reaches a true relative residual of 1e-10 on its own, in about
 the FP64 recurrence's iteration count.  On an ill-conditioned one (a 2-D
 diffusion operator with a 1e6 coefficient contrast, Jacobi-preconditioned)
@@ -55,10 +56,14 @@ def pcg64(A, dinv, f, tol, max_iter, x0=None):
     return x, max_iter
 
 
-def pcg_k32(A, dinv, f, tol, max_iter, factor, cycle_max=30):
+def stall_ratio(factor, claimed):
+    return max(0.5, np.sqrt(factor), np.sqrt(max(claimed, 0.0)))
+
+
+def pcg_k32(A, dinv, f, tol, max_iter, factor, cycle_max=30, max_cycles=0):
     """(x, iterations, true relative residual, stalled)"""
     f32 = np.float32
-    stall = max(0.5, np.sqrt(factor))
+    cycles = 0
     A32 = A.astype(f32)
     d32 = dinv.astype(f32)
     x = np.zeros_like(f)
@@ -86,7 +91,8 @@ def pcg_k32(A, dinv, f, tol, max_iter, factor, cycle_max=30):
             rel = rtrue / fn
             if rel < tol or it >= max_iter:
                 break
-            if rtrue > stall * rbase:
+            cycles += 1
+            if rtrue > stall_ratio(factor, rn / rbase) * rbase or (max_cycles and cycles >= max_cycles):
                 return x, it, rel, True
             rbase = rtrue
             since = 0
@@ -98,8 +104,8 @@ def pcg_k32(A, dinv, f, tol, max_iter, factor, cycle_max=30):
     return x, it, rel, False
 
 
-def solve_mixed(A, dinv, f, tol, max_iter, factor):
-    x, it, rel, stalled = pcg_k32(A, dinv, f, tol, max_iter, factor)
+def solve_mixed(A, dinv, f, tol, max_iter, factor, max_cycles=0):
+    x, it, rel, stalled = pcg_k32(A, dinv, f, tol, max_iter, factor, max_cycles=max_cycles)
     if stalled:
         x, it2 = pcg64(A, dinv, f, tol, max_iter - it, x0=x)
         it += it2
@@ -138,3 +144,24 @@ def test_stalled_fp32_recurrence_hands_over(factor):
     # system is a factor of a few: the hand-over ends as close to the tolerance as it does
     assert rel < 2 * max(1e-9, true64), (rel, true64)
     assert it <= it64 + 200, (it, it64)
+
+
+def test_short_last_cycle_is_not_a_stall():
+    """A cycle that the tolerance ends after a small reduction of the recursive
+    residual (0.9 here) may leave the true residual at 0.93 of the previous
+    one: above 0.5, but within sqrt(0.9), so no hand-over."""
+    assert stall_ratio(1e-2, 0.9) * 1.0 > 0.93
+    assert stall_ratio(1e-2, 1e-2) == 0.5
+    assert stall_ratio(1e-3, 0.3) == pytest.approx(np.sqrt(0.3))
+
+
+@pytest.mark.parametrize("max_cycles", [1, 2])
+def test_cycle_bound_hands_over(max_cycles):
+    A = laplacian()
+    f = np.random.default_rng(2).standard_normal(A.shape[0])
+    dinv = 1.0 / A.diagonal()
+    x64, it64 = pcg64(A, dinv, f, 1e-10, 5000)
+    x, it, rel, stalled = solve_mixed(A, dinv, f, 1e-10, 5000, 1e-2, max_cycles=max_cycles)
+    assert stalled
+    assert rel < 1e-10 * 1.5
+    assert it <= 1.2 * it64 + 5

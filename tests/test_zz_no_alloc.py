@@ -62,3 +62,26 @@ def test_filter_noalloc_matches_filter(cuda):
     assert "rso_filter_noalloc" in g.lib.rso_last_error(g.h).decode()
     assert torch.isnan(out).all()
     g.close()
+
+
+def test_filter_noalloc_leaves_device_memory_unchanged(cuda):
+    """Free device memory (cudaMemGetInfo) is the same before and after calls
+    at radii this handle has not used yet: no call allocates, the first one
+    on the handle included.  Outputs are allocated before the first reading."""
+    from robustoptspline3d_b200 import HierarchyGrid
+    torch = cuda
+    prob = P.cantilever(24, 12, 12)
+    g = HierarchyGrid(prob["emask"], prob["fixed"], prob["load"], prob["normals"])
+    x = torch.tensor(np.random.default_rng(5).standard_normal(g.ne).astype(np.float32), device="cuda")
+    outs = [torch.empty_like(x) for _ in range(4)]
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for radius, out in zip((1.2, 2.6, 4.4, 6.1), outs):
+        st = g.lib.rso_filter_noalloc(g.h, radius, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()))
+        assert st == 0, g.lib.rso_last_error(g.h).decode()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    for out in outs:
+        assert torch.isfinite(out).all()
+    g.close()

@@ -317,6 +317,28 @@ static double dndist(double x, double a) { return -2 * a * (x - 0.5) * std::exp(
 static double inner_(double x, double a) { return x > 1 ? a * (x - 1) + 1 : 1; }
 static double dinner_(double x, double a) { return x > 1 ? a : 1; }
 
+// the pieces above at given points, for the golden fixtures of the
+// reference's own functions (Heaviside, Dirac Grid.cu:76-121; h, dh, inner_,
+// dinner_, overhang, doverhang, normal_distri, dnormal_distri :123-190):
+// out[k * n + i], k in that order
+extern "C" void or_ss_funcs(int n, const double* x, double beta, double a, double mid, double c, double* out) {
+  const double eta = 0.5;
+  const double den = std::tanh(beta * eta) + std::tanh(beta * (1 - eta));
+  for (int i = 0; i < n; i++) {
+    const double t = std::tanh(beta * (x[i] - eta));
+    out[0 * (size_t)n + i] = Hs(x[i], beta);
+    out[1 * (size_t)n + i] = beta * (1 - t * t) / den;
+    out[2 * (size_t)n + i] = hfun(x[i], a);
+    out[3 * (size_t)n + i] = dhfun(x[i], a);
+    out[4 * (size_t)n + i] = inner_(x[i], a);
+    out[5 * (size_t)n + i] = dinner_(x[i], a);
+    out[6 * (size_t)n + i] = overhang(x[i], mid, c);
+    out[7 * (size_t)n + i] = doverhang(x[i], mid, c);
+    out[8 * (size_t)n + i] = ndist(x[i], a);
+    out[9 * (size_t)n + i] = dndist(x[i], a);
+  }
+}
+
 // spline value at an arbitrary point (SplineBasisX + coefficient sum)
 static double spline_value_at(const or_problem* p, const double* c, const double pt[3], bool* inside) {
   const int o = p->order;

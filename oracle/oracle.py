@@ -62,6 +62,8 @@ def _load():
         "or_sensitivity": (None, [_vp, _d, _d]),
         "or_element_energy": (None, [_vp, _d, _d]),
         "or_heaviside": (None, [ctypes.c_int, _d, ctypes.c_double, ctypes.c_double, _u8, _d]),
+        "or_ss_funcs": (None, [ctypes.c_int, _d, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                               ctypes.c_double, _d]),
         "or_heaviside_chain": (None, [ctypes.c_int, _d, ctypes.c_double, _d, _d]),
         "or_filter": (None, [_vp, ctypes.c_double, _d, _d]),
         "or_density_filter": (None, [_vp, ctypes.c_double, _d, _d]),
@@ -126,6 +128,16 @@ def heaviside_chain(rho, beta, g):
     g = np.ascontiguousarray(g, np.float64)
     out = np.zeros_like(rho)
     lib().or_heaviside_chain(rho.size, _p(rho), beta, _p(g), _p(out))
+    return out
+
+
+def ss_funcs(x, beta, a, mid, c):
+    """The oracle's Heaviside, Dirac and self-support penalty functions at x:
+    rows H, Dirac, h, dh, inner_, dinner_, overhang, doverhang, normal_distri,
+    dnormal_distri (grid/Grid.cu:76-190)."""
+    x = np.ascontiguousarray(x, np.float64)
+    out = np.zeros((10, x.size))
+    lib().or_ss_funcs(x.size, _p(x), beta, a, mid, c, _p(out))
     return out
 
 

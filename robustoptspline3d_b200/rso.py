@@ -330,7 +330,12 @@ class HierarchyGrid:
             self.h = None
 
     def __del__(self):
-        self.close()
+        # at interpreter shutdown the stream-ordering wrapper may no longer
+        # import what it needs; the process exit releases the device memory
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def _chk(self, st, what):
         if st:

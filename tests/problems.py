@@ -47,13 +47,14 @@ def cantilever(ex=64, ey=32, ez=32, seed=0):
     return dict(emask=em, fixed=fa, load=la, normals=None, rho=rho, f=f)
 
 
-def ellipsoid(ex=32, ey=16, ez=16, seed=1, shell=3):
+def ellipsoid(ex=32, ey=16, ez=16, seed=1, shell=3, axes=None):
     """Config 1 shape: voxels whose centres lie in the ellipsoid with
-    semi-axes (ex/2-2, ey/2-2, ez/2-2); lowest active node layer clamped;
-    load area = nodes within `shell` voxels of the boundary (only surface
-    nodes become load nodes); analytic outward normals; rho 0.4 +- 0.05."""
+    semi-axes `axes` (default (ex/2-2, ey/2-2, ez/2-2)) centred in the box;
+    lowest active node layer clamped; load area = nodes within `shell` voxels
+    of the boundary (only surface nodes become load nodes); analytic outward
+    normals; rho 0.4 +- 0.05."""
     rng = np.random.default_rng(seed)
-    a, b, c = ex / 2 - 2, ey / 2 - 2, ez / 2 - 2
+    a, b, c = axes if axes is not None else (ex / 2 - 2, ey / 2 - 2, ez / 2 - 2)
     zc, yc, xc = np.meshgrid(np.arange(ez) + 0.5, np.arange(ey) + 0.5, np.arange(ex) + 0.5, indexing="ij")
     em = (((xc - ex / 2) / a) ** 2 + ((yc - ey / 2) / b) ** 2 + ((zc - ez / 2) / c) ** 2 <= 1).astype(np.uint8)
     nx, ny, nz = ex + 1, ey + 1, ez + 1

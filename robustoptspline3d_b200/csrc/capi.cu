@@ -127,6 +127,7 @@ static void free_handle(rso_handle* h) {
   for (auto p : h->sp.work) cudaFree(p);
   for (auto p : h->lanczos_u) cudaFree(p);
   cudaFree(h->e_a); cudaFree(h->e_b); cudaFree(h->e_c); cudaFree(h->e_d); cudaFree(h->e_rhohat);
+  cudaFree(h->shell_pad);
   cudaFree(h->coef_a); cudaFree(h->coef_b); cudaFree(h->coef_c);
   cudaFree(h->coef_df); cudaFree(h->coef_dg); cudaFree(h->fw); cudaFree(h->uw);
   cudaFree(h->wc_buf);

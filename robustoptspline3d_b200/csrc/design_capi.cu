@@ -20,19 +20,20 @@ __global__ void k_d2f_n(const double* __restrict__ a, float* __restrict__ b, lon
   if (i < n) b[i] = (float)a[i];
 }
 
-// padded copy of an optional dense shell mask (NULL stays NULL)
+// padded copy of an optional dense shell mask (NULL stays NULL), in a buffer
+// the handle keeps: the first call with a mask allocates it, later calls reuse it
 static rso_status pad_shell(rso_handle* h, const uint8_t* shell, uint8_t** out) {
   *out = nullptr;
   if (!shell) return RSO_OK;
   const Level& l = h->L[0];
-  RSO_CHECK_CUDA(h, cudaMallocAsync((void**)out, l.NQ, h->stream));
-  RSO_CHECK_CUDA(h, cudaMemsetAsync(*out, 0, l.NQ, h->stream));
-  k_pad_u8e<<<cdiv(l.ne, 256), 256, 0, h->stream>>>(l, shell, *out); rso::note_launch();
+  if (!h->shell_pad) RSO_CHECK_CUDA(h, cudaMalloc((void**)&h->shell_pad, l.NQ));
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(h->shell_pad, 0, l.NQ, h->stream));
+  k_pad_u8e<<<cdiv(l.ne, 256), 256, 0, h->stream>>>(l, shell, h->shell_pad); rso::note_launch();
+  *out = h->shell_pad;
   return launch_check(h, "pad_shell");
 }
 
-static rso_status finish(rso_handle* h, uint8_t* tmp = nullptr) {
-  if (tmp) RSO_CHECK_CUDA(h, cudaFreeAsync(tmp, h->stream));
+static rso_status finish(rso_handle* h, uint8_t* = nullptr) {
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   return RSO_OK;
 }

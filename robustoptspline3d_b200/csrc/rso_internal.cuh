@@ -139,6 +139,7 @@ struct rso_handle {
   long long n_gs_elements = 0;
   // design-iteration scratch
   float *e_a = nullptr, *e_b = nullptr, *e_c = nullptr, *e_d = nullptr, *e_rhohat = nullptr;
+  uint8_t* shell_pad = nullptr;       // padded copy of a caller's shell mask (design_capi.cu), made on first use
   double *coef_a = nullptr, *coef_b = nullptr, *coef_c = nullptr;
   double *coef_df = nullptr, *coef_dg = nullptr;   // MMA inputs
   double *fw = nullptr, *uw = nullptr;             // worst-case force / displacement (padded)

@@ -298,22 +298,28 @@ extern "C" rso_status rso_force_project(rso_handle* h, double* f, int cf) {
   return RSO_OK;
 }
 
+// the padded worst-case force and displacement the handle keeps between calls
+// (allocated by the first call that needs them, here or in a design iteration)
+static rso_status worst_buffers(rso_handle* h) {
+  if (h->fw) return RSO_OK;
+  const long long n3 = 3 * h->L[0].NP;
+  RSO_CHECK_CUDA(h, cudaMalloc(&h->fw, sizeof(double) * n3));
+  RSO_CHECK_CUDA(h, cudaMalloc(&h->uw, sizeof(double) * n3));
+  return RSO_OK;
+}
+
 extern "C" rso_status rso_worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t seed, double* f_worst,
                                      double* u_worst, double* lambda, double* ritz) {
   if (!h || !f_worst || !u_worst || steps < 1 || !(tol > 0)) return RSO_ERR_INVALID_ARG;
   if (!h->operators_ready) { h->err = "call rso_update_operators first"; return RSO_ERR_STATE; }
-  double* fo = nullptr;
-  double* uo = nullptr;
-  const long long n3 = 3 * h->L[0].NP;
-  RSO_CHECK_CUDA(h, cudaMallocAsync(&fo, sizeof(double) * n3, h->stream));
-  RSO_CHECK_CUDA(h, cudaMallocAsync(&uo, sizeof(double) * n3, h->stream));
+  RSO_TRY(worst_buffers(h));
+  double* fo = h->fw;
+  double* uo = h->uw;
   rso_status s = worst_case(h, steps, cf, tol, seed, fo, uo, lambda, ritz, nullptr);
   if (s == RSO_OK) {
     RSO_TRY(unpad_nodes(h, 0, fo, f_worst));
     RSO_TRY(unpad_nodes(h, 0, uo, u_worst));
   }
-  cudaFreeAsync(fo, h->stream);
-  cudaFreeAsync(uo, h->stream);
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   return s;
 }
@@ -322,18 +328,14 @@ extern "C" rso_status rso_modified_pm(rso_handle* h, int cf, uint64_t seed, int 
                                       double* c_worst, int* itn) {
   if (!h || !f || !u || max_itn < 1) return RSO_ERR_INVALID_ARG;
   if (!h->operators_ready) { h->err = "call rso_update_operators first"; return RSO_ERR_STATE; }
-  double* fo = nullptr;
-  double* uo = nullptr;
-  const long long n3 = 3 * h->L[0].NP;
-  RSO_CHECK_CUDA(h, cudaMallocAsync(&fo, sizeof(double) * n3, h->stream));
-  RSO_CHECK_CUDA(h, cudaMallocAsync(&uo, sizeof(double) * n3, h->stream));
+  RSO_TRY(worst_buffers(h));
+  double* fo = h->fw;
+  double* uo = h->uw;
   rso_status s = modified_pm(h, cf, seed, max_itn, fo, uo, c_worst, itn);
   if (s == RSO_OK) {
     RSO_TRY(unpad_nodes(h, 0, fo, f));
     RSO_TRY(unpad_nodes(h, 0, uo, u));
   }
-  cudaFreeAsync(fo, h->stream);
-  cudaFreeAsync(uo, h->stream);
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   return s;
 }

@@ -2,7 +2,6 @@
 // (design-variable, worst-case and MMA entry points live in design.cu,
 // worst.cu and mma.cu.)
 #include "rso_internal.cuh"
-#include <cublas_v2.h>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -111,9 +110,8 @@ static void free_handle(rso_handle* h) {
   }
   cudaFree(h->K0_dev); cudaFree(h->rho); cudaFree(h->rp32); cudaFree(h->rp64);
   cudaFree(h->load_nodes); cudaFree(h->load_normals); cudaFree(h->T1);
-  cudaFree(h->gal_w); cudaFree(h->efix); cudaFree(h->gfix);
-  if (h->cublas) cublasDestroy((cublasHandle_t)h->cublas);
-  cudaFree(h->cublas_ws); cudaFree(h->filt_taps);
+  cudaFree(h->efix); cudaFree(h->gfix);
+  cudaFree(h->filt_taps);
   batch_release(h);
   cudaFree(h->c_nodes); cudaFree(h->c_K); cudaFree(h->c_f); cudaFree(h->c_flag);
   cudaFree(h->red); cudaFree(h->scal); cudaFree(h->xfer); cudaFree(h->fpart);
@@ -340,11 +338,6 @@ extern "C" rso_status rso_set_stream(rso_handle* h, void* stream) {
     if (h->own_stream) cudaStreamDestroy(h->stream);
     h->stream = (cudaStream_t)stream;
     h->own_stream = false;
-    if (h->cublas && (cublasSetStream((cublasHandle_t)h->cublas, h->stream) != CUBLAS_STATUS_SUCCESS ||
-                      cublasSetWorkspace((cublasHandle_t)h->cublas, h->cublas_ws, 32u << 20) != CUBLAS_STATUS_SUCCESS)) {
-      h->err = "cuBLAS stream re-binding failed";
-      return RSO_ERR_CUDA;
-    }
   }
   return RSO_OK;
 }

@@ -16,7 +16,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cooperative_groups.h>
-#include <cublas_v2.h>
 #include <vector>
 
 namespace cg = cooperative_groups;
@@ -506,10 +505,11 @@ __global__ void __launch_bounds__(256) k_prolong_v4(const Level Fl, const Level 
 __device__ __forceinline__ double pw(int F, int o, int A) { return A ? (double)o / F : (double)(F - o) / F; }
 
 // Support-free children enter the first-level coarse element matrices as a
-// plain GEMM, KE[E] = sum_pos w[E][pos] T1[pos] (w = rho^p of child pos, 0
-// for inactive or support-touching children), done by cuBLAS; the
-// support-touching children are added by k_galerkin_fix on the few coarse
-// elements that have them.
+// product KE[E] = sum_pos w[E][pos] T1[pos] (w = rho^p of child pos, 0 for
+// inactive or support-touching children; T1[pos] the 576 entries of child
+// pos's element matrix seen from the coarse element's nodes), done by
+// k_galerkin_first; the support-touching children are added by
+// k_galerkin_fix on the few coarse elements that have them.
 __global__ void k_elem_fixmask(const Level Fl, uint8_t* __restrict__ efix) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= Fl.ne) return;
@@ -521,21 +521,64 @@ __global__ void k_elem_fixmask(const Level Fl, uint8_t* __restrict__ efix) {
   efix[Fl.eidx(x, y, z)] = (uint8_t)m;
 }
 
-__global__ void k_gal_weights(const Level Fl, const Level C, int F, const double* __restrict__ rp,
-                              const uint8_t* __restrict__ efix, double* __restrict__ w) {
-  const long long E = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (E >= C.ne) return;
-  const int X = E % C.ex, Y = (E / C.ex) % C.ey, Z = E / ((long long)C.ex * C.ey);
-  const int F3 = F * F * F;
-  for (int pos = 0; pos < F3; pos++) {
-    const int px = pos % F, py = (pos / F) % F, pz = pos / (F * F);
-    const int x = X * F + px, y = Y * F + py, z = Z * F + pz;
+// KE (576 x ne, column per coarse element) = T1 (576 x F3) . w (F3 x ne),
+// w formed on the fly from the children's rho^p.  A CTA takes GE coarse
+// elements: their weights go to shared memory once, then the 576 rows pass
+// in chunks of 64 staged from T1; a thread accumulates 4 rows x 2 elements
+// in FP64 (each output is one ordered sum over the F3 children).
+constexpr int GE = 32, GM = 64;
+template <int F>
+__global__ void __launch_bounds__(256) k_galerkin_first(const Level Fl, const Level C, const double* __restrict__ rp,
+                                                        const uint8_t* __restrict__ efix,
+                                                        const double* __restrict__ T1, double* __restrict__ KE) {
+  constexpr int F3 = F * F * F;
+  __shared__ __align__(16) double Ws[F3][GE];
+  __shared__ __align__(16) double Ts[F3][GM];
+  const int t = threadIdx.x;
+  const long long E0 = (long long)blockIdx.x * GE;
+  for (int idx = t; idx < F3 * GE; idx += 256) {
+    const int pos = idx / GE, j = idx - pos * GE;
+    const long long E = E0 + j;
     double r = 0.0;
-    if (x < Fl.ex && y < Fl.ey && z < Fl.ez) {
-      const long long e = Fl.eidx(x, y, z);
-      if (Fl.emask[e] && !efix[e]) r = rp[e];
+    if (E < C.ne) {
+      const int X = E % C.ex, Y = (E / C.ex) % C.ey, Z = E / ((long long)C.ex * C.ey);
+      const int x = X * F + pos % F, y = Y * F + (pos / F) % F, z = Z * F + pos / (F * F);
+      if (x < Fl.ex && y < Fl.ey && z < Fl.ez) {
+        const long long e = Fl.eidx(x, y, z);
+        if (Fl.emask[e] && !efix[e]) r = rp[e];
+      }
     }
-    w[E * F3 + pos] = r;
+    Ws[pos][j] = r;
+  }
+  const int ti = t & 15, te = t >> 4;  // rows 4 ti .. 4 ti + 3 of the chunk, elements 2 te, 2 te + 1
+  for (int m0 = 0; m0 < 576; m0 += GM) {
+    __syncthreads();  // Ws complete (first chunk); Ts free (later chunks)
+    for (int idx = t; idx < F3 * GM; idx += 256) {
+      const int k = idx / GM, i = idx - k * GM;
+      Ts[k][i] = T1[(long long)k * 576 + m0 + i];
+    }
+    __syncthreads();
+    double acc[4][2] = {};
+#pragma unroll 8
+    for (int k = 0; k < F3; k++) {
+      const double2 a01 = *reinterpret_cast<const double2*>(&Ts[k][4 * ti]);
+      const double2 a23 = *reinterpret_cast<const double2*>(&Ts[k][4 * ti + 2]);
+      const double2 b = *reinterpret_cast<const double2*>(&Ws[k][2 * te]);
+      const double a[4] = {a01.x, a01.y, a23.x, a23.y};
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        acc[r][0] = fma(a[r], b.x, acc[r][0]);
+        acc[r][1] = fma(a[r], b.y, acc[r][1]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      const long long E = E0 + 2 * te + c;
+      if (E >= C.ne) continue;
+      double* o = KE + E * 576 + m0 + 4 * ti;
+      *reinterpret_cast<double2*>(o) = make_double2(acc[0][c], acc[1][c]);
+      *reinterpret_cast<double2*>(o + 2) = make_double2(acc[2][c], acc[3][c]);
+    }
   }
 }
 
@@ -1214,21 +1257,7 @@ rso_status galerkin_setup(rso_handle* h) {
     RSO_CHECK_CUDA(h, cudaMalloc(&h->gfix, sizeof(int) * list.size()));
     RSO_CHECK_CUDA(h, cudaMemcpy(h->gfix, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice));
   }
-  RSO_CHECK_CUDA(h, cudaMalloc(&h->gal_w, sizeof(double) * (size_t)c.ne * F3));
-  cublasHandle_t cb = nullptr;
-  if (cublasCreate(&cb) != CUBLAS_STATUS_SUCCESS) {
-    h->err = "cublasCreate failed";
-    return RSO_ERR_CUDA;
-  }
-  h->cublas = cb;
-  // a fixed workspace and the handle's stream, set once (rso_set_stream re-binds the stream)
-  const size_t ws = 32u << 20;
-  RSO_CHECK_CUDA(h, cudaMalloc(&h->cublas_ws, ws));
-  if (cublasSetWorkspace(cb, h->cublas_ws, ws) != CUBLAS_STATUS_SUCCESS ||
-      cublasSetStream(cb, h->stream) != CUBLAS_STATUS_SUCCESS) {
-    h->err = "cuBLAS workspace/stream set-up failed";
-    return RSO_ERR_CUDA;
-  }
+  (void)F3;
   return RSO_OK;
 }
 
@@ -1238,16 +1267,12 @@ rso_status galerkin(rso_handle* h) {
     const Level& f = h->L[li - 1];
     if (li == 1)
     {
-      const int F = c.factor, F3 = F * F * F;
-      k_gal_weights<<<cdiv(c.ne, 256), 256, 0, h->stream>>>(f, c, F, h->rp64, h->efix, h->gal_w); rso::note_launch();
-      RSO_TRY(launch_check(h, "galerkin weights"));
-      cublasHandle_t cb = (cublasHandle_t)h->cublas;
-      const double one = 1.0, zero = 0.0;
-      if (cublasDgemm(cb, CUBLAS_OP_N, CUBLAS_OP_N, 576, (int)c.ne, F3, &one, h->T1, 576, h->gal_w, F3, &zero, c.KE,
-                      576) != CUBLAS_STATUS_SUCCESS) {
-        h->err = "cublasDgemm of the first-level Galerkin product failed";
-        return RSO_ERR_CUDA;
-      }
+      const int F = c.factor;
+      const unsigned nblk = (unsigned)cdiv(c.ne, GE);
+      if (F == 4) k_galerkin_first<4><<<nblk, 256, 0, h->stream>>>(f, c, h->rp64, h->efix, h->T1, c.KE);
+      else k_galerkin_first<2><<<nblk, 256, 0, h->stream>>>(f, c, h->rp64, h->efix, h->T1, c.KE);
+      rso::note_launch();
+      RSO_TRY(launch_check(h, "galerkin first level"));
       if (h->n_gfix > 0) {
         k_galerkin_fix<<<h->n_gfix, 288, 0, h->stream>>>(f, c, F, h->rp64, h->K0_dev, h->efix, h->gfix, c.KE);
       }

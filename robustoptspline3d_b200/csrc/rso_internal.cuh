@@ -92,12 +92,9 @@ struct rso_handle {
   double* load_normals = nullptr;     // 3 per load node
   // Galerkin tables
   double* T1 = nullptr;               // F^3 x 576 table for the first coarsening
-  void* cublas = nullptr;             // cublasHandle_t of the first-level Galerkin product
-  double* gal_w = nullptr;            // [coarse element][F^3] rho^p of the support-free children
   uint8_t* efix = nullptr;            // per padded fine element: bit a set if local node a is a support node
   int* gfix = nullptr;                // coarse elements with a child that touches a support node
   int n_gfix = 0;
-  void* cublas_ws = nullptr;          // fixed cuBLAS workspace (no allocation inside calls)
   void* filt_taps = nullptr;          // sensitivity-filter tap table of the last radius used
   long long filt_cap = 0;
   double filt_radius = -1.0;

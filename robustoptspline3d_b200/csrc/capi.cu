@@ -234,7 +234,7 @@ static rso_status setup(rso_handle* h, int ex, int ey, int ez, const uint8_t* em
     ALLOC(h->c_nodes, sizeof(int) * packed.size());
     RSO_CHECK_CUDA(h, cudaMemcpy(h->c_nodes, packed.data(), sizeof(int) * packed.size(), cudaMemcpyHostToDevice));
     const size_t N = 3 * (size_t)h->nc;
-    ALLOC(h->c_K, sizeof(double) * 2 * N * N);
+    ALLOC(h->c_K, sizeof(double) * 3 * N * N);  // factor, inverse, L^-1 scratch
     ALLOC(h->c_f, sizeof(double) * N);
     ALLOC(h->c_flag, sizeof(int));
   }

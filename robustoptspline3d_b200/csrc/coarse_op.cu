@@ -727,56 +727,6 @@ __global__ void k_coarse_dense(const Level C, const double* __restrict__ st, con
   K[(long long)(3 * i + r) * N + 3 * j + c] = st[(long long)(d * 9 + r * 3 + c) * C.NP + n];
 }
 
-// in-place Cholesky (lower) in a single block; flag != 0 on a non-positive pivot
-__global__ void __launch_bounds__(1024) k_cholesky(double* A, int N, int* flag) {
-  // symmetrise first
-  for (long long idx = threadIdx.x; idx < (long long)N * N; idx += blockDim.x) {
-    const int i = idx / N, j = idx % N;
-    if (j > i) {
-      const double v = 0.5 * (A[(long long)i * N + j] + A[(long long)j * N + i]);
-      A[(long long)i * N + j] = v;
-      A[(long long)j * N + i] = v;
-    }
-  }
-  __syncthreads();
-  __shared__ double dsh;
-  for (int j = 0; j < N; j++) {
-    if (threadIdx.x == 0) {
-      double s = A[(long long)j * N + j];
-      if (!(s > 0)) { *flag = 1; s = 1e-300; }
-      s = sqrt(s);
-      A[(long long)j * N + j] = s;
-      dsh = s;
-    }
-    __syncthreads();
-    const double d = dsh;
-    for (int i = j + 1 + threadIdx.x; i < N; i += blockDim.x) A[(long long)i * N + j] /= d;
-    __syncthreads();
-    const int m = N - j - 1;
-    for (long long idx = threadIdx.x; idx < (long long)m * m; idx += blockDim.x) {
-      const int i = j + 1 + idx / m, k = j + 1 + idx % m;
-      if (k <= i) A[(long long)i * N + k] -= A[(long long)i * N + j] * A[(long long)k * N + j];
-    }
-    __syncthreads();
-  }
-}
-
-// X = (L L^T)^-1, one column per thread
-__global__ void k_chol_inverse(const double* __restrict__ Lc, int N, double* __restrict__ X) {
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= N) return;
-  for (int i = 0; i < N; i++) {
-    double t = (i == col) ? 1.0 : 0.0;
-    for (int k = 0; k < i; k++) t -= Lc[(long long)i * N + k] * X[(long long)k * N + col];
-    X[(long long)i * N + col] = t / Lc[(long long)i * N + i];
-  }
-  for (int i = N - 1; i >= 0; i--) {
-    double t = X[(long long)i * N + col];
-    for (int k = i + 1; k < N; k++) t -= Lc[(long long)k * N + i] * X[(long long)k * N + col];
-    X[(long long)i * N + col] = t / Lc[(long long)i * N + i];
-  }
-}
-
 template <typename T>
 __global__ void k_gather_coarse(const Level C, const T* __restrict__ f, const int* __restrict__ cnodes, int nc,
                                 double* __restrict__ b) {
@@ -1296,9 +1246,8 @@ rso_status coarsest_factor(rso_handle* h) {
   // crow map lives right after the c_nodes list (see capi set-up)
   k_coarse_dense<<<cdiv((long long)h->nc * 243, 256), 256, 0, h->stream>>>(c, c.st64, h->c_nodes,
                                                                            h->c_nodes + h->nc, h->nc, h->c_K); rso::note_launch();
-  k_cholesky<<<1, 1024, 0, h->stream>>>(h->c_K, N, h->c_flag); rso::note_launch();
-  k_chol_inverse<<<cdiv(N, 64), 64, 0, h->stream>>>(h->c_K, N, h->c_K + (size_t)N * N); rso::note_launch();
-  RSO_TRY(launch_check(h, "coarsest_factor"));
+  RSO_TRY(launch_check(h, "coarsest assembly"));
+  RSO_TRY(dense_spd_inverse(h, h->c_K, h->c_K + (size_t)N * N, h->c_K + 2 * (size_t)N * N, N, h->c_flag));
   int flag = 0;
   RSO_CHECK_CUDA(h, cudaMemcpyAsync(&flag, h->c_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));

@@ -277,6 +277,11 @@ rso_status prolong(rso_handle* h, int coarse_level, const T* uc, T* uf);
 template <typename T>
 rso_status coarsest_solve(rso_handle* h, const T* f, T* u);
 rso_status galerkin_setup(rso_handle* h);
+// coarsest dense solve (dense.cu): A (N x N) -> Cholesky factor in its lower
+// triangle, X = A^-1, Y scratch; *flag_dev set on a pivot that is not positive
+rso_status dense_spd_inverse(rso_handle* h, double* A, double* X, double* Y, int N, int* flag_dev);
+// A += a R R^T, R row-major N x nr
+rso_status dense_rank_update(rso_handle* h, double* A, int N, const double* R, int nr, double a);
 rso_status galerkin(rso_handle* h);
 rso_status coarsest_factor(rso_handle* h);
 rso_status estimate_lambda(rso_handle* h);

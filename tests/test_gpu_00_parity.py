@@ -163,7 +163,9 @@ def test_coarse_and_transfers_fp32(oracle, cuda, gen, ff, split):
 
 @pytest.mark.parametrize("gen,nl,ff", [(lambda: P.ellipsoid(40, 24, 24), 0, 4),
                                        (lambda: P.ellipsoid(24, 16, 12), 0, 4),
-                                       (lambda: P.cantilever(16, 8, 8), 3, 2)])
+                                       (lambda: P.cantilever(16, 8, 8), 3, 2),
+                                       # coarsest 12 x 6 x 6: 1,911 DOF, many 64-wide tiles of the dense solve
+                                       (lambda: P.cantilever(24, 12, 12), 2, 2)])
 def test_galerkin_stencils_and_transfers(oracle, cuda, gen, nl, ff):
     prob = gen()
     g, o = make(oracle, prob, n_levels=nl, first_factor=ff)

@@ -191,6 +191,8 @@ extern "C" or_problem* or_create(int ex, int ey, int ez, const uint8_t* emask,
   }
   std::sort(ln.begin(), ln.end());
   for (auto& q : ln) p->load_nodes.push_back(q.second);
+  p->has_support = std::any_of(p->support.begin(), p->support.end(), [](uint8_t s) { return s != 0; });
+  if (!p->has_support) rigid_setup(p);
   p->rho.assign(p->L[0].ne, 1.0);
   p->rhop.assign(p->L[0].ne, 1.0);
   return p;
@@ -741,6 +743,30 @@ void orc::coarsest_factor(or_problem* p) {
       double v = 0.5 * (K[(size_t)i * N + j] + K[(size_t)j * N + i]);
       K[(size_t)i * N + j] = K[(size_t)j * N + i] = v;
     }
+  // without supports K is singular, its null space the rigid motions R of the
+  // coarsest nodes (trilinear prolongation reproduces them): factor
+  // K + a R R^T, a the mean diagonal, and K^+ = (K + a R R^T)^-1 - R R^T / a
+  // (the reference's BDCSVD pseudo-inverse, Grid.cpp:4123-4185)
+  double a_rig = 0;
+  int k_rig = 0;
+  if (!p->has_support) {
+    std::vector<double> pos;
+    for (int i = 0; i < nc; i++) {
+      long n = p->cnode[i];
+      pos.push_back((double)(n % c.nx));
+      pos.push_back((double)(n / c.nx % c.ny));
+      pos.push_back((double)(n / ((long)c.nx * c.ny)));
+    }
+    k_rig = rigid_basis(pos, nullptr, p->rigid_coarse, false);
+    for (int i = 0; i < N; i++) a_rig += K[(size_t)i * N + i];
+    a_rig /= N;
+    for (int i = 0; i < N; i++)
+      for (int j = 0; j < N; j++) {
+        double s = 0;
+        for (int q = 0; q < k_rig; q++) s += p->rigid_coarse[(size_t)q * N + i] * p->rigid_coarse[(size_t)q * N + j];
+        K[(size_t)i * N + j] += a_rig * s;
+      }
+  }
   // Cholesky
   std::vector<double> Lc((size_t)N * N, 0.0);
   for (int j = 0; j < N; j++) {
@@ -771,6 +797,13 @@ void orc::coarsest_factor(or_problem* p) {
     }
     for (int i = 0; i < N; i++) p->Kinv[(size_t)i * N + c2] = col[i];
   }
+  if (k_rig)
+    for (int i = 0; i < N; i++)
+      for (int j = 0; j < N; j++) {
+        double s = 0;
+        for (int q = 0; q < k_rig; q++) s += p->rigid_coarse[(size_t)q * N + i] * p->rigid_coarse[(size_t)q * N + j];
+        p->Kinv[(size_t)i * N + j] -= s / a_rig;
+      }
 }
 
 extern "C" void or_coarsest_solve(const or_problem* p, const double* f, double* u) {
@@ -853,6 +886,7 @@ extern "C" int or_solve(or_problem* p, double* u, const double* f, double tol, i
       it++;
       if (rr < tol) break;
     }
+    displacement_project(p, u);
     if (rel_res) *rel_res = rr;
     return it;
   }
@@ -883,6 +917,8 @@ extern "C" int or_solve(or_problem* p, double* u, const double* f, double tol, i
     rz = rz2;
     for (long i = 0; i < 3 * nn; i++) pp[i] = z[i] + beta * pp[i];
   }
+  // support-free problems: the solution without rigid motion (displacementProject)
+  displacement_project(p, u);
   // true residual
   or_residual(p, u, f, r.data());
   for (long i = 0; i < nn; i++)

@@ -30,6 +30,12 @@ struct or_problem {
   std::vector<double> normals;
   std::vector<double> rho, rhop;          // per fine element (box)
   std::vector<int> load_nodes;            // dense node ids (sorted by reference gs id)
+  // support-free problems (no support node): rigid motions, orthonormal
+  bool has_support = true;
+  std::vector<double> rigid_full;         // 3 nn x 6 over the active fine nodes, row (c nn + n), col-major by mode
+  std::vector<double> rigid_load[2];      // load space 3 nl x k[cf], ff (0) and normal-projected cf (1)
+  int rigid_k[2] = {0, 0};
+  std::vector<double> rigid_coarse;       // 3 nc x 6 over the coarsest active nodes (row 3 i + c)
   // coarsest dense solve
   std::vector<long> cnode;                // active coarsest nodes
   std::vector<long> crow;                 // node -> row block (-1 absent)
@@ -50,4 +56,14 @@ void build_topology(or_problem* p, int n_levels, int first_factor);
 void galerkin(or_problem* p);
 void coarsest_factor(or_problem* p);
 double dot3(const double* a, const double* b, long nn);
+// rigid motions of the given node positions (6 columns, rows 3 k + c for
+// node k): translations then rotations p^ (projection.cpp:58-75), turned
+// orthonormal by modified Gram-Schmidt in column order; with `drop`, columns
+// whose residual falls below 1e-6 of their norm are removed
+// (projection.cpp:235-262).  Returns the kept columns (column-major).
+// With `nrm` (3 per node), each node's block of every column is first replaced
+// by its component along the node's normal (projection.cpp:231-233).
+int rigid_basis(const std::vector<double>& pos, const double* nrm, std::vector<double>& Q, bool drop);
+void rigid_setup(or_problem* p);
+void displacement_project(const or_problem* p, double* u);
 }

@@ -18,9 +18,106 @@ static inline double urand(uint64_t seed, uint64_t i) {
   return (double)(h >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
 }
 
+// ---------------------------------------------------------------- rigid motions
+int orc::rigid_basis(const std::vector<double>& pos, const double* nrm, std::vector<double>& Q, bool drop) {
+  const size_t m = pos.size();  // 3 per node
+  std::vector<std::vector<double>> col(6, std::vector<double>(m, 0.0));
+  for (size_t k = 0; k < m / 3; k++) {
+    const double* p = &pos[3 * k];
+    // rows c of [I | p^], p^ = [[0, -z, y], [z, 0, -x], [-y, x, 0]]
+    const double ph[3][3] = {{0, -p[2], p[1]}, {p[2], 0, -p[0]}, {-p[1], p[0], 0}};
+    for (int c = 0; c < 3; c++) {
+      col[c][3 * k + c] = 1.0;
+      for (int j = 0; j < 3; j++) col[3 + j][3 * k + c] = ph[c][j];
+    }
+    if (nrm) {
+      const double* nv = &nrm[3 * k];
+      for (int j = 0; j < 6; j++) {
+        double* b = &col[j][3 * k];
+        const double s = b[0] * nv[0] + b[1] * nv[1] + b[2] * nv[2];
+        for (int c = 0; c < 3; c++) b[c] = s * nv[c];
+      }
+    }
+  }
+  auto dotv = [&](const std::vector<double>& a, const std::vector<double>& b) {
+    double s = 0;
+    for (size_t i = 0; i < m; i++) s += a[i] * b[i];
+    return s;
+  };
+  bool invalid[6] = {false, false, false, false, false, false};
+  for (int i = 0; i < 6; i++) {
+    const double oldres = std::sqrt(dotv(col[i], col[i]));
+    for (int j = 0; j < i; j++) {
+      if (drop && invalid[j]) continue;
+      const double w = dotv(col[i], col[j]);
+      for (size_t t = 0; t < m; t++) col[i][t] -= w * col[j][t];
+    }
+    const double res = std::sqrt(dotv(col[i], col[i]));
+    if (drop && (res / oldres < 1e-6 || oldres < 1e-6)) invalid[i] = true;
+    for (size_t t = 0; t < m; t++) col[i][t] /= res;
+  }
+  Q.clear();
+  int k = 0;
+  for (int i = 0; i < 6; i++) {
+    if (drop && invalid[i]) continue;
+    Q.insert(Q.end(), col[i].begin(), col[i].end());
+    k++;
+  }
+  return k;
+}
+
+// setNodes / setLoadNodes (projection.cpp:47-110, :129-269) for problems
+// without supports: the rigid motions of all active fine nodes (for
+// displacementProject), of the load nodes (for forceProject; normal-projected
+// in constrained-direction modes) and of the coarsest nodes (pseudo-inverse)
+void orc::rigid_setup(or_problem* p) {
+  const Level& f = p->L[0];
+  std::vector<double> pos;
+  std::vector<long> act;
+  for (long n = 0; n < f.nn; n++) {
+    if (!f.vmask[n]) continue;
+    act.push_back(n);
+    pos.push_back((double)(n % f.nx));
+    pos.push_back((double)(n / f.nx % f.ny));
+    pos.push_back((double)(n / ((long)f.nx * f.ny)));
+  }
+  std::vector<double> Q;
+  const int k = rigid_basis(pos, nullptr, Q, false);
+  const size_t m = pos.size();
+  p->rigid_full.assign((size_t)3 * f.nn * 6, 0.0);
+  for (int j = 0; j < k; j++)
+    for (size_t a = 0; a < act.size(); a++)
+      for (int c = 0; c < 3; c++) p->rigid_full[(size_t)j * 3 * f.nn + c * f.nn + act[a]] = Q[j * m + 3 * a + c];
+  std::vector<double> lpos, lnrm;
+  for (int n : p->load_nodes) {
+    lpos.push_back((double)(n % f.nx));
+    lpos.push_back((double)(n / f.nx % f.ny));
+    lpos.push_back((double)(n / ((long)f.nx * f.ny)));
+    for (int c = 0; c < 3; c++) lnrm.push_back(p->normals[3 * (size_t)n + c]);
+  }
+  p->rigid_k[0] = rigid_basis(lpos, nullptr, p->rigid_load[0], true);
+  p->rigid_k[1] = rigid_basis(lpos, lnrm.data(), p->rigid_load[1], true);
+}
+
+// displacementProject (projection.cpp:374-411): u -= R R^T u over the
+// orthonormal rigid motions of the active fine nodes
+void orc::displacement_project(const or_problem* p, double* u) {
+  if (p->has_support) return;
+  const long n3 = 3 * p->L[0].nn;
+  for (int j = 0; j < 6; j++) {
+    const double* r = &p->rigid_full[(size_t)j * n3];
+    double s = 0;
+    for (long i = 0; i < n3; i++) s += r[i] * u[i];
+    for (long i = 0; i < n3; i++) u[i] -= s * r[i];
+  }
+}
+
+extern "C" void or_displacement_project(const or_problem* p, double* u) { displacement_project(p, u); }
+
 // forceProject (projection.cpp:289-360 / projection.cu:165-231): forces kept
 // only on load nodes; in constrained-direction modes only the component
-// along the load normal survives (f -= Nd^T Nd f).
+// along the load normal survives (f -= Nd^T Nd f); without supports the
+// rigid motions of the load set are removed as well (f -= Rd Rd^T f).
 extern "C" void or_force_project(const or_problem* p, double* f, int cf) {
   const long nn = p->L[0].nn;
   std::vector<double> keep(3 * p->load_nodes.size());
@@ -33,6 +130,16 @@ extern "C" void or_force_project(const or_problem* p, double* f, int cf) {
       for (int c = 0; c < 3; c++) v[c] = s * nr[c];
     }
     for (int c = 0; c < 3; c++) keep[3 * k + c] = v[c];
+  }
+  if (!p->has_support) {
+    const int ci = cf ? 1 : 0;
+    const size_t m = keep.size();
+    const std::vector<double>& Q = p->rigid_load[ci];
+    std::vector<double> w(p->rigid_k[ci], 0.0);
+    for (int j = 0; j < p->rigid_k[ci]; j++)
+      for (size_t i = 0; i < m; i++) w[j] += Q[j * m + i] * keep[i];
+    for (int j = 0; j < p->rigid_k[ci]; j++)
+      for (size_t i = 0; i < m; i++) keep[i] -= w[j] * Q[j * m + i];
   }
   for (long i = 0; i < 3 * nn; i++) f[i] = 0;
   for (size_t k = 0; k < p->load_nodes.size(); k++) {
@@ -83,7 +190,7 @@ static void jacobi_eig(int n, std::vector<double> A, std::vector<double>& w, std
 static int solve_tight(or_problem* p, double* u, const double* f, double tol) {
   double rr;
   std::fill(u, u + 3 * p->L[0].nn, 0.0);
-  return or_solve(p, u, f, tol, 500, 1, 1, 1, 0, 1.0, &rr);
+  return or_solve(p, u, f, tol, 500, 1, 1, 1, 0, 1.0, &rr);  // projected when support-free
 }
 
 // dense aggregated worst case (TestSuit::verifyModifiedPM / aggregatedSystem,
@@ -102,12 +209,16 @@ extern "C" double or_dense_worst(or_problem* p, int cf, double tol, double* f_wo
     if (cf) for (int c = 0; c < 3; c++) v[c * nn + n] = p->normals[3 * n + c];
     else v[(col % 3) * nn + n] = 1.0;
   };
+  // basis vectors of the admissible loads (forceProject also removes the
+  // rigid motions of support-free problems; a no-op on the basis otherwise)
   for (int col = 0; col < m; col++) {
     basis(col, b.data());
+    or_force_project(p, b.data(), cf);
     solve_tight(p, U[col].data(), b.data(), tol);
   }
   for (int i = 0; i < m; i++) {
     basis(i, b.data());
+    or_force_project(p, b.data(), cf);
     for (int j = 0; j < m; j++) C[(size_t)i * m + j] = dot3(b.data(), U[j].data(), nn);
   }
   for (int i = 0; i < m; i++)
@@ -124,6 +235,7 @@ extern "C" double or_dense_worst(or_problem* p, int cf, double tol, double* f_wo
   for (int col = 0; col < m; col++) {
     double y = V[(size_t)col * m + best];
     basis(col, b.data());
+    or_force_project(p, b.data(), cf);
     for (long i = 0; i < 3 * nn; i++) {
       if (f_worst) f_worst[i] += y * b[i];
       if (u_worst) u_worst[i] += y * U[col][i];
@@ -213,6 +325,7 @@ extern "C" double or_modified_pm(or_problem* p, int cf, uint64_t seed, int max_i
   int itn = 0;
   while (itn++ < max_itn && (fch > 1e-4 || rr > 1e-2)) {
     rr = or_vcycle(p, u.data(), f.data(), 1, 1, 0, 1.0, 0);
+    displacement_project(p, u.data());
     f = u;
     or_force_project(p, f.data(), cf);
     fn = std::sqrt(dot3(f.data(), f.data(), nn));

@@ -62,6 +62,7 @@ def _load():
         "or_sensitivity": (None, [_vp, _d, _d]),
         "or_element_energy": (None, [_vp, _d, _d]),
         "or_heaviside": (None, [ctypes.c_int, _d, ctypes.c_double, ctypes.c_double, _u8, _d]),
+        "or_displacement_project": (None, [ctypes.c_void_p, _d]),
         "or_ss_funcs": (None, [ctypes.c_int, _d, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                ctypes.c_double, _d]),
         "or_heaviside_chain": (None, [ctypes.c_int, _d, ctypes.c_double, _d, _d]),
@@ -278,6 +279,12 @@ class Problem:
         rr = lib().or_vcycle(self.h, _p(u), _p(np.ascontiguousarray(f, np.float64)), pre, post, kind, omega,
                              symmetric)
         return u, rr
+
+    def displacement_project(self, u):
+        """u without rigid motion (a no-op for problems with supports)."""
+        u = np.ascontiguousarray(u, np.float64).copy()
+        lib().or_displacement_project(self.h, _p(u))
+        return u
 
     def solve(self, f, tol=1e-10, max_iter=200, method=1, pre=1, post=1, kind=0, omega=1.0, u0=None):
         u = self.vec() if u0 is None else np.ascontiguousarray(u0, np.float64).copy()

@@ -358,3 +358,68 @@ def test_mma_case3(oracle):
     ref = so.minimize(f, [0.0, 0.0], jac=df, bounds=[(-1, 1)] * 2, constraints=cons, method="SLSQP", tol=1e-12)
     assert np.allclose(x, ref.x, atol=2e-3)
     assert f(x) - ref.fun < 1e-4
+
+
+def free_box(ex=6, ey=4, ez=4):
+    """A support-free box, load set the x = ex face (normal +x)."""
+    em = np.ones((ez, ey, ex), np.uint8)
+    fa = np.zeros((ez + 1, ey + 1, ex + 1), np.uint8)
+    la = np.zeros_like(fa)
+    la[:, :, ex] = 1
+    nrm = np.zeros((fa.size, 3))
+    nrm[:, 0] = 1.0
+    rho = np.random.default_rng(8).uniform(0.3, 1.0, em.shape)
+    return dict(emask=em, fixed=fa, load=la, normals=nrm, rho=rho)
+
+
+@pytest.mark.parametrize("cf", [0, 1])
+def test_support_free_worst_case_vs_pseudo_inverse(oracle, cf):
+    """Support-free modes (nsff, nscf; optimization/optimization.cpp:99-117):
+    the oracle's coarsest pseudo-inverse, rigid-motion removal of loads
+    (forceProject, projection.cpp:289-360) and of displacements
+    (displacementProject, :374-411) against a dense pseudo-inverse of the
+    scipy-assembled K: solutions of consistent loads, the dense aggregated
+    worst case and Lanczos."""
+    prob = free_box()
+    o = oracle.Problem(prob["emask"], prob["fixed"], prob["load"], prob["normals"], n_levels=2, first_factor=2)
+    o.set_density(prob["rho"].ravel())
+    o.update_stencil()
+    K, _ = assemble(o, prob, oracle.k0())
+    Kp = np.linalg.pinv(K.toarray(), rcond=1e-10)
+    nn = o.nn
+    zz, yy, xx = np.meshgrid(np.arange(o.ez + 1), np.arange(o.ey + 1), np.arange(o.ex + 1), indexing="ij")
+    X = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], 1).astype(float)
+    R = rigid_modes(X)
+    Rf = np.stack([R[:, k].reshape(-1, 3).T.ravel() for k in range(6)], 1)  # SoA rows (c nn + n)
+    # consistent load: a random load on the load nodes without rigid part
+    rng = np.random.default_rng(3)
+    f = o.force_project(rng.standard_normal(3 * nn), cf)
+    assert np.abs(Rf.T @ f).max() < 1e-10 * np.linalg.norm(f) * np.abs(Rf).max()
+    u, _, rr = o.solve(f, tol=1e-12)
+    assert rr < 1e-12
+    assert np.abs(Rf.T @ u).max() < 1e-9 * np.linalg.norm(u) * np.abs(Rf).max()
+    assert np.linalg.norm(u - Kp @ f) < 1e-7 * np.linalg.norm(Kp @ f)
+    # dense worst case: lambda_max of K^+ over unit admissible loads
+    ln = o.load_nodes()
+    if cf:
+        B = np.zeros((3 * nn, len(ln)))
+        for k, n in enumerate(ln):
+            B[n, k] = 1.0  # normal +x
+    else:
+        B = np.zeros((3 * nn, 3 * len(ln)))
+        for k, n in enumerate(ln):
+            for c in range(3):
+                B[c * nn + n, 3 * k + c] = 1.0
+    # admissible subspace: span(B) without the rigid motions of the load set
+    Rl = B.T @ Rf  # in cf mode only the normal components: some motions vanish there
+    Ul, sl, _ = np.linalg.svd(Rl, full_matrices=False)
+    qr = Ul[:, sl > 1e-8 * sl.max()]
+    Pm = np.eye(B.shape[1]) - qr @ qr.T
+    w, V = np.linalg.eigh(Pm)
+    Z = V[:, w > 0.5]
+    lam_ref = np.linalg.eigvalsh(Z.T @ B.T @ Kp @ B @ Z).max()
+    lam_o, fo, uo = o.dense_worst(cf, tol=1e-12)
+    assert abs(lam_o - lam_ref) <= 1e-7 * lam_ref
+    assert abs(np.linalg.norm(fo) - 1) < 1e-9
+    lam_l, _, _, _ = o.lanczos(40, cf, tol=1e-11)
+    assert abs(lam_l - lam_ref) <= 1e-6 * lam_ref

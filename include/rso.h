@@ -182,7 +182,13 @@ void rso_default_config(rso_config* cfg);
  * buffers.  emask: ex*ey*ez bytes (1 = solid voxel).  fixed_area/load_area:
  * node masks (Nn bytes) that play the role of the reference's
  * _inFixedArea/_inLoadArea predicates; load_normals: 3*Nn unit normals used
- * in constrained-direction modes (may be NULL otherwise).
+ * in constrained-direction modes (may be NULL otherwise).  In the
+ * support-free modes (cfg->mode RSO_NO_SUPPORT_*, HierarchyGrid::Mode
+ * grid/Grid.h:170-175) no node is fixed and fixed_area is not read: the
+ * operator is singular on the rigid motions, the coarsest solve becomes a
+ * pseudo-inverse (the reference's BDCSVD, grid/Grid.cpp:4123-4185), every
+ * solution has its rigid motion removed (displacementProject) and every
+ * admissible load the rigid motions of the load set (forceProject).
  * Replaces HierarchyGrid::genFromMesh(solid_bit, reso) (grid/Grid.cpp:978-1237),
  * Grid::build (grid/Grid.cpp:2973-3215), computeProjectionMatrix
  * (grid/Grid.cpp:2694-2836), setNodes/setLoadNodes (optimization/projection.cpp:46-269)
@@ -425,8 +431,15 @@ rso_status rso_selfsupport(rso_handle* h, const float* coeff_dev, double beta, i
                            double* count, double* direction_sum);
 
 /* ---------------------------------------------------------------- worst case */
-/* forceProject (optimization/projection.cu:165-231, projection.cpp:289-360) */
+/* forceProject (optimization/projection.cu:165-231, projection.cpp:289-360):
+ * forces kept on the load nodes, only along the load normal in
+ * constrained-direction mode, and in support-free modes without the rigid
+ * motions of the load set (orthonormal, nearly dependent motions dropped) */
 rso_status rso_force_project(rso_handle* h, double* f_dev, int constrain_direction);
+/* displacementProject (optimization/projection.cpp:374-411): u minus its
+ * projection on the rigid motions of the active fine nodes; a no-op for
+ * problems with supports */
+rso_status rso_displacement_project(rso_handle* h, double* u_dev);
 /* worst-case load: lambda_max of P K^-1 P by Lanczos with full FP64
  * reorthogonalisation, one multigrid solve (to tol) per step.  Replaces
  * modifiedPM (optimization/optimization.cpp:215-353).  ritz_host may be NULL. */

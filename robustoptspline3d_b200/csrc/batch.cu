@@ -472,6 +472,7 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
     }
   }
   for (int b = 0; b < k; b++) {
+    RSO_TRY(displacement_project(h, B.x + b * n3));  // support-free problems
     RSO_TRY(unpad_nodes(h, 0, B.x + b * n3, U + b * nn3));
     if (rel[b] >= tol && fn[b] > 0) status = RSO_ERR_BUDGET_EXCEEDED;
   }

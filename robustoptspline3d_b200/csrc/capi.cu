@@ -114,6 +114,7 @@ static void free_handle(rso_handle* h) {
   cudaFree(h->filt_taps);
   batch_release(h);
   cudaFree(h->c_nodes); cudaFree(h->c_K); cudaFree(h->c_f); cudaFree(h->c_flag);
+  cudaFree(h->rigid_q); cudaFree(h->rigid_m); cudaFree(h->rigid_scr); cudaFree(h->c_R);
   cudaFree(h->red); cudaFree(h->scal); cudaFree(h->xfer); cudaFree(h->fpart);
   if (h->h_scal) cudaFreeHost(h->h_scal);
   cudaFree(h->x); cudaFree(h->r); cudaFree(h->p); cudaFree(h->q); cudaFree(h->z); cudaFree(h->w);
@@ -238,6 +239,7 @@ static rso_status setup(rso_handle* h, int ex, int ey, int ez, const uint8_t* em
     ALLOC(h->c_f, sizeof(double) * N);
     ALLOC(h->c_flag, sizeof(int));
   }
+  if (!h->has_support) RSO_TRY(rigid_setup(h));
   int counts[4];
   RSO_TRY(rso_ref_numbering(h, 0, counts, nullptr, nullptr, nullptr, nullptr, nullptr));
   h->n_gs_elements = counts[3];
@@ -301,12 +303,15 @@ extern "C" rso_status rso_create(const rso_config* cfg, int ex, int ey, int ez, 
     delete h;
     return RSO_ERR_INVALID_ARG;
   }
-  if (h->cfg.mode == RSO_NO_SUPPORT_CONSTRAIN_FORCE_DIRECTION || h->cfg.mode == RSO_NO_SUPPORT_FREE_FORCE) {
-    // the dense coarsest solve needs supports (a support-free operator is singular)
-    g_create_err = "support-free modes are not supported";
+  if (h->cfg.mode < RSO_NO_SUPPORT_CONSTRAIN_FORCE_DIRECTION || h->cfg.mode > RSO_WITH_SUPPORT_FREE_FORCE) {
     delete h;
-    return RSO_ERR_UNSUPPORTED;
+    return RSO_ERR_INVALID_ARG;
   }
+  // support-free modes: no node is fixed (the fixed area is not read); the
+  // operator is singular on the rigid motions, handled by rigid.cu
+  h->has_support = h->cfg.mode == RSO_WITH_SUPPORT_CONSTRAIN_FORCE_DIRECTION ||
+                   h->cfg.mode == RSO_WITH_SUPPORT_FREE_FORCE;
+  if (!h->has_support) fa = nullptr;
   if (rso_status sm = claim_material(h); sm != RSO_OK) {
     delete h;
     return sm;

@@ -1247,12 +1247,26 @@ rso_status coarsest_factor(rso_handle* h) {
   k_coarse_dense<<<cdiv((long long)h->nc * 243, 256), 256, 0, h->stream>>>(c, c.st64, h->c_nodes,
                                                                            h->c_nodes + h->nc, h->nc, h->c_K); rso::note_launch();
   RSO_TRY(launch_check(h, "coarsest assembly"));
+  // support-free problems: K is singular on the rigid motions R of the
+  // coarsest nodes; the pseudo-inverse (the reference's BDCSVD solve,
+  // grid/Grid.cpp:4123-4185) is (K + a R R^T)^-1 - R R^T / a, a the mean diagonal
+  double a_rig = 0;
+  if (!h->has_support && h->c_R) {
+    RSO_TRY(dense_trace(h, h->c_K, N, h->c_f));
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(&a_rig, h->c_f, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+    a_rig /= N;
+    if (!(a_rig > 0)) { h->err = "coarsest operator has no positive diagonal"; return RSO_ERR_STATE; }
+    RSO_TRY(dense_rank_update(h, h->c_K, N, h->c_R, 6, a_rig));
+  }
   RSO_TRY(dense_spd_inverse(h, h->c_K, h->c_K + (size_t)N * N, h->c_K + 2 * (size_t)N * N, N, h->c_flag));
+  if (a_rig > 0) RSO_TRY(dense_rank_update(h, h->c_K + (size_t)N * N, N, h->c_R, 6, -1.0 / a_rig));
   int flag = 0;
   RSO_CHECK_CUDA(h, cudaMemcpyAsync(&flag, h->c_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   if (flag) {
-    h->err = "coarsest operator is not positive definite (a support-free mode needs the pseudo-inverse path)";
+    h->err = h->has_support ? "coarsest operator is not positive definite (no support node reaches it?)"
+                            : "coarsest operator is singular beyond the rigid motions (disconnected parts?)";
     return RSO_ERR_UNSUPPORTED;
   }
   return RSO_OK;

@@ -309,6 +309,26 @@ rso_status dense_spd_inverse(rso_handle* h, double* A, double* X, double* Y, int
   return launch_check(h, "coarsest dense inverse");
 }
 
+__global__ void k_trace(const double* __restrict__ A, int N, double* out) {
+  __shared__ double ws[32];
+  double s = 0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) s += A[(long long)i * N + i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += ws[w];
+    *out = t;
+  }
+}
+
+rso_status dense_trace(rso_handle* h, const double* A, int N, double* out) {
+  k_trace<<<1, 1024, 0, h->stream>>>(A, N, out); rso::note_launch();
+  return launch_check(h, "coarsest trace");
+}
+
 rso_status dense_rank_update(rso_handle* h, double* A, int N, const double* R, int nr, double a) {
   k_rank_update<<<(unsigned)cdiv((long long)N * N, 256), 256, 0, h->stream>>>(A, N, R, nr, a); rso::note_launch();
   return launch_check(h, "coarsest rank update");

@@ -116,6 +116,16 @@ struct rso_handle {
   double* c_K = nullptr;              // N x N workspace / inverse
   double* c_f = nullptr;
   int* c_flag = nullptr;              // factorisation status
+  // support-free problems (RSO_NO_SUPPORT_* modes, rigid.cu): the rigid
+  // motions of the load set (orthonormal, load space, ff and normal-projected
+  // cf), the inverse Gram matrix of the fine nodes' rigid motions about their
+  // centroid (displacement projection), and those of the coarsest nodes
+  bool has_support = true;
+  double* rigid_q = nullptr;          // [2][6][3 n_load]
+  int rigid_k[2] = {0, 0};
+  double* rigid_m = nullptr;          // 6 x 6 inverse Gram matrix, then the centroid (39 doubles)
+  double* rigid_scr = nullptr;        // partial sums of the projections
+  double* c_R = nullptr;              // coarsest rigid motions, 3 nc x 6 row-major, orthonormal
   // reductions
   double* red = nullptr;              // partials
   double* xfer = nullptr;             // restriction scratch: z-filtered fine columns
@@ -323,6 +333,15 @@ rso_status spline_setup(rso_handle* h, int order, int px, int py, int pz);
 
 // worst case (worst.cu)
 rso_status force_project(rso_handle* h, double* f_pad, int cf);
+// support-free problems (rigid.cu): set-up of the rigid motions; removal of
+// the load set's rigid motions from a load-space vector (3 per load node);
+// removal of the fine nodes' rigid motions from a padded FP64 nodal vector
+// (displacementProject); both no-ops when the problem has supports
+rso_status rigid_setup(rso_handle* h);
+rso_status rigid_project_load(rso_handle* h, double* v, int cf);
+rso_status displacement_project(rso_handle* h, double* u_pad);
+// sum of the diagonal of a dense N x N matrix into *out (device)
+rso_status dense_trace(rso_handle* h, const double* A, int N, double* out_dev);
 rso_status worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t seed, double* f_pad,
                       double* u_pad, double* lambda, double* ritz, int* iters);
 rso_status modified_pm(rso_handle* h, int cf, uint64_t seed, int max_itn, double* f_pad, double* u_pad,

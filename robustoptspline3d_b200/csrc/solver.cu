@@ -536,6 +536,7 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
   }
   *used = it;
   if (*stalled) return RSO_OK;
+  RSO_TRY(displacement_project(h, x));  // support-free problems: no rigid motion in the solution
   RSO_TRY(fine_stage_check(h));
   if (info) { info->iterations = it; info->rel_res = rel; }
   if (rel >= tol && fn > 0) { h->err = "PCG did not reach the tolerance within max_iter"; return RSO_ERR_BUDGET_EXCEEDED; }
@@ -612,6 +613,7 @@ rso_status solve_pcg(rso_handle* h, const double* f, double* x, double tol, int 
       RSO_TRY(launch_check(h, "pcg"));
     }
   }
+  RSO_TRY(displacement_project(h, x));
   RSO_TRY(fine_stage_check(h));
   if (info) { info->iterations = it + used; info->rel_res = rel; }
   if (rel >= tol && fn > 0) { h->err = "PCG did not reach the tolerance within max_iter"; return RSO_ERR_BUDGET_EXCEEDED; }
@@ -639,6 +641,7 @@ rso_status solve_vcycles(rso_handle* h, const double* f, double* x, double tol, 
     it++;
     if (!std::isfinite(rel) || rel > 1e4) { h->err = "defect correction diverged"; return RSO_ERR_DIVERGED; }
   }
+  RSO_TRY(displacement_project(h, x));
   RSO_TRY(fine_stage_check(h));
   if (info) { info->iterations = it; info->rel_res = rel; }
   if (rel >= tol && fn > 0) { h->err = "V-cycle iteration did not reach the tolerance"; return RSO_ERR_BUDGET_EXCEEDED; }

@@ -121,6 +121,7 @@ rso_status force_project(rso_handle* h, double* f, int cf) {
   }
   double* v = h->wc_buf + 2 * ls;
   if (nl) { k_gather_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(f, l.NP, h->load_nodes, h->load_normals, nl, cf, v); rso::note_launch(); }
+  RSO_TRY(rigid_project_load(h, v, cf));  // support-free problems: f -= Rd Rd^T f
   RSO_CHECK_CUDA(h, cudaMemsetAsync(f, 0, sizeof(double) * 3 * l.NP, h->stream));
   if (nl) { k_scatter_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(v, h->load_nodes, nl, l.NP, 1.0, f); rso::note_launch(); }
   return launch_check(h, "force_project");
@@ -193,6 +194,7 @@ rso_status worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t see
   double *part = rw, *s1 = rw + MD_MAX * MD_PARTS, *s2 = s1 + MD_MAX, *ab = s2 + MD_MAX;
   k_rand_load<<<cdiv(ls, 128), 128, 0, h->stream>>>(V, nl, seed); rso::note_launch();
   if (cf) { k_project_ls<<<cdiv(nl, 128), 128, 0, h->stream>>>(V, h->load_normals, nl); rso::note_launch(); }
+  RSO_TRY(rigid_project_load(h, V, cf));
   double nv = 0;
   RSO_TRY(dot_host(h, V, V, ls, &nv));
   RSO_TRY(axpby(h, ls, 0.0, V, 1.0 / std::sqrt(nv), V));
@@ -209,6 +211,7 @@ rso_status worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t see
     RSO_TRY(solve_pcg(h, h->w, u, tol, 4000, &si));
     total_it += si.iterations;
     k_gather_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(u, l0.NP, h->load_nodes, h->load_normals, nl, cf, wv); rso::note_launch();
+    RSO_TRY(rigid_project_load(h, wv, cf));
     // alpha = v . w is the first pass's coefficient on v (the newest vector)
     RSO_TRY(reorthogonalise(h, V, ls, it + 1, wv, part, s1));
     RSO_TRY(reorthogonalise(h, V, ls, it + 1, wv, part, s2));
@@ -267,6 +270,7 @@ rso_status modified_pm(rso_handle* h, int cf, uint64_t seed, int max_itn, double
   while (itn++ < max_itn && (fch > 1e-4 || rr > 1e-2)) {
     RSO_TRY(vcycle_fp64(h, u, f, 1, 1, 0, &rr));
     if (!std::isfinite(rr) || rr > 1e4) { h->err = "modified power method diverged"; return RSO_ERR_DIVERGED; }
+    RSO_TRY(displacement_project(h, u));  // support-free problems (optimization.cpp:284-286)
     RSO_CHECK_CUDA(h, cudaMemcpyAsync(f, u, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
     RSO_TRY(force_project(h, f, cf));
     RSO_TRY(dot_host(h, f, f, n3, &fn2));

@@ -106,6 +106,7 @@ SIGNATURES = {
     "rso_set_vcycle_graphs": (_ci, [_vp, _ci]),
     "rso_set_krylov_fp32": (_ci, [_vp, _cd]),
     "rso_set_krylov_fp32_cycles": (_ci, [_vp, _ci]),
+    "rso_displacement_project": (_ci, [_vp, _vp]),
     "rso_voxelize": (_ci, [ctypes.POINTER(ctypes.c_float), _ci, ctypes.POINTER(ctypes.c_int), _ci, _ci, _pu8, _pi,
                            ctypes.POINTER(ctypes.c_float)]),
     "rso_shell_elements": (_ci, [ctypes.POINTER(ctypes.c_float), _ci, ctypes.POINTER(ctypes.c_int), _ci,
@@ -685,6 +686,13 @@ class HierarchyGrid:
         f = f.clone()
         self._chk(self.lib.rso_force_project(self.h, _dev(f, torch.float64), int(constrain_direction)), "rso_force_project")
         return f
+
+    def displacementProject(self, u):
+        """u without the rigid motion of the active nodes (support-free modes; a copy)."""
+        import torch
+        u = u.clone()
+        self._chk(self.lib.rso_displacement_project(self.h, _dev(u, torch.float64)), "rso_displacement_project")
+        return u
 
     def worst_case(self, steps=20, constrain_direction=0, tol=1e-6, seed=1234):
         import torch

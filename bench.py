@@ -187,7 +187,21 @@ def oracle_design_iteration(O, n, em, fa, la, order, parts, coeff, beta=8.0):
     m = O.MMA(len(coeff), 2, 0.0, 1.0)
     m.set_x(coeff)
     m.update(dc * 1e6, np.stack([dv * 1e3, dss * 1e3]), np.array([1e3 * (rho.mean() - 0.3), 1e3 * ssv]))
-    return lam
+    return lam, p.solve_iterations()
+
+
+def cpu_samples(O, sizes, coeff):
+    """One FP64 oracle design iteration per sample size: seconds, PCG
+    iterations over the 20 Lanczos solves, and microseconds per element and
+    PCG iteration (flat when the cost scales with elements x iterations)."""
+    out = []
+    for nr in sizes:
+        emr, far, lar, order, parts, _ = problem(nr)
+        t0 = time.perf_counter()
+        _, its = oracle_design_iteration(O, nr, emr, far, lar, order, parts, coeff)
+        dt = time.perf_counter() - t0
+        out.append({"n": nr, "s": dt, "pcg_iterations": int(its), "us_per_element_iteration": 1e6 * dt / (nr ** 3 * its)})
+    return out
 
 
 def smoother_id(R):
@@ -575,6 +589,8 @@ def main():
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--ref-size", type=int, default=24)
+    ap.add_argument("--ref-sizes", default="24,32,48",
+                    help="sample sizes of the CPU baseline leg (the largest is scaled to 256^3)")
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
@@ -755,13 +771,19 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         from oracle import oracle as O
-        nr = args.ref_size
-        emr, far, lar, _, _, _ = problem(nr)
-        t0 = time.perf_counter()
-        oracle_design_iteration(O, nr, emr, far, lar, order, parts, coeff)
-        dt = time.perf_counter() - t0
-        cpu = {"value": 1.0 / (dt * (256.0 / nr) ** 3), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-               "sample": f"one FP64 oracle design iteration at {nr}^3 took {dt:.2f} s, scaled by (256/{nr})^3"}
+        sizes = [int(v) for v in args.ref_sizes.split(",")]
+        samples = cpu_samples(O, sizes, coeff)
+        big = samples[-1]
+        # scaled from the largest sample by the element count and by the PCG
+        # iterations of this run's own 256^3 iteration (the oracle's count
+        # grows slowly with size; the samples show by how much)
+        its256 = infos[-1]["solve_iterations"]
+        per = big["s"] * (256.0 / big["n"]) ** 3 * max(1.0, its256 / big["pcg_iterations"])
+        cpu = {"value": 1.0 / per, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": (f"one FP64 oracle design iteration at each of {', '.join(f'{v}^3' for v in sizes)}; "
+                          f"the {big['n']}^3 one ({big['s']:.2f} s, {big['pcg_iterations']} PCG iterations) scaled by "
+                          f"(256/{big['n']})^3 and by max(1, {its256} / {big['pcg_iterations']}) iterations"),
+               "samples": samples}
     clocks = clk.summary()
     # the fine operator's binding roof is the FP32 CUDA-core pipe, not HBM:
     # algorithmic flops per second against 148 SMs x 128 lanes x 2 flop per

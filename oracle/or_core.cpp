@@ -199,6 +199,7 @@ extern "C" or_problem* or_create(int ex, int ey, int ez, const uint8_t* emask,
 }
 
 extern "C" void or_destroy(or_problem* p) { delete p; }
+extern "C" long or_solve_iterations(const or_problem* p) { return p->solve_iters; }
 extern "C" int or_n_levels(const or_problem* p) { return (int)p->L.size(); }
 extern "C" void or_level_dims(const or_problem* p, int level, int* d) {
   const Level& l = p->L[level];
@@ -886,6 +887,7 @@ extern "C" int or_solve(or_problem* p, double* u, const double* f, double tol, i
       it++;
       if (rr < tol) break;
     }
+    p->solve_iters += it;
     displacement_project(p, u);
     if (rel_res) *rel_res = rr;
     return it;
@@ -917,6 +919,7 @@ extern "C" int or_solve(or_problem* p, double* u, const double* f, double tol, i
     rz = rz2;
     for (long i = 0; i < 3 * nn; i++) pp[i] = z[i] + beta * pp[i];
   }
+  p->solve_iters += it;
   // support-free problems: the solution without rigid motion (displacementProject)
   displacement_project(p, u);
   // true residual

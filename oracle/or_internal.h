@@ -41,6 +41,7 @@ struct or_problem {
   std::vector<long> crow;                 // node -> row block (-1 absent)
   std::vector<double> Kinv;               // dense inverse (3nc x 3nc)
   int nc = 0;
+  long solve_iters = 0;                   // iterations of every or_solve so far (bench statistics)
   std::vector<double> lam;                // lambda_max(D^-1 K) estimate per level
   // spline
   int order = 0, part[3] = {0, 0, 0}, nb[3] = {0, 0, 0};

@@ -135,6 +135,8 @@ void or_force_project(const or_problem* p, double* f, int constrain_direction);
 /* displacementProject (optimization/projection.cpp:374-411): u -= R R^T u over
  * the rigid motions of the active fine nodes; a no-op with supports */
 void or_displacement_project(const or_problem* p, double* u);
+/* iterations of all solves on this problem so far */
+long or_solve_iterations(const or_problem* p);
 int  or_n_load(const or_problem* p);
 /* dense aggregated worst case: lambda_max of P K^-1 P on the load space and
  * the worst unit force (utils/test_utils.cpp:2598-2645, 2859-2928) */

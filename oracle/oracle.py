@@ -63,6 +63,7 @@ def _load():
         "or_element_energy": (None, [_vp, _d, _d]),
         "or_heaviside": (None, [ctypes.c_int, _d, ctypes.c_double, ctypes.c_double, _u8, _d]),
         "or_displacement_project": (None, [ctypes.c_void_p, _d]),
+        "or_solve_iterations": (ctypes.c_long, [ctypes.c_void_p]),
         "or_ss_funcs": (None, [ctypes.c_int, _d, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                ctypes.c_double, _d]),
         "or_heaviside_chain": (None, [ctypes.c_int, _d, ctypes.c_double, _d, _d]),
@@ -279,6 +280,10 @@ class Problem:
         rr = lib().or_vcycle(self.h, _p(u), _p(np.ascontiguousarray(f, np.float64)), pre, post, kind, omega,
                              symmetric)
         return u, rr
+
+    def solve_iterations(self):
+        """Iterations of all solves on this problem so far."""
+        return lib().or_solve_iterations(self.h)
 
     def displacement_project(self, u):
         """u without rigid motion (a no-op for problems with supports)."""

@@ -182,10 +182,10 @@ static rso_status setup(rso_handle* h, int ex, int ey, int ez, const uint8_t* em
     if (li > 0) {
       ALLOC(l.KE, sizeof(double) * 576 * l.ne);
       ALLOC(l.st64, sizeof(double) * 243 * l.NP);
-      ALLOC(l.st32, sizeof(float) * 243 * l.NP);
+      ALLOC(l.st32, sizeof(float) * st32_len(l.NP));
       RSO_CHECK_CUDA(h, cudaMemset(l.KE, 0, sizeof(double) * 576 * l.ne));
       RSO_CHECK_CUDA(h, cudaMemset(l.st64, 0, sizeof(double) * 243 * l.NP));
-      RSO_CHECK_CUDA(h, cudaMemset(l.st32, 0, sizeof(float) * 243 * l.NP));
+      RSO_CHECK_CUDA(h, cudaMemset(l.st32, 0, sizeof(float) * st32_len(l.NP)));
     }
   }
   Level& l0 = h->L[0];

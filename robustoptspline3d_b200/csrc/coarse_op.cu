@@ -37,9 +37,9 @@ __device__ __forceinline__ void stencil_apply(const Level& L, const T* __restric
 #pragma unroll
     for (int r = 0; r < 3; r++) {
       T s = acc[r];
-      s = fma(st[(d * 9 + r * 3 + 0) * NP + n], u0, s);
-      s = fma(st[(d * 9 + r * 3 + 1) * NP + n], u1, s);
-      s = fma(st[(d * 9 + r * 3 + 2) * NP + n], u2, s);
+      s = fma(st[st_at<T>(NP, d * 9 + r * 3 + 0, n)], u0, s);
+      s = fma(st[st_at<T>(NP, d * 9 + r * 3 + 1, n)], u1, s);
+      s = fma(st[st_at<T>(NP, d * 9 + r * 3 + 2, n)], u2, s);
       acc[r] = s;
     }
   }
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(256) k_coarse(const Level L, const T* __restri
       for (int r = 0; r < 3; r++)
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-          const T sv = st[(d * 9 + r * 3 + c) * NP + n];
+          const T sv = st[st_at<T>(NP, d * 9 + r * 3 + c, n)];
 #pragma unroll
           for (int j = 0; j < KB; j++)
             if (j < nv) acc[j][r] = fma(sv, u[(b0 + j) * VS + nbr + c * NP], acc[j][r]);
@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(256) k_coarse(const Level L, const T* __restri
   T S[9];
   if (MODE == 2 && act) {
 #pragma unroll
-    for (int i = 0; i < 9; i++) S[i] = st[(13 * 9 + i) * NP + n];
+    for (int i = 0; i < 9; i++) S[i] = st[st_at<T>(NP, 13 * 9 + i, n)];
   }
 #pragma unroll
   for (int j = 0; j < KB; j++) {
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(256) k_coarse4(const Level L, const float* __r
       for (int r = 0; r < 3; r++)
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-          const float4 sv = *reinterpret_cast<const float4*>(st + (d * 9 + r * 3 + c) * NP + p0);
+          const float4 sv = *reinterpret_cast<const float4*>(st + st_at<float>(NP, d * 9 + r * 3 + c, p0));
           acc[r][0] = fmaf(sv.x, un[c][0], acc[r][0]);
           acc[r][1] = fmaf(sv.y, un[c][1], acc[r][1]);
           acc[r][2] = fmaf(sv.z, un[c][2], acc[r][2]);
@@ -261,14 +261,12 @@ __global__ void __launch_bounds__(32 * CTY * 3) k_coarse_r(const Level L, const 
   const bool act = in && (L.vclass[n] & NC_ACTIVE) != 0;
   T acc = 0;
   if (act) {
-    const T* sr = st + (long long)(r * 3) * NP + n;
 #pragma unroll
     for (int d = 0; d < 27; d++) {
       const long long nb = n + (d % 3 - 1) + (d / 3 % 3 - 1) * px + (d / 9 - 1) * pxy;
-      const T* sd = sr + (long long)(d * 9) * NP;
-      acc = fma(sd[0], u[nb], acc);
-      acc = fma(sd[NP], u[nb + NP], acc);
-      acc = fma(sd[2 * NP], u[nb + 2 * NP], acc);
+      acc = fma(st[st_at<T>(NP, d * 9 + r * 3 + 0, n)], u[nb], acc);
+      acc = fma(st[st_at<T>(NP, d * 9 + r * 3 + 1, n)], u[nb + NP], acc);
+      acc = fma(st[st_at<T>(NP, d * 9 + r * 3 + 2, n)], u[nb + 2 * NP], acc);
     }
   }
   if (MODE == 0) {
@@ -282,7 +280,7 @@ __global__ void __launch_bounds__(32 * CTY * 3) k_coarse_r(const Level L, const 
   if (!act) { out[n + r * NP] = 0; return; }
   T S[9];
 #pragma unroll
-  for (int i = 0; i < 9; i++) S[i] = st[(13 * 9 + i) * NP + n];
+  for (int i = 0; i < 9; i++) S[i] = st[st_at<T>(NP, 13 * 9 + i, n)];
   // row r of the adjugate of the 3x3 diagonal block
   const T c00 = S[4] * S[8] - S[5] * S[7], c01 = -(S[3] * S[8] - S[5] * S[6]), c02 = S[3] * S[7] - S[4] * S[6];
   const T det = S[0] * c00 + S[1] * c01 + S[2] * c02;
@@ -316,8 +314,8 @@ __global__ void __launch_bounds__(256) k_coarse_gs(const Level L, const T* __res
     T s = f[n + r * NP] - acc[r];
 #pragma unroll
     for (int c = 0; c < 3; c++)
-      if (c != r) s -= st[(13 * 9 + r * 3 + c) * NP + n] * v[c];
-    v[r] = s / st[(13 * 9 + r * 3 + r) * NP + n];
+      if (c != r) s -= st[st_at<T>(NP, 13 * 9 + r * 3 + c, n)] * v[c];
+    v[r] = s / st[st_at<T>(NP, 13 * 9 + r * 3 + r, n)];
   }
   u[n] = v[0]; u[n + NP] = v[1]; u[n + 2 * NP] = v[2];
 }
@@ -708,7 +706,7 @@ __global__ void k_assemble(const Level C, const double* __restrict__ KE, double*
 #pragma unroll
   for (int i = 0; i < 9; i++) {
     st64[(d * 9 + i) * NP + n] = s[i];
-    st32[(d * 9 + i) * NP + n] = (float)s[i];
+    st32[st_at<float>(NP, d * 9 + i, n)] = (float)s[i];
   }
 }
 
@@ -814,7 +812,7 @@ __device__ void bot_jacobi(const Level& L, const T* st, const T* u0v, const T* f
     if (!zero) stencil_apply<T>(L, st, u, n, false, acc);
     T S[9];
 #pragma unroll
-    for (int k = 0; k < 9; k++) S[k] = st[(13 * 9 + k) * NP + n];
+    for (int k = 0; k < 9; k++) S[k] = st[st_at<T>(NP, 13 * 9 + k, n)];
     const T r0 = f[n] - acc[0], r1 = f[n + NP] - acc[1], r2 = f[n + 2 * NP] - acc[2];
     const T A = S[4] * S[8] - S[5] * S[7], B = -(S[3] * S[8] - S[5] * S[6]), C = S[3] * S[7] - S[4] * S[6];
     const T det = S[0] * A + S[1] * B + S[2] * C;

@@ -35,7 +35,7 @@ struct Level {
   uint8_t* vclass = nullptr;      // padded node class
   double* KE = nullptr;           // coarse element matrices, 576 per unpadded element
   double* st64 = nullptr;         // stencil [243][NP]
-  float* st32 = nullptr;
+  float* st32 = nullptr;          // stencil in tiles of 128 nodes (st_at), 243 x round_up(NP, 128)
   double *u64 = nullptr, *f64 = nullptr, *r64 = nullptr, *t64 = nullptr;
   float *u32 = nullptr, *f32 = nullptr, *r32 = nullptr, *t32 = nullptr;
   double lam = 1.0;               // lambda_max(D^-1 K) estimate
@@ -46,6 +46,21 @@ struct Level {
     return (long long)(x + 1) + (long long)qx * ((y + 1) + (long long)qy * (z + 1));
   }
 };
+
+// Index of stencil entry k (0..242) of padded node n.  FP64 stencils are
+// [243][NP]; FP32 stencils, the ones the mixed V-cycle streams, are stored in
+// tiles of 128 consecutive padded nodes, [NP/128][243][128], so that the
+// threads of a warp reading a run of nodes stream one contiguous block
+// (243 x 512 bytes) instead of 243 blocks of 512 bytes a stencil row apart.
+constexpr long long ST_TILE = 128;
+template <typename T>
+__host__ __device__ __forceinline__ long long st_at(long long NP, int k, long long n) {
+  if constexpr (sizeof(T) == 4) return ((n / ST_TILE) * 243 + k) * ST_TILE + (n % ST_TILE);
+  else return (long long)k * NP + n;
+}
+__host__ __device__ __forceinline__ long long st32_len(long long NP) {
+  return 243 * ((NP + ST_TILE - 1) / ST_TILE) * ST_TILE;
+}
 
 // Level is passed to kernels by value: it must stay a plain, trivially
 // copyable record (host-side data such as the unpadded masks lives in the

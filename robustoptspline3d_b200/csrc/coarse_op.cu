@@ -108,47 +108,64 @@ __global__ void __launch_bounds__(256) k_coarse(const Level L, const T* __restri
   }
 }
 
-// FP32 variant for large single-system levels: a thread owns four
-// consecutive padded nodes (px is a multiple of 4, so a group never spans two
-// rows and starts on 16 bytes) and streams the 243 stencil rows, f, the
-// iterate and the node classes with 16-byte loads; the neighbour values of a
-// row of the 3 x 3 x 3 neighbourhood come as one 16-byte load and two scalar
-// ones.  Halo rows are skipped, halo and inactive nodes of a group are written
-// as the per-node kernel leaves them (zero, or f for the residual).
+// FP32 variant for large single-system levels.  A group of four consecutive
+// padded nodes (px is a multiple of 4, so a group never spans two rows and
+// starts on 16 bytes) is taken by three threads, one per neighbour plane
+// dz = -1, 0, +1: each streams the 81 stencil entries of its 9 neighbours
+// (16-byte loads from the tiled FP32 stencil) and their values (one 16-byte
+// load and two scalars per neighbour row), so three times the threads are in
+// flight and each one's chain of loads is a third as long (the levels are a
+// few hundred thousand nodes: one thread per group left the GPU under a wave,
+// bound by each thread's latency).  The partial sums of planes -1 and +1 meet
+// the centre plane's thread in shared memory, which adds them in a fixed
+// order and finishes the node (residual, or damped block Jacobi / Chebyshev
+// step with the diagonal block of its own plane).  Halo rows are skipped;
+// halo and inactive nodes of a group are written as the per-node kernel
+// leaves them (zero, or f for the residual).
+constexpr int C4G = 64;  // node groups per CTA (blockDim (C4G, 3))
 template <int MODE>
-__global__ void __launch_bounds__(256) k_coarse4(const Level L, const float* __restrict__ st,
-                                                 const float* __restrict__ u, const float* __restrict__ f,
-                                                 float* __restrict__ out, float omega,
-                                                 const float* __restrict__ uprev, float c1) {
-  const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(C4G * 3, 3) k_coarse4(const Level L, const float* __restrict__ st,
+                                                     const float* __restrict__ u, const float* __restrict__ f,
+                                                     float* __restrict__ out, float omega,
+                                                     const float* __restrict__ uprev, float c1) {
+  __shared__ float red[2][12][C4G];
+  const int tg = threadIdx.x, pz = threadIdx.y;  // neighbour plane dz = pz - 1
+  const long long g = blockIdx.x * (long long)C4G + tg;
   const long long NP = L.NP, px = L.px, pxy = (long long)L.px * L.py;
   const long long p0 = 4 * g;
-  if (p0 >= NP) return;
-  const int zp = (int)(p0 / pxy);
-  const long long rem = p0 - zp * pxy;
-  const int yp = (int)(rem / px), xp = (int)(rem - yp * px);
-  if (zp < 1 || zp > L.nz || yp < 1 || yp > L.ny) return;  // halo row: stays zero
-  const uchar4 cl4 = *reinterpret_cast<const uchar4*>(L.vclass + p0);
-  const uint8_t cls[4] = {cl4.x, cl4.y, cl4.z, cl4.w};
-  bool act[4];
+  bool work = p0 < NP;
+  int xp = 0;
+  bool act[4] = {false, false, false, false};
+  if (work) {
+    const int zp = (int)(p0 / pxy);
+    const long long rem = p0 - zp * pxy;
+    const int yp = (int)(rem / px);
+    xp = (int)(rem - yp * px);
+    work = !(zp < 1 || zp > L.nz || yp < 1 || yp > L.ny);  // halo row: stays zero
+  }
   bool any = false;
+  if (work) {
+    const uchar4 cl4 = *reinterpret_cast<const uchar4*>(L.vclass + p0);
+    const uint8_t cls[4] = {cl4.x, cl4.y, cl4.z, cl4.w};
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const int x = xp + k - 1;  // node x index
-    act[k] = x >= 0 && x < L.nx && (cls[k] & NC_ACTIVE);
-    any = any || act[k];
+    for (int k = 0; k < 4; k++) {
+      const int x = xp + k - 1;  // node x index
+      act[k] = x >= 0 && x < L.nx && (cls[k] & NC_ACTIVE);
+      any = any || act[k];
+    }
   }
   float acc[3][4];
 #pragma unroll
   for (int r = 0; r < 3; r++)
 #pragma unroll
     for (int k = 0; k < 4; k++) acc[r][k] = 0.f;
-  float S[9][4];
   if (any) {
+    const long long pl = p0 + (long long)(pz - 1) * pxy;
 #pragma unroll
-    for (int d = 0; d < 27; d++) {
-      const long long nb = p0 + (d / 3 % 3 - 1) * px + (d / 9 - 1) * pxy;  // same row offset, dx below
-      const int dx = d % 3 - 1;
+    for (int e = 0; e < 9; e++) {
+      const int d = pz * 9 + e;
+      const long long nb = pl + (e / 3 - 1) * px;  // same row offset, dx below
+      const int dx = e % 3 - 1;
       float un[3][4];
 #pragma unroll
       for (int c = 0; c < 3; c++) {
@@ -174,12 +191,22 @@ __global__ void __launch_bounds__(256) k_coarse4(const Level L, const float* __r
           acc[r][1] = fmaf(sv.y, un[c][1], acc[r][1]);
           acc[r][2] = fmaf(sv.z, un[c][2], acc[r][2]);
           acc[r][3] = fmaf(sv.w, un[c][3], acc[r][3]);
-          if (MODE == 2 && d == 13) {
-            S[r * 3 + c][0] = sv.x; S[r * 3 + c][1] = sv.y; S[r * 3 + c][2] = sv.z; S[r * 3 + c][3] = sv.w;
-          }
         }
     }
   }
+  if (pz != 1) {
+    const int slot = pz >> 1;  // plane -1 -> 0, plane +1 -> 1
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) red[slot][r * 4 + k][tg] = acc[r][k];
+  }
+  __syncthreads();
+  if (pz != 1 || !work) return;
+#pragma unroll
+  for (int r = 0; r < 3; r++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) acc[r][k] = (red[0][r * 4 + k][tg] + acc[r][k]) + red[1][r * 4 + k][tg];
   float res[3][4];
 #pragma unroll
   for (int r = 0; r < 3; r++) {
@@ -203,6 +230,14 @@ __global__ void __launch_bounds__(256) k_coarse4(const Level L, const float* __r
     float4 pv = make_float4(0.f, 0.f, 0.f, 0.f);
     if (uprev) pv = *reinterpret_cast<const float4*>(uprev + p0 + r * NP);
     up[r][0] = pv.x; up[r][1] = pv.y; up[r][2] = pv.z; up[r][3] = pv.w;
+  }
+  // the diagonal blocks, re-read (the centre plane's thread streamed them a
+  // moment ago: cache hits) rather than held in registers through the loop
+  float S[9][4];
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    const float4 sv = *reinterpret_cast<const float4*>(st + st_at<float>(NP, 13 * 9 + i, p0));
+    S[i][0] = sv.x; S[i][1] = sv.y; S[i][2] = sv.z; S[i][3] = sv.w;
   }
   float o[3][4];
 #pragma unroll
@@ -1033,7 +1068,7 @@ rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* 
   if (h->prof_on) prof_begin(h, cls, (double)l.nn);
   if (node_per_thread(h, level)) {
     if (l.nb == 1 && sizeof(T) == 4) {
-      k_coarse4<0><<<cdiv(l.NP / 4, 256), 256, 0, h->stream>>>(l, (const float*)stencil_of<T>(l), (const float*)u,
+      k_coarse4<0><<<cdiv(l.NP / 4, C4G), dim3(C4G, 3), 0, h->stream>>>(l, (const float*)stencil_of<T>(l), (const float*)u,
                                                                (const float*)f, (float*)r, 0.f, nullptr, 0.f);
     } else if (l.nb == 1) {
       k_coarse<T, 0, 1><<<chunk_grid(l, 1), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0));
@@ -1055,7 +1090,7 @@ rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T*
   if (h->prof_on) prof_begin(h, cls, (double)l.nn);
   if (node_per_thread(h, level)) {
     if (l.nb == 1 && sizeof(T) == 4) {
-      k_coarse4<2><<<cdiv(l.NP / 4, 256), 256, 0, h->stream>>>(l, (const float*)stencil_of<T>(l), (const float*)u_in,
+      k_coarse4<2><<<cdiv(l.NP / 4, C4G), dim3(C4G, 3), 0, h->stream>>>(l, (const float*)stencil_of<T>(l), (const float*)u_in,
                                                                (const float*)f, (float*)u_out, (float)omega,
                                                                (const float*)u_prev, (float)c1);
     } else if (l.nb == 1) {

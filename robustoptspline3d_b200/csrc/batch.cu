@@ -287,6 +287,7 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
     RSO_TRY(pad_nodes(h, 0, F + b * nn3, fpad + b * n3));
     RSO_TRY(zero_support(h, B.x + b * n3));
     RSO_TRY(zero_support(h, fpad + b * n3));
+    RSO_TRY(displacement_project(h, fpad + b * n3));  // support-free problems, as rso_solve
   }
   std::vector<int> it(k, 0), done(k, 0);
   std::vector<double> fn(k, 0), rel(k, 0);

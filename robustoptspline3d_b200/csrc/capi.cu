@@ -617,6 +617,9 @@ extern "C" rso_status rso_solve(rso_handle* h, const double* f, double* u, doubl
   RSO_TRY(pad_nodes(h, 0, f, h->w));
   RSO_TRY(zero_support(h, h->x));
   RSO_TRY(zero_support(h, h->w));
+  // support-free problems: no displacement balances the rigid-motion part of
+  // a load, so the solve takes the load without it
+  RSO_TRY(displacement_project(h, h->w));
   cudaEventRecord(e0, h->stream);
   rso_status s = method == RSO_SOLVE_PCG ? solve_pcg(h, h->w, h->x, tol, max_iter, info)
                                          : solve_vcycles(h, h->w, h->x, tol, max_iter, info);

@@ -204,6 +204,10 @@ rso_status worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t see
     double* v = V + ls * it;
     RSO_CHECK_CUDA(h, cudaMemsetAsync(h->w, 0, sizeof(double) * n3, h->stream));
     k_scatter_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(v, h->load_nodes, nl, l0.NP, 1.0, h->w); rso::note_launch();
+    // support-free problems: v is free of the load set's rigid motions up to
+    // rounding, which the Lanczos normalisation can magnify once beta is
+    // small; the solve takes the load exactly without them
+    RSO_TRY(displacement_project(h, h->w));
     double* u = h->lanczos_u[it];
     RSO_CHECK_CUDA(h, cudaMemsetAsync(u, 0, sizeof(double) * n3, h->stream));
     rso_solve_info si = {0, 0, 0};

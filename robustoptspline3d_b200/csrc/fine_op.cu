@@ -75,8 +75,17 @@ __constant__ double cBd[72];  // [c][i][j]
 __constant__ float cBf[72];
 __constant__ double cD0d[9];  // diagonal 3x3 block of local node 0
 __constant__ float cD0f[9];
-__constant__ float2 cBp[72];  // cBf entries duplicated into both lanes (packed FP32 kernel)
-__constant__ float2 cD0p[9];
+// The packed FP32 kernel uses the blocks' finer structure (the isotropic
+// material and the cube's rotations; checked on the host): with
+//   A0, B0, A7, B7 the diagonal and off-diagonal entries of blocks 0 and 7
+//   (full 3 x 3, a I + b (J - I)), P, Q those of the one-bit blocks
+//   ([[P, Q], [Q, P]] on the two axes outside c), R, S those of the two-bit
+//   blocks (R on the 2 x 2 block of the two axes in c, all four entries; S
+//   on the axis outside c)
+// and the node-0 diagonal block D0 = [[Da, Db, Db], [Db, Da, Db], [Db, Db, Da]],
+// cWp holds, duplicated into both lanes: A0 - B0, B0, A7 - B7, B7, P, Q, R, S, Da, Db.
+__constant__ float2 cWp[10];
+enum { W_A0 = 0, W_B0, W_A7, W_B7, W_P, W_Q, W_R, W_S, W_DA, W_DB };
 
 template <typename T>
 __device__ __forceinline__ T bw(int i);
@@ -147,11 +156,34 @@ rso_status upload_walsh(rso_handle* h) {
   RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cBf, Bf, sizeof(Bf), 0, cudaMemcpyHostToDevice, h->stream));
   RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cD0d, D0, sizeof(D0), 0, cudaMemcpyHostToDevice, h->stream));
   RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cD0f, Df, sizeof(Df), 0, cudaMemcpyHostToDevice, h->stream));
-  float2 Bp[72], Dp[9];
-  for (int i = 0; i < 72; i++) Bp[i] = make_float2(Bf[i], Bf[i]);
-  for (int i = 0; i < 9; i++) Dp[i] = make_float2(Df[i], Df[i]);
-  RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cBp, Bp, sizeof(Bp), 0, cudaMemcpyHostToDevice, h->stream));
-  RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cD0p, Dp, sizeof(Dp), 0, cudaMemcpyHostToDevice, h->stream));
+  // the finer structure the packed kernel relies on (see cWp)
+  auto Bv = [&](int c, int i, int j) { return B[c * 9 + i * 3 + j]; };
+  const double A0 = Bv(0, 0, 0), B0 = Bv(0, 0, 1), A7 = Bv(7, 0, 0), B7 = Bv(7, 0, 1);
+  const double Pv = Bv(1, 1, 1), Qv = Bv(1, 1, 2), Rv = Bv(3, 0, 0), Sv = Bv(3, 2, 2);
+  const double Da = D0[0], Db = D0[1];
+  double worst = 0;
+  for (int c = 0; c < 8; c++)
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        const int pc = (c & 1) + ((c >> 1) & 1) + ((c >> 2) & 1);
+        double e = 0;
+        if (b_zero(c, i, j)) e = 0;
+        else if (pc == 0) e = i == j ? A0 : B0;
+        else if (pc == 3) e = i == j ? A7 : B7;
+        else if (pc == 1) e = i == j ? Pv : Qv;
+        else e = ((~c >> i) & 1) ? Sv : Rv;  // the axis outside c: S, else R
+        worst = std::fmax(worst, std::fabs(Bv(c, i, j) - e));
+      }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) worst = std::fmax(worst, std::fabs(D0[i * 3 + j] - (i == j ? Da : Db)));
+  if (worst > 1e-12 * kmax) {
+    h->err = "element matrix lacks the symmetry of an isotropic cube";
+    return RSO_ERR_INVALID_ARG;
+  }
+  const double Wv[10] = {A0 - B0, B0, A7 - B7, B7, Pv, Qv, Rv, Sv, Da, Db};
+  float2 Wp[10];
+  for (int i = 0; i < 10; i++) Wp[i] = make_float2((float)Wv[i], (float)Wv[i]);
+  RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(cWp, Wp, sizeof(Wp), 0, cudaMemcpyHostToDevice, h->stream));
   // the host copies are stack arrays: finish the copies before returning
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   return RSO_OK;
@@ -521,8 +553,10 @@ template <int TYP>
 constexpr int pair_slot() { return pair_rho_off<TYP>() + (36 * 2 * TYP + 31) / 32 * 32; }
 // staging slots of the packed kernel: the Jacobi / Chebyshev step keeps two
 // more stages resident, so that it reads rho^p of the layers around the
-// emitted plane and u at the emitted nodes from shared memory, not registers
-constexpr int pair_slots(int mode, bool tma) { return mode == 2 && tma ? WNSLOT + 2 : WNSLOT; }
+// emitted plane and u at the emitted nodes from shared memory, not registers;
+// it takes 8 slots rather than 6 so that slot indices and phases are a mask
+// and a shift of the stage number, not a division by 6
+constexpr int pair_slots(int mode, bool tma) { return mode == 2 && tma ? 2 * WNSLOT : WNSLOT; }
 template <int TYP>
 constexpr int pair_smem_bytes(int nslot) {
   // slots + corner exchange [2][4 values][3 comps][32 TYP] + 128 bytes to
@@ -570,6 +604,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
   }
   const int ex = x0 - 1 + tx, ey = y0 - 1 + 2 * ty;
   const int NP = (int)L.NP, px = L.px;  // 3 NP < 2^31 (checked by the launcher)
+  const int nb0 = (ex + 2) + px * (ey + 2), pxy32 = px * L.py;  // node (ex + 1, ey + 1, z) at nb0 + pxy32 (z + 1)
   const int xs = x0 & ~3, ox = x0 - xs;
 
   int goff[TMA ? 1 : KC], soff[TMA ? 1 : KC];
@@ -682,7 +717,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
       acc[c] = p_add(own[c], make_float2(xb[(0 * 3 + c) * NT + tid + 1], xb[(1 * 3 + c) * NT + tid + 1]));
       if (wB) acc[c].y += xb[(2 * 3 + c) * NT + tid + WTX] + xb[(3 * 3 + c) * NT + tid + WTX + 1];
     }
-    const int n = (int)L.nidx(ex + 1, ey + 1, zo);
+    const int n = nb0 + pxy32 * (zo + 1);  // L.nidx(ex + 1, ey + 1, zo) in 32 bits
     const bool workA = (clA & NC_ACTIVE) && !(clA & NC_SUPPORT);
     const bool workB = (clB & NC_ACTIVE) && !(clB & NC_SUPPORT);
     float2 res[3];
@@ -724,8 +759,9 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
       const float2 xlo = p_sub(p_add(ra[1], ra[3]), p_add(ra[0], ra[2])), xhi = p_sub(p_add(rb[1], rb[3]), p_add(rb[0], rb[2]));
       const float2 ylo = p_sub(p_add(ra[2], ra[3]), p_add(ra[0], ra[1])), yhi = p_sub(p_add(rb[2], rb[3]), p_add(rb[0], rb[1]));
       const float2 pxz = p_sub(xhi, xlo), pyz = p_sub(yhi, ylo);
-      const float2 a = p_mul(cD0p[0], R), b = p_mul(cD0p[1], pxy_), cc = p_mul(cD0p[2], pxz);
-      const float2 d = p_mul(cD0p[4], R), e = p_mul(cD0p[5], pyz), g = p_mul(cD0p[8], R);
+      // D0 = [[Da, Db, Db], [Db, Da, Db], [Db, Db, Da]]: the three diagonal entries coincide
+      const float2 a = p_mul(cWp[W_DA], R), b = p_mul(cWp[W_DB], pxy_), cc = p_mul(cWp[W_DB], pxz);
+      const float2 d = a, e = p_mul(cWp[W_DB], pyz), g = a;
       const float2 r0 = p_sub(fo[0], acc[0]), r1 = p_sub(fo[1], acc[1]), r2 = p_sub(fo[2], acc[2]);
       const float2 A = p_sub(p_mul(d, g), p_mul(e, e)), B = p_sub(p_mul(cc, e), p_mul(b, g));
       const float2 C = p_sub(p_mul(b, e), p_mul(cc, d));
@@ -765,7 +801,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
     }
     if (z - 1 >= z0) emit(z - 1, sx + ((z - 1) & 1) * 12 * NT);
     if (wA && z >= z0) {
-      const int n = (int)L.nidx(ex + 1, ey + 1, z);
+      const int n = nb0 + pxy32 * (z + 1);
       clA = L.vclass[n];
       if (wB) clB = L.vclass[n + px];
       if (MODE != 1) {
@@ -794,25 +830,59 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
     }
     const int ri = 2 * ty * RX + tx + ox;
     const float2 re = make_float2(sr[ri], sr[ri + RX]);
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-      float2 in[3], o[3];
-#pragma unroll
-      for (int j = 0; j < 3; j++) in[j] = v[c ^ (1 << j)][j];
-#pragma unroll
-      for (int i = 0; i < 3; i++) {
-        float2 s = zero2;
-        bool first = true;
-#pragma unroll
-        for (int j = 0; j < 3; j++)
-          if (!b_zero(c, i, j)) {
-            s = first ? p_mul(cBp[c * 9 + i * 3 + j], in[j]) : p_fma(cBp[c * 9 + i * 3 + j], in[j], s);
-            first = false;
-          }
-        o[i] = p_mul(s, re);
+    // rho^p B: block c maps v[c ^ (1 << j)][j] to v[c ^ (1 << i)][i] (each
+    // entry of v belongs to exactly one block), in the structure of cWp; the
+    // constants enter each block directly, so that nothing stays live across
+    // blocks
+    {
+      // blocks 0 and 7: o_i = rho ((A - B) in_i + B (in_0 + in_1 + in_2))
+      {
+        const float2 a = v[1][0], b = v[2][1], c = v[4][2];
+        const float2 w = p_mul(cWp[W_B0], p_add(p_add(a, b), c));
+        v[1][0] = p_mul(re, p_fma(cWp[W_A0], a, w));
+        v[2][1] = p_mul(re, p_fma(cWp[W_A0], b, w));
+        v[4][2] = p_mul(re, p_fma(cWp[W_A0], c, w));
       }
-#pragma unroll
-      for (int i = 0; i < 3; i++) v[c ^ (1 << i)][i] = o[i];
+      {
+        const float2 a = v[6][0], b = v[5][1], c = v[3][2];
+        const float2 w = p_mul(cWp[W_B7], p_add(p_add(a, b), c));
+        v[6][0] = p_mul(re, p_fma(cWp[W_A7], a, w));
+        v[5][1] = p_mul(re, p_fma(cWp[W_A7], b, w));
+        v[3][2] = p_mul(re, p_fma(cWp[W_A7], c, w));
+      }
+      // one-bit blocks 1, 2, 4: rho [[P, Q], [Q, P]] on the two axes outside
+      // c; the output of the axis in c is zero
+      {
+        const float2 a = v[3][1], b = v[5][2];  // c = 1: axes 1, 2
+        v[3][1] = p_mul(re, p_fma(cWp[W_Q], b, p_mul(cWp[W_P], a)));
+        v[5][2] = p_mul(re, p_fma(cWp[W_Q], a, p_mul(cWp[W_P], b)));
+        v[0][0] = zero2;
+      }
+      {
+        const float2 a = v[3][0], b = v[6][2];  // c = 2: axes 0, 2
+        v[3][0] = p_mul(re, p_fma(cWp[W_Q], b, p_mul(cWp[W_P], a)));
+        v[6][2] = p_mul(re, p_fma(cWp[W_Q], a, p_mul(cWp[W_P], b)));
+        v[0][1] = zero2;
+      }
+      {
+        const float2 a = v[5][0], b = v[6][1];  // c = 4: axes 0, 1
+        v[5][0] = p_mul(re, p_fma(cWp[W_Q], b, p_mul(cWp[W_P], a)));
+        v[6][1] = p_mul(re, p_fma(cWp[W_Q], a, p_mul(cWp[W_P], b)));
+        v[0][2] = zero2;
+      }
+      // two-bit blocks 3, 5, 6: rho R (in_a + in_b) on both axes in c, rho S on the other
+      {
+        const float2 w = p_mul(re, p_mul(cWp[W_R], p_add(v[2][0], v[1][1])));  // c = 3: axes 0, 1
+        v[2][0] = w; v[1][1] = w; v[7][2] = p_mul(re, p_mul(cWp[W_S], v[7][2]));
+      }
+      {
+        const float2 w = p_mul(re, p_mul(cWp[W_R], p_add(v[4][0], v[1][2])));  // c = 5: axes 0, 2
+        v[4][0] = w; v[1][2] = w; v[7][1] = p_mul(re, p_mul(cWp[W_S], v[7][1]));
+      }
+      {
+        const float2 w = p_mul(re, p_mul(cWp[W_R], p_add(v[4][1], v[2][2])));  // c = 6: axes 1, 2
+        v[4][1] = w; v[2][2] = w; v[7][0] = p_mul(re, p_mul(cWp[W_S], v[7][0]));
+      }
     }
     if (MODE == 2 && !LEAN) {
 #pragma unroll

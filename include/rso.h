@@ -300,7 +300,7 @@ rso_status rso_solve_batch(rso_handle* h, int k, const double* F_dev, double* U_
                            rso_solve_info* infos);
 /* Launch-shape autotuner (no counterpart in the reference, whose launch
  * shapes are fixed): times, on this handle's hierarchy with CUDA events, the
- * thread rows of the packed FP32 fine kernel (2 or 4), one thread per node or
+ * thread rows of the packed FP32 fine kernel (2, 4 or 8), one thread per node or
  * per (node, row) on every coarse level, and the first level of the bottom
  * cluster kernel (or none), each timed as mixed-precision solves of a random
  * load, and keeps the fastest for this handle (a candidate must beat the

@@ -3,9 +3,9 @@
 // Three choices depend on the problem's size and shape more than on anything
 // a fixed rule sees, so they are measured on the handle's own hierarchy with
 // CUDA events, one after the other, and the fastest is kept in h->tune:
-//   - thread rows of a CTA of the packed FP32 fine kernel (2 or 4: 32 x 4 or
-//     32 x 8 element columns per CTA; the smaller tile gives small grids more
-//     CTAs, the larger one less halo per node),
+//   - thread rows of a CTA of the packed FP32 fine kernel (2, 4 or 8: 32 x 4,
+//     32 x 8 or 32 x 16 element columns per CTA; the smaller tiles give small
+//     grids more CTAs, the larger ones less halo per node),
 //   - per coarse level, one thread per node (k_coarse) or per (node, row)
 //     (k_coarse_r),
 //   - the first level of the bottom cluster kernel (or none).
@@ -105,7 +105,7 @@ rso_status autotune(rso_handle* h) {
   k_tune_rhs<<<cdiv(l0.NP, 256), 256, 0, h->stream>>>(l0, l0.f64, 4242); note_launch();
   RSO_TRY(launch_check(h, "autotune rhs"));
   // fine kernel tile, with the built-in rules for the rest
-  RSO_TRY(pick(h, {4, 2}, [&](int v) { h->tune.fine_rows = v; }));
+  RSO_TRY(pick(h, {4, 2, 8}, [&](int v) { h->tune.fine_rows = v; }));
   // first level of the bottom cluster kernel, or none
   h->tune.bottom = 1;
   if (nl >= 3 && bottom_level(h) == 1) {
@@ -164,8 +164,8 @@ extern "C" rso_status rso_autotune(rso_handle* h, int* choices_host) {
 extern "C" rso_status rso_set_launch_shapes(rso_handle* h, const int* choices_host, int n) {
   if (!h || !choices_host || n < 2) return RSO_ERR_INVALID_ARG;
   const int nl = (int)h->L.size();
-  if (choices_host[0] != 2 && choices_host[0] != 4) {
-    h->err = "fine thread rows must be 2 or 4";
+  if (choices_host[0] != 2 && choices_host[0] != 4 && choices_host[0] != 8) {
+    h->err = "fine thread rows must be 2, 4 or 8";
     return RSO_ERR_INVALID_ARG;
   }
   const int b = choices_host[1];

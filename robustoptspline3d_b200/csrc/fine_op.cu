@@ -568,7 +568,7 @@ constexpr int pair_smem_bytes(int nslot) {
 // the residual and the Jacobi / Chebyshev step fit 128 registers without
 // spills, K u (MODE 1, which carries u at the emitted nodes) 168
 constexpr int pair_min_blocks(int mode, int typ) {
-  return (mode == 0 ? kPairMinBlocksRes : mode == 2 ? kPairMinBlocksJac : 3) * 4 / typ;
+  return ((mode == 0 ? kPairMinBlocksRes : mode == 2 ? kPairMinBlocksJac : 3) * 4 + typ - 1) / typ;
 }
 
 // TMA: stage u planes and rho^p layers with bulk-tensor copies (tmu: 4-D map
@@ -1165,6 +1165,10 @@ static inline dim3 pair_grid(const Level& l, int pty) {
 
 template <typename T>
 static inline int pcls(int c32, int c64) { return sizeof(T) == 4 ? c32 : c64; }
+// thread rows of the packed kernel's CTA (2, 4 or 8; 4 unless tuned)
+static inline int fine_pty(const rso_handle* h) {
+  return h->tune.fine_rows == 2 || h->tune.fine_rows == 8 ? h->tune.fine_rows : 4;
+}
 
 // cuTensorMapEncodeTiled from the driver, looked up once through the runtime
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -1240,20 +1244,23 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
   // FP32: two columns per thread on packed pairs, staged by TMA; FP64: one
   // column per thread, staged by cp.async
   constexpr bool packed = sizeof(T) == 4;
-  const int pty = h->tune.fine_rows == 2 ? 2 : 4;
-  const int smem = packed ? (pty == 2 ? pair_smem_bytes<2>(pair_slots(MODE, kPairTMA))
-                                      : pair_smem_bytes<4>(pair_slots(MODE, kPairTMA)))
+  const int pty = fine_pty(h);
+  const int smem = packed ? (pty == 2   ? pair_smem_bytes<2>(pair_slots(MODE, kPairTMA))
+                             : pty == 8 ? pair_smem_bytes<8>(pair_slots(MODE, kPairTMA))
+                                        : pair_smem_bytes<4>(pair_slots(MODE, kPairTMA)))
                           : walsh_smem_bytes<T, WTY>();
   const void* kern;
   if constexpr (packed)
-    kern = pty == 2 ? reinterpret_cast<const void*>(k_fine_p<MODE, 2, kPairTMA>)
-                    : reinterpret_cast<const void*>(k_fine_p<MODE, 4, kPairTMA>);
+    kern = pty == 2   ? reinterpret_cast<const void*>(k_fine_p<MODE, 2, kPairTMA>)
+           : pty == 8 ? reinterpret_cast<const void*>(k_fine_p<MODE, 8, kPairTMA>)
+                      : reinterpret_cast<const void*>(k_fine_p<MODE, 4, kPairTMA>);
   else
     kern = reinterpret_cast<const void*>(k_fine_w<T, MODE, WTY>);
   // the shared-memory opt-in is per device and kernel; setting it twice from
   // racing threads is harmless, so an atomic flag per device suffices
-  static std::atomic<bool> attr[2][64];
-  std::atomic<bool>* done = (h->device >= 0 && h->device < 64) ? &attr[pty == 2][h->device] : nullptr;
+  static std::atomic<bool> attr[3][64];
+  const int ti = pty == 2 ? 0 : pty == 4 ? 1 : 2;
+  std::atomic<bool>* done = (h->device >= 0 && h->device < 64) ? &attr[ti][h->device] : nullptr;
   if (!done || !done->load(std::memory_order_acquire)) {
     RSO_CHECK_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     if (done) done->store(true, std::memory_order_release);
@@ -1264,6 +1271,9 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
     if (h->prof_on) prof_begin(h, cls, (double)l.nn);
     if (pty == 2)
       k_fine_p<MODE, 2, kPairTMA><<<pair_grid(l, 2), dim3(WTX, 2), smem, h->stream>>>(
+          l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, mu, mr);
+    else if (pty == 8)
+      k_fine_p<MODE, 8, kPairTMA><<<pair_grid(l, 8), dim3(WTX, 8), smem, h->stream>>>(
           l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, mu, mr);
     else
       k_fine_p<MODE, 4, kPairTMA><<<pair_grid(l, 4), dim3(WTX, 4), smem, h->stream>>>(
@@ -1303,7 +1313,7 @@ rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const doub
 // dot_dev[b * stride] per system of a batch
 rso_status fine_applyK_dot32(rso_handle* h, const float* u, float* f, double* dot_dev, int stride) {
   const Level& l0 = h->L[0];
-  const dim3 g = pair_grid(l0, h->tune.fine_rows == 2 ? 2 : 4);
+  const dim3 g = pair_grid(l0, fine_pty(h));
   const long long nb = (long long)g.x * g.y * g.z;  // all systems
   if (nb > h->fpart_n) {
     h->err = "fine partial-sum buffer smaller than the grid";

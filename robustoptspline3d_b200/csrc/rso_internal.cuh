@@ -169,7 +169,7 @@ struct rso_handle {
   void* prof = nullptr;
   // launch shapes chosen by rso_autotune (autotune.cu); -1 / -2 keep the built-in rules
   struct Tune {
-    int fine_rows = 4;      // thread rows of a CTA of the packed FP32 fine kernel (2 or 4)
+    int fine_rows = 4;      // thread rows of a CTA of the packed FP32 fine kernel (2, 4 or 8)
     int rowsplit[16];       // per level: 1 one thread per (node, row), 0 one per node, -1 by size
     int bottom = -2;        // first level of the bottom cluster kernel, -1 none, -2 by size
     Tune() { for (int& r : rowsplit) r = -1; }

@@ -85,12 +85,12 @@ def test_operator_fp64(oracle, cuda, gen):
     assert rel(r_g, r_o) < 1e-13
 
 
-@pytest.mark.parametrize("rows", [4, 2])
+@pytest.mark.parametrize("rows", [4, 2, 8])
 @pytest.mark.parametrize("gen", [lambda: P.ellipsoid(24, 16, 12), lambda: P.voids_box(20, 12, 12, 3),
                                  lambda: P.cantilever(40, 30, 36)])
 def test_operator_fp32(oracle, cuda, gen, rows):
     """FP32 fine kernels of the mixed V-cycle (residual, K u, Jacobi and Chebyshev steps) against the
-    FP64 oracle, for both tile heights the autotuner chooses between.  Tolerance 2e-5 relative in
+    FP64 oracle, for the three tile heights the autotuner chooses between.  Tolerance 2e-5 relative in
     norm: the inputs are rounded to FP32 and the element products accumulate in FP32.  The
     41 x 31 x 37-node cantilever spans two tiles in x, a ragged last tile in y and two z chunks."""
     prob = gen()

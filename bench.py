@@ -223,6 +223,8 @@ def run_solves(args):
     g.set_density(rho)
     g.update_stencil()
     tuned = g.autotune() if prec == R.rso.MIXED and not args.no_autotune else None
+    if args.fine_rows:
+        g.set_launch_shapes(fine_rows=args.fine_rows)
     if prec == R.rso.MIXED:
         g.set_krylov_fp32(args.krylov32)
     f = torch.zeros(3 * g.nn, dtype=torch.float64, device="cuda")
@@ -588,6 +590,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--fine-rows", type=int, default=0,
+                    help="--mode solve: thread rows of the packed fine kernel's CTA (2, 4 or 8; 0: as tuned)")
     ap.add_argument("--ref-size", type=int, default=24)
     ap.add_argument("--ref-sizes", default="24,32,48",
                     help="sample sizes of the CPU baseline leg (the largest is scaled to 256^3)")

@@ -234,6 +234,17 @@ rso_status rso_load_nodes(rso_handle* h, int* nodes_host, int* n_load);
 /* ---------------------------------------------------------------- operator and multigrid */
 /* element densities (ex*ey*ez floats, inactive entries ignored); Grid rho_e buffer */
 rso_status rso_set_density(rso_handle* h, const float* rho_dev);
+/* The current element densities (ex*ey*ez floats, device), the field
+ * HierarchyGrid::writeDensity saves (grid/Grid.cpp:1267-1300, there as an
+ * OpenVDB grid of element positions and values). */
+rso_status rso_get_density(rso_handle* h, float* rho_dev);
+/* Restart from saved densities: HierarchyGrid::readDensity (grid/Grid.cpp:
+ * 1914-1945) with the points already read from the file: n element positions
+ * (x, y, z per point, host) and their values (host); every other element gets
+ * density 0.  A point outside the grid or on an inactive element is refused
+ * with RSO_ERR_INVALID_ARG ("unmatched grid and file", where the reference
+ * exits).  Then as rso_set_density (call rso_update_operators next). */
+rso_status rso_set_density_points(rso_handle* h, int n, const int32_t* pos_host, const float* values_host);
 /* Galerkin coarse operators and coarsest factorisation; update_stencil
  * (grid/Grid.cpp:4250-4261, grid/Grid.cu:882-1308, grid/Grid.cpp:3697-3752) */
 rso_status rso_update_operators(rso_handle* h);

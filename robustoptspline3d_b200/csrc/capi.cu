@@ -371,6 +371,39 @@ extern "C" rso_status rso_set_density(rso_handle* h, const float* rho) {
   return RSO_OK;
 }
 
+extern "C" rso_status rso_get_density(rso_handle* h, float* rho) {
+  if (!h || !rho) return RSO_ERR_INVALID_ARG;
+  RSO_TRY(unpad_elems_f(h, h->rho, rho));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  return RSO_OK;
+}
+
+extern "C" rso_status rso_set_density_points(rso_handle* h, int n, const int32_t* pos, const float* values) {
+  if (!h || n < 0 || (n > 0 && (!pos || !values))) return RSO_ERR_INVALID_ARG;
+  const Level& l0 = h->L[0];
+  const std::vector<uint8_t>& em = h->h_emask[0];
+  std::vector<float> dense((size_t)l0.ne, 0.0f);
+  for (int i = 0; i < n; i++) {
+    const int x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+    if (x < 0 || y < 0 || z < 0 || x >= l0.ex || y >= l0.ey || z >= l0.ez) {
+      h->err = "density point outside the grid (unmatched grid and file)";
+      return RSO_ERR_INVALID_ARG;
+    }
+    const size_t e = x + (size_t)l0.ex * (y + (size_t)l0.ey * z);
+    if (!em[e]) {
+      h->err = "density point on an inactive element (unmatched grid and file)";
+      return RSO_ERR_INVALID_ARG;
+    }
+    dense[e] = values[i];
+  }
+  // staged in a padded element buffer of the handle (at least ex*ey*ez floats)
+  float* d = h->e_b;
+  RSO_CHECK_CUDA(h, cudaMemcpyAsync(d, dense.data(), sizeof(float) * l0.ne, cudaMemcpyHostToDevice, h->stream));
+  RSO_TRY(rso_set_density(h, d));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  return RSO_OK;
+}
+
 extern "C" rso_status rso_update_operators(rso_handle* h) {
   if (!h) return RSO_ERR_INVALID_ARG;
   RSO_TRY(galerkin(h));

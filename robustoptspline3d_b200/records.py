@@ -53,3 +53,26 @@ class RunRecords:
             write_vector(os.path.join(self.dir, "flast"), np.asarray(f_last, np.float64))
         if u_last is not None:
             write_vector(os.path.join(self.dir, "ulast"), np.asarray(u_last, np.float64))
+
+
+def write_density(prefix, emask, rho):
+    """The densities of the active elements with their integer positions: what
+    HierarchyGrid::writeDensity (grid/Grid.cpp:1267-1300) stores in an
+    OpenVDB grid (absent here), as two raw records: <prefix>.pos, int32
+    x, y, z per element in the layout of bio::write_vectors
+    (utils/binaryIO.h:80-91), and <prefix>.val, float32 values.  emask is the
+    (ez, ey, ex) element mask, rho the dense element field."""
+    emask = np.asarray(emask)
+    z, y, x = np.nonzero(emask)
+    rho = np.asarray(rho, np.float32).reshape(emask.shape)
+    write_vector(prefix + ".pos", np.stack([x, y, z], 1).ravel(), np.int32)
+    write_vector(prefix + ".val", rho[z, y, x], np.float32)
+
+
+def read_density(prefix):
+    """(positions (n, 3) int32 x, y, z; values (n,) float32) written by write_density."""
+    pos = read_vector(prefix + ".pos", np.int32).reshape(-1, 3)
+    val = read_vector(prefix + ".val", np.float32)
+    if len(pos) != len(val):
+        raise ValueError("density records of different lengths")
+    return pos, val

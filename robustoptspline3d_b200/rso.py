@@ -107,6 +107,8 @@ SIGNATURES = {
     "rso_set_krylov_fp32": (_ci, [_vp, _cd]),
     "rso_set_krylov_fp32_cycles": (_ci, [_vp, _ci]),
     "rso_displacement_project": (_ci, [_vp, _vp]),
+    "rso_get_density": (_ci, [_vp, _vp]),
+    "rso_set_density_points": (_ci, [_vp, _ci, _pi, ctypes.POINTER(ctypes.c_float)]),
     "rso_voxelize": (_ci, [ctypes.POINTER(ctypes.c_float), _ci, ctypes.POINTER(ctypes.c_int), _ci, _ci, _pu8, _pi,
                            ctypes.POINTER(ctypes.c_float)]),
     "rso_shell_elements": (_ci, [ctypes.POINTER(ctypes.c_float), _ci, ctypes.POINTER(ctypes.c_int), _ci,
@@ -313,6 +315,7 @@ class HierarchyGrid:
         self.nx, self.ny, self.nz = self.ex + 1, self.ey + 1, self.ez + 1
         self.nn = self.nx * self.ny * self.nz
         self.ne = self.ex * self.ey * self.ez
+        self._emask = emask
         fa = np.ascontiguousarray(fixed_area, dtype=np.uint8).ravel()
         la = np.ascontiguousarray(load_area, dtype=np.uint8).ravel()
         ln = None if load_normals is None else np.ascontiguousarray(load_normals, dtype=np.float64).ravel()
@@ -402,6 +405,30 @@ class HierarchyGrid:
         r = rho if isinstance(rho, torch.Tensor) else torch.as_tensor(np.asarray(rho, np.float32), device="cuda")
         r = r.to(device="cuda", dtype=torch.float32).contiguous()
         self._chk(self.lib.rso_set_density(self.h, _dev(r)), "rso_set_density")
+
+    def get_density(self):
+        """The current element densities (float32 CUDA tensor, ez x ey x ex flattened)."""
+        import torch
+        out = torch.empty(self.ne, dtype=torch.float32, device="cuda")
+        self._chk(self.lib.rso_get_density(self.h, _dev(out)), "rso_get_density")
+        return out
+
+    def writeDensity(self, prefix):
+        """Save the densities of the active elements as HierarchyGrid::writeDensity does
+        (grid/Grid.cpp:1267-1300), as raw records instead of OpenVDB: see records.write_density."""
+        from . import records
+        records.write_density(prefix, self._emask, self.get_density().cpu().numpy())
+
+    def readDensity(self, prefix):
+        """Restart from densities saved by writeDensity (HierarchyGrid::readDensity,
+        grid/Grid.cpp:1914-1945); call update_stencil next."""
+        from . import records
+        pos, val = records.read_density(prefix)
+        pos = np.ascontiguousarray(pos, np.int32)
+        val = np.ascontiguousarray(val, np.float32)
+        self._chk(self.lib.rso_set_density_points(self.h, len(val), _np_ptr(pos, _pi),
+                                                  val.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+                  "rso_set_density_points")
 
     def update_stencil(self):
         self._chk(self.lib.rso_update_operators(self.h), "rso_update_operators")

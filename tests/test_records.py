@@ -30,3 +30,17 @@ def test_run_records_layout(tmp_path):
         assert os.path.exists(os.path.join(tmp_path, name)), name
     assert np.array_equal(read_vector(os.path.join(tmp_path, "trec")), [100.0, 101.0, 102.0])
     assert read_vector(os.path.join(tmp_path, "flast")).size == 6
+
+
+def test_density_records_round_trip(tmp_path):
+    from robustoptspline3d_b200 import records
+    rng = np.random.default_rng(4)
+    em = (rng.uniform(size=(5, 6, 7)) < 0.6).astype(np.uint8)
+    rho = rng.uniform(0, 1, em.shape).astype(np.float32)
+    prefix = str(tmp_path / "density0001")
+    records.write_density(prefix, em, rho)
+    pos, val = records.read_density(prefix)
+    assert len(val) == em.sum()
+    back = np.zeros_like(rho)
+    back[pos[:, 2], pos[:, 1], pos[:, 0]] = val
+    assert np.array_equal(back, rho * em)

@@ -12,7 +12,7 @@ exceed the 126 MB L2, so no flush is inserted between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--size S]
   python bench.py --mode solve [--precision mixed|fp64] [--size S]
-  python bench.py --mode batch|problems|scale|mesh
+  python bench.py --mode batch|problems|scale|mesh|surface
 
 `--mode solve` times single multigrid-preconditioned CG solves (to relative
 residual 1e-6) on the density of the seeded initial design, with a seeded
@@ -521,6 +521,69 @@ def run_mesh(args):
     print(json.dumps(out), flush=True)
 
 
+def run_surface(args):
+    """Surface-point self-support on the seeded 256^3 design (32^3 tricubic
+    coefficients): the rho = 0.5 crossings of the 66^3 background grid thinned
+    to 200,000 points (rso_surface_points), then the overhang constraint
+    (mode 4, 135 degrees) with its coefficient gradient at those points
+    (rso_surface_selfsupport).  Both are synchronous C-ABI calls with device
+    coefficients; the median host wall time of --steps calls after --warmup.
+    The CPU column runs the oracle's restatement of the same two steps once,
+    at the full size, on one core."""
+    import torch
+    import robustoptspline3d_b200 as R
+    n = args.size
+    em, fa, la, order, parts, coeff = problem(n)
+    g = R.HierarchyGrid(em, fa, la, None, R.Config())
+    g.set_spline_partition(parts, parts, parts, order)
+    c = torch.as_tensor(coeff, dtype=torch.float32, device="cuda")
+    mc, npts = 64, 200000
+    lib = g.lib
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 1)):
+            out = fn()
+        ts = []
+        for _ in range(max(args.steps, 1)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return float(np.median(ts)) * 1e3, out
+
+    l0 = lib.rso_launch_count()
+    ms_pts, (_, counts) = timed(lambda: g.generate_spline_surface_nodes(c, mc_res=mc, n_points=npts))
+    l1 = lib.rso_launch_count()
+    ms_ss, res = timed(lambda: g.deal_surface_points(c, 8.0, 4))
+    l2 = lib.rso_launch_count()
+    calls = max(args.warmup, 1) + max(args.steps, 1)
+    out = {"metric": "surface-point self-support @256^3 (sampling + constraint + gradient)",
+           "value": 1e3 / (ms_pts + ms_ss), "unit": "evaluations/s", "higher_is_better": True,
+           "ms_sampling": ms_pts, "ms_constraint": ms_ss, "counts": counts,
+           "constraint": {"value": res[0], "count": res[3], "probe_sum": res[4]},
+           "gpu_launches_per_call": {"sampling": (l1 - l0) // calls, "constraint": (l2 - l1) // calls},
+           "data": "synthetic (seeded design of the design-iteration bench)",
+           "config": {"workload": f"{n}^3 box, order {order}, {parts + order}^3 coefficients, background {mc}^3 "
+                                  f"(+2), {npts} points, mode 4 (overhang sigmoid), beta 8",
+                      "timing": "host wall clock around synchronous C-ABI calls, device coefficients"}}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        o = O.Problem(em, fa, la, n_levels=1)   # the spline and the mask only; no hierarchy
+        o.spline_setup(order, [parts] * 3)
+        cd = np.asarray(coeff, np.float32).astype(np.float64)
+        t0 = time.perf_counter()
+        pts, _ = o.surface_points(cd, mc=mc, n_points=npts)
+        t1 = time.perf_counter()
+        o.surface_selfsupport(cd, pts, 8.0, 4)
+        t2 = time.perf_counter()
+        out["cpu_baseline"] = {"value": 1.0 / (t2 - t0), "unit": "evaluations/s", "cores": 1, "kind": "port",
+                               "ms_sampling": (t1 - t0) * 1e3, "ms_constraint": (t2 - t1) * 1e3,
+                               "sample": "one full evaluation (same sizes)"}
+    g.close()
+    print(json.dumps(out), flush=True)
+
+
 def run_scale(args):
     """One worst-case design iteration on the 512 x 256 x 256 voids box (the
     FP32-operator-at-scale configuration), mixed and plain FP64; the FP64 path
@@ -600,7 +663,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--krylov32", type=float, default=1e-2,
                     help="mixed PCG with the FP32 Krylov recurrence, true-residual replacement factor (0: FP64 recurrence)")
-    ap.add_argument("--mode", default="design", choices=["design", "solve", "batch", "problems", "scale", "mesh"])
+    ap.add_argument("--mode", default="design", choices=["design", "solve", "batch", "problems", "scale", "mesh",
+                                                          "surface"])
     ap.add_argument("--systems", type=int, default=16)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
@@ -618,6 +682,9 @@ def main():
         return
     if args.mode == "mesh":
         run_mesh(args)
+        return
+    if args.mode == "surface":
+        run_surface(args)
         return
     if args.impl == "reference":
         # host-only arm: rank 0 times the CPU path, other ranks exit at once

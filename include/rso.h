@@ -441,6 +441,44 @@ rso_status rso_selfsupport(rso_handle* h, const float* coeff_dev, double beta, i
                            double default_angle, float* per_element_dev, float* dc_dev, double* value,
                            double* count, double* direction_sum);
 
+/* ---------------------------------------------------------------- surface-point self-support
+ * deal_surface_points (optimization/optimization.cpp:1185-1221).  Points are
+ * element-unit coordinates, SoA (x[0..n), y[0..n), z[0..n)). */
+typedef struct rso_surface_info {
+  long long n_crossings;   /* background-grid edges crossing rho = 0.5 */
+  long long n_first_pick;  /* candidates after the first equal-distance pick */
+  long long n_in_model;    /* candidates inside an active element */
+  int n_points;            /* points kept (= n_points requested) */
+  int reserved;
+} rso_surface_info;
+/* Grid::generate_spline_surface_nodes (grid/Grid.cpp:4067-4112) with
+ * compute_background_mcPoints_value (grid/Grid.cu:4066-4175) and
+ * compute_surface_nodes_in_model (grid/Grid.cpp:3861-4060): the crossings of
+ * rho = 0.5 on the (mc_res+2)^3 background grid of the model box (NULL: the
+ * bounding box of the active elements; else {xmin, ymin, zmin, xmax, ymax,
+ * zmax}), one per crossing grid edge in edge order, thinned to n_points as the
+ * reference does.  The points stay on the handle. */
+rso_status rso_surface_points(rso_handle* h, const float* coeff_dev, int mc_res, int n_points,
+                              const float* model_box_host, rso_surface_info* info);
+/* Grid::uploadSurfacePoints: use the given points (3 n floats, device or host) */
+rso_status rso_set_surface_points(rso_handle* h, const float* xyz, int n_points);
+/* copy the points out (3 n floats; xyz may be NULL to query n) */
+rso_status rso_get_surface_points(rso_handle* h, float* xyz, int capacity, int* n_points);
+/* compute_spline_surface_point_normal .. scale_spline_selfsupp_constraint_dcoeff
+ * (grid/Grid.cu:5709-6505, grid/Grid.cpp:4263-4280): normals, orientation,
+ * flags, the per-point constraint of GlobalSSMode `mode` (p-norm 8,
+ * h-function 10, sigmoid 0.09), its mean (p-norm: (mean)^(1/8) - 1) and its
+ * coefficient gradient divided by the count.  per_point (n) and dc (n_coeff)
+ * may be NULL. */
+rso_status rso_surface_selfsupport(rso_handle* h, const float* coeff_dev, double beta, int mode,
+                                   double opt_angle, double default_angle, float* per_point_dev,
+                                   float* dc_dev, double* value, double* count, double* direction_sum);
+/* outward normals of the last evaluation (3 n doubles, SoA) and the flags
+ * (2 n bytes: at the default angle, compute_selfsupp_flag_actual
+ * grid/Grid.cu:5945-5992, then at the optimisation angle, :5994-6040);
+ * either may be NULL */
+rso_status rso_get_surface_normals(rso_handle* h, double* normals, uint8_t* flags);
+
 /* ---------------------------------------------------------------- worst case */
 /* forceProject (optimization/projection.cu:165-231, projection.cpp:289-360):
  * forces kept on the load nodes, only along the load normal in

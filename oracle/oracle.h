@@ -130,6 +130,23 @@ double or_selfsupport(const or_problem* p, const double* c, double beta, int mod
                       double opt_angle, double default_angle, double* per_element,
                       double* dc, double* count_out, double* direction_sum);
 
+/* surface-point self-support (or_surface.cpp; grid/Grid.cu:4066-4175,
+ * :5709-6505, grid/Grid.cpp:3831-4112).  box = {xmin, ymin, zmin, xmax, ymax,
+ * zmax} in element units.  or_mc_values fills (mc+2)^3 background values
+ * (x fastest) and, if pos3 is not NULL, their coordinates (SoA); or_equidistant the clamped equal-distance picks (returns their
+ * number); or_surface_points writes npts points (SoA, 3*npts) and info[4] =
+ * {crossings, after the first pick, inside the model, written}. */
+void or_mc_values(const or_problem* p, const double* c, int mc, const float* box, float* val, float* pos3);
+long or_equidistant(long range, long m, long* out);
+int  or_surface_points(const or_problem* p, const double* c, int mc, int npts, const float* box,
+                       float* xyz, long* info);
+/* normals (3n SoA), per (n), flags (2n: actual, virtual) and dc (n_coeff,
+ * divided by the count) may be NULL; returns the constraint value */
+double or_surface_selfsupport(const or_problem* p, const double* c, const float* xyz, long n, double beta,
+                              int mode, double opt_angle, double default_angle, double* normals,
+                              double* per, uint8_t* flags, double* dc, double* count_out,
+                              double* dirsum_out);
+
 /* worst-case machinery */
 void or_force_project(const or_problem* p, double* f, int constrain_direction);
 /* displacementProject (optimization/projection.cpp:374-411): u -= R R^T u over

@@ -18,6 +18,7 @@ _u8 = ctypes.POINTER(ctypes.c_uint8)
 _i32 = ctypes.POINTER(ctypes.c_int)
 _u32 = ctypes.POINTER(ctypes.c_uint32)
 _f32 = ctypes.POINTER(ctypes.c_float)
+_i64 = ctypes.POINTER(ctypes.c_int64)
 _vp = ctypes.c_void_p
 
 
@@ -77,6 +78,11 @@ def _load():
         "or_density2coeff_adjoint": (None, [_vp, _d, _u8, _d]),
         "or_selfsupport": (ctypes.c_double, [_vp, _d, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_double, _d, _d, _d, _d]),
+        "or_mc_values": (None, [_vp, _d, ctypes.c_int, _f32, _f32, _f32]),
+        "or_equidistant": (ctypes.c_long, [ctypes.c_long, ctypes.c_long, _i64]),
+        "or_surface_points": (ctypes.c_int, [_vp, _d, ctypes.c_int, ctypes.c_int, _f32, _f32, _i64]),
+        "or_surface_selfsupport": (ctypes.c_double, [_vp, _d, _f32, ctypes.c_long, ctypes.c_double, ctypes.c_int,
+                                                     ctypes.c_double, ctypes.c_double, _d, _d, _u8, _d, _d, _d]),
         "or_force_project": (None, [_vp, _d, ctypes.c_int]),
         "or_dense_worst": (ctypes.c_double, [_vp, ctypes.c_int, ctypes.c_double, _d, _d]),
         "or_lanczos": (ctypes.c_double, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_uint64,
@@ -156,6 +162,7 @@ class Problem:
         la = np.ascontiguousarray(load_area, dtype=np.uint8).ravel()
         ln = None if load_normals is None else np.ascontiguousarray(load_normals, dtype=np.float64).ravel()
         self._keep = (emask, fa, la, ln)
+        self.emask = emask
         self.h = lib().or_create(self.ex, self.ey, self.ez, _p(emask.ravel(), _u8), _p(fa, _u8), _p(la, _u8),
                                  _p(ln), E, nu, penal, rhomin, n_levels, first_factor)
         self.penal = penal
@@ -364,6 +371,49 @@ class Problem:
         v = lib().or_selfsupport(self.h, _p(np.ascontiguousarray(c, np.float64)), beta, mode, opt_angle,
                                  default_angle, _p(per), _p(dc), ctypes.byref(cnt), ctypes.byref(dsum))
         return v, per, dc, cnt.value, dsum.value
+
+    # surface-point self-support
+    def model_box(self):
+        """bounding box of the active elements, {xmin, ymin, zmin, xmax, ymax, zmax}"""
+        em = self.emask.reshape(self.ez, self.ey, self.ex)
+        lo, hi = [], []
+        for ax in (2, 1, 0):
+            occ = np.flatnonzero(em.any(axis=tuple(a for a in range(3) if a != ax)))
+            lo.append(float(occ[0]))
+            hi.append(float(occ[-1] + 1))
+        return np.array(lo + hi, np.float32)
+
+    def mc_values(self, c, mc=64, box=None):
+        """background values (mc+2)^3 and their coordinates (3, (mc+2)^3)"""
+        box = self.model_box() if box is None else np.asarray(box, np.float32)
+        out = np.zeros((mc + 2) ** 3, np.float32)
+        pos = np.zeros((3, (mc + 2) ** 3), np.float32)
+        lib().or_mc_values(self.h, _p(np.ascontiguousarray(c, np.float64)), mc, _p(box, _f32), _p(out, _f32),
+                           _p(pos, _f32))
+        return out, pos
+
+    def surface_points(self, c, mc=64, n_points=200000, box=None):
+        box = self.model_box() if box is None else np.asarray(box, np.float32)
+        xyz = np.zeros(3 * max(n_points, 0), np.float32)
+        info = np.zeros(4, np.int64)
+        lib().or_surface_points(self.h, _p(np.ascontiguousarray(c, np.float64)), mc, n_points, _p(box, _f32),
+                                _p(xyz, _f32), _p(info, _i64))
+        return xyz.reshape(3, -1), info
+
+    def surface_selfsupport(self, c, xyz, beta, mode=4, opt_angle=0.75 * np.pi, default_angle=0.75 * np.pi):
+        xyz = np.ascontiguousarray(xyz, np.float32).reshape(3, -1)
+        n = xyz.shape[1]
+        nrm = np.zeros(3 * n)
+        per = np.zeros(n)
+        flags = np.zeros(2 * n, np.uint8)
+        dc = np.zeros(self.n_coeff)
+        cnt = ctypes.c_double(0)
+        dsum = ctypes.c_double(0)
+        v = lib().or_surface_selfsupport(self.h, _p(np.ascontiguousarray(c, np.float64)), _p(xyz, _f32), n, beta,
+                                         mode, opt_angle, default_angle, _p(nrm), _p(per), _p(flags, _u8), _p(dc),
+                                         ctypes.byref(cnt), ctypes.byref(dsum))
+        return dict(value=v, normals=nrm.reshape(3, n), per=per, flags=flags.reshape(2, n), dc=dc,
+                    count=cnt.value, dirsum=dsum.value)
 
     # worst case
     def force_project(self, f, cf):

@@ -12,7 +12,9 @@ a shim for the CUDA keywords, and tests/golden/make_golden.py runs them to
 write the golden fixtures the oracle is pinned against.
 
 Each spec names a file, a regular expression matching the first line of the
-definition, and a mode:
+definition, a mode, and optionally an anchor: a regular expression whose
+first match starts the search (for a lambda whose text repeats in other
+functions).  Modes:
   def   the definition from its first line (and a 'template<...>' line just
         above it) through its matching closing brace (and a ';' after it)
   body  only the brace-enclosed body of the matched function
@@ -51,6 +53,24 @@ SPECS = [
     ("lib_bits.inc", "culib/lib.cuh", r"__device__ bool read_gbit\(T word, int id\)", "def"),
     ("lib_bits.inc", "culib/lib.cuh", r"__device__ T clamp\(T value, T low, T upp\)", "def"),
     ("lib_bits.inc", "culib/lib.cuh", r"struct gBitSAT \{", "def"),
+    # surface-point self-support (deal_surface_points, optimization/optimization.cpp:1185-1221)
+    ("surf_funcs.inc", "grid/Grid.cu", r"__device__ float oh\(float x", "def"),
+    ("surf_funcs.inc", "grid/Grid.cu", r"__device__ float doh\(float x", "def"),
+    ("surf_funcs.inc", "grid/Grid.cu", r"__device__ float norm\(float v\[3\]\)", "def"),
+    ("surf_funcs.inc", "grid/Grid.cu", r"__device__ float dot\(float v1\[3\]", "def"),
+    ("surf_funcs.inc", "grid/Grid.cpp", r"std::vector<int> generateEquidistantIntegers\(int range", "def"),
+    ("surf_mc.inc", "grid/Grid.cu", r"auto calc_node = \[=\] __device__\(int id\)", "expr",
+     r"void Grid::compute_background_mcPoints_value\("),
+    ("surf_normal.inc", "grid/Grid.cu", r"auto calc_normal = \[=\] __device__\(int node_id\)", "expr",
+     r"void grid::Grid::compute_spline_surface_point_normal\(void\)"),
+    ("surf_dir.inc", "grid/Grid.cu", r"auto calc_node = \[=\] __device__\(int node_id\)", "expr",
+     r"float grid::Grid::correct_spline_surface_point_normal_direction\(float beta\)"),
+    ("surf_flag.inc", "grid/Grid.cu", r"auto calc_node = \[=\] __device__\(int node_id\)", "expr",
+     r"void grid::Grid::compute_selfsupp_flag_actual\(void\)"),
+    ("surf_ss.inc", "grid/Grid.cu", r"auto calc_node = \[=\] __device__\(int node_id\)", "expr",
+     r"void grid::Grid::compute_spline_selfsupp_constraint\(void\)"),
+    ("surf_dss.inc", "grid/Grid.cu", r"auto calc_node_value = \[=\] __device__\(int node_id\)", "expr",
+     r"void grid::Grid::compute_spline_selfsupp_constraint_dcoeff\(void\)"),
 ]
 
 
@@ -86,8 +106,14 @@ def _match_brace(text, start):
     raise ValueError("unbalanced braces")
 
 
-def extract(text, pattern, mode):
-    m = re.search(pattern, text)
+def extract(text, pattern, mode, anchor=None):
+    pos = 0
+    if anchor:
+        a = re.search(anchor, text)
+        if not a:
+            raise ValueError(f"anchor not found: {anchor}")
+        pos = a.end()
+    m = re.compile(pattern).search(text, pos)
     if not m:
         raise ValueError(f"pattern not found: {pattern}")
     if mode == "expr":
@@ -111,11 +137,13 @@ def extract(text, pattern, mode):
 def main(ref_root, out_dir):
     os.makedirs(out_dir, exist_ok=True)
     chunks = {}
-    for out, src, pattern, mode in SPECS:
+    for spec in SPECS:
+        out, src, pattern, mode = spec[:4]
+        anchor = spec[4] if len(spec) > 4 else None
         path = os.path.join(ref_root, src)
         with open(path, encoding="utf-8", errors="replace") as f:
             text = f.read()
-        line, code = extract(text, pattern, mode)
+        line, code = extract(text, pattern, mode, anchor)
         chunks.setdefault(out, []).append(f"// {src}:{line}\n#line {line} \"{src}\"\n{code}\n")
     for out, parts in chunks.items():
         with open(os.path.join(out_dir, out), "w") as f:

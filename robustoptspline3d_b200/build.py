@@ -24,7 +24,7 @@ FILE_FLAGS = {"voxelize.cu": ["-fmad=false"], "boundary.cu": ["-fmad=false"]}
 SOURCES = ["capi.cu", "topology.cu", "fine_op.cu", "coarse_op.cu", "reduce.cu", "solver.cu", "design.cu",
            "design_capi.cu", "worst.cu", "mma.cu", "driver.cu", "prof.cu",
            "filter_noalloc.cu", "batch.cu", "autotune.cu", "oc.cu", "voxelize.cu",
-           "boundary.cu", "dense.cu", "rigid.cu"]
+           "boundary.cu", "dense.cu", "rigid.cu", "surface.cu"]
 
 
 def _compile(src, verbose=False):

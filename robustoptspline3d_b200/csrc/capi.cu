@@ -131,6 +131,7 @@ static void free_handle(rso_handle* h) {
   cudaFree(h->coef_df); cudaFree(h->coef_dg); cudaFree(h->fw); cudaFree(h->uw);
   cudaFree(h->wc_buf);
   vcycle_graphs_free(h);
+  surface_free(h);
   prof_free(h);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   delete h;

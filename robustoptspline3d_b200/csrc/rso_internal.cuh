@@ -189,6 +189,7 @@ struct rso_handle {
   void* vcg = nullptr;                             // captured FP32 V-cycles (solver.cu)
   void* cap_prof = nullptr;                        // event pairs of the V-cycle capture in progress (prof.cu)
   bool vc_graphs = true;                           // replay captured V-cycles (rso_set_vcycle_graphs)
+  void* surf = nullptr;                            // surface-point self-support state (surface.cu)
 };
 
 namespace rso {
@@ -211,6 +212,8 @@ void prof_harvest(rso_handle* h, void* pairs);
 // captured V-cycles (solver.cu)
 void vcycle_graphs_harvest(rso_handle* h);
 void vcycle_graphs_free(rso_handle* h);
+// surface-point self-support state (surface.cu)
+void surface_free(rso_handle* h);
 }  // namespace rso
 
 // ---------------------------------------------------------------- helpers

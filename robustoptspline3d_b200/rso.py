@@ -15,6 +15,8 @@ Names follow the reference:
   Grid.coeff2density             -> rso_coeff2density     (grid/Grid.cu:3441)
   Grid.ddensity2dcoeff           -> rso_density2coeff_adjoint (grid/Grid.cu:3566)
   deal_background_points         -> rso_selfsupport       (optimization/optimization.cpp:1223)
+  deal_surface_points            -> rso_surface_points + rso_surface_selfsupport
+                                                          (optimization/optimization.cpp:1185)
   forceProject / modifiedPM      -> rso_force_project / rso_modified_pm / rso_worst_case
   MMA::mma_t::update             -> rso_mma_update        (optimization/mma_t.cpp:18)
 """
@@ -61,6 +63,11 @@ class _IterInfo(ctypes.Structure):
                 ("ss_value", ctypes.c_double), ("ms_total", ctypes.c_double), ("ms_operators", ctypes.c_double),
                 ("ms_worst", ctypes.c_double), ("ms_adjoint", ctypes.c_double), ("ms_selfsupport", ctypes.c_double),
                 ("ms_mma", ctypes.c_double), ("solve_iterations", ctypes.c_int), ("mma_converged", ctypes.c_int)]
+
+
+class _SurfaceInfo(ctypes.Structure):
+    _fields_ = [("n_crossings", ctypes.c_longlong), ("n_first_pick", ctypes.c_longlong),
+                ("n_in_model", ctypes.c_longlong), ("n_points", ctypes.c_int), ("reserved", ctypes.c_int)]
 
 
 class _Region(ctypes.Structure):
@@ -153,6 +160,11 @@ SIGNATURES = {
     "rso_coeff2density": (_ci, [_vp, _vp, _vp, _vp]),
     "rso_density2coeff_adjoint": (_ci, [_vp, _vp, _vp, _vp]),
     "rso_selfsupport": (_ci, [_vp, _vp, _cd, _ci, _cd, _cd, _vp, _vp, _pd, _pd, _pd]),
+    "rso_surface_points": (_ci, [_vp, _vp, _ci, _ci, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_SurfaceInfo)]),
+    "rso_set_surface_points": (_ci, [_vp, _vp, _ci]),
+    "rso_get_surface_points": (_ci, [_vp, _vp, _ci, _pi]),
+    "rso_surface_selfsupport": (_ci, [_vp, _vp, _cd, _ci, _cd, _cd, _vp, _vp, _pd, _pd, _pd]),
+    "rso_get_surface_normals": (_ci, [_vp, _vp, _vp]),
     "rso_force_project": (_ci, [_vp, _vp, _ci]),
     "rso_worst_case": (_ci, [_vp, _ci, _ci, _cd, ctypes.c_uint64, _vp, _vp, _pd, _pd]),
     "rso_modified_pm": (_ci, [_vp, _ci, ctypes.c_uint64, _ci, _vp, _vp, _pd, _pi]),
@@ -706,6 +718,68 @@ class HierarchyGrid:
         self._chk(self.lib.rso_selfsupport(self.h, _dev(c), beta, mode, opt_angle, default_angle, _dev(per), _dev(dc),
                                            ctypes.byref(val), ctypes.byref(cnt), ctypes.byref(ds)), "rso_selfsupport")
         return val.value, per, dc, cnt.value, ds.value
+
+    # ------------------------------------------------------------ surface-point self-support
+    def generate_spline_surface_nodes(self, coeff, mc_res=64, n_points=200000, model_box=None):
+        """Sample rho = 0.5 of the spline design (Grid::generate_spline_surface_nodes,
+        grid/Grid.cpp:4067-4112); the points stay on the handle.  Returns the
+        points, a (3, n) CUDA tensor, and the sampling counts."""
+        c = self._efield(coeff)
+        box = None
+        if model_box is not None:
+            box = np.ascontiguousarray(model_box, np.float32)
+            if box.size != 6:
+                raise RSOError("model_box holds xmin, ymin, zmin, xmax, ymax, zmax")
+        info = _SurfaceInfo()
+        self._chk(self.lib.rso_surface_points(self.h, _dev(c), int(mc_res), int(n_points),
+                                              _np_ptr(box, ctypes.POINTER(ctypes.c_float)), ctypes.byref(info)),
+                  "rso_surface_points")
+        counts = dict(n_crossings=info.n_crossings, n_first_pick=info.n_first_pick, n_in_model=info.n_in_model,
+                      n_points=info.n_points)
+        return self.surface_points(), counts
+
+    def uploadSurfacePoints(self, xyz):
+        """Use the given points (3, n) for the surface constraint."""
+        import torch
+        x = xyz if isinstance(xyz, torch.Tensor) else torch.as_tensor(np.asarray(xyz, np.float32))
+        x = x.to(device="cuda", dtype=torch.float32).contiguous()
+        n = x.numel() // 3
+        self._chk(self.lib.rso_set_surface_points(self.h, _dev(x.view(-1)), n), "rso_set_surface_points")
+
+    def surface_points(self):
+        import torch
+        n = ctypes.c_int(0)
+        self._chk(self.lib.rso_get_surface_points(self.h, None, 0, ctypes.byref(n)), "rso_get_surface_points")
+        out = torch.empty(3 * n.value, dtype=torch.float32, device="cuda")
+        if n.value:
+            self._chk(self.lib.rso_get_surface_points(self.h, _dev(out), n.value, ctypes.byref(n)),
+                      "rso_get_surface_points")
+        return out.view(3, -1)
+
+    def deal_surface_points(self, coeff, beta, mode=4, opt_angle=0.75 * np.pi, default_angle=0.75 * np.pi):
+        """The constraint at the handle's surface points (grid/Grid.cu:5709-6505):
+        (value, per-point values, dvalue/dcoeff, count, probe sum)."""
+        import torch
+        c = self._efield(coeff)
+        n = ctypes.c_int(0)
+        self._chk(self.lib.rso_get_surface_points(self.h, None, 0, ctypes.byref(n)), "rso_get_surface_points")
+        per = torch.empty(max(n.value, 1), dtype=torch.float32, device="cuda")
+        dc = torch.empty(self.n_coeff, dtype=torch.float32, device="cuda")
+        val, cnt, ds = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_double(0)
+        self._chk(self.lib.rso_surface_selfsupport(self.h, _dev(c), beta, mode, opt_angle, default_angle, _dev(per),
+                                                   _dev(dc), ctypes.byref(val), ctypes.byref(cnt), ctypes.byref(ds)),
+                  "rso_surface_selfsupport")
+        return val.value, per[:n.value], dc, cnt.value, ds.value
+
+    def surface_normals(self):
+        """Outward normals (3, n) float64 and flags (2, n) of the last evaluation."""
+        import torch
+        n = ctypes.c_int(0)
+        self._chk(self.lib.rso_get_surface_points(self.h, None, 0, ctypes.byref(n)), "rso_get_surface_points")
+        nrm = torch.empty(3 * max(n.value, 1), dtype=torch.float64, device="cuda")
+        fl = torch.empty(2 * max(n.value, 1), dtype=torch.uint8, device="cuda")
+        self._chk(self.lib.rso_get_surface_normals(self.h, _dev(nrm), _dev(fl)), "rso_get_surface_normals")
+        return nrm[:3 * n.value].view(3, -1), fl[:2 * n.value].view(2, -1)
 
     # ------------------------------------------------------------ worst case
     def forceProject(self, f, constrain_direction):

@@ -16,10 +16,16 @@ as .npz files beside this script:
               and coeff2density (grid/Grid.cu:3405-3502) on a masked 16^3 grid
   filter.npz  filterSensitivity_kernel (grid/Grid.cu:4210-4309) on a masked
               16^3 grid at four radii
+  surface.npz the surface-point self-support pieces on a 16^3 box: background
+              marching-cubes values and positions (grid/Grid.cu:4109-4160),
+              generateEquidistantIntegers (grid/Grid.cpp:3831-3847), and at
+              seeded points the normals, orientation probes, flags, per-point
+              constraint values, means and coefficient gradients of all six
+              modes (grid/Grid.cu:5709-6505, grid/Grid.cpp:4263-4280)
 
 Needs the reference's sources (REF, default /root/reference) and g++; the
 fixtures it writes are committed, so the tests need neither.  Run:
-  python tests/golden/make_golden.py
+  python tests/golden/make_golden.py [fixture ...]   (default: all)
 """
 import os
 import subprocess
@@ -70,10 +76,41 @@ def masked_cube(e, seed):
     return m.astype(np.uint8)
 
 
-def main():
+def surface_fixture(p):
+    e, order, parts, mc = 16, 3, (4, 3, 5), 16
+    nb = [order + q for q in parts]
+    rng = np.random.default_rng(31)
+    coeff = rng.normal(0.5, 0.15, nb[0] * nb[1] * nb[2]).astype(np.float32)
+    # points inside the box where the spline support holds every one of them
+    pts = rng.uniform(0.25, e - 0.25, (3, 500)).astype(np.float32)
+    coeff.tofile(p("coeff")); pts.tofile(p("pts"))
+    beta, opt_ratio, default_ratio = 8.0, 0.75, 0.75
+    run(["surface", e, order, *parts, p("coeff"), mc, pts.shape[1], p("pts"), beta, opt_ratio, default_ratio,
+         p("mc"), p("eq"), p("po"), p("dc"), p("sc")])
+    n3 = (mc + 2) ** 3
+    npt = pts.shape[1]
+    po = np.fromfile(p("po"), np.float32)
+    out = dict(ereso=e, order=order, parts=np.array(parts, np.int32), mc=mc, coeff=coeff, pts=pts, beta=beta,
+               opt_ratio=opt_ratio, default_ratio=default_ratio,
+               mc_out=np.fromfile(p("mc"), np.float32).reshape(4, n3),
+               equi_pairs=np.array([[100, 10], [1000, 300], [1574, 1500], [12345, 600], [50, 49], [7, 3]], np.int64),
+               equi=np.fromfile(p("eq"), np.int32),
+               normals=po[:3 * npt].reshape(3, npt), direction=po[3 * npt:4 * npt], flag=po[4 * npt:5 * npt],
+               per=po[5 * npt:].reshape(6, npt),
+               dc=np.fromfile(p("dc"), np.float32).reshape(6, -1),
+               scalars=np.fromfile(p("sc"), np.float32))
+    np.savez_compressed(os.path.join(HERE, "surface.npz"), **out)
+
+
+def main(which=()):
     subprocess.run(["make", "-s", "-C", ORACLE, "ref"], check=True)
     with tempfile.TemporaryDirectory() as td:
         p = lambda name: os.path.join(td, name)  # noqa: E731
+        if which:
+            if "surface" in which:
+                surface_fixture(p)
+            print("wrote", ", ".join(f"{w}.npz" for w in which))
+            return 0
 
         # ------------------------------------------------------------- functions
         x = np.concatenate([np.linspace(-0.5, 2.5, 601), np.random.default_rng(1).uniform(-1, 3, 200),
@@ -145,8 +182,9 @@ def main():
             outs.append(np.fromfile(p("o"), np.float32))
         np.savez_compressed(os.path.join(HERE, "filter.npz"), ereso=e, mask=mask, sens=g,
                             radii=np.array(radii), out=np.stack(outs))
+        surface_fixture(p)
     print("wrote", ", ".join(f for f in sorted(os.listdir(HERE)) if f.endswith(".npz")))
 
 
 if __name__ == "__main__":
-    sys.exit(main())
+    sys.exit(main(tuple(sys.argv[1:])))

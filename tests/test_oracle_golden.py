@@ -2,8 +2,11 @@
 reference's own code (tests/golden/make_golden.py runs definitions extracted
 unmodified from the reference's sources and compiled on the host).  These pin
 the oracle's Heaviside projection and its chain (a17), the sensitivity filter
-(a18), the knot series, basis functions and density map of the spline (a19)
-and the self-support penalty functions (a21) to the reference's arithmetic.
+(a18), the knot series, basis functions and density map of the spline (a19),
+the self-support penalty functions (a21) and the surface-point self-support
+pieces (background marching-cubes values, equal-distance picks, normals,
+orientation, flags, per-point constraint and coefficient gradient) to the
+reference's arithmetic.
 
 The reference computes in FP32 and the oracle in FP64, so values agree to
 FP32 rounding: tolerances are stated per test relative to the magnitude of
@@ -121,3 +124,59 @@ def test_golden_filter(oracle):
     for r, ref in zip(g["radii"], g["out"]):
         out = o.filter(float(r), dense)
         assert close(out[flat], ref, 4e-6), r
+
+
+def surface_problem(oracle, g):
+    e = int(g["ereso"])
+    o = box_problem(oracle, np.ones((e, e, e), np.uint8))
+    o.spline_setup(int(g["order"]), [int(v) for v in g["parts"]])
+    return o
+
+
+def test_golden_surface_background(oracle):
+    """Background marching-cubes grid of a 16^3 model box at resolution 16
+    (grid/Grid.cu:4109-4160): cell-centre coordinates bit-identical (same float
+    arithmetic), values (spline - 0.5, 0 - 0.5 outside the box) within 1e-6;
+    equal-distance picks (grid/Grid.cpp:3831-3847) identical except where the
+    reference's last pick is one past the list, which the oracle clamps."""
+    g = golden("surface.npz")
+    o = surface_problem(oracle, g)
+    e, mc = int(g["ereso"]), int(g["mc"])
+    val, pos = o.mc_values(g["coeff"].astype(np.float64), mc, box=np.array([0, 0, 0, e, e, e], np.float32))
+    ref = g["mc_out"]
+    assert np.array_equal(pos, ref[:3])
+    assert np.abs(val - ref[3]).max() <= 1e-6
+    assert np.array_equal(val <= 0, ref[3] <= 0)
+    off = 0
+    for rng_, m in g["equi_pairs"]:
+        ref_idx = g["equi"][off:off + m]
+        off += m
+        idx = np.zeros(m, np.int64)
+        assert oracle.lib().or_equidistant(int(rng_), int(m), idx.ctypes.data_as(oracle._i64)) == m
+        assert np.array_equal(idx, np.minimum(ref_idx, rng_ - 1)), (rng_, m)
+    assert off == g["equi"].size
+
+
+def test_golden_surface_constraint(oracle):
+    """At 500 seeded points of the 16^3 box (order 3, 4x3x5 partitions, beta 8,
+    135 degree angles): the outward normals (spline gradient, flipped by the
+    orientation probes of grid/Grid.cu:5800-5943) within 2e-6 of the largest,
+    the probe sum and the overhang flags exact, and for each of the six modes
+    the per-point values within 1e-5, the count exact, the mean within 1e-5
+    and the coefficient gradient within 1e-5 of its largest entry (the
+    reference accumulates it in FP32)."""
+    g = golden("surface.npz")
+    o = surface_problem(oracle, g)
+    c = g["coeff"].astype(np.float64)
+    opt = float(np.float32(g["opt_ratio"] * np.pi))
+    dft = float(np.float32(g["default_ratio"] * np.pi))
+    sc = g["scalars"]
+    for mode in range(6):
+        r = o.surface_selfsupport(c, g["pts"], float(g["beta"]), mode, opt, dft)
+        assert r["dirsum"] == sc[0]
+        assert close(r["normals"], g["normals"], 2e-6)
+        assert np.array_equal(r["flags"][0], g["flag"].astype(np.uint8))
+        assert close(r["per"], g["per"][mode], 1e-5), mode
+        assert r["count"] == sc[1 + 2 * mode], mode
+        assert abs(r["value"] - sc[2 + 2 * mode]) <= 1e-5 * max(1.0, abs(sc[2 + 2 * mode])), mode
+        assert close(r["dc"], g["dc"][mode], 1e-5), mode

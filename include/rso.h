@@ -538,6 +538,12 @@ typedef struct {
   double opt_angle, default_angle;
   double sens_scale, vol_scale, ss_scale;  /* driver scalings (optimization.cpp:1008-1024) */
   uint64_t seed;
+  /* self-support variant: 0 evaluates it on the background elements
+   * (deal_background_points, optimization/optimization.cpp:1223-1242); n > 0
+   * on n surface points sampled from a ss_mc_res^3 background grid of the
+   * active elements' bounding box (deal_surface_points, :1185-1221) */
+  int ss_points;
+  int ss_mc_res;
 } rso_iter_params;
 
 typedef struct {

@@ -57,9 +57,15 @@ static rso_status evaluate_design(rso_handle* h, const double* c, const rso_iter
                      &ev->lambda, nullptr, &ev->iters));
   RSO_TRY(dot_host(h, h->fw, h->uw, n3, &ev->c_worst));
   const double t2 = now_ms();
-  // self-support (deal_background_points)
+  // self-support (deal_background_points, or deal_surface_points with surface points)
   ev->ss = 0;
-  if (ss) {
+  if (ss && prm->ss_points > 0) {
+    float box[6];
+    active_box(h, box);
+    RSO_TRY(surface_points(h, c, prm->ss_mc_res > 0 ? prm->ss_mc_res : 64, prm->ss_points, box, nullptr));
+    RSO_TRY(surface_selfsupport(h, c, prm->beta, prm->ss_mode, prm->opt_angle, prm->default_angle, nullptr, h->coef_b,
+                                &ev->ss, nullptr, nullptr));
+  } else if (ss) {
     RSO_TRY(selfsupport(h, c, prm->beta, prm->ss_mode, prm->opt_angle, prm->default_angle, nullptr, h->coef_b, &ev->ss,
                         nullptr, nullptr));
     RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -142,6 +148,8 @@ extern "C" void rso_default_iter_params(rso_iter_params* p) {
   p->vol_scale = 1e3;
   p->ss_scale = 1e3;
   p->seed = 1234;
+  p->ss_points = 0;
+  p->ss_mc_res = 64;
 }
 
 extern "C" rso_status rso_design_iteration(rso_handle* h, rso_mma* mma, const rso_iter_params* prm,

@@ -214,6 +214,14 @@ void vcycle_graphs_harvest(rso_handle* h);
 void vcycle_graphs_free(rso_handle* h);
 // surface-point self-support state (surface.cu)
 void surface_free(rso_handle* h);
+// bounding box {xmin, ymin, zmin, xmax, ymax, zmax} of the active elements
+void active_box(rso_handle* h, float box[6]);
+// the rho = 0.5 samples (kept on the handle) and the constraint at them;
+// c: n_coeff doubles on the device, dc (device, may be NULL) divided by the count
+rso_status surface_points(rso_handle* h, const double* c, int mc, int npts, const float* box, rso_surface_info* info);
+rso_status surface_selfsupport(rso_handle* h, const double* c, double beta, int mode, double opt_angle,
+                               double default_angle, float* per_out, double* dc, double* value, double* count,
+                               double* dirsum);
 }  // namespace rso
 
 // ---------------------------------------------------------------- helpers

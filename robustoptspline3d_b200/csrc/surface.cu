@@ -50,9 +50,7 @@ namespace rso {
 
 namespace {
 
-constexpr int SC_THREADS = 256;                 // compaction CTA
-constexpr int SC_PER_THREAD = 16;               // consecutive entries per thread
-constexpr int SC_CHUNK = SC_THREADS * SC_PER_THREAD;
+constexpr int SC_THREADS = 256;                 // compaction CTA; each thread takes PT consecutive entries
 constexpr int SP_THREADS = 256;                 // per-point kernels
 
 struct SplineP {
@@ -187,11 +185,11 @@ __device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned* total)
   return before;
 }
 
-template <class P>
+template <class P, int PT>
 __global__ void __launch_bounds__(SC_THREADS) k_sc_count(P pred, long long n, unsigned* __restrict__ cnt) {
-  const long long base = blockIdx.x * (long long)SC_CHUNK + (long long)threadIdx.x * SC_PER_THREAD;
+  const long long base = blockIdx.x * (long long)(SC_THREADS * PT) + (long long)threadIdx.x * PT;
   unsigned k = 0;
-  for (int i = 0; i < SC_PER_THREAD; i++)
+  for (int i = 0; i < PT; i++)
     if (base + i < n && pred(base + i)) k++;
   unsigned total;
   block_excl_scan(k, &total);
@@ -216,14 +214,15 @@ __global__ void __launch_bounds__(SC_THREADS) k_sc_scan(unsigned* __restrict__ c
   if (threadIdx.x == 0) cnt[nb] = total;
 }
 
-template <class P, class E>
+template <class P, class E, int PT>
 __global__ void __launch_bounds__(SC_THREADS) k_sc_emit(P pred, E emit, long long n, const unsigned* __restrict__ off) {
-  const long long base = blockIdx.x * (long long)SC_CHUNK + (long long)threadIdx.x * SC_PER_THREAD;
+  static_assert(PT <= 32, "one flag bit per entry");
+  const long long base = blockIdx.x * (long long)(SC_THREADS * PT) + (long long)threadIdx.x * PT;
   unsigned flags = 0, k = 0;
-  for (int i = 0; i < SC_PER_THREAD; i++)
+  for (int i = 0; i < PT; i++)
     if (base + i < n && pred(base + i)) { flags |= 1u << i; k++; }
   unsigned pos = off[blockIdx.x] + block_excl_scan(k, nullptr);
-  for (int i = 0; i < SC_PER_THREAD; i++)
+  for (int i = 0; i < PT; i++)
     if (flags >> i & 1u) emit(pos++, base + i);
 }
 
@@ -476,6 +475,8 @@ struct SurfState {
   double* scal = nullptr;             // probe sum, penalty sum, down count
   double* h_scal = nullptr;           // pinned mirror
   unsigned* h_cnt = nullptr;
+  bool have_box = false;              // bounding box of the active elements
+  float box[6];
 };
 
 static SurfState* surf(rso_handle* h) {
@@ -545,22 +546,51 @@ static SplineP spline_p(const rso_handle* h) {
   return S;
 }
 
-// order-preserving compaction of [0, n) under pred; returns the kept count
-template <class P, class E>
+// order-preserving compaction of [0, n) under pred, PT entries per thread;
+// returns the kept count
+template <int PT, class P, class E>
 static rso_status compact(rso_handle* h, P pred, E emit, long long n, long long* kept) {
   SurfState* s = surf(h);
-  const long long nb = (n + SC_CHUNK - 1) / SC_CHUNK;
+  const long long nb = (n + SC_THREADS * PT - 1) / (SC_THREADS * PT);
   *kept = 0;
   if (nb == 0) return RSO_OK;
   RSO_TRY(grow(h, &s->cnt, &s->cnt_cap, nb + 1));
-  k_sc_count<P><<<(int)nb, SC_THREADS, 0, h->stream>>>(pred, n, s->cnt); note_launch();
+  k_sc_count<P, PT><<<(int)nb, SC_THREADS, 0, h->stream>>>(pred, n, s->cnt); note_launch();
   k_sc_scan<<<1, SC_THREADS, 0, h->stream>>>(s->cnt, (int)nb); note_launch();
-  k_sc_emit<P, E><<<(int)nb, SC_THREADS, 0, h->stream>>>(pred, emit, n, s->cnt); note_launch();
+  k_sc_emit<P, E, PT><<<(int)nb, SC_THREADS, 0, h->stream>>>(pred, emit, n, s->cnt); note_launch();
   RSO_TRY(launch_check(h, "surface compaction"));
   RSO_CHECK_CUDA(h, cudaMemcpyAsync(s->h_cnt, s->cnt + nb, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   *kept = s->h_cnt[0];
   return RSO_OK;
+}
+
+// computed once per handle (the element mask does not change after rso_create)
+void active_box(rso_handle* h, float box[6]) {
+  SurfState* s = surf(h);
+  if (!s->have_box) {
+    const Level& l = h->L[0];
+    int lo[3] = {l.ex, l.ey, l.ez}, hi[3] = {-1, -1, -1};
+    const int dims[3] = {l.ex, l.ey, l.ez};
+    const uint8_t* m = h->h_emask[0].data();
+    for (int z = 0; z < l.ez; z++)
+      for (int y = 0; y < l.ey; y++, m += l.ex) {
+        int x0 = 0, x1 = l.ex - 1;
+        while (x0 < l.ex && !m[x0]) x0++;
+        if (x0 == l.ex) continue;
+        while (!m[x1]) x1--;
+        lo[0] = std::min(lo[0], x0); hi[0] = std::max(hi[0], x1);
+        lo[1] = std::min(lo[1], y); hi[1] = std::max(hi[1], y);
+        lo[2] = std::min(lo[2], z); hi[2] = std::max(hi[2], z);
+      }
+    for (int a = 0; a < 3; a++) {
+      if (hi[a] < 0) { lo[a] = 0; hi[a] = dims[a] - 1; }
+      s->box[a] = (float)lo[a];
+      s->box[3 + a] = (float)(hi[a] + 1);
+    }
+    s->have_box = true;
+  }
+  std::memcpy(box, s->box, sizeof(float) * 6);
 }
 
 rso_status surface_points(rso_handle* h, const double* c, int mc, int npts, const float* box,
@@ -584,7 +614,8 @@ rso_status surface_points(rso_handle* h, const double* c, int mc, int npts, cons
   // crossing edges, in edge order
   RSO_TRY(grow(h, &s->edges, &s->edge_cap, 3 * n3));
   long long num = 0;
-  RSO_TRY(compact(h, EdgePred{s->mcval, G.n}, EdgeEmit{s->edges}, 3 * n3, &num));
+  // 16 edges per thread (cheap tests), 2 candidates per thread in the pick (a crossing each)
+  RSO_TRY(compact<16>(h, EdgePred{s->mcval, G.n}, EdgeEmit{s->edges}, 3 * n3, &num));
   // first pick (3 npts of them when there are more than 2 npts per point), inside the model
   const bool thin = npts > 0 && num / npts > 2;
   const long long m1 = thin ? std::min<long long>(3ll * npts, num) : num;
@@ -593,7 +624,7 @@ rso_status surface_points(rso_handle* h, const double* c, int mc, int npts, cons
   if (m1 > 0) {
     PickPred pp{l, G, s->mcval, s->edges, num, thin ? 3ll * npts : num};
     PickEmit pe{G, s->mcval, s->edges, num, thin ? 3ll * npts : num, s->kept, s->kept_cap};
-    RSO_TRY(compact(h, pp, pe, m1, &nk));
+    RSO_TRY(compact<2>(h, pp, pe, m1, &nk));
   }
   if (npts > 0) {
     k_final_pick<<<cdiv(npts, SP_THREADS), SP_THREADS, 0, h->stream>>>(s->kept, s->kept_cap, nk, npts, s->xyz);
@@ -660,27 +691,13 @@ extern "C" rso_status rso_surface_points(rso_handle* h, const float* coeff, int 
                                          const float* model_box, rso_surface_info* info) {
   if (!h || !coeff || mc_res < 1 || mc_res > 1022 || n_points < 0) return RSO_ERR_INVALID_ARG;
   if (!h->sp.order) { h->err = "spline not set up"; return RSO_ERR_STATE; }
-  const Level& l = h->L[0];
   float box[6];
   if (model_box) {
     std::memcpy(box, model_box, sizeof(box));
     for (int a = 0; a < 3; a++)
       if (!(box[3 + a] > box[a])) { h->err = "empty model box"; return RSO_ERR_INVALID_ARG; }
   } else {
-    // bounding box of the active elements
-    int lo[3] = {l.ex, l.ey, l.ez}, hi[3] = {-1, -1, -1};
-    const int dims[3] = {l.ex, l.ey, l.ez};
-    const std::vector<uint8_t>& em = h->h_emask[0];
-    for (long long e = 0; e < (long long)em.size(); e++) {
-      if (!em[e]) continue;
-      const int ix[3] = {(int)(e % l.ex), (int)(e / l.ex % l.ey), (int)(e / ((long long)l.ex * l.ey))};
-      for (int a = 0; a < 3; a++) { lo[a] = std::min(lo[a], ix[a]); hi[a] = std::max(hi[a], ix[a]); }
-    }
-    for (int a = 0; a < 3; a++) {
-      if (hi[a] < 0) { lo[a] = 0; hi[a] = dims[a] - 1; }
-      box[a] = (float)lo[a];
-      box[3 + a] = (float)(hi[a] + 1);
-    }
+    active_box(h, box);
   }
   RSO_TRY(coeff_in(h, coeff));
   RSO_TRY(surface_points(h, h->coef_a, mc_res, n_points, box, info));

@@ -55,7 +55,8 @@ class _IterParams(ctypes.Structure):
                 ("filter_mode", ctypes.c_int), ("lanczos_steps", ctypes.c_int), ("solve_tol", ctypes.c_double),
                 ("constrain_direction", ctypes.c_int), ("ss_mode", ctypes.c_int), ("opt_angle", ctypes.c_double),
                 ("default_angle", ctypes.c_double), ("sens_scale", ctypes.c_double), ("vol_scale", ctypes.c_double),
-                ("ss_scale", ctypes.c_double), ("seed", ctypes.c_uint64)]
+                ("ss_scale", ctypes.c_double), ("seed", ctypes.c_uint64), ("ss_points", ctypes.c_int),
+                ("ss_mc_res", ctypes.c_int)]
 
 
 class _IterInfo(ctypes.Structure):
@@ -303,6 +304,8 @@ class IterParams:
     vol_scale: float = 1e3
     ss_scale: float = 1e3
     seed: int = 1234
+    ss_points: int = 0       # > 0: the self-support constraint on that many surface points
+    ss_mc_res: int = 64
 
     def _c(self):
         c = _IterParams()

@@ -180,3 +180,36 @@ def test_surface_gradient_fd(oracle, cuda, mode):
               o.surface_selfsupport(cm, gd["pts"], 8.0, mode)["value"]) / (2 * h)
         assert abs(fd - dc[i]) <= 1e-5 * np.abs(dc).max() + 1e-4 * abs(fd), (i, fd, dc[i])
     g.close()
+
+
+def test_design_gradient_surface_points(oracle, cuda):
+    """The design driver with the surface-point variant (IterParams.ss_points):
+    its self-support value and gradient equal those of the sampling and the
+    constraint called on their own, and match the oracle at the oracle's
+    points (the coefficients are FP32 values, as the C ABI takes them)."""
+    import robustoptspline3d_b200 as R
+    n = 16
+    em = np.ones((n, n, n), np.uint8)
+    fa = np.zeros((n + 1,) * 3, np.uint8)
+    fa[0] = 1
+    la = np.zeros_like(fa)
+    la[n] = 1
+    g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=R.rso.FP64, smoother=R.rso.SMOOTH_JACOBI, omega=0.6))
+    nc = g.set_spline_partition(4, 4, 4, 4)
+    c32 = np.random.default_rng(5).uniform(0, 1, nc).astype(np.float32)
+    for mode in (4, 5):
+        prm = R.IterParams(beta=8.0, filter_mode=1, lanczos_steps=6, solve_tol=1e-8, ss_mode=mode, ss_points=500,
+                           ss_mc_res=20)
+        vals, _, _, gs = g.design_gradient(c32.astype(np.float64), prm)
+        pts, counts = g.generate_spline_surface_nodes(c32, mc_res=20, n_points=500)
+        val, _, dc, _, _ = g.deal_surface_points(c32, 8.0, mode)
+        assert vals["ss"] == val
+        assert maxrel(gs.cpu().numpy(), dc.cpu().numpy()) <= 1e-6
+        o = oracle.Problem(em, fa, la, n_levels=1)
+        o.spline_setup(4, (4, 4, 4))
+        opts, oinfo = o.surface_points(c32.astype(np.float64), mc=20, n_points=500)
+        assert counts["n_crossings"] == oinfo[0]
+        r = o.surface_selfsupport(c32.astype(np.float64), opts, 8.0, mode)
+        assert abs(val - r["value"]) <= 1e-9 * max(1.0, abs(r["value"]))
+        assert maxrel(gs.cpu().numpy(), r["dc"]) <= 1e-6
+    g.close()

@@ -208,6 +208,25 @@ def smoother_id(R):
     return {"chebyshev": R.rso.SMOOTH_CHEBYSHEV, "jacobi": R.rso.SMOOTH_JACOBI, "gs": R.rso.SMOOTH_GS}[SMOOTHER]
 
 
+def kernel_classes(g):
+    """Per-class CUDA-event profile recorded on handle g: launches, mean
+    microseconds and algorithmic GB/s of each class that ran."""
+    import ctypes
+    lib = g.lib
+    name = ctypes.create_string_buffer(64)
+    cnt, tot, b, fl = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    classes = {}
+    for cls in range(16):
+        if lib.rso_profile_class(g.h, cls, name, 64, ctypes.byref(cnt), ctypes.byref(tot), ctypes.byref(b),
+                                 ctypes.byref(fl)) != 0:
+            break
+        if cnt.value:
+            avg = tot.value / cnt.value / 1e3
+            classes[name.value.decode()] = {"launches": cnt.value, "avg_us": avg * 1e6,
+                                            "algorithmic_GBps": b.value / avg / 1e9}
+    return classes
+
+
 def run_solves(args):
     """Multigrid-preconditioned CG solves on the initial design's density."""
     import ctypes
@@ -242,17 +261,7 @@ def run_solves(args):
         ms += t
         worst = max(worst, rr)
     lib.rso_set_profiling(g.h, 0)
-    name = ctypes.create_string_buffer(64)
-    cnt, tot, b, fl = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
-    classes = {}
-    for cls in range(16):
-        if lib.rso_profile_class(g.h, cls, name, 64, ctypes.byref(cnt), ctypes.byref(tot), ctypes.byref(b),
-                                 ctypes.byref(fl)) != 0:
-            break
-        if cnt.value:
-            avg = tot.value / cnt.value / 1e3
-            classes[name.value.decode()] = {"launches": cnt.value, "avg_us": avg * 1e6,
-                                            "algorithmic_GBps": b.value / avg / 1e9}
+    classes = kernel_classes(g)
     print(json.dumps({"metric": f"multigrid PCG solve @{n}^3 to rel.resid 1e-6 ({args.precision})",
                       "value": ms / args.steps, "unit": "ms/solve", "higher_is_better": False,
                       "iterations_per_solve": its / args.steps, "ms_per_iteration": ms / its,
@@ -619,8 +628,15 @@ def run_scale(args):
             torch.cuda.synchronize()
             times.append(time.perf_counter() - t1)
         x_new = mma.get()[0]
+        # one more iteration with per-class CUDA-event timing (not among the timed ones)
+        g.lib.rso_profile_reset(g.h)
+        g.lib.rso_set_profiling(g.h, 1)
+        mma.set_x(c0)
+        g.design_iteration(mma, prm)
+        g.lib.rso_set_profiling(g.h, 0)
         res[prec] = dict(vals=vals, gl=gl.cpu().numpy(), x=x_new, s=min(times[1:]), info=info, setup_s=setup_s,
-                         levels=[g.level_dims(i)[:3].tolist() for i in range(g.n_levels())])
+                         levels=[g.level_dims(i)[:3].tolist() for i in range(g.n_levels())],
+                         classes=kernel_classes(g), nodes=int(np.prod(g.level_dims(0)[3:6])))
         mma.close()
         g.close()
         del g, gl, gv, gs, c0
@@ -637,6 +653,9 @@ def run_scale(args):
                               "dlambda_dcoeff": rel(m["gl"], d["gl"]),
                               "coefficients_after_mma": rel(m["x"], d["x"])},
            "setup_s": {"mixed": m["setup_s"], "fp64": d["setup_s"]},
+           "kernel_classes": {"mixed": m["classes"], "fp64": d["classes"]},
+           "fine_ns_per_node": {k: v["avg_us"] * 1e3 / m["nodes"] for k, v in m["classes"].items()
+                                if k.startswith("fine_")},
            "config": {"workload": "511x256x256 voxels (embedded 512x256x256), 200 spherical voids r~U[4,20]",
                       "load": "x=511 node plane, force along +x (constrained direction)", "support": "x=0 nodes",
                       "spline": f"order {order}, partition {parts}", "solve_tol": {"mixed": 1e-6, "fp64": 1e-10},

@@ -76,3 +76,18 @@ def read_density(prefix):
     if len(pos) != len(val):
         raise ValueError("density records of different lengths")
     return pos, val
+
+
+def write_coeff(path, coeff):
+    """The spline coefficients as float32 raw elements (HierarchyGrid::writeCoeff,
+    grid/Grid.cpp:2140-2156, written by the drivers as <out>/coeff)."""
+    write_vector(path, np.asarray(coeff, np.float32).ravel(), np.float32)
+
+
+def read_coeff(path, n_coeff=None):
+    """Coefficients written by write_coeff; with n_coeff, the count is checked
+    against the handle's spline (a file of another partition is refused)."""
+    c = read_vector(path, np.float32)
+    if n_coeff is not None and c.size != n_coeff:
+        raise ValueError(f"coefficient file holds {c.size} values, the spline has {n_coeff}")
+    return c

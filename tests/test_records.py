@@ -44,3 +44,17 @@ def test_density_records_round_trip(tmp_path):
     back = np.zeros_like(rho)
     back[pos[:, 2], pos[:, 1], pos[:, 0]] = val
     assert np.array_equal(back, rho * em)
+
+
+def test_coeff_round_trip(tmp_path):
+    """writeCoeff's layout: float32 raw elements; a file of another size is refused."""
+    import pytest
+    from robustoptspline3d_b200 import records
+    c = np.random.default_rng(3).uniform(0, 1, 7 * 8 * 9)
+    p = str(tmp_path / "coeff")
+    records.write_coeff(p, c)
+    assert os.path.getsize(p) == 4 * c.size
+    back = records.read_coeff(p, c.size)
+    assert back.dtype == np.float32 and np.array_equal(back, c.astype(np.float32))
+    with pytest.raises(ValueError):
+        records.read_coeff(p, c.size + 1)

@@ -325,6 +325,14 @@ rso_status rso_autotune(rso_handle* h, int* choices_host);
  * bottom level -2 restores the built-in size rule, a row-split entry of -1
  * too), e.g. to reuse choices measured once for many handles. */
 rso_status rso_set_launch_shapes(rso_handle* h, const int* choices_host, int n);
+/* Node planes per z chunk of the packed FP32 fine kernel (4, 8, 16 or 32; 0
+ * restores the size rule: the longest chunk that gives the grid 4 CTAs per
+ * SM).  A CTA marches its chunk plane by plane and re-reads the plane below
+ * it, so short chunks fill the GPU on small grids at the price of that plane;
+ * rso_autotune measures the lengths.  rso_fine_zchunk returns the length in
+ * use. */
+rso_status rso_set_fine_zchunk(rso_handle* h, int planes);
+int rso_fine_zchunk(const rso_handle* h);
 /* Replay of the FP32 V-cycle (the mixed-precision preconditioner) from CUDA
  * graphs (no counterpart in the reference, which launches every kernel):
  * on by default.  The V-cycle is captured the second time its launch
@@ -334,6 +342,17 @@ rso_status rso_set_launch_shapes(rso_handle* h, const int* choices_host, int n);
  * handle's own or one set by rso_set_stream other than the legacy default
  * stream; if a capture fails the handle keeps to plain launches. */
 rso_status rso_set_vcycle_graphs(rso_handle* h, int on);
+/* Device-controlled solves (no counterpart in the reference): with on != 0
+ * the mixed-precision PCG loop with the FP32 recurrence runs as one CUDA
+ * graph per solve, a conditional WHILE node whose body holds the iteration
+ * (q = K p, the residual update, the V-cycle, the direction update) and a
+ * conditional IF node for the FP64 residual replacement; the decisions the
+ * host takes between iterations otherwise (replace, stop, stall) are taken by
+ * one-thread kernels on the same scalars, so the iterations, iterates and
+ * residuals are those of the host-driven loop.  Used when the V-cycle graphs
+ * are on and per-kernel profiling is off; a failed capture falls back to the
+ * host-driven loop.  Off by default. */
+rso_status rso_set_solve_graphs(rso_handle* h, int on);
 /* Krylov recurrence of the mixed-precision PCG (no counterpart in the
  * reference, whose CG is FP64).  0 < replace_factor < 1 (1e-2 by default in
  * mixed precision): the recurrence runs in FP32 (FP32 operator, FP32

@@ -5,7 +5,9 @@
 // CUDA events, one after the other, and the fastest is kept in h->tune:
 //   - thread rows of a CTA of the packed FP32 fine kernel (2, 4 or 8: 32 x 4,
 //     32 x 8 or 32 x 16 element columns per CTA; the smaller tiles give small
-//     grids more CTAs, the larger ones less halo per node),
+//     grids more CTAs, the larger ones less halo per node) and the node planes
+//     of its z chunks (32 down to 4: shorter chunks give small grids more CTAs
+//     and each re-reads one plane),
 //   - per coarse level, one thread per node (k_coarse) or per (node, row)
 //     (k_coarse_r),
 //   - the first level of the bottom cluster kernel (or none).
@@ -106,6 +108,14 @@ rso_status autotune(rso_handle* h) {
   RSO_TRY(launch_check(h, "autotune rhs"));
   // fine kernel tile, with the built-in rules for the rest
   RSO_TRY(pick(h, {4, 2, 8}, [&](int v) { h->tune.fine_rows = v; }));
+  // its z chunk: the size rule's choice first, then the other lengths
+  {
+    h->tune.fine_zc = 0;
+    std::vector<int> zc = {fine_zc(h)};
+    for (int v = kFineZcMax; v >= kFineZcMin; v /= 2)
+      if (v != zc.front()) zc.push_back(v);
+    RSO_TRY(pick(h, zc, [&](int v) { h->tune.fine_zc = v; }));
+  }
   // first level of the bottom cluster kernel, or none
   h->tune.bottom = 1;
   if (nl >= 3 && bottom_level(h) == 1) {
@@ -154,7 +164,7 @@ extern "C" rso_status rso_autotune(rso_handle* h, int* choices_host) {
     return st;
   }
   if (choices_host) {
-    choices_host[0] = h->tune.fine_rows;
+    choices_host[0] = h->tune.fine_rows;  // the z chunk is read with rso_fine_zchunk
     choices_host[1] = bottom_level(h);
     for (int li = 0; li < (int)h->L.size(); li++) choices_host[2 + li] = li > 0 && li < 16 ? h->tune.rowsplit[li] : -1;
   }
@@ -174,6 +184,7 @@ extern "C" rso_status rso_set_launch_shapes(rso_handle* h, const int* choices_ho
     return RSO_ERR_INVALID_ARG;
   }
   rso_handle::Tune t;
+  t.fine_zc = h->tune.fine_zc;  // set on its own (rso_set_fine_zchunk)
   t.fine_rows = choices_host[0];
   t.bottom = b;
   for (int li = 0; li < nl && 2 + li < n && li < 16; li++) {

@@ -131,6 +131,7 @@ static void free_handle(rso_handle* h) {
   cudaFree(h->coef_df); cudaFree(h->coef_dg); cudaFree(h->fw); cudaFree(h->uw);
   cudaFree(h->wc_buf);
   vcycle_graphs_free(h);
+  solve_graphs_free(h);
   surface_free(h);
   prof_free(h);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -167,7 +168,8 @@ static rso_status setup(rso_handle* h, int ex, int ey, int ez, const uint8_t* em
     // one partial per CTA of the fine operator kernels: 31 x 7 nodes per
     // z-chunk of 32 planes (FP64), 31 x 3 or 31 x 7 (packed FP32, 2 or 4 rows)
     const Level& f0 = h->L[0];
-    h->fpart_n = (long long)cdiv(f0.nx, 31) * cdiv(f0.ny, 3) * cdiv(f0.nz, 32);
+    // the smallest fine-kernel tile: 2 thread rows (3 new element rows), z chunks of kFineZcMin planes
+    h->fpart_n = (long long)cdiv(f0.nx, 31) * cdiv(f0.ny, 3) * cdiv(f0.nz, kFineZcMin);
     ALLOC(h->fpart, sizeof(double) * h->fpart_n);
   }
   // per-level buffers
@@ -487,6 +489,20 @@ extern "C" rso_status rso_prolong_fp32(rso_handle* h, int cl, const double* uc, 
 extern "C" rso_status rso_set_vcycle_graphs(rso_handle* h, int on) {
   if (!h) return RSO_ERR_INVALID_ARG;
   h->vc_graphs = on != 0;
+  return RSO_OK;
+}
+
+extern "C" rso_status rso_set_fine_zchunk(rso_handle* h, int planes) {
+  if (!h || (planes != 0 && planes != 4 && planes != 8 && planes != 16 && planes != 32)) return RSO_ERR_INVALID_ARG;
+  h->tune.fine_zc = planes;
+  return RSO_OK;
+}
+
+extern "C" int rso_fine_zchunk(const rso_handle* h) { return h ? fine_zc(h) : 0; }
+
+extern "C" rso_status rso_set_solve_graphs(rso_handle* h, int on) {
+  if (!h) return RSO_ERR_INVALID_ARG;
+  h->solve_graphs = on != 0;
   return RSO_OK;
 }
 

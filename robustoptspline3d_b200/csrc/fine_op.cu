@@ -579,7 +579,7 @@ template <int MODE, int TYP, bool TMA>
 __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
     k_fine_p(const Level L, const float* __restrict__ u, const float* __restrict__ f, float* __restrict__ out,
              const float* __restrict__ rp, float omega, double* __restrict__ dotp, const float* __restrict__ uprev,
-             float c1, const __grid_constant__ CUtensorMap tmu, const __grid_constant__ CUtensorMap tmr) {
+             float c1, int fzc, const __grid_constant__ CUtensorMap tmu, const __grid_constant__ CUtensorMap tmr) {
   constexpr int RX = 36, ROWS = 2 * TYP, NPL = RX * (ROWS + 1), NT = WTX * TYP;
   constexpr int NS = pair_slots(MODE, TMA);
   constexpr bool LEAN = MODE == 2 && TMA;  // operands of the emitted plane re-read from the slots
@@ -593,8 +593,9 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
   float* sx = ss + NS * SLOT;                  // [2][4][3][NT] corner exchange, by plane parity
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * WTX + tx;
   const int x0 = blockIdx.x * (WTX - 1), y0 = blockIdx.y * (ROWS - 1);
-  const int nzc = (L.nz + FZC - 1) / FZC, bsys = blockIdx.z / nzc;
-  const int z0 = (blockIdx.z - bsys * nzc) * FZC, z1 = min(z0 + FZC, L.nz);
+  // blockIdx.z = z chunk of fzc node planes + (number of chunks) * system
+  const int nzc = (L.nz + fzc - 1) / fzc, bsys = blockIdx.z / nzc;
+  const int z0 = (blockIdx.z - bsys * nzc) * fzc, z1 = min(z0 + fzc, L.nz);
   {
     const long long off = (long long)bsys * 3 * L.NP;
     u += off;
@@ -1159,8 +1160,9 @@ static inline dim3 march_grid(const Level& l) {
 }
 constexpr bool kPairTMA = true;  // packed kernel stages with TMA (else cp.async)
 // thread rows pty of the packed FP32 kernel (2 pty element rows; rso_autotune picks 2 or 4)
-static inline dim3 pair_grid(const Level& l, int pty) {
-  return dim3(cdiv(l.nx, WTX - 1), cdiv(l.ny, 2 * pty - 1), cdiv(l.nz, FZC) * l.nb);
+// and its z chunk of fzc node planes
+static inline dim3 pair_grid(const Level& l, int pty, int fzc) {
+  return dim3(cdiv(l.nx, WTX - 1), cdiv(l.ny, 2 * pty - 1), cdiv(l.nz, fzc) * l.nb);
 }
 
 template <typename T>
@@ -1168,6 +1170,23 @@ static inline int pcls(int c32, int c64) { return sizeof(T) == 4 ? c32 : c64; }
 // thread rows of the packed kernel's CTA (2, 4 or 8; 4 unless tuned)
 static inline int fine_pty(const rso_handle* h) {
   return h->tune.fine_rows == 2 || h->tune.fine_rows == 8 ? h->tune.fine_rows : 4;
+}
+// z chunk of the packed kernel: the tuned value, else the largest of 32, 16,
+// 8, 4 planes that gives the grid at least 4 CTAs per SM (a CTA marches its
+// chunk plane by plane, so small levels need short chunks to fill the GPU;
+// each chunk re-reads one plane below it)
+int fine_zc(const rso_handle* h) {
+  const int t = h->tune.fine_zc;
+  if (t == 4 || t == 8 || t == 16 || t == 32) return t;
+  const Level& l = h->L[0];
+  const int pty = fine_pty(h);
+  int zc = kFineZcMax;
+  while (zc > kFineZcMin) {
+    const dim3 g = pair_grid(l, pty, zc);
+    if ((long long)g.x * g.y * g.z >= 4LL * 148) break;
+    zc /= 2;
+  }
+  return zc;
 }
 
 // cuTensorMapEncodeTiled from the driver, looked up once through the runtime
@@ -1266,18 +1285,19 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
     if (done) done->store(true, std::memory_order_release);
   }
   if constexpr (packed) {
+    const int fzc = fine_zc(h);
     CUtensorMap mu{}, mr{};
     if (kPairTMA) RSO_TRY(pair_tensor_maps(h, l, u, rp, 2 * pty, &mu, &mr));
     if (h->prof_on) prof_begin(h, cls, (double)l.nn);
     if (pty == 2)
-      k_fine_p<MODE, 2, kPairTMA><<<pair_grid(l, 2), dim3(WTX, 2), smem, h->stream>>>(
-          l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, mu, mr);
+      k_fine_p<MODE, 2, kPairTMA><<<pair_grid(l, 2, fzc), dim3(WTX, 2), smem, h->stream>>>(
+          l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, fzc, mu, mr);
     else if (pty == 8)
-      k_fine_p<MODE, 8, kPairTMA><<<pair_grid(l, 8), dim3(WTX, 8), smem, h->stream>>>(
-          l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, mu, mr);
+      k_fine_p<MODE, 8, kPairTMA><<<pair_grid(l, 8, fzc), dim3(WTX, 8), smem, h->stream>>>(
+          l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, fzc, mu, mr);
     else
-      k_fine_p<MODE, 4, kPairTMA><<<pair_grid(l, 4), dim3(WTX, 4), smem, h->stream>>>(
-          l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, mu, mr);
+      k_fine_p<MODE, 4, kPairTMA><<<pair_grid(l, 4, fzc), dim3(WTX, 4), smem, h->stream>>>(
+          l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, fzc, mu, mr);
   } else {
     if (h->prof_on) prof_begin(h, cls, (double)l.nn);
     k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega, dotp,
@@ -1313,7 +1333,7 @@ rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const doub
 // dot_dev[b * stride] per system of a batch
 rso_status fine_applyK_dot32(rso_handle* h, const float* u, float* f, double* dot_dev, int stride) {
   const Level& l0 = h->L[0];
-  const dim3 g = pair_grid(l0, fine_pty(h));
+  const dim3 g = pair_grid(l0, fine_pty(h), fine_zc(h));
   const long long nb = (long long)g.x * g.y * g.z;  // all systems
   if (nb > h->fpart_n) {
     h->err = "fine partial-sum buffer smaller than the grid";

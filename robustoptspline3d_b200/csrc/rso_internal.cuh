@@ -170,6 +170,7 @@ struct rso_handle {
   // launch shapes chosen by rso_autotune (autotune.cu); -1 / -2 keep the built-in rules
   struct Tune {
     int fine_rows = 4;      // thread rows of a CTA of the packed FP32 fine kernel (2, 4 or 8)
+    int fine_zc = 0;        // node planes per z chunk of that kernel (4, 8, 16 or 32; 0: by size)
     int rowsplit[16];       // per level: 1 one thread per (node, row), 0 one per node, -1 by size
     int bottom = -2;        // first level of the bottom cluster kernel, -1 none, -2 by size
     Tune() { for (int& r : rowsplit) r = -1; }
@@ -189,6 +190,10 @@ struct rso_handle {
   void* vcg = nullptr;                             // captured FP32 V-cycles (solver.cu)
   void* cap_prof = nullptr;                        // event pairs of the V-cycle capture in progress (prof.cu)
   bool vc_graphs = true;                           // replay captured V-cycles (rso_set_vcycle_graphs)
+  // run the FP32-Krylov PCG loop as one captured graph whose iterations and
+  // residual replacements are decided on the device (rso_set_solve_graphs)
+  bool solve_graphs = false;
+  void* sgc = nullptr;                             // captured solve graphs (solver.cu)
   void* surf = nullptr;                            // surface-point self-support state (surface.cu)
 };
 
@@ -212,6 +217,10 @@ void prof_harvest(rso_handle* h, void* pairs);
 // captured V-cycles (solver.cu)
 void vcycle_graphs_harvest(rso_handle* h);
 void vcycle_graphs_free(rso_handle* h);
+void solve_graphs_free(rso_handle* h);
+// node planes per z chunk of the packed FP32 fine kernel (fine_op.cu)
+constexpr int kFineZcMax = 32, kFineZcMin = 4;
+int fine_zc(const rso_handle* h);
 // surface-point self-support state (surface.cu)
 void surface_free(rso_handle* h);
 // bounding box {xmin, ymin, zmin, xmax, ymax, zmax} of the active elements

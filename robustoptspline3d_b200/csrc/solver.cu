@@ -248,10 +248,12 @@ void push_bits(std::vector<uint64_t>& k, X v) {
   k.push_back(b);
 }
 
-std::vector<uint64_t> vc_key(const rso_handle* h) {
+// rotating = false leaves the rotating level vectors (u32, r32, t32) out
+std::vector<uint64_t> vc_key(const rso_handle* h, bool rotating = true) {
   std::vector<uint64_t> k;
   for (const Level& l : h->L) {
-    push_bits(k, l.u32); push_bits(k, l.f32); push_bits(k, l.r32); push_bits(k, l.t32);
+    push_bits(k, rotating ? l.u32 : nullptr); push_bits(k, l.f32);
+    push_bits(k, rotating ? l.r32 : nullptr); push_bits(k, rotating ? l.t32 : nullptr);
     push_bits(k, l.st32); push_bits(k, l.vclass); push_bits(k, l.emask);
     push_bits(k, l.NP); push_bits(k, l.nn); push_bits(k, l.nb); push_bits(k, l.lam);
     push_bits(k, l.nx); push_bits(k, l.ny); push_bits(k, l.nz); push_bits(k, l.px); push_bits(k, l.py);
@@ -261,7 +263,7 @@ std::vector<uint64_t> vc_key(const rso_handle* h) {
   push_bits(k, h->c_K); push_bits(k, h->c_nodes); push_bits(k, h->c_f); push_bits(k, h->c_fb); push_bits(k, h->nc);
   push_bits(k, h->cfg.smoother); push_bits(k, h->cfg.pre); push_bits(k, h->cfg.post);
   push_bits(k, h->cfg.omega); push_bits(k, h->cfg.cheb_lower); push_bits(k, h->prof_on);
-  push_bits(k, h->tune.fine_rows); push_bits(k, h->tune.bottom);
+  push_bits(k, h->tune.fine_rows); push_bits(k, h->tune.fine_zc); push_bits(k, h->tune.bottom);
   for (int r : h->tune.rowsplit) push_bits(k, r);
   return k;
 }
@@ -444,6 +446,322 @@ constexpr int kCycleMax = 30;
 double stall_ratio(double factor, double claimed) {
   return std::max(std::max(0.5, std::sqrt(factor)), std::sqrt(std::max(claimed, 0.0)));
 }
+// ---------------------------------------------------------------- device-controlled solve
+// The loop of solve_pcg_k32 below as one CUDA graph of kSolveUnroll
+// iterations, each three conditional IF nodes: the first holds q = K p with
+// p.q, alpha, the recursive residual update and a one-thread control kernel
+// (k_pcg_ctl_a); the second the FP64 residual replacement and its control
+// kernel (k_pcg_ctl_b); the third the V-cycle, r.z, beta and the direction
+// update.  The control kernels take the host loop's decisions on the same
+// device scalars with the same double arithmetic, so the graph reproduces the
+// host loop's iterations; when the solve stops they switch off every later
+// iteration of the graph.  The graph is straight-line (no WHILE node), so a
+// launch ends after at most kSolveUnroll iterations whatever the control
+// kernels decide; the host launches it again while the solve goes on.
+constexpr int kSolveUnroll = 16;
+struct PcgCtl {
+  double fn, tol, krylov32, rbase, rel, rnorm;
+  int max_iter, cycles_max, it, since, cycles, replace, status, done, n_rep, n_cont;
+};
+enum { PCG_RUNNING = 0, PCG_STALLED = 1, PCG_NONFINITE = 2 };
+struct PcgGo {
+  cudaGraphConditionalHandle go[kSolveUnroll];  // one per unrolled iteration
+};
+
+__device__ __forceinline__ void pcg_stop(PcgCtl* c, const PcgGo& g, int i) {
+  c->done = 1;
+  for (int j = i + 1; j < kSolveUnroll; j++) cudaGraphSetConditional(g.go[j], 0);
+}
+
+// after the recursive residual update: s[5] = r.r
+__global__ void k_pcg_ctl_a(PcgCtl* c, const double* s, PcgGo g, int i, cudaGraphConditionalHandle hr,
+                            cudaGraphConditionalHandle hc) {
+  const double rnorm = sqrt(s[5]);
+  c->it++;
+  c->since++;
+  c->rnorm = rnorm;
+  if (!isfinite(rnorm)) {
+    c->status = PCG_NONFINITE;
+    c->replace = 0;
+    cudaGraphSetConditional(hr, 0);
+    cudaGraphSetConditional(hc, 0);
+    pcg_stop(c, g, i);
+    return;
+  }
+  const bool rep = rnorm < c->krylov32 * c->rbase || rnorm < c->tol * c->fn || c->it >= c->max_iter ||
+                   c->since >= kCycleMax;
+  c->replace = rep;
+  if (rep) {
+    c->n_rep++;
+  } else {
+    c->rel = rnorm / c->fn;
+    c->n_cont++;
+  }
+  cudaGraphSetConditional(hr, rep ? 1u : 0u);
+  cudaGraphSetConditional(hc, rep ? 0u : 1u);
+}
+
+__device__ __forceinline__ double stall_ratio_dev(double factor, double claimed) {
+  return fmax(fmax(0.5, sqrt(factor)), sqrt(fmax(claimed, 0.0)));
+}
+
+// after the replacement: s[8] = true r.r
+__global__ void k_pcg_ctl_b(PcgCtl* c, const double* s, PcgGo g, int i, cudaGraphConditionalHandle hc) {
+  const double rtrue = sqrt(s[8]);
+  c->rel = rtrue / c->fn;
+  if (!isfinite(c->rel)) {
+    c->status = PCG_NONFINITE;
+    pcg_stop(c, g, i);
+    return;
+  }
+  if (c->rel < c->tol || c->it >= c->max_iter) {
+    pcg_stop(c, g, i);
+    return;
+  }
+  c->cycles++;
+  if (rtrue > stall_ratio_dev(c->krylov32, c->rnorm / c->rbase) * c->rbase ||
+      (c->cycles_max > 0 && c->cycles >= c->cycles_max)) {
+    c->status = PCG_STALLED;  // the true residual of x is in r
+    pcg_stop(c, g, i);
+    return;
+  }
+  c->rbase = rtrue;
+  c->since = 0;
+  c->n_cont++;
+  cudaGraphSetConditional(hc, 1);
+}
+
+// the direction update of k_cg32_step_dir with the step taken or not as the
+// control block says (after a replacement x has taken it already)
+__global__ void k_cg32_step_dir_ctl(long long n4, const double* __restrict__ alpha, const double* __restrict__ beta,
+                                    const float4* __restrict__ z, float4* __restrict__ p, double2* __restrict__ x,
+                                    const PcgCtl* __restrict__ c) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n4) return;
+  const float4 pi = p[i], zi = z[i];
+  if (!c->replace) {
+    const double a = *alpha;
+    double2 x0 = x[2 * i], x1 = x[2 * i + 1];
+    x0.x += a * pi.x;
+    x0.y += a * pi.y;
+    x1.x += a * pi.z;
+    x1.y += a * pi.w;
+    x[2 * i] = x0;
+    x[2 * i + 1] = x1;
+  }
+  const float b = (float)*beta;
+  p[i] = make_float4(zi.x + b * pi.x, zi.y + b * pi.y, zi.z + b * pi.z, zi.w + b * pi.w);
+}
+
+namespace {
+struct SolveGraph {
+  std::vector<uint64_t> key;
+  cudaGraphExec_t exec = nullptr;
+  long long k_iter = 0, k_rep = 0, k_cont = 0;  // kernels per iteration / replacement / continuation
+};
+struct SolveGraphs {
+  std::vector<SolveGraph> graphs;
+  PcgCtl* ctl = nullptr;
+  PcgCtl* h_ctl = nullptr;
+  cudaStream_t cs = nullptr;
+  bool broken = false;
+};
+constexpr size_t kMaxSolveGraphs = 4;
+
+// the launches a captured body records go to the capture stream
+struct StreamSwap {
+  rso_handle* h;
+  cudaStream_t saved;
+  StreamSwap(rso_handle* hh, cudaStream_t s) : h(hh), saved(hh->stream) { h->stream = s; }
+  ~StreamSwap() { h->stream = saved; }
+};
+
+long long count_kernels(cudaGraph_t g) {
+  size_t n = 0;
+  cudaGraphGetNodes(g, nullptr, &n);
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (n) cudaGraphGetNodes(g, nodes.data(), &n);
+  long long k = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+  }
+  return k;
+}
+
+// adds to G an IF node on handle hc after `dep` (none if null) whose body
+// records the launches of `body`, captured on stream cs
+template <class F>
+rso_status add_if(rso_handle* h, cudaGraph_t G, cudaGraphNode_t* dep, cudaGraphConditionalHandle hc,
+                  cudaStream_t cs, F body, cudaGraphNode_t* node, long long* kernels) {
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = hc;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  if (cudaGraphAddNode(node, G, dep, dep ? 1 : 0, &cp) != cudaSuccess) return RSO_ERR_CUDA;
+  cudaGraph_t bg = cp.conditional.phGraph_out[0];
+  if (cudaStreamBeginCaptureToGraph(cs, bg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+    return RSO_ERR_CUDA;
+  rso_status r;
+  {
+    StreamSwap sw(h, cs);
+    r = body();
+  }
+  cudaGraph_t out = nullptr;
+  if (cudaStreamEndCapture(cs, &out) != cudaSuccess) r = RSO_ERR_CUDA;
+  *kernels = count_kernels(bg);
+  return r;
+}
+}  // namespace
+
+void solve_graphs_free(rso_handle* h) {
+  SolveGraphs* c = (SolveGraphs*)h->sgc;
+  if (!c) return;
+  for (auto& g : c->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  cudaFree(c->ctl);
+  if (c->h_ctl) cudaFreeHost(c->h_ctl);
+  if (c->cs) cudaStreamDestroy(c->cs);
+  delete c;
+  h->sgc = nullptr;
+}
+
+// Builds the unrolled graph of the loop for iterate x and right-hand side f
+// (FP64, padded); the V-cycle's rotating level vectors are left as they were.
+static rso_status build_solve_graph(rso_handle* h, SolveGraphs* c, const double* f, double* x, SolveGraph* g) {
+  Level& l0 = h->L[0];
+  const long long n3 = 3 * l0.NP, n4 = n3 / 4;
+  double* s = h->scal;
+  float* r32 = l0.f32;
+  float* p32 = reinterpret_cast<float*>(h->z);
+  float* q32 = reinterpret_cast<float*>(h->q);
+  PcgCtl* ctl = c->ctl;
+  const std::vector<uint64_t> rot = vc_rotating(h);
+  cudaGraph_t G = nullptr;
+  rso_status st = RSO_OK;
+  do {
+    if (cudaGraphCreate(&G, 0) != cudaSuccess) { st = RSO_ERR_CUDA; break; }
+    PcgGo go;
+    cudaGraphConditionalHandle hr[kSolveUnroll], hc[kSolveUnroll];
+    for (int i = 0; i < kSolveUnroll && st == RSO_OK; i++)
+      if (cudaGraphConditionalHandleCreate(&go.go[i], G, 1, cudaGraphCondAssignDefault) != cudaSuccess ||
+          cudaGraphConditionalHandleCreate(&hr[i], G, 0, cudaGraphCondAssignDefault) != cudaSuccess ||
+          cudaGraphConditionalHandleCreate(&hc[i], G, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+        st = RSO_ERR_CUDA;
+    if (st != RSO_OK) break;
+    cudaGraphNode_t prev = nullptr, node = nullptr;
+    for (int i = 0; i < kSolveUnroll && st == RSO_OK; i++) {
+      long long k1 = 0, kr = 0, kc = 0;
+      st = add_if(h, G, prev ? &prev : nullptr, go.go[i], c->cs, [&]() -> rso_status {
+        RSO_TRY(fine_applyK_dot32(h, p32, q32, s + 1));
+        k_cg_alpha<<<1, 1, 0, h->stream>>>(s);
+        RSO_TRY(cg32_resid_rr(h, n3, s + 2, q32, r32, s + 5));
+        k_pcg_ctl_a<<<1, 1, 0, h->stream>>>(ctl, s, go, i, hr[i], hc[i]);
+        return launch_check(h, "pcg graph");
+      }, &node, &k1);
+      if (st != RSO_OK) break;
+      prev = node;
+      // the FP64 residual replacement
+      st = add_if(h, G, &prev, hr[i], c->cs, [&]() -> rso_status {
+        k_cg32_step<<<cdiv(n4, 256), 256, 0, h->stream>>>(n4, s + 2, reinterpret_cast<const float4*>(p32),
+                                                          reinterpret_cast<double2*>(x));
+        RSO_TRY(fine_residual<double>(h, x, f, h->r, h->rp64));
+        RSO_TRY(dot(h, h->r, h->r, n3, s + 8));
+        k_pcg_ctl_b<<<1, 1, 0, h->stream>>>(ctl, s, go, i, hc[i]);
+        k_d2f<<<cdiv(n3, 256), 256, 0, h->stream>>>(h->r, r32, n3);
+        return launch_check(h, "pcg graph");
+      }, &node, &kr);
+      if (st != RSO_OK) break;
+      prev = node;
+      // the V-cycle and the direction update
+      st = add_if(h, G, &prev, hc[i], c->cs, [&]() -> rso_status {
+        RSO_TRY(vcycle_mixed_launches(h));
+        const float* z32 = l0.u32;
+        RSO_TRY(dot_ff(h, r32, z32, n3, s + 3));
+        k_cg_beta<<<1, 1, 0, h->stream>>>(s);
+        k_cg32_step_dir_ctl<<<cdiv(n4, 256), 256, 0, h->stream>>>(
+            n4, s + 2, s + 4, reinterpret_cast<const float4*>(z32), reinterpret_cast<float4*>(p32),
+            reinterpret_cast<double2*>(x), ctl);
+        return launch_check(h, "pcg graph");
+      }, &node, &kc);
+      if (st != RSO_OK) break;
+      prev = node;
+      vc_set_rotating(h, rot);  // every unrolled V-cycle starts from the same vectors
+      g->k_iter = k1; g->k_rep = kr; g->k_cont = kc;
+    }
+    if (st != RSO_OK) break;
+    if (cudaGraphInstantiate(&g->exec, G, 0) != cudaSuccess) { g->exec = nullptr; st = RSO_ERR_CUDA; }
+  } while (false);
+  if (G) cudaGraphDestroy(G);
+  vc_set_rotating(h, rot);
+  cudaGetLastError();  // a failed capture leaves its error here
+  return st;
+}
+
+// Runs the loop from the state solve_pcg_k32 prepared (p, r32, q, s[0] = r.z)
+// on the device.  Returns RSO_ERR_UNSUPPORTED when no graph could be made
+// (nothing has run then; the host loop takes over).
+static rso_status pcg32_graph(rso_handle* h, const double* f, double* x, double tol, int max_iter, double fn,
+                              double rbase, int* it, double* rel, bool* stalled) {
+  if (!h->sgc) h->sgc = new SolveGraphs();
+  SolveGraphs* c = (SolveGraphs*)h->sgc;
+  if (c->broken) return RSO_ERR_UNSUPPORTED;
+  if (!c->ctl) {
+    if (cudaMalloc((void**)&c->ctl, sizeof(PcgCtl)) != cudaSuccess ||
+        cudaMallocHost((void**)&c->h_ctl, sizeof(PcgCtl)) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->cs, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      c->broken = true;
+      return RSO_ERR_UNSUPPORTED;
+    }
+  }
+  // what vc_key holds without the rotating level vectors (the graph does not
+  // depend on which of them a V-cycle starts from), and the loop's own vectors
+  std::vector<uint64_t> key = vc_key(h, false);
+  push_bits(key, f); push_bits(key, x); push_bits(key, h->z); push_bits(key, h->q); push_bits(key, h->r);
+  push_bits(key, h->rp64); push_bits(key, h->scal);
+  SolveGraph* g = nullptr;
+  for (auto& e : c->graphs)
+    if (e.key == key) g = &e;
+  if (!g) {
+    SolveGraph ng;
+    ng.key = key;
+    if (build_solve_graph(h, c, f, x, &ng) != RSO_OK) {
+      if (ng.exec) cudaGraphExecDestroy(ng.exec);
+      c->broken = true;
+      return RSO_ERR_UNSUPPORTED;
+    }
+    if (c->graphs.size() >= kMaxSolveGraphs) {
+      cudaGraphExecDestroy(c->graphs.front().exec);
+      c->graphs.erase(c->graphs.begin());
+    }
+    c->graphs.push_back(ng);
+    g = &c->graphs.back();
+  }
+  PcgCtl& hc = *c->h_ctl;
+  hc = PcgCtl{};
+  hc.fn = fn; hc.tol = tol; hc.krylov32 = h->krylov32; hc.rbase = rbase;
+  hc.max_iter = max_iter; hc.cycles_max = h->krylov32_cycles;
+  RSO_CHECK_CUDA(h, cudaMemcpyAsync(c->ctl, c->h_ctl, sizeof(PcgCtl), cudaMemcpyHostToDevice, h->stream));
+  // each launch runs at most kSolveUnroll iterations; the control block says
+  // when the solve has stopped
+  const int max_launches = max_iter / kSolveUnroll + 2;
+  for (int launch = 0;; launch++) {
+    RSO_CHECK_CUDA(h, cudaGraphLaunch(g->exec, h->stream));
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(c->h_ctl, c->ctl, sizeof(PcgCtl), cudaMemcpyDeviceToHost, h->stream));
+    RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (hc.done) break;
+    if (launch + 1 >= max_launches) { h->err = "device-controlled PCG did not stop"; return RSO_ERR_STATE; }
+  }
+  note_launches(g->k_iter * hc.it + g->k_rep * hc.n_rep + g->k_cont * hc.n_cont);
+  *it = hc.it;
+  *rel = hc.rel;
+  if (hc.status == PCG_NONFINITE) { h->err = "non-finite residual in PCG"; return RSO_ERR_NONFINITE; }
+  *stalled = hc.status == PCG_STALLED;
+  return RSO_OK;
+}
+
 static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, double tol, int max_iter,
                                 rso_solve_info* info, bool* stalled, int* used) {
   Level& l0 = h->L[0];
@@ -484,6 +802,13 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
     RSO_TRY(vcycle_mixed(h));
     RSO_CHECK_CUDA(h, cudaMemcpyAsync(p32, l0.u32, sizeof(float) * n3, cudaMemcpyDeviceToDevice, h->stream));
     RSO_TRY(dot_ff(h, r32, l0.u32, n3, s + 0));
+    rso_status gs = RSO_ERR_UNSUPPORTED;
+    if (h->solve_graphs && h->vc_graphs && !h->prof_on && h->stream && max_iter > 0)
+      gs = pcg32_graph(h, f, x, tol, max_iter, fn, rbase, &it, &rel, stalled);
+    if (gs != RSO_ERR_UNSUPPORTED) {
+      RSO_TRY(gs);
+      max_iter = 0;  // the loop below has run on the device
+    }
     while (it < max_iter) {
       RSO_TRY(fine_applyK_dot32(h, p32, q32, s + 1));
       k_cg_alpha<<<1, 1, 0, h->stream>>>(s); rso::note_launch();

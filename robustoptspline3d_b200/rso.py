@@ -112,6 +112,9 @@ SIGNATURES = {
     "rso_residual": (_ci, [_vp, _vp, _vp, _vp]),
     "rso_fine_sweep_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
     "rso_set_vcycle_graphs": (_ci, [_vp, _ci]),
+    "rso_set_solve_graphs": (_ci, [_vp, _ci]),
+    "rso_set_fine_zchunk": (_ci, [_vp, _ci]),
+    "rso_fine_zchunk": (_ci, [_vp]),
     "rso_set_krylov_fp32": (_ci, [_vp, _cd]),
     "rso_set_krylov_fp32_cycles": (_ci, [_vp, _ci]),
     "rso_displacement_project": (_ci, [_vp, _vp]),
@@ -470,7 +473,8 @@ class HierarchyGrid:
         (rso_autotune); returns the choices."""
         c = np.zeros(2 + self.n_levels(), np.int32)
         self._chk(self.lib.rso_autotune(self.h, _np_ptr(c, _pi)), "rso_autotune")
-        return {"fine_rows": int(c[0]), "bottom_level": int(c[1]), "row_split": [int(x) for x in c[2:]]}
+        return {"fine_rows": int(c[0]), "fine_zchunk": self.fine_zchunk(), "bottom_level": int(c[1]),
+                "row_split": [int(x) for x in c[2:]]}
 
     def set_launch_shapes(self, fine_rows=4, bottom_level=-2, row_split=None):
         """Launch shapes in rso_autotune's terms (rso_set_launch_shapes)."""
@@ -516,6 +520,17 @@ class HierarchyGrid:
     def set_vcycle_graphs(self, on):
         """Replay captured FP32 V-cycles from CUDA graphs (default) or launch every kernel."""
         self._chk(self.lib.rso_set_vcycle_graphs(self.h, 1 if on else 0), "rso_set_vcycle_graphs")
+
+    def set_fine_zchunk(self, planes=0):
+        """Node planes per z chunk of the FP32 fine kernel (4, 8, 16, 32; 0: by size)."""
+        self._chk(self.lib.rso_set_fine_zchunk(self.h, int(planes)), "rso_set_fine_zchunk")
+
+    def fine_zchunk(self):
+        return int(self.lib.rso_fine_zchunk(self.h))
+
+    def set_solve_graphs(self, on):
+        """Run the mixed PCG loop as one device-controlled CUDA graph per solve."""
+        self._chk(self.lib.rso_set_solve_graphs(self.h, 1 if on else 0), "rso_set_solve_graphs")
 
     def fine_sweep_fp32(self, op, u, f=None, uprev=None, omega=1.0, c1=0.0):
         """One FP32 fine-level sweep (op 0 residual, 1 K u, 2 Jacobi/Chebyshev step), FP64 in and out."""

@@ -43,6 +43,7 @@ def test_autotune_choices_solve_alike(cuda, gen):
     u_ref = u_ref.cpu().numpy()
     ch = g.autotune()
     assert ch["fine_rows"] in (2, 4, 8)
+    assert ch["fine_zchunk"] in (4, 8, 16, 32)
     assert ch["bottom_level"] == -1 or 1 <= ch["bottom_level"] <= nl - 2
     assert len(ch["row_split"]) == nl and all(r in (-1, 0, 1) for r in ch["row_split"])
     u, it, _, _ = g.solve(f, tol=1e-10, max_iter=300)
@@ -65,4 +66,34 @@ def test_launch_shapes_rejected(cuda):
         g.set_launch_shapes(3)
     with pytest.raises(RSOError):
         g.set_launch_shapes(4, bottom_level=g.n_levels())
+    g.close()
+
+
+@pytest.mark.parametrize("rows", [2, 4, 8])
+def test_fine_zchunk_sweeps_identical(cuda, rows):
+    """The z chunk only cuts the march into pieces that re-read the plane below
+    them: residual, K u and Jacobi / Chebyshev sweeps are bit-identical for
+    chunks of 4, 8, 16 and 32 node planes (with 41 planes the last chunk is
+    short), and PCG solves agree to 1e-8 with iteration counts within one
+    (the p.q partial sums are grouped by chunk)."""
+    g = make(P.cantilever(40, 24, 40))
+    g.set_launch_shapes(fine_rows=rows)
+    rng = np.random.default_rng(7)
+    u = cuda.tensor(rng.standard_normal(3 * g.nn), dtype=cuda.float64, device="cuda")
+    f = cuda.tensor(rhs(g), dtype=cuda.float64, device="cuda")
+    ref = None
+    for zc in (32, 16, 8, 4):
+        g.set_fine_zchunk(zc)
+        assert g.fine_zchunk() == zc
+        out = [g.fine_sweep_fp32(0, u, f).cpu().numpy(), g.fine_sweep_fp32(1, u).cpu().numpy(),
+               g.fine_sweep_fp32(2, u, f, uprev=u, omega=0.7, c1=0.3).cpu().numpy()]
+        x, it, rr, _ = g.solve(f, tol=1e-10, max_iter=300)
+        if ref is None:
+            ref = (out, x.cpu().numpy(), it)
+            continue
+        for a, b in zip(out, ref[0]):
+            assert np.array_equal(a, b), zc
+        assert abs(it - ref[2]) <= 1 and rel(x.cpu().numpy(), ref[1]) < 1e-8
+    g.set_fine_zchunk(0)
+    assert g.fine_zchunk() in (4, 8, 16, 32)
     g.close()

@@ -8,8 +8,8 @@
 //     grids more CTAs, the larger ones less halo per node) and the node planes
 //     of its z chunks (32 down to 4: shorter chunks give small grids more CTAs
 //     and each re-reads one plane),
-//   - per coarse level, one thread per node (k_coarse) or per (node, row)
-//     (k_coarse_r),
+//   - per coarse level, one thread per node (k_coarse4 / k_coarse), per
+//     (node, row) (k_coarse_r) or nine per node (k_coarse_r9),
 //   - the first level of the bottom cluster kernel (or none).
 // Each candidate is timed as whole solves (see solve_ms).
 // The candidates compute the same arithmetic; only launch shapes differ.  The
@@ -119,7 +119,7 @@ rso_status autotune(rso_handle* h) {
   // first level of the bottom cluster kernel, or none
   h->tune.bottom = 1;
   if (nl >= 3 && bottom_level(h) == 1) {
-    std::vector<int> cands = {-2, -1};
+    std::vector<int> cands = {-1};  // the built-in rule (none) first
     for (int lb = nl - 2; lb >= 1; lb--) {
       bool small = true;
       for (int li = lb; li < nl; li++) small = small && h->L[li].nn <= kTuneBottomMaxNodes;
@@ -131,9 +131,14 @@ rso_status autotune(rso_handle* h) {
   }
   // coarse kernel variant of each level the bottom kernel does not take
   const int lb = bottom_level(h);
-  for (int li = 1; li < nl - 1 && li < 16 && (lb < 0 || li < lb); li++)
-    RSO_TRY(pick(h, {h->L[li].nn > 100000 ? 0 : 1, h->L[li].nn > 100000 ? 1 : 0},
-                 [&](int v) { h->tune.rowsplit[li] = v; }));
+  for (int li = 1; li < nl - 1 && li < 16 && (lb < 0 || li < lb); li++) {
+    // the size rule's variant first, then the others
+    h->tune.rowsplit[li] = -1;
+    std::vector<int> v = {coarse_variant_of(h, li)};
+    for (int k = 0; k <= 2; k++)
+      if (k != v.front()) v.push_back(k);
+    RSO_TRY(pick(h, v, [&](int x) { h->tune.rowsplit[li] = x; }));
+  }
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
   // graphs captured for the rejected candidates are never replayed again
   vcycle_graphs_free(h);
@@ -189,8 +194,8 @@ extern "C" rso_status rso_set_launch_shapes(rso_handle* h, const int* choices_ho
   t.bottom = b;
   for (int li = 0; li < nl && 2 + li < n && li < 16; li++) {
     const int r = choices_host[2 + li];
-    if (r < -1 || r > 1) {
-      h->err = "row split choices are -1, 0 or 1";
+    if (r < -1 || r > 2) {
+      h->err = "coarse kernel choices are -1 (size rule), 0 (per node), 1 (per node and row) or 2 (nine per node)";
       return RSO_ERR_INVALID_ARG;
     }
     t.rowsplit[li] = li > 0 ? r : -1;

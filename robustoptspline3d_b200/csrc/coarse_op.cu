@@ -329,6 +329,77 @@ __global__ void __launch_bounds__(32 * CTY * 3) k_coarse_r(const Level L, const 
   out[n + r * NP] = ur + c1 * (ur - pr) + (omega / det) * (a0 * r0 + a1 * r1 + a2 * r2);
 }
 
+// Small levels (a few thousand to a few ten thousand nodes): the per-row
+// kernel above leaves most of the GPU idle and each thread with a chain of 81
+// stencil and 81 vector loads.  Here nine threads share a node: thread (r, pz)
+// takes row r over the nine neighbours of plane z - 1 + pz (27 loads of each),
+// and the three planes' partial sums meet in shared memory.  Same arithmetic
+// per plane as k_coarse_r, summed plane by plane (the FP32 result may differ in
+// the last bits).  MODE 0 residual, MODE 2 damped block Jacobi / Chebyshev step.
+constexpr int CTY9 = 2;
+template <typename T, int MODE>
+__global__ void __launch_bounds__(32 * CTY9 * 9) k_coarse_r9(const Level L, const T* __restrict__ st,
+                                                             const T* __restrict__ u, const T* __restrict__ f,
+                                                             T* __restrict__ out, T omega,
+                                                             const T* __restrict__ uprev, T c1) {
+  __shared__ T spart[3][3][CTY9][32];  // [plane][row]
+  __shared__ T sres[3][CTY9][32];
+  const int bsys = blockIdx.z / L.nz;
+  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * CTY9 + threadIdx.y, z = blockIdx.z - bsys * L.nz;
+  {
+    const long long off = (long long)bsys * 3 * L.NP;
+    u += off;
+    f += off;
+    out += off;
+    if (uprev != nullptr) uprev += off;
+  }
+  const int r = threadIdx.z % 3, pz = threadIdx.z / 3;
+  const bool in = x < L.nx && y < L.ny;
+  const long long NP = L.NP, px = L.px, pxy = (long long)L.px * L.py;
+  const long long n = in ? L.nidx(x, y, z) : 0;
+  const bool act = in && (L.vclass[n] & NC_ACTIVE) != 0;
+  T acc = 0;
+  if (act) {
+#pragma unroll
+    for (int d9 = 0; d9 < 9; d9++) {
+      const int d = pz * 9 + d9;
+      const long long nb = n + (d % 3 - 1) + (d / 3 % 3 - 1) * px + (d / 9 - 1) * pxy;
+      acc = fma(st[st_at<T>(NP, d * 9 + r * 3 + 0, n)], u[nb], acc);
+      acc = fma(st[st_at<T>(NP, d * 9 + r * 3 + 1, n)], u[nb + NP], acc);
+      acc = fma(st[st_at<T>(NP, d * 9 + r * 3 + 2, n)], u[nb + 2 * NP], acc);
+    }
+  }
+  spart[pz][r][threadIdx.y][threadIdx.x] = acc;
+  __syncthreads();
+  if (pz == 0) {
+    const T a = spart[0][r][threadIdx.y][threadIdx.x] + spart[1][r][threadIdx.y][threadIdx.x] +
+                spart[2][r][threadIdx.y][threadIdx.x];
+    if (MODE == 0) {
+      if (in) out[n + r * NP] = f[n + r * NP] - a;
+      return;
+    }
+    sres[r][threadIdx.y][threadIdx.x] = act ? f[n + r * NP] - a : T(0);
+  }
+  if (MODE == 0) return;
+  __syncthreads();
+  if (pz != 0 || !in) return;
+  if (!act) { out[n + r * NP] = 0; return; }
+  T S[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) S[i] = st[st_at<T>(NP, 13 * 9 + i, n)];
+  // row r of the adjugate of the 3x3 diagonal block
+  const T c00 = S[4] * S[8] - S[5] * S[7], c01 = -(S[3] * S[8] - S[5] * S[6]), c02 = S[3] * S[7] - S[4] * S[6];
+  const T det = S[0] * c00 + S[1] * c01 + S[2] * c02;
+  T a0, a1, a2;
+  if (r == 0) { a0 = c00; a1 = -(S[1] * S[8] - S[2] * S[7]); a2 = S[1] * S[5] - S[2] * S[4]; }
+  else if (r == 1) { a0 = c01; a1 = S[0] * S[8] - S[2] * S[6]; a2 = -(S[0] * S[5] - S[2] * S[3]); }
+  else { a0 = c02; a1 = -(S[0] * S[7] - S[1] * S[6]); a2 = S[0] * S[4] - S[1] * S[3]; }
+  const T r0 = sres[0][threadIdx.y][threadIdx.x], r1 = sres[1][threadIdx.y][threadIdx.x],
+          r2 = sres[2][threadIdx.y][threadIdx.x];
+  const T ur = u[n + r * NP], pr = uprev ? uprev[n + r * NP] : T(0);
+  out[n + r * NP] = ur + c1 * (ur - pr) + (omega / det) * (a0 * r0 + a1 * r1 + a2 * r2);
+}
+
 // one colour of the point Gauss-Seidel sweep on stored stencils (gs_relax_kernel grid/Grid.cu:1497-1609)
 template <typename T>
 __global__ void __launch_bounds__(256) k_coarse_gs(const Level L, const T* __restrict__ st, T* __restrict__ u,
@@ -787,16 +858,16 @@ __global__ void k_gemv_scatter(const Level C, const double* __restrict__ Kinv, c
 }
 
 // ---------------------------------------------------------------- bottom of the V-cycle
-// The small levels (at most kBottomMaxNodes nodes each) and the coarsest
-// solve run as one kernel on an 8-CTA thread-block cluster: a sweep on a
-// 17^3-node level is a few microseconds of work, less than a launch, so
-// every phase (Jacobi sweeps, residual, restriction, dense coarsest solve,
-// prolongation) is separated by a cluster barrier instead of a launch.  A
-// cluster rather than one CTA because a single SM cannot pull the level's
-// stencils from L2 fast enough.  Damped Jacobi only; results are left in the
-// levels' u vectors exactly as the per-level launches leave them.
+// The small levels and the coarsest solve as one kernel on an 8-CTA
+// thread-block cluster: every phase (Jacobi / Chebyshev sweeps, residual,
+// restriction, dense coarsest solve, prolongation) is separated by a cluster
+// barrier instead of a launch.  Results are left in the levels' u vectors
+// exactly as the per-level launches leave them.  Measured on cubes from 32^3
+// to 256^3 the phases wait on load latency with 8 SMs working, and the
+// per-level launches over the whole GPU are faster (the 17^3 to 5^3 levels of
+// a 256^3 hierarchy: 3 % of a solve), so it runs only when rso_autotune finds
+// it faster on the handle's own problem.
 constexpr int BOT_CTAS = 8, BOT_THREADS = 1024, BOT_MAX_LEVELS = 12;
-static const long long kBottomMaxNodes = 6000;
 
 constexpr int BOT_MAX_SWEEPS = 8;
 template <typename T>
@@ -1048,12 +1119,17 @@ const double* stencil_of<double>(const Level& l) { return l.st64; }
 template <>
 const float* stencil_of<float>(const Level& l) { return l.st32; }
 
-// one thread per node on large levels, per (node, row) on small ones, unless
-// rso_autotune measured the level
-static bool node_per_thread(const rso_handle* h, int level) {
+// kernel variant of a coarse level: 0 one thread per node (large levels), 1
+// one per (node, row) (the rest), 2 nine per node (k_coarse_r9: only when
+// rso_autotune finds it faster; on cubes from 32^3 to 256^3 it measured
+// slower than 1 on every level), unless rso_autotune measured the level
+static int coarse_variant(const rso_handle* h, int level) {
   const int t = level < 16 ? h->tune.rowsplit[level] : -1;
-  return t >= 0 ? t == 0 : h->L[level].nn > kRowSplitMaxNodes;
+  if (t >= 0 && t <= 2) return t;
+  return h->L[level].nn > kRowSplitMaxNodes ? 0 : 1;
 }
+static bool node_per_thread(const rso_handle* h, int level) { return coarse_variant(h, level) == 0; }
+int coarse_variant_of(const rso_handle* h, int level) { return coarse_variant(h, level); }
 
 // profiling class of a coarse sweep: the streamed FP32 kernel has its own
 static int coarse_class(const rso_handle* h, int level, int elem_size) {
@@ -1076,6 +1152,8 @@ rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* 
       k_coarse<T, 0, 4><<<chunk_grid(l, 4), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0));
     }
     rso::note_launch();
+  } else if (coarse_variant(h, level) == 2) {
+    k_coarse_r9<T, 0><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY9), l.nz * l.nb), dim3(32, CTY9, 9), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0)); rso::note_launch();
   } else {
     k_coarse_r<T, 0><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz * l.nb), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u, f, r, T(0), (const T*)nullptr, T(0)); rso::note_launch();
   }
@@ -1099,6 +1177,8 @@ rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T*
       k_coarse<T, 2, 4><<<chunk_grid(l, 4), dim3(32, 8), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1);
     }
     rso::note_launch();
+  } else if (coarse_variant(h, level) == 2) {
+    k_coarse_r9<T, 2><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY9), l.nz * l.nb), dim3(32, CTY9, 9), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1); rso::note_launch();
   } else {
     k_coarse_r<T, 2><<<dim3(cdiv(l.nx, 32), cdiv(l.ny, CTY), l.nz * l.nb), dim3(32, CTY, 3), 0, h->stream>>>(l, stencil_of<T>(l), u_in, f, u_out, (T)omega, u_prev, (T)c1); rso::note_launch();
   }
@@ -1174,8 +1254,8 @@ rso_status coarsest_solve(rso_handle* h, const T* f, T* u) {
 }
 
 // index of the first level handled by k_bottom (-1: none).  It needs damped
-// Jacobi, at least one smoothed level above the coarsest, and every level from
-// it down small enough.
+// Jacobi or Chebyshev, at least one smoothed level above the coarsest, and a
+// level chosen by rso_autotune.
 int bottom_level(const rso_handle* h) {
   const int nl = (int)h->L.size();
   if (h->cfg.smoother == RSO_SMOOTH_GS || nl < 3 || nl > BOT_MAX_LEVELS || h->nc == 0) return -1;
@@ -1183,9 +1263,10 @@ int bottom_level(const rso_handle* h) {
   // a level chosen by rso_autotune: any level from 1 to nl - 2, or none
   if (h->tune.bottom == -1) return -1;
   if (h->tune.bottom >= 1 && h->tune.bottom <= nl - 2) return h->tune.bottom;
-  int lb = nl - 1;
-  while (lb - 1 >= 1 && h->L[lb - 1].nn <= kBottomMaxNodes) lb--;
-  return lb <= nl - 2 ? lb : -1;
+  // built-in rule: none.  The cluster kernel's phases run on 8 SMs and wait on
+  // load latency; separate launches over the whole GPU measured faster on
+  // cubes from 32^3 to 256^3 (rso_autotune still tries it)
+  return -1;
 }
 
 template <typename T>

@@ -171,7 +171,7 @@ struct rso_handle {
   struct Tune {
     int fine_rows = 4;      // thread rows of a CTA of the packed FP32 fine kernel (2, 4 or 8)
     int fine_zc = 0;        // node planes per z chunk of that kernel (4, 8, 16 or 32; 0: by size)
-    int rowsplit[16];       // per level: 1 one thread per (node, row), 0 one per node, -1 by size
+    int rowsplit[16];       // per level: 0 one thread per node, 1 per (node, row), 2 nine per node, -1 by size
     int bottom = -2;        // first level of the bottom cluster kernel, -1 none, -2 by size
     Tune() { for (int& r : rowsplit) r = -1; }
   } tune;
@@ -221,6 +221,8 @@ void solve_graphs_free(rso_handle* h);
 // node planes per z chunk of the packed FP32 fine kernel (fine_op.cu)
 constexpr int kFineZcMax = 32, kFineZcMin = 4;
 int fine_zc(const rso_handle* h);
+// kernel variant of a coarse level: 0 per node, 1 per (node, row), 2 nine threads per node (coarse_op.cu)
+int coarse_variant_of(const rso_handle* h, int level);
 // surface-point self-support state (surface.cu)
 void surface_free(rso_handle* h);
 // bounding box {xmin, ymin, zmin, xmax, ymax, zmax} of the active elements

@@ -45,12 +45,12 @@ def test_autotune_choices_solve_alike(cuda, gen):
     assert ch["fine_rows"] in (2, 4, 8)
     assert ch["fine_zchunk"] in (4, 8, 16, 32)
     assert ch["bottom_level"] == -1 or 1 <= ch["bottom_level"] <= nl - 2
-    assert len(ch["row_split"]) == nl and all(r in (-1, 0, 1) for r in ch["row_split"])
+    assert len(ch["row_split"]) == nl and all(r in (-1, 0, 1, 2) for r in ch["row_split"])
     u, it, _, _ = g.solve(f, tol=1e-10, max_iter=300)
     assert abs(it - it_ref) <= 1 and rel(u.cpu().numpy(), u_ref) < 1e-8
     for rows in (2, 4):
         for bottom in [-1] + list(range(1, nl - 1)):
-            for split in (0, 1):
+            for split in (0, 1, 2):
                 g.set_launch_shapes(rows, bottom, [-1] + [split] * (nl - 1))
                 u, it, rr, _ = g.solve(f, tol=1e-10, max_iter=300)
                 assert rr < 1e-10
@@ -96,4 +96,25 @@ def test_fine_zchunk_sweeps_identical(cuda, rows):
         assert abs(it - ref[2]) <= 1 and rel(x.cpu().numpy(), ref[1]) < 1e-8
     g.set_fine_zchunk(0)
     assert g.fine_zchunk() in (4, 8, 16, 32)
+    g.close()
+
+
+def test_coarse_variants_sweep_alike(cuda):
+    """The three coarse kernels (one thread per node, per (node, row), nine per
+    node) compute the same residual and Jacobi / Chebyshev step on every
+    coarse level: equal to FP32 rounding of the stencil sums."""
+    g = make(P.cantilever(64, 32, 32))
+    nl = g.n_levels()
+    rng = np.random.default_rng(3)
+    for li in range(1, nl - 1):
+        nn = int(np.prod(g.level_dims(li)[3:6]))
+        u = cuda.tensor(rng.standard_normal(3 * nn), dtype=cuda.float64, device="cuda")
+        f = cuda.tensor(rng.standard_normal(3 * nn), dtype=cuda.float64, device="cuda")
+        outs = []
+        for v in (0, 1, 2):
+            g.set_launch_shapes(4, -1, [-1] + [v] * (nl - 1))
+            outs.append((g.coarse_sweep_fp32(li, 0, u, f).cpu().numpy(),
+                         g.coarse_sweep_fp32(li, 2, u, f, uprev=u, omega=0.6, c1=0.2).cpu().numpy()))
+        for a, b in outs[1:]:
+            assert rel(a, outs[0][0]) < 1e-5 and rel(b, outs[0][1]) < 1e-5, li
     g.close()

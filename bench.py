@@ -39,14 +39,18 @@ sys.path.insert(0, ROOT)
 METRIC = ("worst-case TO design iterations/s @256^3 (mixed: FP32 V-cycle and CG recurrence, FP64 residual "
           "replacement; true rel.resid 1e-6)")
 UNIT = "iter/s"
-# V-cycle smoother: 2 + 2 Chebyshev steps for D^-1 K on [0.1 lambda_max,
-# lambda_max].  On this workload a 256^3 solve takes about 11-12 PCG
-# iterations with it, 14 with the interval [lambda_max/4, lambda_max], 16 with
-# damped Jacobi (omega = 0.8) and 18 with omega = 0.6, at the same cost per
-# iteration.
+# V-cycle smoother: 2 + 2 Chebyshev steps for D^-1 K on [0.07 lambda_max,
+# lambda_max].  On this workload a 256^3 solve of the seeded design's density
+# takes 11 PCG iterations with it (32.3 ms), 11 with 0.05, 12 with 0.1
+# (34.8 ms), 16 with 0.03 and 37 with 0.02 (the interval then reaches below
+# what the power-iteration estimate of lambda_max supports), 14 with
+# [lambda_max/4, lambda_max], 16 with damped Jacobi (omega = 0.8) and 18 with
+# omega = 0.6, at the same cost per iteration; 3 + 3 and 4 + 4 steps take 9
+# and 8 iterations but longer (33.8 and 36.5 ms with 0.05).  A design
+# iteration's 20 Lanczos solves take 265 PCG iterations at 0.07, 275 at 0.1.
 SMOOTHER = "chebyshev"
 OMEGA = 0.8
-CHEB_LOWER = 0.1
+CHEB_LOWER = 0.07
 
 
 def problem(n, seed=2026):
@@ -682,11 +686,16 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--krylov32", type=float, default=1e-2,
                     help="mixed PCG with the FP32 Krylov recurrence, true-residual replacement factor (0: FP64 recurrence)")
+    ap.add_argument("--cheb-lower", type=float, default=None,
+                    help="lower end of the Chebyshev smoother's interval as a fraction of lambda_max")
     ap.add_argument("--mode", default="design", choices=["design", "solve", "batch", "problems", "scale", "mesh",
                                                           "surface"])
     ap.add_argument("--systems", type=int, default=16)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
+    if args.cheb_lower is not None:
+        global CHEB_LOWER
+        CHEB_LOWER = args.cheb_lower
     if args.mode == "solve":
         run_solves(args)
         return

@@ -575,7 +575,9 @@ constexpr int pair_min_blocks(int mode, int typ) {
 // (px, py, pz, 3 nb) of u, box 36 x (2 TYP + 1) x 1 x 3; tmr: 3-D map
 // (qx, qy, qz) of rho^p, box 36 x 2 TYP x 1; out-of-range boxes read zero);
 // otherwise every thread stages 16-byte chunks with cp.async.
-template <int MODE, int TYP, bool TMA>
+// DOT (MODE 2 only): also sum f . out into per-CTA partials (dotp); a
+// separate instantiation so the plain step carries none of it
+template <int MODE, int TYP, bool TMA, bool DOT = false>
 __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
     k_fine_p(const Level L, const float* __restrict__ u, const float* __restrict__ f, float* __restrict__ out,
              const float* __restrict__ rp, float omega, double* __restrict__ dotp, const float* __restrict__ uprev,
@@ -700,7 +702,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
   const float2 zero2 = make_float2(0.f, 0.f);
   float2 F[4][3], Gt[4][3], uc[3], uo[3], own[3], fo[3], po[3], ra[4], rb[4];
   uint8_t clA = 0, clB = 0;
-  double pq = 0;
+  double pq = 0;  // with dotp: MODE 1 u . (K u); with DOT (MODE 2) f . out
   face(ss + ((z0 - 1 + NS) % NS) * SLOT, F, uc);
 #pragma unroll
   for (int q = 0; q < 4; q++) {
@@ -779,6 +781,15 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
       for (int c = 0; c < 3; c++) {
         const float2 v = p_fma(id, dl[c], p_fma(cc1, p_sub(uo[c], po[c]), uo[c]));
         res[c] = make_float2(workA ? v.x : 0.f, workB ? v.y : 0.f);
+      }
+      // DOT: this thread's share of f . out (the CG step's r . z when this
+      // is the V-cycle's last sweep)
+      if constexpr (DOT) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          pq += (double)fo[c].x * (double)res[c].x;
+          if (wB) pq += (double)fo[c].y * (double)res[c].y;
+        }
       }
     }
 #pragma unroll
@@ -926,7 +937,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
   }
   __syncthreads();
   emit(z1 - 1, sx + ((z1 - 1) & 1) * 12 * NT);
-  if (MODE == 1 && dotp != nullptr) {
+  if ((MODE == 1 || DOT) && dotp != nullptr) {
     __shared__ double sred[TYP];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) pq += __shfl_down_sync(0xffffffffu, pq, o);
@@ -1268,18 +1279,26 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
                              : pty == 8 ? pair_smem_bytes<8>(pair_slots(MODE, kPairTMA))
                                         : pair_smem_bytes<4>(pair_slots(MODE, kPairTMA)))
                           : walsh_smem_bytes<T, WTY>();
+  // MODE 2 with dotp: the instantiation that also sums f . out
+  const bool jdot = MODE == 2 && dotp != nullptr;
   const void* kern;
-  if constexpr (packed)
-    kern = pty == 2   ? reinterpret_cast<const void*>(k_fine_p<MODE, 2, kPairTMA>)
-           : pty == 8 ? reinterpret_cast<const void*>(k_fine_p<MODE, 8, kPairTMA>)
-                      : reinterpret_cast<const void*>(k_fine_p<MODE, 4, kPairTMA>);
-  else
+  if constexpr (packed) {
+    if (jdot)
+      kern = pty == 2   ? reinterpret_cast<const void*>(k_fine_p<MODE, 2, kPairTMA, true>)
+             : pty == 8 ? reinterpret_cast<const void*>(k_fine_p<MODE, 8, kPairTMA, true>)
+                        : reinterpret_cast<const void*>(k_fine_p<MODE, 4, kPairTMA, true>);
+    else
+      kern = pty == 2   ? reinterpret_cast<const void*>(k_fine_p<MODE, 2, kPairTMA>)
+             : pty == 8 ? reinterpret_cast<const void*>(k_fine_p<MODE, 8, kPairTMA>)
+                        : reinterpret_cast<const void*>(k_fine_p<MODE, 4, kPairTMA>);
+  } else {
     kern = reinterpret_cast<const void*>(k_fine_w<T, MODE, WTY>);
+  }
   // the shared-memory opt-in is per device and kernel; setting it twice from
   // racing threads is harmless, so an atomic flag per device suffices
-  static std::atomic<bool> attr[3][64];
+  static std::atomic<bool> attr[3][2][64];
   const int ti = pty == 2 ? 0 : pty == 4 ? 1 : 2;
-  std::atomic<bool>* done = (h->device >= 0 && h->device < 64) ? &attr[ti][h->device] : nullptr;
+  std::atomic<bool>* done = (h->device >= 0 && h->device < 64) ? &attr[ti][jdot ? 1 : 0][h->device] : nullptr;
   if (!done || !done->load(std::memory_order_acquire)) {
     RSO_CHECK_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     if (done) done->store(true, std::memory_order_release);
@@ -1289,15 +1308,25 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
     CUtensorMap mu{}, mr{};
     if (kPairTMA) RSO_TRY(pair_tensor_maps(h, l, u, rp, 2 * pty, &mu, &mr));
     if (h->prof_on) prof_begin(h, cls, (double)l.nn);
-    if (pty == 2)
+    if (jdot) {
+      if (pty == 2)
+        k_fine_p<MODE, 2, kPairTMA, true><<<pair_grid(l, 2, fzc), dim3(WTX, 2), smem, h->stream>>>(
+            l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, fzc, mu, mr);
+      else if (pty == 8)
+        k_fine_p<MODE, 8, kPairTMA, true><<<pair_grid(l, 8, fzc), dim3(WTX, 8), smem, h->stream>>>(
+            l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, fzc, mu, mr);
+      else
+        k_fine_p<MODE, 4, kPairTMA, true><<<pair_grid(l, 4, fzc), dim3(WTX, 4), smem, h->stream>>>(
+            l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, fzc, mu, mr);
+    } else if (pty == 2)
       k_fine_p<MODE, 2, kPairTMA><<<pair_grid(l, 2, fzc), dim3(WTX, 2), smem, h->stream>>>(
-          l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, fzc, mu, mr);
+          l, u, f, out, rp, (float)omega, MODE == 2 ? nullptr : dotp, uprev, (float)c1, fzc, mu, mr);
     else if (pty == 8)
       k_fine_p<MODE, 8, kPairTMA><<<pair_grid(l, 8, fzc), dim3(WTX, 8), smem, h->stream>>>(
-          l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, fzc, mu, mr);
+          l, u, f, out, rp, (float)omega, MODE == 2 ? nullptr : dotp, uprev, (float)c1, fzc, mu, mr);
     else
       k_fine_p<MODE, 4, kPairTMA><<<pair_grid(l, 4, fzc), dim3(WTX, 4), smem, h->stream>>>(
-          l, u, f, out, rp, (float)omega, dotp, uprev, (float)c1, fzc, mu, mr);
+          l, u, f, out, rp, (float)omega, MODE == 2 ? nullptr : dotp, uprev, (float)c1, fzc, mu, mr);
   } else {
     if (h->prof_on) prof_begin(h, cls, (double)l.nn);
     k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega, dotp,
@@ -1348,6 +1377,21 @@ rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const
                        const T* u_prev, double c1) {
   return launch_fine<T, 2>(h, u_in, f, u_out, rp, omega, pcls<T>(PC_FINE_JAC32, PC_FINE_JAC64), "fine_jacobi", nullptr,
                            u_prev, c1);
+}
+// the FP32 step with dot_dev = f . u_out in the same pass (single system)
+rso_status fine_jacobi_dot32(rso_handle* h, const float* u_in, const float* f, float* u_out, double omega,
+                             const float* u_prev, double c1, double* dot_dev) {
+  const Level& l0 = h->L[0];
+  const dim3 g = pair_grid(l0, fine_pty(h), fine_zc(h));
+  const long long nb = (long long)g.x * g.y * g.z;
+  if (l0.nb != 1 || nb > h->fpart_n) {
+    h->err = "fine partial-sum buffer smaller than the grid";
+    return RSO_ERR_STATE;
+  }
+  const rso_status st = launch_fine<float, 2>(h, u_in, f, u_out, h->rp32, omega, PC_FINE_JAC32, "fine_jacobi_dot32",
+                                              h->fpart, u_prev, c1);
+  if (st != RSO_OK) return st;
+  return reduce_partials(h, h->fpart, (int)nb, dot_dev);
 }
 template <typename T>
 rso_status fine_jacobi0(rso_handle* h, const T* f, T* u_out, const T* rp, double omega) {

@@ -194,6 +194,9 @@ struct rso_handle {
   // residual replacements are decided on the device (rso_set_solve_graphs)
   bool solve_graphs = false;
   void* sgc = nullptr;                             // captured solve graphs (solver.cu)
+  // when set, the FP32 V-cycle's last fine sweep also sums f . u into this
+  // device scalar (the CG step's r . z; solver.cu)
+  double* vc_zdot = nullptr;
   void* surf = nullptr;                            // surface-point self-support state (surface.cu)
 };
 
@@ -302,6 +305,9 @@ rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const doub
 template <typename T>
 rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const T* rp, double omega,
                        const T* u_prev = nullptr, double c1 = 0.0);
+// the FP32 Jacobi / Chebyshev step with dot_dev = f . u_out from the same pass
+rso_status fine_jacobi_dot32(rso_handle* h, const float* u_in, const float* f, float* u_out, double omega,
+                             const float* u_prev, double c1, double* dot_dev);
 template <typename T>
 rso_status fine_jacobi0(rso_handle* h, const T* f, T* u_out, const T* rp, double omega);
 template <typename T>

@@ -64,8 +64,9 @@ void smoother_steps(const rso_handle* h, double lam, int m, double* om, double* 
 // sweep on the fine level then needs no operator application).  Jacobi and
 // Chebyshev steps rotate three level vectors: u (current), t (next) and r
 // (previous iterate; free while the level is being smoothed).
+// last_dot (FP32 fine level only): the last step also sums f . u into it
 template <typename T>
-static rso_status smooth(rso_handle* h, int li, int sweeps, int reverse, bool zero = false) {
+static rso_status smooth(rso_handle* h, int li, int sweeps, int reverse, bool zero = false, double* last_dot = nullptr) {
   Level& l = h->L[li];
   if (h->cfg.smoother == RSO_SMOOTH_GS) {
     for (int s = 0; s < sweeps; s++)
@@ -83,8 +84,12 @@ static rso_status smooth(rso_handle* h, int li, int sweeps, int reverse, bool ze
   for (int s = 0; s < sweeps; s++) {
     // previous iterate: none before the second step; zero when the smoothing started from zero
     const T* prev = (!cheb || s == 0 || (zero && s == 1)) ? nullptr : LV<T>::r(l);
+    const bool dot_here = last_dot != nullptr && li == 0 && s == sweeps - 1 && !(zero && s == 0);
     if (li == 0 && zero && s == 0) RSO_TRY(fine_jacobi0<T>(h, LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om[0]));
-    else if (li == 0) RSO_TRY(fine_jacobi<T>(h, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om[s], prev, c1[s]));
+    else if (dot_here) {
+      if constexpr (sizeof(T) == 4)
+        RSO_TRY(fine_jacobi_dot32(h, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), om[s], prev, c1[s], last_dot));
+    } else if (li == 0) RSO_TRY(fine_jacobi<T>(h, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om[s], prev, c1[s]));
     else RSO_TRY(coarse_jacobi<T>(h, li, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), om[s], prev, c1[s]));
     if (cheb) {  // previous <- current <- next
       T* old_prev = LV<T>::r(l);
@@ -134,9 +139,11 @@ rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric, bool u
     RSO_TRY(bottom_vcycle<T>(h, lb, pre, post));
   }
   // up-sweep from the level above the coarsest (or above the cluster kernel's levels)
+  // the FP32 V-cycle's last fine step may also sum f . u (h->vc_zdot)
+  double* zdot = sizeof(T) == 4 && h->L[0].nb == 1 ? h->vc_zdot : nullptr;
   for (int li = lb > 0 ? lb - 1 : nl - 2; li >= 0; li--) {
     RSO_TRY(prolong<T>(h, li + 1, LV<T>::u(h->L[li + 1]), LV<T>::u(h->L[li])));
-    RSO_TRY(smooth<T>(h, li, post, symmetric ? 1 : 0));
+    RSO_TRY(smooth<T>(h, li, post, symmetric ? 1 : 0, false, li == 0 ? zdot : nullptr));
   }
   return RSO_OK;
 }
@@ -262,7 +269,7 @@ std::vector<uint64_t> vc_key(const rso_handle* h, bool rotating = true) {
   push_bits(k, h->rp32); push_bits(k, h->xfer); push_bits(k, h->xfer_n);
   push_bits(k, h->c_K); push_bits(k, h->c_nodes); push_bits(k, h->c_f); push_bits(k, h->c_fb); push_bits(k, h->nc);
   push_bits(k, h->cfg.smoother); push_bits(k, h->cfg.pre); push_bits(k, h->cfg.post);
-  push_bits(k, h->cfg.omega); push_bits(k, h->cfg.cheb_lower); push_bits(k, h->prof_on);
+  push_bits(k, h->cfg.omega); push_bits(k, h->cfg.cheb_lower); push_bits(k, h->prof_on); push_bits(k, h->vc_zdot);
   push_bits(k, h->tune.fine_rows); push_bits(k, h->tune.fine_zc); push_bits(k, h->tune.bottom);
   for (int r : h->tune.rowsplit) push_bits(k, r);
   return k;
@@ -676,9 +683,9 @@ static rso_status build_solve_graph(rso_handle* h, SolveGraphs* c, const double*
       prev = node;
       // the V-cycle and the direction update
       st = add_if(h, G, &prev, hc[i], c->cs, [&]() -> rso_status {
-        RSO_TRY(vcycle_mixed_launches(h));
+        RSO_TRY(vcycle_mixed_launches(h));  // r . z into s[3] from its last fine step when h->vc_zdot says so
         const float* z32 = l0.u32;
-        RSO_TRY(dot_ff(h, r32, z32, n3, s + 3));
+        if (h->vc_zdot != s + 3) RSO_TRY(dot_ff(h, r32, z32, n3, s + 3));
         k_cg_beta<<<1, 1, 0, h->stream>>>(s);
         k_cg32_step_dir_ctl<<<cdiv(n4, 256), 256, 0, h->stream>>>(
             n4, s + 2, s + 4, reinterpret_cast<const float4*>(z32), reinterpret_cast<float4*>(p32),
@@ -799,9 +806,18 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
     // buffer seen as FP32, so old doubles split across its entries) must be zero
     RSO_CHECK_CUDA(h, cudaMemsetAsync(q32, 0, sizeof(float) * n3, h->stream));
     k_d2f<<<cdiv(n3, 256), 256, 0, h->stream>>>(h->r, r32, n3); rso::note_launch();
+    // r . z comes out of the V-cycle's last fine step when it is a Jacobi or
+    // Chebyshev step (after a post-smoothing), else from its own pass
+    const bool fuse = h->cfg.smoother != RSO_SMOOTH_GS && h->cfg.post >= 1;
+    struct ZdotReset {
+      rso_handle* h;
+      ~ZdotReset() { h->vc_zdot = nullptr; }
+    } zreset{h};
+    h->vc_zdot = fuse ? s + 0 : nullptr;
     RSO_TRY(vcycle_mixed(h));
     RSO_CHECK_CUDA(h, cudaMemcpyAsync(p32, l0.u32, sizeof(float) * n3, cudaMemcpyDeviceToDevice, h->stream));
-    RSO_TRY(dot_ff(h, r32, l0.u32, n3, s + 0));
+    if (!fuse) RSO_TRY(dot_ff(h, r32, l0.u32, n3, s + 0));
+    h->vc_zdot = fuse ? s + 3 : nullptr;
     rso_status gs = RSO_ERR_UNSUPPORTED;
     if (h->solve_graphs && h->vc_graphs && !h->prof_on && h->stream && max_iter > 0)
       gs = pcg32_graph(h, f, x, tol, max_iter, fn, rbase, &it, &rel, stalled);
@@ -845,7 +861,7 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
       }
       RSO_TRY(vcycle_mixed(h));
       const float* z32 = l0.u32;
-      RSO_TRY(dot_ff(h, r32, z32, n3, s + 3));
+      if (!fuse) RSO_TRY(dot_ff(h, r32, z32, n3, s + 3));
       k_cg_beta<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
       if (replace)
         k_cg32_step_dir<true><<<cdiv(n4, 256), 256, 0, h->stream>>>(

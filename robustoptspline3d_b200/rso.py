@@ -473,14 +473,27 @@ class HierarchyGrid:
         (rso_autotune); returns the choices."""
         c = np.zeros(2 + self.n_levels(), np.int32)
         self._chk(self.lib.rso_autotune(self.h, _np_ptr(c, _pi)), "rso_autotune")
-        return {"fine_rows": int(c[0]), "fine_zchunk": self.fine_zchunk(), "bottom_level": int(c[1]),
-                "row_split": [int(x) for x in c[2:]]}
+        self._shapes = {"fine_rows": int(c[0]), "fine_zchunk": self.fine_zchunk(), "bottom_level": int(c[1]),
+                        "row_split": [int(x) for x in c[2:]]}
+        return dict(self._shapes)
+
+    def launch_shapes(self):
+        """The launch shapes last chosen by autotune() or set_launch_shapes() (the
+        built-in rules' markers when neither ran)."""
+        sh = getattr(self, "_shapes", None)
+        if sh is None:
+            sh = {"fine_rows": 4, "fine_zchunk": self.fine_zchunk(), "bottom_level": -2,
+                  "row_split": [-1] * self.n_levels()}
+        return dict(sh)
 
     def set_launch_shapes(self, fine_rows=4, bottom_level=-2, row_split=None):
         """Launch shapes in rso_autotune's terms (rso_set_launch_shapes)."""
         rs = list(row_split or [])
         c = np.array([fine_rows, bottom_level] + rs, np.int32)
         self._chk(self.lib.rso_set_launch_shapes(self.h, _np_ptr(c, _pi), len(c)), "rso_set_launch_shapes")
+        nl = self.n_levels()
+        self._shapes = {"fine_rows": int(fine_rows), "fine_zchunk": self.fine_zchunk(), "bottom_level": int(bottom_level),
+                        "row_split": [int(x) for x in rs[:nl]] + [-1] * max(0, nl - len(rs))}
 
     def updateDensities(self, rho, sens, vgoal, step=0.1, damp=0.5, shell=None, variant=0):
         """OC density update (rso_oc_update_density): returns (new rho, info dict)."""

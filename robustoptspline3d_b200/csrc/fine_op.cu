@@ -703,6 +703,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
   float2 F[4][3], Gt[4][3], uc[3], uo[3], own[3], fo[3], po[3], ra[4], rb[4];
   uint8_t clA = 0, clB = 0;
   double pq = 0;  // with dotp: MODE 1 u . (K u); with DOT (MODE 2) f . out
+  float2 zq = make_float2(0.f, 0.f);  // DOT: f . out of the two columns along the march
   face(ss + ((z0 - 1 + NS) % NS) * SLOT, F, uc);
 #pragma unroll
   for (int q = 0; q < 4; q++) {
@@ -783,13 +784,11 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
         res[c] = make_float2(workA ? v.x : 0.f, workB ? v.y : 0.f);
       }
       // DOT: this thread's share of f . out (the CG step's r . z when this
-      // is the V-cycle's last sweep)
+      // is the V-cycle's last sweep), summed in FP32 along the march (one
+      // packed fma per component) and in FP64 across threads
       if constexpr (DOT) {
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-          pq += (double)fo[c].x * (double)res[c].x;
-          if (wB) pq += (double)fo[c].y * (double)res[c].y;
-        }
+        for (int c = 0; c < 3; c++) zq = p_fma(fo[c], res[c], zq);
       }
     }
 #pragma unroll
@@ -937,6 +936,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
   }
   __syncthreads();
   emit(z1 - 1, sx + ((z1 - 1) & 1) * 12 * NT);
+  if constexpr (DOT) pq = (double)zq.x + (wB ? (double)zq.y : 0.0);
   if ((MODE == 1 || DOT) && dotp != nullptr) {
     __shared__ double sred[TYP];
 #pragma unroll

@@ -418,29 +418,49 @@ __global__ void __launch_bounds__(SP_THREADS) k_sumd_partial(const double* __res
 }
 
 // dc += w . (dN N N, N dN N, N N dN) / count over the order^3 coefficients of each point
+// dc += w . (dN N N, N dN N, N N dN) / count over the order^3 coefficients of
+// each point.  A warp whose points all fall in the same knot cell (a run of
+// nearby samples, or the copies of the first point that pad a short list)
+// sums its contributions with shuffles and adds each once; other warps add
+// per point.
 __global__ void __launch_bounds__(SP_THREADS) k_surf_grad(SplineP S, const float* __restrict__ xyz, int n,
                                                           const double* __restrict__ w,
                                                           const double* __restrict__ down_sum, int mode,
                                                           double* __restrict__ dc) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const double w0 = w[k], w1 = w[n + k], w2 = w[2 * (long long)n + k];
-  if (w0 == 0 && w1 == 0 && w2 == 0) return;
+  const int lane = threadIdx.x & 31;
+  bool has = k < n;
+  double w0 = 0, w1 = 0, w2 = 0;
+  if (has) {
+    w0 = w[k]; w1 = w[n + k]; w2 = w[2 * (long long)n + k];
+    has = !(w0 == 0 && w1 == 0 && w2 == 0);
+  }
+  const int o = S.order;
+  int I[3] = {0, 0, 0};
+  double N[3][5] = {}, D[3][5] = {};
+  if (has) {
+    const double pt[3] = {(double)xyz[k], (double)xyz[n + k], (double)xyz[2 * n + k]};
+    for (int a = 0; a < 3 && has; a++) has = basis_vd(S, a, pt[a], &I[a], N[a], D[a]);
+  }
   const double cnt = mode % 2 == 0 ? *down_sum : (double)n;
   const double scale = cnt == 0 ? 0.0 : 1.0 / cnt;
-  const int o = S.order;
-  int I[3];
-  double N[3][5], D[3][5];
-  const double pt[3] = {(double)xyz[k], (double)xyz[n + k], (double)xyz[2 * n + k]};
-  for (int a = 0; a < 3; a++)
-    if (!basis_vd(S, a, pt[a], &I[a], N[a], D[a])) return;
+  const long long key = has ? cidx(S, I[0], I[1], I[2]) : -1;
+  const long long key0 = __shfl_sync(0xffffffffu, key, 0);
+  const bool uniform = __all_sync(0xffffffffu, key == key0) && key0 >= 0;
   for (int q = 0; q < o; q++)
     for (int b = 0; b < o; b++) {
       const double nyz = N[1][b] * N[2][q];
       const double t1 = w1 * D[1][b] * N[2][q] + w2 * N[1][b] * D[2][q];
       for (int a = 0; a < o; a++) {
-        const double v = scale * (w0 * D[0][a] * nyz + N[0][a] * t1);
-        atomicAdd(&dc[cidx(S, I[0] - o + a, I[1] - o + b, I[2] - o + q)], v);
+        double v = has ? scale * (w0 * D[0][a] * nyz + N[0][a] * t1) : 0.0;
+        const long long ci = cidx(S, I[0] - o + a, I[1] - o + b, I[2] - o + q);
+        if (uniform) {
+#pragma unroll
+          for (int sh = 16; sh > 0; sh >>= 1) v += __shfl_xor_sync(0xffffffffu, v, sh);
+          if (lane == 0) atomicAdd(&dc[ci], v);
+        } else if (has) {
+          atomicAdd(&dc[ci], v);
+        }
       }
     }
 }

@@ -216,11 +216,14 @@ constexpr int walsh_smem_bytes() {
 // MODE 2: out = u + c1 (u - uprev) + omega D^-1 (f - K u), D = 3x3 diagonal
 //         block: damped block Jacobi for c1 = 0, a Chebyshev step otherwise
 //         (uprev NULL reads as zero)
-template <typename T, int MODE, int TY>
+// RR (MODE 0 only): also write an FP32 copy of r (out32) and sum r . r into
+// per-CTA partials (dotp); a separate instantiation so the plain residual
+// carries none of it
+template <typename T, int MODE, int TY, bool RR = false>
 __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
     k_fine_w(const Level L, const T* __restrict__ u, const T* __restrict__ f, T* __restrict__ out,
              const T* __restrict__ rp, T omega, double* __restrict__ dotp, const T* __restrict__ uprev,
-             T c1) {
+             T c1, float* __restrict__ out32) {
   // Staged rows are 16-byte aligned windows of RX entries starting at the
   // tile's first padded x index rounded down to a multiple of 4 (ox = offset
   // of the tile inside the window), copied in 16-byte chunks.
@@ -312,7 +315,7 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
   // layers around it
   T F[4][3], Gt[4][3], uc[3], uo[3], own[3], fo[3], po[3], ra[4], rb[4];
   uint8_t clo = 0;
-  double pq = 0;  // MODE 1 with dotp: this thread's share of u . (K u)
+  double pq = 0;  // with dotp: MODE 1 this thread's share of u . (K u), MODE 0 of r . r
   face(ss + ((z0 - 1 + WNSLOT) % WNSLOT) * SLOT, F, uc);
 #pragma unroll
   for (int q = 0; q < 4; q++) {
@@ -334,7 +337,14 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
     const bool work = (clo & NC_ACTIVE) && !(clo & NC_SUPPORT);
     if (MODE == 0) {
 #pragma unroll
-      for (int c = 0; c < 3; c++) out[n + c * NP] = fo[c] - (work ? acc[c] : T(0));
+      for (int c = 0; c < 3; c++) {
+        const T r = fo[c] - (work ? acc[c] : T(0));
+        out[n + c * NP] = r;
+        if constexpr (RR) {  // an FP32 copy of r and r . r from the same pass
+          out32[n + c * NP] = (float)r;
+          pq += (double)r * (double)r;
+        }
+      }
     } else if (MODE == 1) {
       const bool pass = (clo & NC_SUPPORT) != 0;
 #pragma unroll
@@ -461,8 +471,8 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
   }
   __syncthreads();
   emit(z1 - 1, sx + ((z1 - 1) & 1) * 9 * NE);
-  if (MODE == 1 && dotp != nullptr) {
-    // per-CTA partial of u . (K u), summed by a second pass on the host side
+  if ((MODE == 1 || RR) && dotp != nullptr) {
+    // per-CTA partial of u . (K u) or r . r, summed by a second pass
     __shared__ double sred[TY];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) pq += __shfl_down_sync(0xffffffffu, pq, o);
@@ -1260,7 +1270,8 @@ rso_status fine_stage_check(rso_handle* h) {
 
 template <typename T, int MODE>
 static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, const T* rp, double omega, int cls,
-                              const char* what, double* dotp = nullptr, const T* uprev = nullptr, double c1 = 0.0) {
+                              const char* what, double* dotp = nullptr, const T* uprev = nullptr, double c1 = 0.0,
+                              float* out32 = nullptr) {
   const Level& l = h->L[0];
   if (3 * l.NP >= (1LL << 31)) {
     h->err = "fine level too large for 32-bit in-plane offsets";
@@ -1291,6 +1302,8 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
       kern = pty == 2   ? reinterpret_cast<const void*>(k_fine_p<MODE, 2, kPairTMA>)
              : pty == 8 ? reinterpret_cast<const void*>(k_fine_p<MODE, 8, kPairTMA>)
                         : reinterpret_cast<const void*>(k_fine_p<MODE, 4, kPairTMA>);
+  } else if (MODE == 0 && out32 != nullptr) {
+    kern = reinterpret_cast<const void*>(k_fine_w<T, MODE, WTY, true>);
   } else {
     kern = reinterpret_cast<const void*>(k_fine_w<T, MODE, WTY>);
   }
@@ -1298,7 +1311,8 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
   // racing threads is harmless, so an atomic flag per device suffices
   static std::atomic<bool> attr[3][2][64];
   const int ti = pty == 2 ? 0 : pty == 4 ? 1 : 2;
-  std::atomic<bool>* done = (h->device >= 0 && h->device < 64) ? &attr[ti][jdot ? 1 : 0][h->device] : nullptr;
+  const bool second = jdot || (MODE == 0 && out32 != nullptr);  // the instantiation with the extra outputs
+  std::atomic<bool>* done = (h->device >= 0 && h->device < 64) ? &attr[ti][second ? 1 : 0][h->device] : nullptr;
   if (!done || !done->load(std::memory_order_acquire)) {
     RSO_CHECK_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     if (done) done->store(true, std::memory_order_release);
@@ -1329,8 +1343,12 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
           l, u, f, out, rp, (float)omega, MODE == 2 ? nullptr : dotp, uprev, (float)c1, fzc, mu, mr);
   } else {
     if (h->prof_on) prof_begin(h, cls, (double)l.nn);
-    k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega, dotp,
-                                                                                 uprev, (T)c1);
+    if (MODE == 0 && out32 != nullptr)
+      k_fine_w<T, MODE, WTY, true><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(l, u, f, out, rp, (T)omega,
+                                                                                       dotp, uprev, (T)c1, out32);
+    else
+      k_fine_w<T, MODE, WTY><<<march_grid(l), dim3(WTX, WTY), smem, h->stream>>>(
+          l, u, f, out, rp, (T)omega, MODE == 0 ? nullptr : dotp, uprev, (T)c1, nullptr);
   }
   rso::note_launch();
   if (h->prof_on) prof_end(h, cls);
@@ -1340,6 +1358,22 @@ static rso_status launch_fine(rso_handle* h, const T* u, const T* f, T* out, con
 template <typename T>
 rso_status fine_residual(rso_handle* h, const T* u, const T* f, T* r, const T* rp) {
   return launch_fine<T, 0>(h, u, f, r, rp, 0.0, pcls<T>(PC_FINE_RES32, PC_FINE_RES64), "fine_residual");
+}
+// the FP64 residual with its FP32 copy r32 and r . r (dot_dev) from the same
+// pass (single system; the entries the operator does not write are left as they are)
+rso_status fine_residual64_rr(rso_handle* h, const double* u, const double* f, double* r, float* r32,
+                              double* dot_dev) {
+  const Level& l0 = h->L[0];
+  const dim3 g = march_grid(l0);
+  const long long nb = (long long)g.x * g.y * g.z;
+  if (l0.nb != 1 || nb > h->fpart_n) {
+    h->err = "fine partial-sum buffer smaller than the grid";
+    return RSO_ERR_STATE;
+  }
+  const rso_status st = launch_fine<double, 0>(h, u, f, r, h->rp64, 0.0, PC_FINE_RES64, "fine_residual64_rr",
+                                               h->fpart, nullptr, 0.0, r32);
+  if (st != RSO_OK) return st;
+  return reduce_partials(h, h->fpart, (int)nb, dot_dev);
 }
 template <typename T>
 rso_status fine_applyK(rso_handle* h, const T* u, T* f, const T* rp) {

@@ -308,6 +308,9 @@ rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const
 // the FP32 Jacobi / Chebyshev step with dot_dev = f . u_out from the same pass
 rso_status fine_jacobi_dot32(rso_handle* h, const float* u_in, const float* f, float* u_out, double omega,
                              const float* u_prev, double c1, double* dot_dev);
+// the FP64 residual with its FP32 copy and r . r from the same pass
+rso_status fine_residual64_rr(rso_handle* h, const double* u, const double* f, double* r, float* r32,
+                              double* dot_dev);
 template <typename T>
 rso_status fine_jacobi0(rso_handle* h, const T* f, T* u_out, const T* rp, double omega);
 template <typename T>

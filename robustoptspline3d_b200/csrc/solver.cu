@@ -673,10 +673,8 @@ static rso_status build_solve_graph(rso_handle* h, SolveGraphs* c, const double*
       st = add_if(h, G, &prev, hr[i], c->cs, [&]() -> rso_status {
         k_cg32_step<<<cdiv(n4, 256), 256, 0, h->stream>>>(n4, s + 2, reinterpret_cast<const float4*>(p32),
                                                           reinterpret_cast<double2*>(x));
-        RSO_TRY(fine_residual<double>(h, x, f, h->r, h->rp64));
-        RSO_TRY(dot(h, h->r, h->r, n3, s + 8));
+        RSO_TRY(fine_residual64_rr(h, x, f, h->r, r32, s + 8));  // r, its FP32 copy and r . r
         k_pcg_ctl_b<<<1, 1, 0, h->stream>>>(ctl, s, go, i, hc[i]);
-        k_d2f<<<cdiv(n3, 256), 256, 0, h->stream>>>(h->r, r32, n3);
         return launch_check(h, "pcg graph");
       }, &node, &kr);
       if (st != RSO_OK) break;
@@ -787,6 +785,16 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
     RSO_TRY(fine_residual<double>(h, x, f, h->r, h->rp64));
     return dot_host(h, h->r, h->r, n3, rn2);
   };
+  // in a replacement: the true residual with its FP32 copy (the recurrence's
+  // new r) and r . r from one pass; the padding of r32 keeps the zeros the
+  // first copy gave it
+  auto true_residual_rr = [&](double* rn2) -> rso_status {
+    RSO_TRY(fine_residual64_rr(h, x, f, h->r, r32, h->scal + 15));
+    RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->h_scal + 15, h->scal + 15, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+    *rn2 = h->h_scal[15];
+    return RSO_OK;
+  };
   double fn2 = 0, rn2 = 0;
   RSO_TRY(dot_host(h, f, f, n3, &fn2));
   RSO_TRY(true_residual(&rn2));
@@ -842,7 +850,7 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
         k_cg32_step<<<cdiv(n4, 256), 256, 0, h->stream>>>(n4, s + 2, reinterpret_cast<const float4*>(p32),
                                                           reinterpret_cast<double2*>(x));
         rso::note_launch();
-        RSO_TRY(true_residual(&rn2));
+        RSO_TRY(true_residual_rr(&rn2));
         const double rtrue = std::sqrt(rn2);
         rel = rtrue / fn;
         if (!std::isfinite(rel)) { h->err = "non-finite residual in PCG"; return RSO_ERR_NONFINITE; }
@@ -855,7 +863,6 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
         }
         rbase = rtrue;
         since = 0;
-        k_d2f<<<cdiv(n3, 256), 256, 0, h->stream>>>(h->r, r32, n3); rso::note_launch();
       } else {
         rel = rnorm / fn;
       }

@@ -51,6 +51,7 @@ UNIT = "iter/s"
 SMOOTHER = "chebyshev"
 OMEGA = 0.8
 CHEB_LOWER = 0.07
+SMOOTH_STEPS = 2  # Chebyshev steps before and after the coarse correction
 
 
 def problem(n, seed=2026):
@@ -240,7 +241,7 @@ def run_solves(args):
     em, fa, la, order, parts, coeff = problem(n)
     prec = R.rso.MIXED if args.precision == "mixed" else R.rso.FP64
     g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=prec, smoother=smoother_id(R), omega=OMEGA, cheb_lower=CHEB_LOWER,
-                                                    pre=2, post=2, poisson_ratio=0.3))
+                                                    pre=SMOOTH_STEPS, post=SMOOTH_STEPS, poisson_ratio=0.3))
     nc = g.set_spline_partition(parts, parts, parts, order)
     rho = g.projectDensities(g.coeff2density(np.asarray(coeff, np.float32)[:nc]), 8.0)
     g.set_density(rho)
@@ -313,7 +314,7 @@ def run_batch(args):
     em, fa, la, rho, F = batch_problem(n, k)
     prec = R.rso.MIXED if args.precision == "mixed" else R.rso.FP64
     g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=prec, smoother=smoother_id(R), omega=OMEGA,
-                                                    cheb_lower=CHEB_LOWER, pre=2, post=2, poisson_ratio=0.3))
+                                                    cheb_lower=CHEB_LOWER, pre=SMOOTH_STEPS, post=SMOOTH_STEPS, poisson_ratio=0.3))
     g.set_density(rho.ravel())
     g.update_stencil()
     if prec == R.rso.MIXED and not args.no_autotune:
@@ -340,7 +341,7 @@ def run_batch(args):
                       "batch_vs_sequential": t_seq / t_batch,
                       "iterations": [i for i, _ in infos], "sequential_iterations": its,
                       "data": "synthetic", "config": {"workload": "config 3a (16 top-face patch loads, bottom clamped)",
-                                                      "smoother": f"{SMOOTHER} 2+2", "levels": g_levels(n)}}),
+                                                      "smoother": f"{SMOOTHER} {SMOOTH_STEPS}+{SMOOTH_STEPS}", "levels": g_levels(n)}}),
           flush=True)
     g.close()
 
@@ -378,7 +379,7 @@ def run_problems(args):
     for i, n in enumerate(sizes):
         em, fa, la, rho, f = cube_problem(int(n), 100 + i)
         g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=R.rso.MIXED, smoother=smoother_id(R), omega=OMEGA,
-                                                        cheb_lower=CHEB_LOWER, pre=2, post=2, poisson_ratio=0.4,
+                                                        cheb_lower=CHEB_LOWER, pre=SMOOTH_STEPS, post=SMOOTH_STEPS, poisson_ratio=0.4,
                                                         youngs_modulus=1e6))
         g.set_density(rho.ravel())
         g.update_stencil()
@@ -428,7 +429,7 @@ def run_problems(args):
                       "concurrent_bottom_cluster_solves_per_s": len(grids) / t_con_b,
                       "sizes": [int(n) for n in sizes], "iterations": its, "iterations_concurrent": its_c,
                       "iterations_concurrent_bottom_cluster": its_cb,
-                      "data": "synthetic", "config": {"workload": "config 3b", "smoother": f"{SMOOTHER} 2+2"}}),
+                      "data": "synthetic", "config": {"workload": "config 3b", "smoother": f"{SMOOTHER} {SMOOTH_STEPS}+{SMOOTH_STEPS}"}}),
           flush=True)
     for g in grids:
         g.close()
@@ -635,7 +636,7 @@ def run_scale(args):
     for prec, tol in ((R.rso.MIXED, 1e-6), (R.rso.FP64, 1e-10)):
         t0 = time.perf_counter()
         g = R.HierarchyGrid(em, fa, la, normals, R.Config(precision=prec, smoother=smoother_id(R), omega=OMEGA,
-                                                          cheb_lower=CHEB_LOWER, pre=2, post=2, poisson_ratio=0.3,
+                                                          cheb_lower=CHEB_LOWER, pre=SMOOTH_STEPS, post=SMOOTH_STEPS, poisson_ratio=0.3,
                                                           mode=R.rso.WITH_SUPPORT_CF))
         nc = g.set_spline_partition(*parts, order)
         coeff = np.clip(np.random.default_rng(2026).normal(0.5, 0.15, nc), 0.0, 1.0)
@@ -684,7 +685,7 @@ def run_scale(args):
            "config": {"workload": "511x256x256 voxels (embedded 512x256x256), 200 spherical voids r~U[4,20]",
                       "load": "x=511 node plane, force along +x (constrained direction)", "support": "x=0 nodes",
                       "spline": f"order {order}, partition {parts}", "solve_tol": {"mixed": 1e-6, "fp64": 1e-10},
-                      "smoother": f"{SMOOTHER} 2+2 on [{CHEB_LOWER}, 1] x lambda_max",
+                      "smoother": f"{SMOOTHER} {SMOOTH_STEPS}+{SMOOTH_STEPS} on [{CHEB_LOWER}, 1] x lambda_max",
                       "smoother_state": "FP32 (BF16/FP16 state not built)", "filter": "none (exact gradients)"},
            "data": "synthetic"}
     print(json.dumps(out))
@@ -709,14 +710,17 @@ def main():
                     help="mixed PCG with the FP32 Krylov recurrence, true-residual replacement factor (0: FP64 recurrence)")
     ap.add_argument("--cheb-lower", type=float, default=None,
                     help="lower end of the Chebyshev smoother's interval as a fraction of lambda_max")
+    ap.add_argument("--smooth-steps", type=int, default=2,
+                    help="Chebyshev smoothing steps before and after each coarse correction")
     ap.add_argument("--mode", default="design", choices=["design", "solve", "batch", "problems", "scale", "mesh",
                                                           "surface"])
     ap.add_argument("--systems", type=int, default=16)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
+    global CHEB_LOWER, SMOOTH_STEPS
     if args.cheb_lower is not None:
-        global CHEB_LOWER
         CHEB_LOWER = args.cheb_lower
+    SMOOTH_STEPS = args.smooth_steps
     if args.mode == "solve":
         run_solves(args)
         return
@@ -751,7 +755,7 @@ def main():
 
     def make(precision):
         g = R.HierarchyGrid(em, fa, la, None, R.Config(precision=precision, smoother=smoother_id(R), omega=OMEGA, cheb_lower=CHEB_LOWER,
-                                                        pre=2, post=2, poisson_ratio=0.3))
+                                                        pre=SMOOTH_STEPS, post=SMOOTH_STEPS, poisson_ratio=0.3))
         nc = g.set_spline_partition(parts, parts, parts, order)
         if precision == R.rso.MIXED:
             g.set_krylov_fp32(args.krylov32)
@@ -926,7 +930,7 @@ def main():
                 "vs_baseline": None, "dtype": "f32 V-cycle and CG recurrence + f64 iterate, residual replacement, Lanczos, MMA", "data": "synthetic",
                 "config": {"workload": f"{n}^3 worst-case spline TO iteration (config 4 shape)", "elements": n ** 3,
                            "spline": "order 4, 32^3 coefficients", "lanczos_steps": 20, "solve_tol": 1e-6,
-                           "smoother": f"{SMOOTHER} 2+2 on [{CHEB_LOWER}, 1] x lambda_max",
+                           "smoother": f"{SMOOTHER} {SMOOTH_STEPS}+{SMOOTH_STEPS} on [{CHEB_LOWER}, 1] x lambda_max",
                            "preconditioner": "one V-cycle per CG iteration",
                            "krylov": (f"FP32 recurrence, true FP64 residual replacing it every {args.krylov32:g} "
                                       "reduction and at the end") if args.krylov32 > 0 else "FP64 recurrence",

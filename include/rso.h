@@ -272,6 +272,9 @@ rso_status rso_coarse_sweep_fp32(rso_handle* h, int level, int op, const double*
  * grid/Grid.cu:2717-2734, in the precision of the mixed V-cycle). */
 rso_status rso_prolong_fp32(rso_handle* h, int coarse_level, const double* uc_dev, const double* uf_dev,
                             double* out_dev);
+/* FP32 restriction fc = R rf (Grid::restrict_residual, grid/Grid.cu:2615-2635,
+ * in the precision of the mixed V-cycle). */
+rso_status rso_restrict_fp32(rso_handle* h, int coarse_level, const double* rf_dev, double* fc_dev);
 /* coarse-level stencil (243 x Nn_level doubles, [d][row][col][node]); rxStencil */
 rso_status rso_get_stencil(rso_handle* h, int level, double* out_dev);
 /* coarse residual on stored stencils; update_residual_kernel_1 (grid/Grid.cu:2169-2267) */

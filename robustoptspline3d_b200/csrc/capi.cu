@@ -486,6 +486,19 @@ extern "C" rso_status rso_prolong_fp32(rso_handle* h, int cl, const double* uc, 
   return RSO_OK;
 }
 
+extern "C" rso_status rso_restrict_fp32(rso_handle* h, int cl, const double* rf, double* fc) {
+  if (!h || !rf || !fc || cl < 1 || cl >= (int)h->L.size()) return RSO_ERR_INVALID_ARG;
+  Level& c = h->L[cl];
+  Level& f = h->L[cl - 1];
+  RSO_TRY(pad_nodes(h, cl - 1, rf, f.r64));
+  RSO_TRY(to_f32(h, f.r64, f.r32, 3 * f.NP));
+  RSO_TRY(restrict_<float>(h, cl, f.r32, c.f32));
+  RSO_TRY(to_f64(h, c.f32, c.f64, 3 * c.NP));
+  RSO_TRY(unpad_nodes(h, cl, c.f64, fc));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  return RSO_OK;
+}
+
 extern "C" rso_status rso_set_vcycle_graphs(rso_handle* h, int on) {
   if (!h) return RSO_ERR_INVALID_ARG;
   h->vc_graphs = on != 0;

@@ -453,18 +453,51 @@ __global__ void k_restrict_z(const Level Fl, int nZ, const T* __restrict__ rf, T
   t[i] = s0; t[i + comp] = s1; t[i + 2 * comp] = s2;
 }
 
-template <typename T, int F>
+// FP32, single system: pass 1 over four consecutive padded fine nodes per
+// thread (16-byte loads and stores; px is a multiple of 4), into t laid out
+// like the fine level's padded planes, t[c][Z][py][px].  Same arithmetic, in
+// the same order, as k_restrict_z; the padding entries of t are never read.
+template <int F>
+__global__ void __launch_bounds__(256) k_restrict_z_v4(const Level Fl, int nZ, const float* __restrict__ rf,
+                                                       float* __restrict__ t) {
+  const long long pxy = (long long)Fl.px * Fl.py, off = 4 * (blockIdx.x * (long long)blockDim.x + threadIdx.x);
+  const int Z = blockIdx.y;
+  if (off >= pxy) return;
+  float4 s[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) s[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+  for (int dz = -F + 1; dz < F; dz++) {
+    const int z = F * Z + dz;
+    if (z < 0 || z >= Fl.nz) continue;
+    const float* src = rf + pxy * (z + 1) + off;
+    const float w = (float)(F - (dz < 0 ? -dz : dz)) / (float)F;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float4 v = *reinterpret_cast<const float4*>(src + c * Fl.NP);
+      s[c].x += w * v.x; s[c].y += w * v.y; s[c].z += w * v.z; s[c].w += w * v.w;
+    }
+  }
+  const long long comp = pxy * nZ;
+#pragma unroll
+  for (int c = 0; c < 3; c++) *reinterpret_cast<float4*>(t + c * comp + Z * pxy + off) = s[c];
+}
+
+// PAD: t laid out like the fine level's padded planes, t[c][Z][py][px] (the
+// layout k_restrict_z_v4 writes)
+template <typename T, int F, bool PAD = false>
 __global__ void k_restrict_xy(const Level Fl, const Level C, const T* __restrict__ t, T* __restrict__ fc) {
   const int bsys = blockIdx.z / C.nz;
   const int X = blockIdx.x * 32 + threadIdx.x, Y = blockIdx.y * 8 + threadIdx.y, Z = blockIdx.z - bsys * C.nz;
   if (X >= C.nx || Y >= C.ny) return;
-  t += (long long)bsys * 3 * Fl.nx * Fl.ny * C.nz;
+  const long long plane = PAD ? (long long)Fl.px * Fl.py : (long long)Fl.nx * Fl.ny, comp = plane * C.nz;
+  const long long rowl = PAD ? Fl.px : Fl.nx, o0 = PAD ? Fl.px + 1 : 0;  // t index of fine (x, y): o0 + y rowl + x
+  t += (long long)bsys * 3 * comp;
   fc += (long long)bsys * 3 * C.NP;
   const long long nC = C.nidx(X, Y, Z);
   T s0 = 0, s1 = 0, s2 = 0;
   if (C.vclass[nC] & NC_ACTIVE) {
-    const long long plane = (long long)Fl.nx * Fl.ny, comp = plane * C.nz;
-    const T* tz = t + (long long)Z * plane;
+    const T* tz = t + (long long)Z * plane + o0;
 #pragma unroll
     for (int dy = -F + 1; dy < F; dy++) {
       const int y = F * Y + dy;
@@ -475,7 +508,7 @@ __global__ void k_restrict_xy(const Level Fl, const Level C, const T* __restrict
         const int x = F * X + dx;
         if (x < 0 || x >= Fl.nx) continue;
         const T w = wy * ((T)(F - (dx < 0 ? -dx : dx)) / (T)F);
-        const long long i = (long long)y * Fl.nx + x;
+        const long long i = (long long)y * rowl + x;
         s0 += w * tz[i]; s1 += w * tz[i + comp]; s2 += w * tz[i + 2 * comp];
       }
     }
@@ -603,6 +636,71 @@ __global__ void __launch_bounds__(256) k_prolong_v4(const Level Fl, const Level 
 #pragma unroll
   for (int c = 0; c < 3; c++)
     *reinterpret_cast<float4*>(uf + p0 + c * NP) = make_float4(u[c][0], u[c][1], u[c][2], u[c][3]);
+}
+
+// FP32, single system: one warp per fine row (y, z).  The lanes first fold the
+// row's coarse columns along y and z into shared memory (E[c][X], X = 0..C.nx,
+// index C.nx the zero halo), then update four consecutive padded fine nodes
+// each with 16-byte loads and stores, taking every node's two x-corners from
+// E: 12 coarse loads per coarse column instead of up to 36 per four nodes.
+// Same arithmetic, in the same order, as k_prolong.
+constexpr int PROW_WARPS = 8;
+template <int F>
+__global__ void __launch_bounds__(32 * PROW_WARPS) k_prolong_row(const Level Fl, const Level C,
+                                                                 const float* __restrict__ uc, float* __restrict__ uf) {
+  extern __shared__ float sE_all[];  // [PROW_WARPS][3][C.nx + 1]
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int y = blockIdx.x * PROW_WARPS + w, z = blockIdx.y;
+  if (y >= Fl.ny) return;  // whole warp
+  const int ncol = C.nx + 1;
+  float* sE = sE_all + w * 3 * ncol;
+  const int Y0 = y / F, Z0 = z / F, oy = y - F * Y0, oz = z - F * Z0;
+  const float wy[2] = {(float)(F - oy) / (float)F, (float)oy / (float)F};
+  const float wz[2] = {(float)(F - oz) / (float)F, (float)oz / (float)F};
+  const long long cpx = C.px, cpxy = (long long)C.px * C.py;
+  for (int X = lane; X < ncol; X += 32) {
+    const long long c0 = C.nidx(X, Y0, Z0);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      float s = 0;
+#pragma unroll
+      for (int k = 0; k < 4; k++) s += wy[k & 1] * wz[k >> 1] * uc[c0 + (k & 1) * cpx + (k >> 1) * cpxy + c * C.NP];
+      sE[c * ncol + X] = s;
+    }
+  }
+  __syncwarp();
+  const long long NP = Fl.NP, rb = (long long)Fl.px * ((y + 1) + (long long)Fl.py * (z + 1));
+  for (int gq = lane; 4 * gq < Fl.px; gq += 32) {
+    const long long p0 = rb + 4 * gq;
+    const uchar4 cl4 = *reinterpret_cast<const uchar4*>(Fl.vclass + p0);
+    const uint8_t cls[4] = {cl4.x, cl4.y, cl4.z, cl4.w};
+    bool upd[4];
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int x = 4 * gq - 1 + k;
+      upd[k] = x >= 0 && x < Fl.nx && (cls[k] & NC_ACTIVE) && !(cls[k] & NC_SUPPORT);
+      any = any || upd[k];
+    }
+    if (!any) continue;
+    float u[3][4];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float4 m = *reinterpret_cast<const float4*>(uf + p0 + c * NP);
+      u[c][0] = m.x; u[c][1] = m.y; u[c][2] = m.z; u[c][3] = m.w;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      if (!upd[k]) continue;
+      const int x = 4 * gq - 1 + k, X0 = x / F, ox = x - F * X0;
+      const float w1 = (float)ox / (float)F, w0 = (float)(F - ox) / (float)F;
+#pragma unroll
+      for (int c = 0; c < 3; c++) u[c][k] = u[c][k] + (w0 * sE[c * ncol + X0] + w1 * sE[c * ncol + X0 + 1]);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      *reinterpret_cast<float4*>(uf + p0 + c * NP) = make_float4(u[c][0], u[c][1], u[c][2], u[c][3]);
+  }
 }
 
 // ---------------------------------------------------------------- Galerkin
@@ -1206,6 +1304,21 @@ rso_status restrict_(rso_handle* h, int cl, const T* rf, T* fc) {
   }
   T* t = reinterpret_cast<T*>(h->xfer);
   const dim3 gz(cdiv(f.nx, 32), cdiv(f.ny, 8), c.nz * c.nb);
+  // FP32, one system: the z pass on 16-byte vectors into padded planes (the
+  // scratch holds 2 xfer_n floats, 3 px py nz_coarse of them here)
+  if (sizeof(T) == 4 && c.nb == 1 && (c.factor == 4 || c.factor == 2) &&
+      (size_t)3 * f.px * f.py * c.nz <= 2 * h->xfer_n) {
+    const dim3 g4((unsigned)cdiv((long long)f.px * f.py / 4, 256), c.nz);
+    float* t4 = reinterpret_cast<float*>(h->xfer);
+    if (c.factor == 4) {
+      k_restrict_z_v4<4><<<g4, 256, 0, h->stream>>>(f, c.nz, (const float*)rf, t4); rso::note_launch();
+      k_restrict_xy<float, 4, true><<<node_grid(c), dim3(32, 8), 0, h->stream>>>(f, c, t4, (float*)fc); rso::note_launch();
+    } else {
+      k_restrict_z_v4<2><<<g4, 256, 0, h->stream>>>(f, c.nz, (const float*)rf, t4); rso::note_launch();
+      k_restrict_xy<float, 2, true><<<node_grid(c), dim3(32, 8), 0, h->stream>>>(f, c, t4, (float*)fc); rso::note_launch();
+    }
+    return launch_check(h, "restrict");
+  }
   if (c.factor == 4) {
     k_restrict_z<T, 4><<<gz, dim3(32, 8), 0, h->stream>>>(f, c.nz, rf, t); rso::note_launch();
     k_restrict_xy<T, 4><<<node_grid(c), dim3(32, 8), 0, h->stream>>>(f, c, t, fc); rso::note_launch();
@@ -1222,7 +1335,15 @@ template <typename T>
 rso_status prolong(rso_handle* h, int cl, const T* uc, T* uf) {
   const Level& f = h->L[cl - 1];
   const Level& c = h->L[cl];
-  if (sizeof(T) == 4 && f.nb == 1 && (c.factor == 4 || c.factor == 2)) {
+  const size_t row_smem = sizeof(float) * PROW_WARPS * 3 * (c.nx + 1);
+  if (sizeof(T) == 4 && f.nb == 1 && (c.factor == 4 || c.factor == 2) && row_smem <= 48 * 1024) {
+    const dim3 g((unsigned)cdiv(f.ny, PROW_WARPS), f.nz);
+    if (c.factor == 4)
+      k_prolong_row<4><<<g, dim3(32, PROW_WARPS), row_smem, h->stream>>>(f, c, (const float*)uc, (float*)uf);
+    else
+      k_prolong_row<2><<<g, dim3(32, PROW_WARPS), row_smem, h->stream>>>(f, c, (const float*)uc, (float*)uf);
+    rso::note_launch();
+  } else if (sizeof(T) == 4 && f.nb == 1 && (c.factor == 4 || c.factor == 2)) {
     const unsigned nblk = (unsigned)cdiv(f.NP / 4, 256);
     if (c.factor == 4)
       k_prolong_v4<4><<<nblk, 256, 0, h->stream>>>(f, c, (const float*)uc, (float*)uf);

@@ -206,6 +206,7 @@ rso_status upload_walsh(rso_handle* h) {
 // Node planes of u (3 components, 33 x (TY+1)) and element layers of rho^p are
 // staged with cp.async WPD stages ahead in WNSLOT slots.
 constexpr int WTX = 32, FZC = 32, WPD = 2, WNSLOT = 4;
+static_assert((WNSLOT & (WNSLOT - 1)) == 0, "slot indices are masks of the stage number");
 
 template <typename T, int TY>
 constexpr int walsh_smem_bytes() {
@@ -276,7 +277,7 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
   const long long pxy = (long long)L.px * L.py, qxy = (long long)L.qx * L.qy;
   // stage s: node plane s of u and element layer s of rho^p (zero outside)
   auto issue = [&](int s) {
-    T* dst = ss + ((s + WNSLOT) % WNSLOT) * SLOT;
+    T* dst = ss + ((s + WNSLOT) & (WNSLOT - 1)) * SLOT;
     const long long po = pxy * (s + 1), qo = qxy * (s + 1);
 #pragma unroll
     for (int kk = 0; kk < KC; kk++) {
@@ -316,7 +317,7 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
   T F[4][3], Gt[4][3], uc[3], uo[3], own[3], fo[3], po[3], ra[4], rb[4];
   uint8_t clo = 0;
   double pq = 0;  // with dotp: MODE 1 this thread's share of u . (K u), MODE 0 of r . r
-  face(ss + ((z0 - 1 + WNSLOT) % WNSLOT) * SLOT, F, uc);
+  face(ss + ((z0 - 1 + WNSLOT) & (WNSLOT - 1)) * SLOT, F, uc);
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     Gt[q][0] = Gt[q][1] = Gt[q][2] = T(0);
@@ -399,8 +400,8 @@ __global__ void __launch_bounds__(WTX* TY, sizeof(T) == 8 ? 2 : 3)
         }
       }
     }
-    const T* su = ss + ((z + 1 + WNSLOT) % WNSLOT) * SLOT;
-    const T* sr = ss + ((z + WNSLOT) % WNSLOT) * SLOT + 3 * NPL;
+    const T* su = ss + ((z + 1 + WNSLOT) & (WNSLOT - 1)) * SLOT;
+    const T* sr = ss + ((z + WNSLOT) & (WNSLOT - 1)) * SLOT + 3 * NPL;
     T v[8][3], un[3];
     {
       T Fn[4][3];
@@ -594,6 +595,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
              float c1, int fzc, const __grid_constant__ CUtensorMap tmu, const __grid_constant__ CUtensorMap tmr) {
   constexpr int RX = 36, ROWS = 2 * TYP, NPL = RX * (ROWS + 1), NT = WTX * TYP;
   constexpr int NS = pair_slots(MODE, TMA);
+  static_assert((NS & (NS - 1)) == 0, "slot indices are masks of the stage number");
   constexpr bool LEAN = MODE == 2 && TMA;  // operands of the emitted plane re-read from the slots
   constexpr int RHO = pair_rho_off<TYP>(), SLOT = pair_slot<TYP>();
   constexpr uint32_t STAGE_BYTES = sizeof(float) * (3 * NPL + RX * ROWS);  // both boxes of a stage
@@ -645,13 +647,13 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
   const long long pxy = (long long)L.px * L.py, qxy = (long long)L.qx * L.qy;
   __shared__ __align__(8) uint64_t bars[NS];
   bool gave_up = false;
-  // stage s (node plane s, element layer s) into slot (s + NS) % NS
+  // stage s (node plane s, element layer s) into slot (s + NS) mod NS (NS a power of two, s >= -1)
   auto issue = [&](int s) {
-    float* dst = ss + ((s + NS) % NS) * SLOT;
+    float* dst = ss + ((s + NS) & (NS - 1)) * SLOT;
     if constexpr (TMA) {
       // thread 0 only; stages past z1 are never read and not issued
       if (s > z1) return;
-      uint64_t* bar = &bars[(s + NS) % NS];
+      uint64_t* bar = &bars[(s + NS) & (NS - 1)];
       mbar_expect_tx(bar, STAGE_BYTES);
       tma_load_4d(dst, &tmu, xs, y0, s + 1, 3 * bsys, bar);
       tma_load_3d(dst + RHO, &tmr, xs, y0, s + 1, bar);
@@ -671,8 +673,8 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
   };
   // TMA: wait until stage s has landed (the k-th use of a slot completes phase k)
   auto wait_stage = [&](int s) {
-    const uint32_t parity = (uint32_t)((s - (z0 - 1)) / NS) & 1u;
-    if (!mbar_wait(&bars[(s + NS) % NS], parity)) gave_up = true;
+    const uint32_t parity = ((uint32_t)(s - (z0 - 1)) / NS) & 1u;  // s >= z0 - 1
+    if (!mbar_wait(&bars[(s + NS) & (NS - 1)], parity)) gave_up = true;
   };
   // xy modes of the face nodes of both columns on a staged plane (lane 0:
   // column A, lane 1: column B), and u at the two emitted nodes
@@ -714,7 +716,7 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
   uint8_t clA = 0, clB = 0;
   double pq = 0;  // with dotp: MODE 1 u . (K u); with DOT (MODE 2) f . out
   float2 zq = make_float2(0.f, 0.f);  // DOT: f . out of the two columns along the march
-  face(ss + ((z0 - 1 + NS) % NS) * SLOT, F, uc);
+  face(ss + ((z0 - 1 + NS) & (NS - 1)) * SLOT, F, uc);
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     Gt[q][0] = Gt[q][1] = Gt[q][2] = zero2;
@@ -754,9 +756,9 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
         // u at the two nodes from plane zo, rho^p from layers zo - 1 and zo
         // (stages zo - 1 and zo stay resident until stage zo + NS is issued)
         const int base = 2 * ty * RX + tx + ox;
-        const float* pu = ss + ((zo + NS) % NS) * SLOT + base;
-        const float* pa = ss + ((zo - 1 + NS) % NS) * SLOT + RHO + base;
-        const float* pb = ss + ((zo + NS) % NS) * SLOT + RHO + base;
+        const float* pu = ss + ((zo + NS) & (NS - 1)) * SLOT + base;
+        const float* pa = ss + ((zo - 1 + NS) & (NS - 1)) * SLOT + RHO + base;
+        const float* pb = ss + ((zo + NS) & (NS - 1)) * SLOT + RHO + base;
 #pragma unroll
         for (int c = 0; c < 3; c++) uo[c] = make_float2(pu[c * NPL + RX + 1], pu[c * NPL + 2 * RX + 1]);
         ra[0] = make_float2(pa[0], pa[RX]);
@@ -834,8 +836,8 @@ __global__ void __launch_bounds__(32 * TYP, pair_min_blocks(MODE, TYP))
         }
       }
     }
-    const float* su = ss + ((z + 1 + NS) % NS) * SLOT;
-    const float* sr = ss + ((z + NS) % NS) * SLOT + RHO;
+    const float* su = ss + ((z + 1 + NS) & (NS - 1)) * SLOT;
+    const float* sr = ss + ((z + NS) & (NS - 1)) * SLOT + RHO;
     float2 v[8][3], un[3];
     {
       float2 Fn[4][3];

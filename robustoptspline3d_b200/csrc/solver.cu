@@ -432,6 +432,48 @@ __global__ void k_cg32_step(long long n4, const double* __restrict__ alpha, cons
   x[2 * i + 1] = x1;
 }
 
+// Deferred FP64 steps: x += alpha_j p_j for the k directions waiting in the
+// ring, in their order (the step k_cg32_step_dir takes every iteration, taken
+// later with the same operations in the same order, so x is bit-identical at
+// every point where it is read)
+constexpr int kStepRing = 4;
+struct StepRing {
+  const float4* p[kStepRing];
+};
+__global__ void k_cg32_flush(long long n4, const double* __restrict__ alpha, const StepRing R, int k,
+                             double2* __restrict__ x) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n4) return;
+  double2 x0 = x[2 * i], x1 = x[2 * i + 1];
+#pragma unroll
+  for (int j = 0; j < kStepRing; j++) {
+    if (j >= k) break;
+    const float4 pi = R.p[j][i];
+    const double a = alpha[j];
+    x0.x += a * pi.x;
+    x0.y += a * pi.y;
+    x1.x += a * pi.z;
+    x1.y += a * pi.w;
+  }
+  x[2 * i] = x0;
+  x[2 * i + 1] = x1;
+}
+// p_out = z + beta p_in in FP32 (the direction update of k_cg32_step_dir);
+// p_out may be p_in
+__global__ void k_cg32_dir(long long n4, const double* __restrict__ beta, const float4* __restrict__ z,
+                           const float4* p_in, float4* p_out) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n4) return;
+  const float4 pi = p_in[i], zi = z[i];
+  const float b = (float)*beta;
+  p_out[i] = make_float4(zi.x + b * pi.x, zi.y + b * pi.y, zi.z + b * pi.z, zi.w + b * pi.w);
+}
+// alpha = rz / pq, also kept for the deferred step
+__global__ void k_cg_alpha_keep(double* s, double* keep) {
+  s[2] = s[0] / s[1];
+  *keep = s[2];
+}
+
 // Mixed-precision PCG with the Krylov recurrence in FP32 (no counterpart in
 // the reference, whose CG is FP64): p, q = K p, r and z are FP32 and the
 // iterate x accumulates alpha p in FP64.  The recursive FP32 residual drifts
@@ -833,9 +875,32 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
       RSO_TRY(gs);
       max_iter = 0;  // the loop below has run on the device
     }
+    // one system: the FP64 steps wait in a ring of four FP32 directions (the
+    // two halves of the FP64 buffers z and p) and enter x at the next
+    // replacement or when the ring is full, so a step reads each direction
+    // once more instead of x's 16 bytes per entry every iteration
+    const bool defer = l0.nb == 1;
+    float* ring[kStepRing] = {p32, p32 + n3, reinterpret_cast<float*>(h->p), reinterpret_cast<float*>(h->p) + n3};
+    double* ring_alpha = h->scal + 40;
+    int pend = 0;     // steps waiting: directions ring[0 .. pend), step sizes ring_alpha[0 .. pend)
+    float* pc = p32;  // the current direction, ring[pend] until its step size is known
+    auto flush = [&]() -> rso_status {
+      if (pend == 0) return RSO_OK;
+      StepRing R;
+      for (int j = 0; j < kStepRing; j++) R.p[j] = reinterpret_cast<const float4*>(ring[j < pend ? j : 0]);
+      k_cg32_flush<<<cdiv(n4, 256), 256, 0, h->stream>>>(n4, ring_alpha, R, pend, reinterpret_cast<double2*>(x));
+      rso::note_launch();
+      pend = 0;
+      return launch_check(h, "pcg32 deferred steps");
+    };
     while (it < max_iter) {
-      RSO_TRY(fine_applyK_dot32(h, p32, q32, s + 1));
-      k_cg_alpha<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
+      RSO_TRY(fine_applyK_dot32(h, pc, q32, s + 1));
+      if (defer) {
+        k_cg_alpha_keep<<<1, 1, 0, h->stream>>>(s, ring_alpha + pend); rso::note_launch();
+        pend++;
+      } else {
+        k_cg_alpha<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
+      }
       RSO_TRY(cg32_resid_rr(h, n3, s + 2, q32, r32, s + 5));
       RSO_CHECK_CUDA(h, cudaMemcpyAsync(h->h_scal + 5, s + 5, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
       RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -847,9 +912,13 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
       const bool replace =
           rnorm < h->krylov32 * rbase || rnorm < tol * fn || it >= max_iter || since >= kCycleMax;
       if (replace) {
-        k_cg32_step<<<cdiv(n4, 256), 256, 0, h->stream>>>(n4, s + 2, reinterpret_cast<const float4*>(p32),
-                                                          reinterpret_cast<double2*>(x));
-        rso::note_launch();
+        if (defer) {
+          RSO_TRY(flush());
+        } else {
+          k_cg32_step<<<cdiv(n4, 256), 256, 0, h->stream>>>(n4, s + 2, reinterpret_cast<const float4*>(pc),
+                                                            reinterpret_cast<double2*>(x));
+          rso::note_launch();
+        }
         RSO_TRY(true_residual_rr(&rn2));
         const double rtrue = std::sqrt(rn2);
         rel = rtrue / fn;
@@ -870,14 +939,22 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
       const float* z32 = l0.u32;
       if (!fuse) RSO_TRY(dot_ff(h, r32, z32, n3, s + 3));
       k_cg_beta<<<1, 1, 0, h->stream>>>(s); rso::note_launch();
-      if (replace)
+      if (defer) {
+        if (pend == kStepRing) RSO_TRY(flush());
+        float* pn = ring[pend];  // pc itself right after a flush of one step
+        k_cg32_dir<<<cdiv(n4, 256), 256, 0, h->stream>>>(n4, s + 4, reinterpret_cast<const float4*>(z32),
+                                                         reinterpret_cast<const float4*>(pc),
+                                                         reinterpret_cast<float4*>(pn));
+        pc = pn;
+      } else if (replace) {
         k_cg32_step_dir<true><<<cdiv(n4, 256), 256, 0, h->stream>>>(
-            n4, s + 2, s + 4, reinterpret_cast<const float4*>(z32), reinterpret_cast<float4*>(p32),
+            n4, s + 2, s + 4, reinterpret_cast<const float4*>(z32), reinterpret_cast<float4*>(pc),
             reinterpret_cast<double2*>(x));
-      else
+      } else {
         k_cg32_step_dir<false><<<cdiv(n4, 256), 256, 0, h->stream>>>(
-            n4, s + 2, s + 4, reinterpret_cast<const float4*>(z32), reinterpret_cast<float4*>(p32),
+            n4, s + 2, s + 4, reinterpret_cast<const float4*>(z32), reinterpret_cast<float4*>(pc),
             reinterpret_cast<double2*>(x));
+      }
       rso::note_launch();
       RSO_TRY(launch_check(h, "pcg32"));
     }

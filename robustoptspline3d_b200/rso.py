@@ -137,6 +137,7 @@ SIGNATURES = {
                                   ctypes.c_double, _vp, _pd]),
     "rso_coarse_sweep_fp32": (_ci, [_vp, _ci, _ci, _vp, _vp, _vp, ctypes.c_double, ctypes.c_double, _vp]),
     "rso_prolong_fp32": (_ci, [_vp, _ci, _vp, _vp, _vp]),
+    "rso_restrict_fp32": (_ci, [_vp, _ci, _vp, _vp]),
     "rso_autotune": (_ci, [_vp, _pi]),
     "rso_set_launch_shapes": (_ci, [_vp, _pi, _ci]),
     "rso_get_stencil": (_ci, [_vp, _ci, _vp]),
@@ -570,6 +571,15 @@ class HierarchyGrid:
         out = torch.empty_like(uf)
         self._chk(self.lib.rso_prolong_fp32(self.h, coarse_level, _dev(uc, torch.float64), _dev(uf, torch.float64),
                                             _dev(out)), "rso_prolong_fp32")
+        return out
+
+    def restrict_fp32(self, coarse_level, rf):
+        """R rf in FP32 (the mixed V-cycle's restriction), FP64 in and out."""
+        import torch
+        d = self.level_dims(coarse_level)
+        out = torch.empty(3 * int(d[3] * d[4] * d[5]), dtype=torch.float64, device="cuda")
+        self._chk(self.lib.rso_restrict_fp32(self.h, coarse_level, _dev(rf, torch.float64), _dev(out)),
+                  "rso_restrict_fp32")
         return out
 
     def stencil(self, level):

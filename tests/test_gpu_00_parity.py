@@ -118,9 +118,9 @@ def test_operator_fp32(oracle, cuda, gen, rows):
 def test_coarse_and_transfers_fp32(oracle, cuda, gen, ff, split):
     """FP32 kernels of the mixed V-cycle below the fine level against the FP64 oracle: coarse
     residual and Jacobi / Chebyshev steps with both coarse kernel variants (one thread per node
-    with 16-byte streams, split = 0; one per node and row, split = 1), the prolongation, and the
-    fine level's first step from zero.  Tolerance 2e-5 relative in norm (FP32 stencils and
-    vectors)."""
+    with 16-byte streams, split = 0; one per node and row, split = 1), the prolongation, the
+    restriction, and the fine level's first step from zero.  Tolerance 2e-5 relative in norm
+    (FP32 stencils and vectors)."""
     prob = gen()
     g, o = make(oracle, prob, first_factor=ff)
     g.update_stencil()
@@ -152,6 +152,8 @@ def test_coarse_and_transfers_fp32(oracle, cuda, gen, ff, split):
         if lvl == 1:
             po[np.tile((o.node_class() & 4) > 0, 3)] = 0
         assert rel(g.prolong_fp32(lvl, t(uc, cuda), t(uf, cuda)).cpu().numpy(), po) < tol, lvl
+        rf = rng.standard_normal(3 * nnf) * np.tile(vmf, 3)
+        assert rel(g.restrict_fp32(lvl, t(rf, cuda)).cpu().numpy(), o.restrict(lvl, rf)) < tol, lvl
     cls = o.node_class()
     dead = np.tile(((cls & 4) > 0) | ((cls & 1) == 0), 3)
     f = rng.standard_normal(3 * o.nn)

@@ -247,8 +247,13 @@ def run_solves(args):
     g.set_density(rho)
     g.update_stencil()
     tuned = g.autotune() if prec == R.rso.MIXED and not args.no_autotune else None
-    if args.fine_rows:
-        g.set_launch_shapes(fine_rows=args.fine_rows)
+    if args.fine_rows or args.bottom_level != -3:
+        sh = g.launch_shapes()
+        g.set_launch_shapes(fine_rows=args.fine_rows or sh["fine_rows"],
+                            bottom_level=sh["bottom_level"] if args.bottom_level == -3 else args.bottom_level,
+                            row_split=sh["row_split"])
+    if args.bottom_kernel >= 0:
+        g.set_bottom_kernel(args.bottom_kernel)
     if prec == R.rso.MIXED:
         g.set_krylov_fp32(args.krylov32)
     f = torch.zeros(3 * g.nn, dtype=torch.float64, device="cuda")
@@ -271,7 +276,7 @@ def run_solves(args):
                       "value": ms / args.steps, "unit": "ms/solve", "higher_is_better": False,
                       "iterations_per_solve": its / args.steps, "ms_per_iteration": ms / its,
                       "max_true_rel_residual": worst, "krylov32_replace_factor": args.krylov32,
-                      "levels": g_levels(n), "kernel_classes": classes, "launch_shapes": tuned}), flush=True)
+                      "levels": g_levels(n), "kernel_classes": classes, "launch_shapes": g.launch_shapes()}), flush=True)
     g.close()
 
 
@@ -700,6 +705,10 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--fine-rows", type=int, default=0,
                     help="--mode solve: thread rows of the packed fine kernel's CTA (2, 4 or 8; 0: as tuned)")
+    ap.add_argument("--bottom-level", type=int, default=-3,
+                    help="--mode solve: first level of the bottom kernel (-1 none, -2 built-in rule; default as tuned)")
+    ap.add_argument("--bottom-kernel", type=int, default=-1,
+                    help="--mode solve: bottom kernel kind (1 persistent grid-wide, 0 cluster; default as tuned)")
     ap.add_argument("--ref-size", type=int, default=24)
     ap.add_argument("--ref-sizes", default="24,32,48",
                     help="sample sizes of the CPU baseline leg (the largest is scaled to 256^3)")

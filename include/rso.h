@@ -315,18 +315,22 @@ rso_status rso_solve_batch(rso_handle* h, int k, const double* F_dev, double* U_
 /* Launch-shape autotuner (no counterpart in the reference, whose launch
  * shapes are fixed): times, on this handle's hierarchy with CUDA events, the
  * thread rows of the packed FP32 fine kernel (2, 4 or 8), one thread per node or
- * per (node, row) on every coarse level, and the first level of the bottom
- * cluster kernel (or none), each timed as mixed-precision solves of a random
- * load, and keeps the fastest for this handle (a candidate must beat the
- * built-in rule by 1 %).  The candidates compute the same arithmetic.  Needs
+ * per (node, row) on every coarse level, the z chunk of the fine kernel, and
+ * the first level and kind of the bottom kernel (or none), each timed as
+ * mixed-precision solves of a random load, and keeps the fastest for this
+ * handle (a candidate must beat the built-in rule by 3 %).  The candidates compute the same arithmetic.  Needs
  * rso_update_operators first, mixed precision and a Jacobi or Chebyshev
  * smoother; overwrites the solver's work vectors; takes a few dozen solves.  choices_host (NULL or
- * 2 + number of levels ints): fine rows, bottom level (-1 none), then per
- * level 0 = node per thread, 1 = row split, -1 not tuned. */
+ * 2 + number of levels ints): fine rows, bottom level (-1 none; its kind is
+ * read with rso_bottom_kernel), then per level 0 = node per thread, 1 = row
+ * split, 2 = nine per node, -1 not tuned. */
 rso_status rso_autotune(rso_handle* h, int* choices_host);
 /* Sets the launch shapes directly, in rso_autotune's format (n >= 2 ints;
  * bottom level -2 restores the built-in size rule, a row-split entry of -1
- * too), e.g. to reuse choices measured once for many handles. */
+ * too), e.g. to reuse choices measured once for many handles.  The built-in
+ * bottom rule, for the FP32 V-cycle of mixed precision with bottom kernel
+ * kind 1: the persistent kernel from the first coarse level of at most 60,000
+ * nodes above the coarsest. */
 rso_status rso_set_launch_shapes(rso_handle* h, const int* choices_host, int n);
 /* Node planes per z chunk of the packed FP32 fine kernel (4, 8, 16 or 32; 0
  * restores the size rule: the longest chunk that gives the grid 4 CTAs per
@@ -336,6 +340,16 @@ rso_status rso_set_launch_shapes(rso_handle* h, const int* choices_host, int n);
  * use. */
 rso_status rso_set_fine_zchunk(rso_handle* h, int planes);
 int rso_fine_zchunk(const rso_handle* h);
+/* Kernel of the bottom of the FP32 V-cycle, when the launch shapes give it a
+ * first level (no counterpart in the reference, which launches every level's
+ * kernels): kind 1 (default) one persistent cooperative kernel over the whole
+ * GPU, every CTA resident at once, its phases (sweeps, residuals, transfers,
+ * the coarsest solve) separated by a grid-wide barrier whose waits give up
+ * after about 2 s (the solve then fails with RSO_ERR_CUDA); kind 0 one kernel
+ * on an 8-CTA thread-block cluster.  rso_autotune measures both;
+ * rso_bottom_kernel returns the kind in use. */
+rso_status rso_set_bottom_kernel(rso_handle* h, int kind);
+int rso_bottom_kernel(const rso_handle* h);
 /* Replay of the FP32 V-cycle (the mixed-precision preconditioner) from CUDA
  * graphs (no counterpart in the reference, which launches every kernel):
  * on by default.  The V-cycle is captured the second time its launch
@@ -347,9 +361,10 @@ int rso_fine_zchunk(const rso_handle* h);
 rso_status rso_set_vcycle_graphs(rso_handle* h, int on);
 /* Device-controlled solves (no counterpart in the reference): with on != 0
  * the mixed-precision PCG loop with the FP32 recurrence runs as one CUDA
- * graph per solve, a conditional WHILE node whose body holds the iteration
- * (q = K p, the residual update, the V-cycle, the direction update) and a
- * conditional IF node for the FP64 residual replacement; the decisions the
+ * graph per solve: 16 unrolled iterations, each of conditional IF nodes for
+ * the iteration (q = K p, the residual update), the FP64 residual
+ * replacement, and the V-cycle with the direction update (a straight-line
+ * graph: a launch ends whatever the device decides); the decisions the
  * host takes between iterations otherwise (replace, stop, stall) are taken by
  * one-thread kernels on the same scalars, so the iterations, iterates and
  * residuals are those of the host-driven loop.  Used when the V-cycle graphs

@@ -10,7 +10,7 @@
 //     and each re-reads one plane),
 //   - per coarse level, one thread per node (k_coarse4 / k_coarse), per
 //     (node, row) (k_coarse_r) or nine per node (k_coarse_r9),
-//   - the first level of the bottom cluster kernel (or none).
+//   - the first level of the bottom kernel and its kind (or none).
 // Each candidate is timed as whole solves (see solve_ms).
 // The candidates compute the same arithmetic; only launch shapes differ.  The
 // solver's work vectors are overwritten.
@@ -56,8 +56,6 @@ rso_status time_ms(rso_handle* h, int warm, int reps, F&& body, double* ms) {
   return RSO_OK;
 }
 
-// largest level the bottom cluster kernel is tried from (8 CTAs sweep it)
-constexpr long long kTuneBottomMaxNodes = 60000;
 
 // Every candidate is timed as mixed-precision PCG solves to relative residual
 // 1e-6 of a random load (the FP64 level vectors of the fine level hold it and
@@ -116,16 +114,26 @@ rso_status autotune(rso_handle* h) {
       if (v != zc.front()) zc.push_back(v);
     RSO_TRY(pick(h, zc, [&](int v) { h->tune.fine_zc = v; }));
   }
-  // first level of the bottom cluster kernel, or none
+  // first level of the bottom kernel and its kind (2 level + kind: 1 the
+  // persistent grid-wide kernel, 0 the cluster kernel), or none
   h->tune.bottom = 1;
   if (nl >= 3 && bottom_level(h) == 1) {
-    std::vector<int> cands = {-1};  // the built-in rule (none) first
+    // the built-in rule's choice first
+    h->tune.bottom = -2;
+    h->tune.bottom_kind = 1;
+    const int rule = bottom_level(h);
+    std::vector<int> cands = {rule > 0 ? 2 * rule + 1 : -1};
+    if (rule > 0) cands.push_back(-1);
     for (int lb = nl - 2; lb >= 1; lb--) {
       bool small = true;
-      for (int li = lb; li < nl; li++) small = small && h->L[li].nn <= kTuneBottomMaxNodes;
-      if (small) cands.push_back(lb);
+      for (int li = lb; li < nl; li++) small = small && h->L[li].nn <= kBottomMaxNodes;
+      for (int kind = 1; small && kind >= 0; kind--)
+        if (2 * lb + kind != cands.front()) cands.push_back(2 * lb + kind);
     }
-    RSO_TRY(pick(h, cands, [&](int v) { h->tune.bottom = v; }));
+    RSO_TRY(pick(h, cands, [&](int v) {
+      h->tune.bottom = v < 0 ? -1 : v / 2;
+      if (v >= 0) h->tune.bottom_kind = v % 2;
+    }));
   } else {
     h->tune.bottom = -2;
   }
@@ -189,7 +197,8 @@ extern "C" rso_status rso_set_launch_shapes(rso_handle* h, const int* choices_ho
     return RSO_ERR_INVALID_ARG;
   }
   rso_handle::Tune t;
-  t.fine_zc = h->tune.fine_zc;  // set on its own (rso_set_fine_zchunk)
+  t.fine_zc = h->tune.fine_zc;  // set on their own (rso_set_fine_zchunk, rso_set_bottom_kernel)
+  t.bottom_kind = h->tune.bottom_kind;
   t.fine_rows = choices_host[0];
   t.bottom = b;
   for (int li = 0; li < nl && 2 + li < n && li < 16; li++) {

@@ -115,7 +115,7 @@ static void free_handle(rso_handle* h) {
   batch_release(h);
   cudaFree(h->c_nodes); cudaFree(h->c_K); cudaFree(h->c_f); cudaFree(h->c_flag);
   cudaFree(h->rigid_q); cudaFree(h->rigid_m); cudaFree(h->rigid_scr); cudaFree(h->c_R);
-  cudaFree(h->red); cudaFree(h->scal); cudaFree(h->xfer); cudaFree(h->fpart);
+  cudaFree(h->red); cudaFree(h->gbar); cudaFree(h->scal); cudaFree(h->xfer); cudaFree(h->fpart);
   if (h->h_scal) cudaFreeHost(h->h_scal);
   cudaFree(h->x); cudaFree(h->r); cudaFree(h->p); cudaFree(h->q); cudaFree(h->z); cudaFree(h->w);
   cudaFree(h->stage_a); cudaFree(h->stage_b);
@@ -150,6 +150,8 @@ static rso_status setup(rso_handle* h, int ex, int ey, int ez, const uint8_t* em
   RSO_CHECK_CUDA(h, cudaMemcpy(h->K0_dev, h->K0, sizeof(double) * 576, cudaMemcpyHostToDevice));
   RSO_TRY(upload_K0(h));
   ALLOC(h->red, sizeof(double) * 4096);
+  ALLOC(h->gbar, sizeof(unsigned) * 4);
+  RSO_CHECK_CUDA(h, cudaMemset(h->gbar, 0, sizeof(unsigned) * 4));
   ALLOC(h->scal, sizeof(double) * 64);
   RSO_CHECK_CUDA(h, cudaMallocHost((void**)&h->h_scal, sizeof(double) * 64));
   RSO_CHECK_CUDA(h, cudaMemset(h->scal, 0, sizeof(double) * 64));
@@ -512,6 +514,14 @@ extern "C" rso_status rso_set_fine_zchunk(rso_handle* h, int planes) {
 }
 
 extern "C" int rso_fine_zchunk(const rso_handle* h) { return h ? fine_zc(h) : 0; }
+
+extern "C" rso_status rso_set_bottom_kernel(rso_handle* h, int kind) {
+  if (!h || (kind != 0 && kind != 1)) return RSO_ERR_INVALID_ARG;
+  h->tune.bottom_kind = kind;
+  return RSO_OK;
+}
+
+extern "C" int rso_bottom_kernel(const rso_handle* h) { return h ? h->tune.bottom_kind : -1; }
 
 extern "C" rso_status rso_set_solve_graphs(rso_handle* h, int on) {
   if (!h) return RSO_ERR_INVALID_ARG;

@@ -13,6 +13,8 @@
 // which applies R K P to assembled stencils).  Stencils are then assembled
 // from the element matrices, in FP64 and FP32.
 #include "rso_internal.cuh"
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cooperative_groups.h>
@@ -25,8 +27,10 @@ namespace rso {
 static const double DIRICHLET_W = 1e6;  // grid/Grid.cu:14
 
 // ---------------------------------------------------------------- stencil kernels
+// u is a plain pointer: the bottom kernels write it in earlier phases of the
+// same launch, so its loads must be coherent ones
 template <typename T>
-__device__ __forceinline__ void stencil_apply(const Level& L, const T* __restrict__ st, const T* __restrict__ u,
+__device__ __forceinline__ void stencil_apply(const Level& L, const T* __restrict__ st, const T* u,
                                               long long n, bool skip_centre, T acc[3]) {
   const long long NP = L.NP, px = L.px, pxy = (long long)L.px * L.py;
 #pragma unroll
@@ -274,14 +278,16 @@ __global__ void __launch_bounds__(C4G * 3, 3) k_coarse4(const Level L, const flo
 // Jacobi update exchanges the three residual components through shared
 // memory.
 constexpr int CTY = 4;
-template <typename T, int MODE>
-__global__ void __launch_bounds__(32 * CTY * 3) k_coarse_r(const Level L, const T* __restrict__ st,
-                                                           const T* __restrict__ u, const T* __restrict__ f,
-                                                           T* __restrict__ out, T omega,
-                                                           const T* __restrict__ uprev, T c1) {
-  __shared__ T sres[3][CTY][32];
-  const int bsys = blockIdx.z / L.nz;
-  const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * CTY + threadIdx.y, z = blockIdx.z - bsys * L.nz;
+// thread (x, y, r) of a 32 x CTY x 3 tile at plane z of system bsys; ZERO:
+// u read as zero (a first step from a zero iterate).  sres is the tile's
+// shared exchange; every thread of the CTA calls this (MODE 2 synchronises it)
+// The vectors are plain pointers here: the persistent bottom kernel writes
+// them in earlier phases of the same launch, so their loads must be coherent
+// ones (the per-level kernel's own parameters carry __restrict__).
+template <typename T, int MODE, bool ZERO = false>
+__device__ __forceinline__ void coarse_r_node(const Level& L, const T* __restrict__ st, const T* u, const T* f,
+                                              T* out, T omega, const T* uprev, T c1, int x, int y, int z, int bsys,
+                                              T (*sres)[CTY][32]) {
   {
     const long long off = (long long)bsys * 3 * L.NP;
     u += off;
@@ -295,7 +301,7 @@ __global__ void __launch_bounds__(32 * CTY * 3) k_coarse_r(const Level L, const 
   const long long n = in ? L.nidx(x, y, z) : 0;
   const bool act = in && (L.vclass[n] & NC_ACTIVE) != 0;
   T acc = 0;
-  if (act) {
+  if (act && !ZERO) {
 #pragma unroll
     for (int d = 0; d < 27; d++) {
       const long long nb = n + (d % 3 - 1) + (d / 3 % 3 - 1) * px + (d / 9 - 1) * pxy;
@@ -325,8 +331,18 @@ __global__ void __launch_bounds__(32 * CTY * 3) k_coarse_r(const Level L, const 
   else { a0 = c02; a1 = -(S[0] * S[7] - S[1] * S[6]); a2 = S[0] * S[4] - S[1] * S[3]; }
   const T r0 = sres[0][threadIdx.y][threadIdx.x], r1 = sres[1][threadIdx.y][threadIdx.x],
           r2 = sres[2][threadIdx.y][threadIdx.x];
-  const T ur = u[n + r * NP], pr = uprev ? uprev[n + r * NP] : T(0);
+  const T ur = ZERO ? T(0) : u[n + r * NP], pr = uprev ? uprev[n + r * NP] : T(0);
   out[n + r * NP] = ur + c1 * (ur - pr) + (omega / det) * (a0 * r0 + a1 * r1 + a2 * r2);
+}
+template <typename T, int MODE>
+__global__ void __launch_bounds__(32 * CTY * 3) k_coarse_r(const Level L, const T* __restrict__ st,
+                                                           const T* __restrict__ u, const T* __restrict__ f,
+                                                           T* __restrict__ out, T omega,
+                                                           const T* __restrict__ uprev, T c1) {
+  __shared__ T sres[3][CTY][32];
+  const int bsys = blockIdx.z / L.nz;
+  coarse_r_node<T, MODE>(L, st, u, f, out, omega, uprev, c1, blockIdx.x * 32 + threadIdx.x,
+                         blockIdx.y * CTY + threadIdx.y, blockIdx.z - bsys * L.nz, bsys, sres);
 }
 
 // Small levels (a few thousand to a few ten thousand nodes): the per-row
@@ -1203,6 +1219,177 @@ __global__ void __cluster_dims__(BOT_CTAS, 1, 1) __launch_bounds__(BOT_THREADS, 
   }
 }
 
+// The same bottom of the V-cycle as one persistent kernel over the whole GPU:
+// a cooperative launch (every CTA resident at once) whose phases are
+// separated by a grid-wide barrier.  The sweeps and residuals run as the
+// row-split per-level kernel does (tiles of 32 x CTY nodes, three threads per
+// node, the same arithmetic: bit-identical sweeps), the transfers and the
+// coarsest solve as in k_bottom.
+constexpr int GB_THREADS = 32 * CTY * 3;
+// a barrier wait gives up after this many SM clock cycles (about 2 s)
+constexpr long long kGbarCycles = 4000000000LL;
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// grid-wide barrier on bar = {arrivals, generation, gave-up flag}: one arrival
+// per CTA; the last resets the count and advances the generation.  gen (thread
+// 0's copy of the generation) moves on with it.  Returns false on every
+// thread of every CTA once some wait has given up (bar[2] set): the kernel
+// then returns, and the host reports it after the solve.
+__device__ bool gbar_sync(unsigned* bar, unsigned& gen, int tid) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (tid == 0) {
+    int ok = *reinterpret_cast<volatile unsigned*>(bar + 2) == 0u;
+    if (ok) {
+      const unsigned g = gen;
+      __threadfence();
+      if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+        atomicExch(bar, 0u);
+        __threadfence();
+        atomicExch(bar + 1, g + 1);
+      } else {
+        const long long t0 = clock64();
+        while (ld_acquire_gpu(bar + 1) == g) {
+          if (*reinterpret_cast<volatile unsigned*>(bar + 2) != 0u) { ok = 0; break; }
+          if (clock64() - t0 > kGbarCycles) {
+            atomicExch(bar + 2, 1u);
+            ok = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+      gen = g + 1;
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// one row-split sweep (MODE 2) or residual (MODE 0) of a level, tile by tile
+template <typename T, int MODE, bool ZERO>
+__device__ void gb_sweep(const Level& L, const T* st, const T* u, const T* f, T* out, T omega, const T* uprev, T c1,
+                         T (*sres)[CTY][32]) {
+  const int tx = (L.nx + 31) / 32, ty = (L.ny + CTY - 1) / CTY;
+  const long long nt = (long long)tx * ty * L.nz * L.nb;
+  for (long long t = blockIdx.x; t < nt; t += gridDim.x) {
+    const int bx = (int)(t % tx);
+    const long long q = t / tx;
+    const int by = (int)(q % ty);
+    const long long zb = q / ty;
+    const int bsys = (int)(zb / L.nz), z = (int)(zb - (long long)bsys * L.nz);
+    coarse_r_node<T, MODE, ZERO>(L, st, u, f, out, omega, uprev, c1, bx * 32 + threadIdx.x, by * CTY + threadIdx.y,
+                                 z, bsys, sres);
+    __syncthreads();  // sres is reused by the next tile
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(GB_THREADS) k_bottom_grid(const __grid_constant__ BottomArgs<T> A, unsigned* bar) {
+  __shared__ T sres[3][CTY][32];
+  const int tid = threadIdx.x + 32 * (threadIdx.y + CTY * threadIdx.z);
+  const int g0 = blockIdx.x * GB_THREADS + tid, gs = gridDim.x * GB_THREADS;
+  unsigned gen = 0;
+  if (tid == 0) gen = ld_acquire_gpu(bar + 1);
+#define GB_SYNC() \
+  if (!gbar_sync(bar, gen, tid)) return
+  T* ucur[BOT_MAX_LEVELS];
+  // down: pre-smoothing from a zero iterate, residual, restriction
+  for (int li = A.lb; li < A.nl - 1; li++) {
+    const Level& L = A.L[li];
+    const T* st = bv_st<T>(L);
+    T* u = bv_u<T>(L);
+    T *cur = u, *oth = bv_t<T>(L), *prv = bv_r<T>(L);
+    for (int s = 0; s < A.pre; s++) {
+      if (s == 0)
+        gb_sweep<T, 2, true>(L, st, cur, bv_f<T>(L), oth, A.om[li][s], (const T*)nullptr, A.c1[li][s], sres);
+      else
+        gb_sweep<T, 2, false>(L, st, cur, bv_f<T>(L), oth, A.om[li][s], s <= 1 ? (const T*)nullptr : prv,
+                              A.c1[li][s], sres);
+      GB_SYNC();
+      T* w = prv; prv = cur; cur = oth; oth = w;
+    }
+    if (A.pre == 0) {
+      for (long long i = g0; i < 3 * L.NP * L.nb; i += gs) u[i] = T(0);
+      GB_SYNC();
+    }
+    ucur[li] = cur;
+    gb_sweep<T, 0, false>(L, st, cur, bv_f<T>(L), oth, T(0), (const T*)nullptr, T(0), sres);
+    GB_SYNC();
+    bot_restrict<T>(L, A.L[li + 1], oth, bv_f<T>(A.L[li + 1]), g0, gs);
+    GB_SYNC();
+  }
+  // coarsest: u = Kinv f at the listed nodes, zero elsewhere; one warp per row
+  {
+    const Level& C = A.L[A.nl - 1];
+    T* u = bv_u<T>(C);
+    const T* f = bv_f<T>(C);
+    const long long VS = 3 * C.NP;
+    const int N = 3 * A.nc;
+    for (long long i = g0; i < VS * C.nb; i += gs) u[i] = T(0);
+    for (long long ib = g0; ib < (long long)A.nc * C.nb; ib += gs) {
+      const long long b = ib / A.nc, i = ib - b * A.nc;
+      const long long n = A.cnodes[i] + b * VS;
+      double* cf = A.cf + b * N;
+      cf[3 * i + 0] = (double)f[n];
+      cf[3 * i + 1] = (double)f[n + C.NP];
+      cf[3 * i + 2] = (double)f[n + 2 * C.NP];
+    }
+    GB_SYNC();
+    const int lane = tid & 31, warp = g0 >> 5, nwarps = gs >> 5;
+    for (long long rb = warp; rb < (long long)N * C.nb; rb += nwarps) {
+      const long long b = rb / N;
+      const int row = (int)(rb - b * N);
+      const double* cf = A.cf + b * N;
+      const double* k = A.kinv + (long long)row * N;
+      double sum = 0;
+      for (int j = lane; j < N; j += 32) sum += k[j] * cf[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+      if (lane == 0) u[b * VS + A.cnodes[row / 3] + (row % 3) * C.NP] = (T)sum;
+    }
+    ucur[A.nl - 1] = u;
+    GB_SYNC();
+  }
+  // up: prolongation and post-smoothing; the top level ends in its u
+  for (int li = A.nl - 2; li >= A.lb; li--) {
+    const Level& L = A.L[li];
+    const T* st = bv_st<T>(L);
+    T* u = bv_u<T>(L);
+    T *cur = ucur[li], *oth, *prv;
+    T* bufs[3] = {u, bv_t<T>(L), bv_r<T>(L)};
+    {
+      int k = 0;
+      T* rest[2];
+      for (int q = 0; q < 3; q++)
+        if (bufs[q] != cur) rest[k++] = bufs[q];
+      oth = rest[0];
+      prv = rest[1];
+    }
+    bot_prolong<T>(L, A.L[li + 1], ucur[li + 1], cur, g0, gs);
+    GB_SYNC();
+    for (int s = 0; s < A.post; s++) {
+      gb_sweep<T, 2, false>(L, st, cur, bv_f<T>(L), oth, A.om[li][s], s == 0 ? (const T*)nullptr : prv,
+                            A.c1[li][s], sres);
+      GB_SYNC();
+      T* w = prv; prv = cur; cur = oth; oth = w;
+    }
+    ucur[li] = cur;
+    if (li == A.lb && cur != u) {
+      bot_copy<T>(L, cur, u, g0, gs);
+      GB_SYNC();
+    }
+  }
+#undef GB_SYNC
+}
+
 // ---------------------------------------------------------------- host wrappers
 // grids over the nodes of a level for every system it carries
 static inline dim3 node_grid(const Level& l) { return dim3(cdiv(l.nx, 32), cdiv(l.ny, 8), l.nz * l.nb); }
@@ -1374,19 +1561,24 @@ rso_status coarsest_solve(rso_handle* h, const T* f, T* u) {
   return launch_check(h, "coarsest_solve");
 }
 
-// index of the first level handled by k_bottom (-1: none).  It needs damped
-// Jacobi or Chebyshev, at least one smoothed level above the coarsest, and a
-// level chosen by rso_autotune.
-int bottom_level(const rso_handle* h) {
+// index of the first level handled by the bottom kernel (-1: none).  It needs
+// damped Jacobi or Chebyshev and at least one smoothed level above the
+// coarsest; the level is rso_autotune's choice or the built-in rule's.
+int bottom_level(const rso_handle* h, bool fp32) {
   const int nl = (int)h->L.size();
   if (h->cfg.smoother == RSO_SMOOTH_GS || nl < 3 || nl > BOT_MAX_LEVELS || h->nc == 0) return -1;
   if (h->cfg.pre > BOT_MAX_SWEEPS || h->cfg.post > BOT_MAX_SWEEPS) return -1;
   // a level chosen by rso_autotune: any level from 1 to nl - 2, or none
   if (h->tune.bottom == -1) return -1;
   if (h->tune.bottom >= 1 && h->tune.bottom <= nl - 2) return h->tune.bottom;
-  // built-in rule: none.  The cluster kernel's phases run on 8 SMs and wait on
-  // load latency; separate launches over the whole GPU measured faster on
-  // cubes from 32^3 to 256^3 (rso_autotune still tries it)
+  // built-in rule, for the FP32 V-cycle of mixed precision (the FP64 one keeps
+  // its per-level launches): the persistent grid-wide kernel from the first
+  // level of at most kBottomMaxNodes nodes, whose sweeps are latency-bound
+  // (256^3: from 33^3, 35.2 -> 33.6 ms per solve; 64^3: from 17^3, 5.6 ->
+  // 4.2 ms); the cluster kernel only when rso_autotune finds it faster
+  if (!fp32 || h->cfg.precision != RSO_MIXED || h->tune.bottom_kind != 1) return -1;
+  for (int li = 1; li <= nl - 2; li++)
+    if (h->L[li].nn <= kBottomMaxNodes) return li;
   return -1;
 }
 
@@ -1409,8 +1601,41 @@ rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post) {
   A.cnodes = h->c_nodes;
   A.nc = h->nc;
   A.cf = h->L[0].nb > 1 ? h->c_fb : h->c_f;
-  k_bottom<T><<<BOT_CTAS, BOT_THREADS, 0, h->stream>>>(A); rso::note_launch();
-  return launch_check(h, "bottom_vcycle");
+  if (h->tune.bottom_kind == 0) {
+    k_bottom<T><<<BOT_CTAS, BOT_THREADS, 0, h->stream>>>(A); rso::note_launch();
+    return launch_check(h, "bottom_vcycle");
+  }
+  // the persistent kernel: as many CTAs as the largest level has tiles, at
+  // most as many as are resident at once (a cooperative launch refuses more)
+  static std::atomic<int> occ_cache[2][64];
+  const int ti = sizeof(T) == 4 ? 0 : 1;
+  const int dev = h->device >= 0 && h->device < 64 ? h->device : 0;
+  int occ = occ_cache[ti][dev].load(std::memory_order_relaxed);
+  if (occ <= 0) {
+    RSO_CHECK_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bottom_grid<T>, GB_THREADS, 0));
+    occ_cache[ti][dev].store(occ, std::memory_order_relaxed);
+  }
+  int sms = 0;
+  RSO_CHECK_CUDA(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  long long need = 1;
+  for (int li = lb; li < nl; li++) {
+    const Level& l = h->L[li];
+    need = std::max(need, (long long)cdiv(l.nx, 32) * cdiv(l.ny, CTY) * l.nz * l.nb);
+  }
+  const int grid = (int)std::max<long long>(1, std::min<long long>(need, (long long)occ * sms));
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(grid);
+  lc.blockDim = dim3(32, CTY, 3);
+  lc.dynamicSmemBytes = 0;
+  lc.stream = h->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  RSO_CHECK_CUDA(h, cudaLaunchKernelEx(&lc, k_bottom_grid<T>, A, h->gbar));
+  rso::note_launch();
+  return launch_check(h, "bottom_vcycle (grid)");
 }
 template rso_status bottom_vcycle<double>(rso_handle*, int, int, int);
 template rso_status bottom_vcycle<float>(rso_handle*, int, int, int);

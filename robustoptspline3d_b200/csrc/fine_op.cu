@@ -1258,9 +1258,17 @@ static rso_status pair_tensor_maps(rso_handle* h, const Level& l, const float* u
 // fails if a staged-copy wait of the fine kernels gave up since the last call
 // (never in a healthy run); resets the device-wide count
 rso_status fine_stage_check(rso_handle* h) {
-  unsigned int n = 0, zero = 0;
+  unsigned int n = 0, zero = 0, gb = 0;
   RSO_CHECK_CUDA(h, cudaMemcpyFromSymbolAsync(&n, g_stage_timeouts, sizeof(n), 0, cudaMemcpyDeviceToHost, h->stream));
+  if (h->gbar) RSO_CHECK_CUDA(h, cudaMemcpyAsync(&gb, h->gbar + 2, sizeof(gb), cudaMemcpyDeviceToHost, h->stream));
   RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (gb != 0) {
+    // nothing runs on the stream now: the barrier starts afresh
+    RSO_CHECK_CUDA(h, cudaMemsetAsync(h->gbar, 0, sizeof(unsigned) * 4, h->stream));
+    RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+    h->err = "a grid-barrier wait of the persistent bottom kernel timed out";
+    return RSO_ERR_CUDA;
+  }
   if (n != 0) {
     RSO_CHECK_CUDA(h, cudaMemcpyToSymbolAsync(g_stage_timeouts, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, h->stream));
     RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));

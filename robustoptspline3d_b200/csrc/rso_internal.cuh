@@ -143,6 +143,7 @@ struct rso_handle {
   double* c_R = nullptr;              // coarsest rigid motions, 3 nc x 6 row-major, orthonormal
   // reductions
   double* red = nullptr;              // partials
+  unsigned* gbar = nullptr;           // grid barrier of the persistent bottom kernel: arrivals, generation, gave-up flag
   double* xfer = nullptr;             // restriction scratch: z-filtered fine columns
   size_t xfer_n = 0;                  // its capacity in doubles
   double* fpart = nullptr;            // per-CTA partial sums of the fine operator kernel
@@ -172,7 +173,8 @@ struct rso_handle {
     int fine_rows = 4;      // thread rows of a CTA of the packed FP32 fine kernel (2, 4 or 8)
     int fine_zc = 0;        // node planes per z chunk of that kernel (4, 8, 16 or 32; 0: by size)
     int rowsplit[16];       // per level: 0 one thread per node, 1 per (node, row), 2 nine per node, -1 by size
-    int bottom = -2;        // first level of the bottom cluster kernel, -1 none, -2 by size
+    int bottom = -2;        // first level of the bottom kernel, -1 none, -2 by size
+    int bottom_kind = 1;    // bottom kernel: 1 the persistent grid-wide kernel, 0 the 8-CTA cluster kernel
     Tune() { for (int& r : rowsplit) r = -1; }
   } tune;
   // reliable-update PCG (mixed precision): the Krylov recurrence in FP32,
@@ -297,7 +299,10 @@ template <typename T>
 rso_status fine_applyK(rso_handle* h, const T* u, T* f, const T* rp);
 constexpr int kMaxSweeps = 16;
 void smoother_steps(const rso_handle* h, double lam, int m, double* om, double* c1);
-int bottom_level(const rso_handle* h);
+// levels of at most this many nodes are the bottom kernels' (the built-in
+// rule's first level; the largest rso_autotune tries)
+constexpr long long kBottomMaxNodes = 60000;
+int bottom_level(const rso_handle* h, bool fp32 = true);
 template <typename T>
 rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post);
 rso_status fine_applyK_dot(rso_handle* h, const double* u, double* f, const double* rp, double* dot_dev,

@@ -115,8 +115,8 @@ static rso_status level_residual(rso_handle* h, int li) {
 template <typename T>
 rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric, bool u0_zero) {
   const int nl = (int)h->L.size();
-  // levels from lb down run inside one cluster kernel (bottom_vcycle)
-  const int lb = bottom_level(h);
+  // levels from lb down run inside one bottom kernel (bottom_vcycle)
+  const int lb = bottom_level(h, sizeof(T) == 4);
   const int top = lb > 0 ? lb : nl;
   for (int li = 0; li < top; li++) {
     Level& l = h->L[li];

@@ -115,6 +115,8 @@ SIGNATURES = {
     "rso_set_solve_graphs": (_ci, [_vp, _ci]),
     "rso_set_fine_zchunk": (_ci, [_vp, _ci]),
     "rso_fine_zchunk": (_ci, [_vp]),
+    "rso_set_bottom_kernel": (_ci, [_vp, _ci]),
+    "rso_bottom_kernel": (_ci, [_vp]),
     "rso_set_krylov_fp32": (_ci, [_vp, _cd]),
     "rso_set_krylov_fp32_cycles": (_ci, [_vp, _ci]),
     "rso_displacement_project": (_ci, [_vp, _vp]),
@@ -475,7 +477,7 @@ class HierarchyGrid:
         c = np.zeros(2 + self.n_levels(), np.int32)
         self._chk(self.lib.rso_autotune(self.h, _np_ptr(c, _pi)), "rso_autotune")
         self._shapes = {"fine_rows": int(c[0]), "fine_zchunk": self.fine_zchunk(), "bottom_level": int(c[1]),
-                        "row_split": [int(x) for x in c[2:]]}
+                        "bottom_kernel": self.bottom_kernel(), "row_split": [int(x) for x in c[2:]]}
         return dict(self._shapes)
 
     def launch_shapes(self):
@@ -484,7 +486,7 @@ class HierarchyGrid:
         sh = getattr(self, "_shapes", None)
         if sh is None:
             sh = {"fine_rows": 4, "fine_zchunk": self.fine_zchunk(), "bottom_level": -2,
-                  "row_split": [-1] * self.n_levels()}
+                  "bottom_kernel": self.bottom_kernel(), "row_split": [-1] * self.n_levels()}
         return dict(sh)
 
     def set_launch_shapes(self, fine_rows=4, bottom_level=-2, row_split=None):
@@ -494,6 +496,7 @@ class HierarchyGrid:
         self._chk(self.lib.rso_set_launch_shapes(self.h, _np_ptr(c, _pi), len(c)), "rso_set_launch_shapes")
         nl = self.n_levels()
         self._shapes = {"fine_rows": int(fine_rows), "fine_zchunk": self.fine_zchunk(), "bottom_level": int(bottom_level),
+                        "bottom_kernel": self.bottom_kernel(),
                         "row_split": [int(x) for x in rs[:nl]] + [-1] * max(0, nl - len(rs))}
 
     def updateDensities(self, rho, sens, vgoal, step=0.1, damp=0.5, shell=None, variant=0):
@@ -541,6 +544,13 @@ class HierarchyGrid:
 
     def fine_zchunk(self):
         return int(self.lib.rso_fine_zchunk(self.h))
+
+    def set_bottom_kernel(self, kind):
+        """Bottom of the FP32 V-cycle: 1 persistent grid-wide kernel, 0 8-CTA cluster kernel."""
+        self._chk(self.lib.rso_set_bottom_kernel(self.h, int(kind)), "rso_set_bottom_kernel")
+
+    def bottom_kernel(self):
+        return int(self.lib.rso_bottom_kernel(self.h))
 
     def set_solve_graphs(self, on):
         """Run the mixed PCG loop as one device-controlled CUDA graph per solve."""

@@ -1,7 +1,7 @@
 """Launch-shape autotuner (rso_autotune / rso_set_launch_shapes) through the C ABI.
 The alternatives compute the same arithmetic in other launch shapes, so every
-forced combination of fine tile height, coarse kernel variant and bottom-kernel
-level must solve to the same answer: the solves run to relative residual 1e-10
+forced combination of fine tile height, coarse kernel variant, bottom-kernel
+level and bottom-kernel kind must solve to the same answer: the solves run to relative residual 1e-10
 and must agree to 1e-8 relative with iteration counts within one."""
 import numpy as np
 import pytest
@@ -48,14 +48,44 @@ def test_autotune_choices_solve_alike(cuda, gen):
     assert len(ch["row_split"]) == nl and all(r in (-1, 0, 1, 2) for r in ch["row_split"])
     u, it, _, _ = g.solve(f, tol=1e-10, max_iter=300)
     assert abs(it - it_ref) <= 1 and rel(u.cpu().numpy(), u_ref) < 1e-8
+    assert ch["bottom_kernel"] in (0, 1)
     for rows in (2, 4):
         for bottom in [-1] + list(range(1, nl - 1)):
-            for split in (0, 1, 2):
-                g.set_launch_shapes(rows, bottom, [-1] + [split] * (nl - 1))
+            for kind in ((1, 0) if bottom > 0 else (1,)):
+                g.set_bottom_kernel(kind)
+                for split in (0, 1, 2):
+                    g.set_launch_shapes(rows, bottom, [-1] + [split] * (nl - 1))
+                    u, it, rr, _ = g.solve(f, tol=1e-10, max_iter=300)
+                    assert rr < 1e-10
+                    assert abs(it - it_ref) <= 1, (rows, bottom, kind, split)
+                    assert rel(u.cpu().numpy(), u_ref) < 1e-8, (rows, bottom, kind, split)
+    g.close()
+
+
+def test_bottom_kernels_agree(cuda):
+    """The persistent grid-wide bottom kernel and the cluster kernel run the same
+    phases (their sweeps in other launch shapes): V-cycle-preconditioned solves
+    from every first level agree with per-level launches to 1e-8, repeated
+    solves replay captured V-cycles, and an unknown kind is refused."""
+    from robustoptspline3d_b200 import RSOError
+    g = make(P.ellipsoid(48, 32, 32))
+    nl = g.n_levels()
+    f = cuda.tensor(rhs(g, 7), dtype=cuda.float64, device="cuda")
+    g.set_launch_shapes(4, -1)
+    u_ref, it_ref, _, _ = g.solve(f, tol=1e-10, max_iter=300)
+    u_ref = u_ref.cpu().numpy()
+    for kind in (1, 0):
+        g.set_bottom_kernel(kind)
+        assert g.bottom_kernel() == kind
+        for bottom in range(1, nl - 1):
+            g.set_launch_shapes(4, bottom)
+            assert g.launch_shapes()["bottom_kernel"] == kind
+            for _ in range(3):  # captured on the second occurrence, replayed on the third
                 u, it, rr, _ = g.solve(f, tol=1e-10, max_iter=300)
-                assert rr < 1e-10
-                assert abs(it - it_ref) <= 1, (rows, bottom, split)
-                assert rel(u.cpu().numpy(), u_ref) < 1e-8, (rows, bottom, split)
+                assert rr < 1e-10 and abs(it - it_ref) <= 1, (kind, bottom, it, it_ref)
+                assert rel(u.cpu().numpy(), u_ref) < 1e-8, (kind, bottom)
+    with pytest.raises(RSOError):
+        g.set_bottom_kernel(2)
     g.close()
 
 

@@ -1601,8 +1601,12 @@ rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post) {
   A.cnodes = h->c_nodes;
   A.nc = h->nc;
   A.cf = h->L[0].nb > 1 ? h->c_fb : h->c_f;
+  double bnodes = 0;
+  for (int li = lb; li < nl; li++) bnodes += (double)h->L[li].nn * h->L[li].nb;
   if (h->tune.bottom_kind == 0) {
+    if (h->prof_on) prof_begin(h, PC_BOTTOM, bnodes);
     k_bottom<T><<<BOT_CTAS, BOT_THREADS, 0, h->stream>>>(A); rso::note_launch();
+    if (h->prof_on) prof_end(h, PC_BOTTOM);
     return launch_check(h, "bottom_vcycle");
   }
   // the persistent kernel: as many CTAs as the largest level has tiles, at
@@ -1633,8 +1637,10 @@ rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post) {
   at[0].val.cooperative = 1;
   lc.attrs = at;
   lc.numAttrs = 1;
+  if (h->prof_on) prof_begin(h, PC_BOTTOM, bnodes);
   RSO_CHECK_CUDA(h, cudaLaunchKernelEx(&lc, k_bottom_grid<T>, A, h->gbar));
   rso::note_launch();
+  if (h->prof_on) prof_end(h, PC_BOTTOM);
   return launch_check(h, "bottom_vcycle (grid)");
 }
 template rso_status bottom_vcycle<double>(rso_handle*, int, int, int);

@@ -36,6 +36,9 @@ static const ProfClassInfo kInfo[PC_N] = {
     {"coarse_stencil_fp64", 243 * 8 + 24 + 24 + 24 + 1, 486},
     // the same operator, four nodes per thread on 16-byte streams (large FP32 levels)
     {"coarse_stencil_fp32_streamed", 243 * 4 + 12 + 12 + 12 + 1, 486},
+    // the whole bottom of a V-cycle in one launch (its levels' nodes counted
+    // once; no per-node traffic figure)
+    {"vcycle_bottom", 0, 0},
 };
 
 struct Prof {

@@ -206,7 +206,7 @@ namespace rso {
 // launch accounting and profiling (prof.cu)
 enum ProfClass {
   PC_FINE_JAC32, PC_FINE_RES32, PC_FINE_GS32, PC_FINE_APPLYK64, PC_FINE_RES64, PC_FINE_JAC64, PC_FINE_GS64,
-  PC_COARSE32, PC_COARSE64, PC_COARSE32_STREAM, PC_N
+  PC_COARSE32, PC_COARSE64, PC_COARSE32_STREAM, PC_BOTTOM, PC_N
 };
 void note_launch();
 void note_launches(long long n);

@@ -1063,9 +1063,11 @@ __device__ void bot_residual(const Level& L, const T* st, const T* u0v, const T*
   }
 }
 
-template <typename T>
+// FC: the coarsening factor when known at compile time (its loops unrolled,
+// so a thread's loads are all in flight at once), 0 to read it from C
+template <typename T, int FC = 0>
 __device__ void bot_restrict(const Level& Fl, const Level& C, const T* rf0, T* fc0, int g0, int gs) {
-  const int F = C.factor;
+  const int F = FC > 0 ? FC : C.factor;
   for (long long ib = g0; ib < C.nn * C.nb; ib += gs) {
     const long long b = ib / C.nn, i = ib - b * C.nn;
     const T* rf = rf0 + b * 3 * Fl.NP;
@@ -1074,13 +1076,16 @@ __device__ void bot_restrict(const Level& Fl, const Level& C, const T* rf0, T* f
     const long long nC = C.nidx(X, Y, Z);
     T s0 = 0, s1 = 0, s2 = 0;
     if (C.vclass[nC] & NC_ACTIVE) {
+#pragma unroll
       for (int dz = -F + 1; dz < F; dz++) {
         const int z = F * Z + dz;
         if (z < 0 || z >= Fl.nz) continue;
+#pragma unroll
         for (int dy = -F + 1; dy < F; dy++) {
           const int y = F * Y + dy;
           if (y < 0 || y >= Fl.ny) continue;
           const T wyz = (T)(F - abs(dy)) / (T)F * ((T)(F - abs(dz)) / (T)F);
+#pragma unroll
           for (int dx = -F + 1; dx < F; dx++) {
             const int x = F * X + dx;
             if (x < 0 || x >= Fl.nx) continue;
@@ -1092,6 +1097,44 @@ __device__ void bot_restrict(const Level& Fl, const Level& C, const T* rf0, T* f
       }
     }
     fc[nC] = s0; fc[nC + C.NP] = s1; fc[nC + 2 * C.NP] = s2;
+  }
+}
+
+// the restriction with one thread per (coarse node, component) and the
+// factor known at compile time: a thread's (2F - 1)^3 loads are independent
+// and unrolled (the same sums in the same order as bot_restrict)
+template <typename T, int F>
+__device__ void bot_restrict3(const Level& Fl, const Level& C, const T* rf0, T* fc0, int g0, int gs) {
+  for (long long it = g0; it < 3 * C.nn * C.nb; it += gs) {
+    const int c = (int)(it % 3);
+    const long long ib = it / 3;
+    const long long b = ib / C.nn, i = ib - b * C.nn;
+    const T* rf = rf0 + b * 3 * Fl.NP + c * Fl.NP;
+    T* fc = fc0 + b * 3 * C.NP + c * C.NP;
+    const int X = (int)(i % C.nx), Y = (int)((i / C.nx) % C.ny), Z = (int)(i / ((long long)C.nx * C.ny));
+    const long long nC = C.nidx(X, Y, Z);
+    T sum = 0;
+    if (C.vclass[nC] & NC_ACTIVE) {
+#pragma unroll
+      for (int dz = -F + 1; dz < F; dz++) {
+        const int z = F * Z + dz;
+        if (z < 0 || z >= Fl.nz) continue;
+#pragma unroll
+        for (int dy = -F + 1; dy < F; dy++) {
+          const int y = F * Y + dy;
+          if (y < 0 || y >= Fl.ny) continue;
+          const T wyz = (T)(F - abs(dy)) / (T)F * ((T)(F - abs(dz)) / (T)F);
+#pragma unroll
+          for (int dx = -F + 1; dx < F; dx++) {
+            const int x = F * X + dx;
+            if (x < 0 || x >= Fl.nx) continue;
+            const T w = wyz * ((T)(F - abs(dx)) / (T)F);
+            sum += w * rf[Fl.nidx(x, y, z)];
+          }
+        }
+      }
+    }
+    fc[nC] = sum;
   }
 }
 
@@ -1117,6 +1160,35 @@ __device__ void bot_prolong(const Level& Fl, const Level& C, const T* uc0, T* uf
       s0 += w * uc[nC]; s1 += w * uc[nC + C.NP]; s2 += w * uc[nC + 2 * C.NP];
     }
     uf[n] += s0; uf[n + Fl.NP] += s1; uf[n + 2 * Fl.NP] += s2;
+  }
+}
+
+// the prolongation with one thread per (fine node, component): the same
+// sums in the same order as bot_prolong, a third of the loads per thread
+template <typename T>
+__device__ void bot_prolong3(const Level& Fl, const Level& C, const T* uc0, T* uf0, int g0, int gs) {
+  const int F = C.factor;
+  for (long long it = g0; it < 3 * Fl.nn * Fl.nb; it += gs) {
+    const int c = (int)(it % 3);
+    const long long ib = it / 3;
+    const long long b = ib / Fl.nn, i = ib - b * Fl.nn;
+    const T* uc = uc0 + b * 3 * C.NP + c * C.NP;
+    T* uf = uf0 + b * 3 * Fl.NP + c * Fl.NP;
+    const int x = (int)(i % Fl.nx), y = (int)((i / Fl.nx) % Fl.ny), z = (int)(i / ((long long)Fl.nx * Fl.ny));
+    const long long n = Fl.nidx(x, y, z);
+    const uint8_t cls = Fl.vclass[n];
+    if (!(cls & NC_ACTIVE) || (cls & NC_SUPPORT)) continue;
+    const int X0 = x / F, Y0 = y / F, Z0 = z / F;
+    const int ox = x - F * X0, oy = y - F * Y0, oz = z - F * Z0;
+    T sum = 0;
+#pragma unroll
+    for (int A = 0; A < 8; A++) {
+      const int ax = A & 1, ay = (A >> 1) & 1, az = A >> 2;
+      const T w = (ax ? (T)ox : (T)(F - ox)) / (T)F * ((ay ? (T)oy : (T)(F - oy)) / (T)F) *
+                  ((az ? (T)oz : (T)(F - oz)) / (T)F);
+      sum += w * uc[C.nidx(X0 + ax, Y0 + ay, Z0 + az)];
+    }
+    uf[n] += sum;
   }
 }
 
@@ -1225,7 +1297,6 @@ __global__ void __cluster_dims__(BOT_CTAS, 1, 1) __launch_bounds__(BOT_THREADS, 
 // row-split per-level kernel does (tiles of 32 x CTY nodes, three threads per
 // node, the same arithmetic: bit-identical sweeps), the transfers and the
 // coarsest solve as in k_bottom.
-constexpr int GB_THREADS = 32 * CTY * 3;
 // a barrier wait gives up after this many SM clock cycles (about 2 s)
 constexpr long long kGbarCycles = 4000000000LL;
 
@@ -1275,8 +1346,8 @@ __device__ bool gbar_sync(unsigned* bar, unsigned& gen, int tid) {
 
 // one row-split sweep (MODE 2) or residual (MODE 0) of a level, tile by tile
 template <typename T, int MODE, bool ZERO>
-__device__ void gb_sweep(const Level& L, const T* st, const T* u, const T* f, T* out, T omega, const T* uprev, T c1,
-                         T (*sres)[CTY][32]) {
+__device__ void gb_sweep_rows(const Level& L, const T* st, const T* u, const T* f, T* out, T omega, const T* uprev,
+                              T c1, T (*sres)[CTY][32]) {
   const int tx = (L.nx + 31) / 32, ty = (L.ny + CTY - 1) / CTY;
   const long long nt = (long long)tx * ty * L.nz * L.nb;
   for (long long t = blockIdx.x; t < nt; t += gridDim.x) {
@@ -1291,11 +1362,164 @@ __device__ void gb_sweep(const Level& L, const T* st, const T* u, const T* f, T*
   }
 }
 
+// FP32: the sweeps of the persistent kernel on groups of four consecutive
+// padded nodes, nine threads per group, one per neighbour row (plane dz, row
+// dy): a thread loads its row's u (a 16-byte vector and two scalars per
+// component) and the 27 stencil vectors of its three neighbours, 36 loads
+// where a row-split thread makes 162, so a small level's sweep is a few load
+// latencies long.  The nine partial sums meet in shared memory in a fixed
+// order; four of the group's threads then finish one node each as k_coarse4
+// does (residual, or damped block Jacobi / Chebyshev step; halo rows
+// unwritten).
+constexpr int G9 = 32;  // node groups per tile (9 G9 threads)
+template <int MODE, bool ZERO>
+__device__ void gb_sweep4(const Level& L, const float* __restrict__ st, const float* u0v, const float* f0v,
+                          float* out0v, float omega, const float* up0v, float c1, float (*red)[12][G9]) {
+  const int tg = threadIdx.x % G9, q = threadIdx.x / G9;  // q = 3 (dz + 1) + (dy + 1)
+  const int pz = q / 3, py = q - 3 * pz;
+  const long long NP = L.NP, px = L.px, pxy = (long long)L.px * L.py;
+  const long long ng = NP / 4, ngt = ng * L.nb;
+  const long long ntile = (ngt + G9 - 1) / G9;
+  for (long long t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const long long gg = t * G9 + tg;
+    const long long bsys = gg < ngt ? gg / ng : 0, g = gg - bsys * ng;
+    const long long vo = bsys * 3 * NP;
+    const float* u = u0v + vo;
+    const long long p0 = 4 * g;
+    bool work = gg < ngt;
+    int xp = 0;
+    bool act[4] = {false, false, false, false};
+    if (work) {
+      const int zp = (int)(p0 / pxy);
+      const long long rem = p0 - zp * pxy;
+      const int yp = (int)(rem / px);
+      xp = (int)(rem - yp * px);
+      work = !(zp < 1 || zp > L.nz || yp < 1 || yp > L.ny);  // halo row: stays zero
+    }
+    bool any = false;
+    if (work) {
+      const uchar4 cl4 = *reinterpret_cast<const uchar4*>(L.vclass + p0);
+      const uint8_t cls[4] = {cl4.x, cl4.y, cl4.z, cl4.w};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int x = xp + k - 1;
+        act[k] = x >= 0 && x < L.nx && (cls[k] & NC_ACTIVE);
+        any = any || act[k];
+      }
+    }
+    float acc[3][4];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) acc[r][k] = 0.f;
+    if (any && !ZERO) {
+      const long long nb = p0 + (long long)(pz - 1) * pxy + (long long)(py - 1) * px;
+      float w[3][6];  // u at x offsets -1 .. 4 of the group's row in this neighbour row
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const float* uc = u + nb + c * NP;
+        const float4 m = *reinterpret_cast<const float4*>(uc);
+        // at xp = 0 the left neighbour is outside the row (the group's first
+        // node is halo, its result discarded); likewise the right one at the end
+        w[c][0] = xp > 0 ? uc[-1] : 0.f;
+        w[c][1] = m.x; w[c][2] = m.y; w[c][3] = m.z; w[c][4] = m.w;
+        w[c][5] = xp + 4 < px ? uc[4] : 0.f;
+      }
+#pragma unroll
+      for (int dx = 0; dx < 3; dx++) {
+        const int d = q * 3 + dx;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            const float4 sv = *reinterpret_cast<const float4*>(st + st_at<float>(NP, d * 9 + r * 3 + c, p0));
+            acc[r][0] = fmaf(sv.x, w[c][dx + 0], acc[r][0]);
+            acc[r][1] = fmaf(sv.y, w[c][dx + 1], acc[r][1]);
+            acc[r][2] = fmaf(sv.z, w[c][dx + 2], acc[r][2]);
+            acc[r][3] = fmaf(sv.w, w[c][dx + 3], acc[r][3]);
+          }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) red[q][r * 4 + k][tg] = acc[r][k];
+    __syncthreads();
+    if (q < 4 && work) {
+      // thread q finishes node k = q of the group: its rows' nine partial
+      // sums in the order dz, dy = (-1, -1) .. (1, 1)
+      const int k = q;
+      const long long n = p0 + k;
+      float a[3];
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        float sum = red[0][r * 4 + k][tg];
+#pragma unroll
+        for (int sl = 1; sl < 9; sl++) sum += red[sl][r * 4 + k][tg];
+        a[r] = sum;
+      }
+      const float* f = f0v + vo;
+      float* out = out0v + vo;
+      float res[3];
+#pragma unroll
+      for (int r = 0; r < 3; r++) res[r] = f[n + r * NP] - (act[k] ? a[r] : 0.f);
+      if (MODE == 0) {
+#pragma unroll
+        for (int r = 0; r < 3; r++) out[n + r * NP] = res[r];
+      } else if (!act[k]) {
+#pragma unroll
+        for (int r = 0; r < 3; r++) out[n + r * NP] = 0.f;
+      } else {
+        float Sk[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) Sk[i] = st[st_at<float>(NP, 13 * 9 + i, n)];
+        float uo[3], up[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          uo[r] = ZERO ? 0.f : u[n + r * NP];
+          up[r] = up0v ? up0v[vo + n + r * NP] : 0.f;
+        }
+        const float r0 = res[0], r1 = res[1], r2 = res[2];
+        const float A = Sk[4] * Sk[8] - Sk[5] * Sk[7], B = -(Sk[3] * Sk[8] - Sk[5] * Sk[6]),
+                    C = Sk[3] * Sk[7] - Sk[4] * Sk[6];
+        const float det = Sk[0] * A + Sk[1] * B + Sk[2] * C;
+        const float id = omega / det;
+        const float i01 = -(Sk[1] * Sk[8] - Sk[2] * Sk[7]), i02 = Sk[1] * Sk[5] - Sk[2] * Sk[4];
+        const float i11 = Sk[0] * Sk[8] - Sk[2] * Sk[6], i12 = -(Sk[0] * Sk[5] - Sk[2] * Sk[3]);
+        const float i21 = -(Sk[0] * Sk[7] - Sk[1] * Sk[6]), i22 = Sk[0] * Sk[4] - Sk[1] * Sk[3];
+        out[n] = uo[0] + c1 * (uo[0] - up[0]) + id * (A * r0 + i01 * r1 + i02 * r2);
+        out[n + NP] = uo[1] + c1 * (uo[1] - up[1]) + id * (B * r0 + i11 * r1 + i12 * r2);
+        out[n + 2 * NP] = uo[2] + c1 * (uo[2] - up[2]) + id * (C * r0 + i21 * r1 + i22 * r2);
+      }
+    }
+    __syncthreads();  // red is reused by the next tile
+  }
+}
+
+// threads of a CTA of the persistent kernel: nine per group of G9 four-node
+// groups (FP32), 32 x CTY x 3 for the row-split sweeps (FP64)
 template <typename T>
-__global__ void __launch_bounds__(GB_THREADS) k_bottom_grid(const __grid_constant__ BottomArgs<T> A, unsigned* bar) {
-  __shared__ T sres[3][CTY][32];
-  const int tid = threadIdx.x + 32 * (threadIdx.y + CTY * threadIdx.z);
-  const int g0 = blockIdx.x * GB_THREADS + tid, gs = gridDim.x * GB_THREADS;
+constexpr int gb_threads() { return sizeof(T) == 4 ? 9 * G9 : 32 * CTY * 3; }
+// shared exchange of a sweep: [9][12][G9] floats (FP32), [3][CTY][32] T (FP64)
+template <typename T>
+constexpr int gb_smem() { return sizeof(T) == 4 ? 9 * 12 * G9 * 4 : 3 * CTY * 32 * (int)sizeof(T); }
+
+template <typename T, int MODE, bool ZERO>
+__device__ __forceinline__ void gb_sweep(const Level& L, const T* st, const T* u, const T* f, T* out, T omega,
+                                         const T* uprev, T c1, unsigned char* sm) {
+  if constexpr (sizeof(T) == 4)
+    gb_sweep4<MODE, ZERO>(L, st, u, f, out, omega, uprev, c1, reinterpret_cast<float (*)[12][G9]>(sm));
+  else
+    gb_sweep_rows<T, MODE, ZERO>(L, st, u, f, out, omega, uprev, c1, reinterpret_cast<T (*)[CTY][32]>(sm));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(gb_threads<T>(), sizeof(T) == 4 ? 2 : 1) k_bottom_grid(const __grid_constant__ BottomArgs<T> A,
+                                                                 unsigned* bar) {
+  __shared__ __align__(16) unsigned char sres[gb_smem<T>()];
+  constexpr int NT = gb_threads<T>();
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int g0 = blockIdx.x * NT + tid, gs = gridDim.x * NT;
   unsigned gen = 0;
   if (tid == 0) gen = ld_acquire_gpu(bar + 1);
 #define GB_SYNC() \
@@ -1323,34 +1547,34 @@ __global__ void __launch_bounds__(GB_THREADS) k_bottom_grid(const __grid_constan
     ucur[li] = cur;
     gb_sweep<T, 0, false>(L, st, cur, bv_f<T>(L), oth, T(0), (const T*)nullptr, T(0), sres);
     GB_SYNC();
-    bot_restrict<T>(L, A.L[li + 1], oth, bv_f<T>(A.L[li + 1]), g0, gs);
+    if (A.L[li + 1].factor == 2)
+      bot_restrict3<T, 2>(L, A.L[li + 1], oth, bv_f<T>(A.L[li + 1]), g0, gs);
+    else
+      bot_restrict<T>(L, A.L[li + 1], oth, bv_f<T>(A.L[li + 1]), g0, gs);
+    if (li + 1 == A.nl - 1) {  // the coarsest iterate is zero outside the listed nodes
+      const Level& C = A.L[li + 1];
+      T* uc = bv_u<T>(C);
+      for (long long i = g0; i < 3 * C.NP * C.nb; i += gs) uc[i] = T(0);
+    }
     GB_SYNC();
   }
-  // coarsest: u = Kinv f at the listed nodes, zero elsewhere; one warp per row
+  // coarsest: u = Kinv f at the listed nodes (zeroed elsewhere above); one
+  // warp per row, f read through the node list
   {
     const Level& C = A.L[A.nl - 1];
     T* u = bv_u<T>(C);
     const T* f = bv_f<T>(C);
     const long long VS = 3 * C.NP;
     const int N = 3 * A.nc;
-    for (long long i = g0; i < VS * C.nb; i += gs) u[i] = T(0);
-    for (long long ib = g0; ib < (long long)A.nc * C.nb; ib += gs) {
-      const long long b = ib / A.nc, i = ib - b * A.nc;
-      const long long n = A.cnodes[i] + b * VS;
-      double* cf = A.cf + b * N;
-      cf[3 * i + 0] = (double)f[n];
-      cf[3 * i + 1] = (double)f[n + C.NP];
-      cf[3 * i + 2] = (double)f[n + 2 * C.NP];
-    }
-    GB_SYNC();
     const int lane = tid & 31, warp = g0 >> 5, nwarps = gs >> 5;
     for (long long rb = warp; rb < (long long)N * C.nb; rb += nwarps) {
       const long long b = rb / N;
       const int row = (int)(rb - b * N);
-      const double* cf = A.cf + b * N;
+      const T* fb = f + b * VS;
       const double* k = A.kinv + (long long)row * N;
       double sum = 0;
-      for (int j = lane; j < N; j += 32) sum += k[j] * cf[j];
+#pragma unroll 4
+      for (int j = lane; j < N; j += 32) sum += k[j] * (double)fb[A.cnodes[j / 3] + (j % 3) * C.NP];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
       if (lane == 0) u[b * VS + A.cnodes[row / 3] + (row % 3) * C.NP] = (T)sum;
@@ -1373,7 +1597,7 @@ __global__ void __launch_bounds__(GB_THREADS) k_bottom_grid(const __grid_constan
       oth = rest[0];
       prv = rest[1];
     }
-    bot_prolong<T>(L, A.L[li + 1], ucur[li + 1], cur, g0, gs);
+    bot_prolong3<T>(L, A.L[li + 1], ucur[li + 1], cur, g0, gs);
     GB_SYNC();
     for (int s = 0; s < A.post; s++) {
       gb_sweep<T, 2, false>(L, st, cur, bv_f<T>(L), oth, A.om[li][s], s == 0 ? (const T*)nullptr : prv,
@@ -1616,7 +1840,7 @@ rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post) {
   const int dev = h->device >= 0 && h->device < 64 ? h->device : 0;
   int occ = occ_cache[ti][dev].load(std::memory_order_relaxed);
   if (occ <= 0) {
-    RSO_CHECK_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bottom_grid<T>, GB_THREADS, 0));
+    RSO_CHECK_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_bottom_grid<T>, gb_threads<T>(), 0));
     occ_cache[ti][dev].store(occ, std::memory_order_relaxed);
   }
   int sms = 0;
@@ -1624,12 +1848,13 @@ rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post) {
   long long need = 1;
   for (int li = lb; li < nl; li++) {
     const Level& l = h->L[li];
-    need = std::max(need, (long long)cdiv(l.nx, 32) * cdiv(l.ny, CTY) * l.nz * l.nb);
+    need = std::max(need, sizeof(T) == 4 ? (long long)cdiv(l.NP / 4 * l.nb, G9)
+                                         : (long long)cdiv(l.nx, 32) * cdiv(l.ny, CTY) * l.nz * l.nb);
   }
   const int grid = (int)std::max<long long>(1, std::min<long long>(need, (long long)occ * sms));
   cudaLaunchConfig_t lc = {};
   lc.gridDim = dim3(grid);
-  lc.blockDim = dim3(32, CTY, 3);
+  lc.blockDim = sizeof(T) == 4 ? dim3(gb_threads<T>()) : dim3(32, CTY, 3);
   lc.dynamicSmemBytes = 0;
   lc.stream = h->stream;
   cudaLaunchAttribute at[1];

@@ -350,6 +350,14 @@ int rso_fine_zchunk(const rso_handle* h);
  * rso_bottom_kernel returns the kind in use. */
 rso_status rso_set_bottom_kernel(rso_handle* h, int kind);
 int rso_bottom_kernel(const rso_handle* h);
+/* Self-test of the persistent kernel's bounded barrier wait (no counterpart in
+ * the reference): a cooperative launch of 4 CTAs passes 8 grid barriers whose
+ * arrival target is the grid plus short_by (0 or 1); with short_by = 1 no
+ * barrier completes, every wait gives up after limit_ms (0 < limit_ms <= 1000)
+ * and the kernel returns.  *gave_up receives whether a wait gave up; the
+ * barrier state is reset afterwards, so the handle stays usable.  No fault and
+ * no hang either way. */
+rso_status rso_grid_barrier_selftest(rso_handle* h, int short_by, double limit_ms, int* gave_up);
 /* Replay of the FP32 V-cycle (the mixed-precision preconditioner) from CUDA
  * graphs (no counterpart in the reference, which launches every kernel):
  * on by default.  The V-cycle is captured the second time its launch

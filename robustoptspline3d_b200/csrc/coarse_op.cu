@@ -1311,15 +1311,19 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
 // 0's copy of the generation) moves on with it.  Returns false on every
 // thread of every CTA once some wait has given up (bar[2] set): the kernel
 // then returns, and the host reports it after the solve.
-__device__ bool gbar_sync(unsigned* bar, unsigned& gen, int tid) {
+// (target, limit: the arrivals that complete the barrier and the wait's bound
+// in clock cycles; the self-test sets them, the bottom kernel keeps the grid
+// size and kGbarCycles)
+__device__ bool gbar_sync(unsigned* bar, unsigned& gen, int tid, unsigned target = 0, long long limit = kGbarCycles) {
   __shared__ int s_ok;
+  if (target == 0) target = gridDim.x;
   __syncthreads();
   if (tid == 0) {
     int ok = *reinterpret_cast<volatile unsigned*>(bar + 2) == 0u;
     if (ok) {
       const unsigned g = gen;
       __threadfence();
-      if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      if (atomicAdd(bar, 1u) == target - 1) {
         atomicExch(bar, 0u);
         __threadfence();
         atomicExch(bar + 1, g + 1);
@@ -1327,7 +1331,7 @@ __device__ bool gbar_sync(unsigned* bar, unsigned& gen, int tid) {
         const long long t0 = clock64();
         while (ld_acquire_gpu(bar + 1) == g) {
           if (*reinterpret_cast<volatile unsigned*>(bar + 2) != 0u) { ok = 0; break; }
-          if (clock64() - t0 > kGbarCycles) {
+          if (clock64() - t0 > limit) {
             atomicExch(bar + 2, 1u);
             ok = 0;
             break;
@@ -1390,10 +1394,12 @@ __device__ void gb_sweep4(const Level& L, const float* __restrict__ st, const fl
     int xp = 0;
     bool act[4] = {false, false, false, false};
     if (work) {
-      const int zp = (int)(p0 / pxy);
-      const long long rem = p0 - zp * pxy;
-      const int yp = (int)(rem / px);
-      xp = (int)(rem - yp * px);
+      // the levels of this kernel are small (NP < 2^31): 32-bit divisions
+      const unsigned p0u = (unsigned)p0, pxyu = (unsigned)pxy, pxu = (unsigned)px;
+      const int zp = (int)(p0u / pxyu);
+      const unsigned rem = p0u - (unsigned)zp * pxyu;
+      const int yp = (int)(rem / pxu);
+      xp = (int)(rem - (unsigned)yp * pxu);
       work = !(zp < 1 || zp > L.nz || yp < 1 || yp > L.ny);  // halo row: stays zero
     }
     bool any = false;
@@ -1833,6 +1839,11 @@ rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post) {
     if (h->prof_on) prof_end(h, PC_BOTTOM);
     return launch_check(h, "bottom_vcycle");
   }
+  for (int li = lb; li < nl; li++)
+    if (h->L[li].NP * h->L[li].nb >= (1LL << 31)) {
+      h->err = "the persistent bottom kernel takes levels below 2^31 padded nodes";
+      return RSO_ERR_UNSUPPORTED;
+    }
   // the persistent kernel: as many CTAs as the largest level has tiles, at
   // most as many as are resident at once (a cooperative launch refuses more)
   static std::atomic<int> occ_cache[2][64];
@@ -1868,6 +1879,17 @@ rso_status bottom_vcycle(rso_handle* h, int lb, int pre, int post) {
   if (h->prof_on) prof_end(h, PC_BOTTOM);
   return launch_check(h, "bottom_vcycle (grid)");
 }
+// Self-test of the bounded barrier wait: a cooperative launch of a few CTAs
+// passes `rounds` barriers whose arrival target is the grid size plus
+// short_by; with short_by > 0 no barrier completes, so every CTA's wait gives
+// up after limit cycles, sets the flag and returns (no fault, no hang).
+__global__ void k_gbar_selftest(unsigned* bar, int rounds, unsigned short_by, long long limit) {
+  unsigned gen = 0;
+  if (threadIdx.x == 0) gen = ld_acquire_gpu(bar + 1);
+  for (int r = 0; r < rounds; r++)
+    if (!gbar_sync(bar, gen, threadIdx.x, gridDim.x + short_by, limit)) return;
+}
+
 template rso_status bottom_vcycle<double>(rso_handle*, int, int, int);
 template rso_status bottom_vcycle<float>(rso_handle*, int, int, int);
 
@@ -2016,3 +2038,36 @@ template rso_status coarsest_solve<double>(rso_handle*, const double*, double*);
 template rso_status coarsest_solve<float>(rso_handle*, const float*, float*);
 
 }  // namespace rso
+
+using namespace rso;
+
+extern "C" rso_status rso_grid_barrier_selftest(rso_handle* h, int short_by, double limit_ms, int* gave_up) {
+  if (!h || !gave_up || short_by < 0 || short_by > 1 || !(limit_ms > 0) || limit_ms > 1000) return RSO_ERR_INVALID_ARG;
+  if (!h->gbar) {
+    h->err = "grid barrier state not allocated";
+    return RSO_ERR_STATE;
+  }
+  const int dev = h->device >= 0 ? h->device : 0;
+  int khz = 0;
+  RSO_CHECK_CUDA(h, cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev));
+  const long long limit = (long long)(limit_ms * (khz > 0 ? khz : 2000000));
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(h->gbar, 0, sizeof(unsigned) * 4, h->stream));
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(4);
+  lc.blockDim = dim3(128);
+  lc.stream = h->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  RSO_CHECK_CUDA(h, cudaLaunchKernelEx(&lc, k_gbar_selftest, h->gbar, 8, (unsigned)short_by, limit));
+  note_launch();
+  unsigned flag = 0;
+  RSO_CHECK_CUDA(h, cudaMemcpyAsync(&flag, h->gbar + 2, sizeof(flag), cudaMemcpyDeviceToHost, h->stream));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  RSO_CHECK_CUDA(h, cudaMemsetAsync(h->gbar, 0, sizeof(unsigned) * 4, h->stream));
+  RSO_CHECK_CUDA(h, cudaStreamSynchronize(h->stream));
+  *gave_up = flag != 0;
+  return RSO_OK;
+}

@@ -1026,9 +1026,11 @@ __global__ void __launch_bounds__(256) k_fine_jacobi0_v4(const Level L, const fl
   const long long NP = L.NP, px = L.px, pxy = (long long)L.px * L.py;
   const long long p0 = 4 * g;
   if (p0 >= NP) return;
-  const int zp = (int)(p0 / pxy);
-  const long long rem = p0 - zp * pxy;
-  const int yp = (int)(rem / px), xp = (int)(rem - yp * px);
+  // NP < 2^31 (checked by the launcher): 32-bit divisions
+  const unsigned p0u = (unsigned)p0, pxyu = (unsigned)pxy, pxu = (unsigned)px;
+  const int zp = (int)(p0u / pxyu);
+  const unsigned rem = p0u - (unsigned)zp * pxyu;
+  const int yp = (int)(rem / pxu), xp = (int)(rem - (unsigned)yp * pxu);
   if (zp < 1 || zp > L.nz || yp < 1 || yp > L.ny) return;
   const uchar4 cl4 = *reinterpret_cast<const uchar4*>(L.vclass + p0);
   const uint8_t cls[4] = {cl4.x, cl4.y, cl4.z, cl4.w};
@@ -1440,7 +1442,7 @@ rso_status fine_jacobi_dot32(rso_handle* h, const float* u_in, const float* f, f
 template <typename T>
 rso_status fine_jacobi0(rso_handle* h, const T* f, T* u_out, const T* rp, double omega) {
   const Level& l = h->L[0];
-  if (sizeof(T) == 4 && l.nb == 1) {
+  if (sizeof(T) == 4 && l.nb == 1 && l.NP < (1LL << 31)) {
     k_fine_jacobi0_v4<<<cdiv(l.NP / 4, 256), 256, 0, h->stream>>>(l, (const float*)f, (float*)u_out,
                                                                  (const float*)rp, (float)omega);
     rso::note_launch();

@@ -117,6 +117,7 @@ SIGNATURES = {
     "rso_fine_zchunk": (_ci, [_vp]),
     "rso_set_bottom_kernel": (_ci, [_vp, _ci]),
     "rso_bottom_kernel": (_ci, [_vp]),
+    "rso_grid_barrier_selftest": (_ci, [_vp, _ci, _cd, _pi]),
     "rso_set_krylov_fp32": (_ci, [_vp, _cd]),
     "rso_set_krylov_fp32_cycles": (_ci, [_vp, _ci]),
     "rso_displacement_project": (_ci, [_vp, _vp]),
@@ -551,6 +552,13 @@ class HierarchyGrid:
 
     def bottom_kernel(self):
         return int(self.lib.rso_bottom_kernel(self.h))
+
+    def grid_barrier_selftest(self, short_by=0, limit_ms=10.0):
+        """Bounded-wait self-test of the persistent kernel's grid barrier: 1 if a wait gave up."""
+        out = ctypes.c_int(0)
+        self._chk(self.lib.rso_grid_barrier_selftest(self.h, int(short_by), float(limit_ms), ctypes.byref(out)),
+                  "rso_grid_barrier_selftest")
+        return int(out.value)
 
     def set_solve_graphs(self, on):
         """Run the mixed PCG loop as one device-controlled CUDA graph per solve."""

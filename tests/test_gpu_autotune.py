@@ -148,3 +148,26 @@ def test_coarse_variants_sweep_alike(cuda):
         for a, b in outs[1:]:
             assert rel(a, outs[0][0]) < 1e-5 and rel(b, outs[0][1]) < 1e-5, li
     g.close()
+
+
+def test_grid_barrier_wait_gives_up(cuda):
+    """The persistent bottom kernel's barrier waits are bounded: with an
+    arrival target one above the grid no barrier completes, every wait gives up
+    after the limit and the launch returns (no fault, no hang); barriers that
+    complete report nothing; the handle then solves with the persistent kernel
+    as before."""
+    import time
+    g = make(P.cantilever(48, 24, 24))
+    f = cuda.tensor(rhs(g), dtype=cuda.float64, device="cuda")
+    g.set_bottom_kernel(1)
+    g.set_launch_shapes(4, 1)
+    u_ref, it_ref, _, _ = g.solve(f, tol=1e-10, max_iter=300)
+    assert g.grid_barrier_selftest(short_by=0, limit_ms=50.0) == 0
+    t0 = time.perf_counter()
+    assert g.grid_barrier_selftest(short_by=1, limit_ms=5.0) == 1
+    assert time.perf_counter() - t0 < 5.0
+    assert g.grid_barrier_selftest(short_by=0, limit_ms=50.0) == 0
+    u, it, rr, _ = g.solve(f, tol=1e-10, max_iter=300)
+    assert rr < 1e-10 and it == it_ref
+    assert np.array_equal(u.cpu().numpy(), u_ref.cpu().numpy())
+    g.close()

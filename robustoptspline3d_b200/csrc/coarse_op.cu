@@ -141,10 +141,12 @@ __global__ void __launch_bounds__(C4G * 3, 3) k_coarse4(const Level L, const flo
   int xp = 0;
   bool act[4] = {false, false, false, false};
   if (work) {
-    const int zp = (int)(p0 / pxy);
-    const long long rem = p0 - zp * pxy;
-    const int yp = (int)(rem / px);
-    xp = (int)(rem - yp * px);
+    // NP < 2^31 (checked by the launchers): 32-bit divisions
+    const unsigned p0u = (unsigned)p0, pxyu = (unsigned)pxy, pxu = (unsigned)px;
+    const int zp = (int)(p0u / pxyu);
+    const unsigned rem = p0u - (unsigned)zp * pxyu;
+    const int yp = (int)(rem / pxu);
+    xp = (int)(rem - (unsigned)yp * pxu);
     work = !(zp < 1 || zp > L.nz || yp < 1 || yp > L.ny);  // halo row: stays zero
   }
   bool any = false;
@@ -1105,13 +1107,16 @@ __device__ void bot_restrict(const Level& Fl, const Level& C, const T* rf0, T* f
 // and unrolled (the same sums in the same order as bot_restrict)
 template <typename T, int F>
 __device__ void bot_restrict3(const Level& Fl, const Level& C, const T* rf0, T* fc0, int g0, int gs) {
-  for (long long it = g0; it < 3 * C.nn * C.nb; it += gs) {
-    const int c = (int)(it % 3);
-    const long long ib = it / 3;
-    const long long b = ib / C.nn, i = ib - b * C.nn;
-    const T* rf = rf0 + b * 3 * Fl.NP + c * Fl.NP;
-    T* fc = fc0 + b * 3 * C.NP + c * C.NP;
-    const int X = (int)(i % C.nx), Y = (int)((i / C.nx) % C.ny), Z = (int)(i / ((long long)C.nx * C.ny));
+  // the levels of the persistent kernel are below 2^31 nodes (checked by its
+  // launcher): 32-bit index arithmetic
+  const unsigned nn = (unsigned)C.nn, nx = (unsigned)C.nx, ny = (unsigned)C.ny;
+  for (unsigned it = g0; it < 3u * nn * (unsigned)C.nb; it += gs) {
+    const unsigned ib = it / 3u, c = it - 3u * ib;
+    const unsigned b = ib / nn, i = ib - b * nn;
+    const T* rf = rf0 + (long long)b * 3 * Fl.NP + c * Fl.NP;
+    T* fc = fc0 + (long long)b * 3 * C.NP + c * C.NP;
+    const unsigned iy = i / nx, Z = iy / ny;
+    const int X = (int)(i - iy * nx), Y = (int)(iy - Z * ny);
     const long long nC = C.nidx(X, Y, Z);
     T sum = 0;
     if (C.vclass[nC] & NC_ACTIVE) {
@@ -1168,13 +1173,15 @@ __device__ void bot_prolong(const Level& Fl, const Level& C, const T* uc0, T* uf
 template <typename T>
 __device__ void bot_prolong3(const Level& Fl, const Level& C, const T* uc0, T* uf0, int g0, int gs) {
   const int F = C.factor;
-  for (long long it = g0; it < 3 * Fl.nn * Fl.nb; it += gs) {
-    const int c = (int)(it % 3);
-    const long long ib = it / 3;
-    const long long b = ib / Fl.nn, i = ib - b * Fl.nn;
-    const T* uc = uc0 + b * 3 * C.NP + c * C.NP;
-    T* uf = uf0 + b * 3 * Fl.NP + c * Fl.NP;
-    const int x = (int)(i % Fl.nx), y = (int)((i / Fl.nx) % Fl.ny), z = (int)(i / ((long long)Fl.nx * Fl.ny));
+  // 32-bit index arithmetic, as in bot_restrict3
+  const unsigned nn = (unsigned)Fl.nn, nx = (unsigned)Fl.nx, ny = (unsigned)Fl.ny;
+  for (unsigned it = g0; it < 3u * nn * (unsigned)Fl.nb; it += gs) {
+    const unsigned ib = it / 3u, c = it - 3u * ib;
+    const unsigned b = ib / nn, i = ib - b * nn;
+    const T* uc = uc0 + (long long)b * 3 * C.NP + c * C.NP;
+    T* uf = uf0 + (long long)b * 3 * Fl.NP + c * Fl.NP;
+    const unsigned iy = i / nx, zz = iy / ny;
+    const int x = (int)(i - iy * nx), y = (int)(iy - zz * ny), z = (int)zz;
     const long long n = Fl.nidx(x, y, z);
     const uint8_t cls = Fl.vclass[n];
     if (!(cls & NC_ACTIVE) || (cls & NC_SUPPORT)) continue;
@@ -1386,7 +1393,7 @@ __device__ void gb_sweep4(const Level& L, const float* __restrict__ st, const fl
   const long long ntile = (ngt + G9 - 1) / G9;
   for (long long t = blockIdx.x; t < ntile; t += gridDim.x) {
     const long long gg = t * G9 + tg;
-    const long long bsys = gg < ngt ? gg / ng : 0, g = gg - bsys * ng;
+    const long long bsys = gg < ngt ? (long long)((unsigned)gg / (unsigned)ng) : 0, g = gg - bsys * ng;
     const long long vo = bsys * 3 * NP;
     const float* u = u0v + vo;
     const long long p0 = 4 * g;
@@ -1658,7 +1665,7 @@ rso_status coarse_residual(rso_handle* h, int level, const T* u, const T* f, T* 
   const int cls = coarse_class(h, level, sizeof(T));
   if (h->prof_on) prof_begin(h, cls, (double)l.nn);
   if (node_per_thread(h, level)) {
-    if (l.nb == 1 && sizeof(T) == 4) {
+    if (l.nb == 1 && sizeof(T) == 4 && l.NP < (1LL << 31)) {
       k_coarse4<0><<<cdiv(l.NP / 4, C4G), dim3(C4G, 3), 0, h->stream>>>(l, (const float*)stencil_of<T>(l), (const float*)u,
                                                                (const float*)f, (float*)r, 0.f, nullptr, 0.f);
     } else if (l.nb == 1) {
@@ -1682,7 +1689,7 @@ rso_status coarse_jacobi(rso_handle* h, int level, const T* u_in, const T* f, T*
   const int cls = coarse_class(h, level, sizeof(T));
   if (h->prof_on) prof_begin(h, cls, (double)l.nn);
   if (node_per_thread(h, level)) {
-    if (l.nb == 1 && sizeof(T) == 4) {
+    if (l.nb == 1 && sizeof(T) == 4 && l.NP < (1LL << 31)) {
       k_coarse4<2><<<cdiv(l.NP / 4, C4G), dim3(C4G, 3), 0, h->stream>>>(l, (const float*)stencil_of<T>(l), (const float*)u_in,
                                                                (const float*)f, (float*)u_out, (float)omega,
                                                                (const float*)u_prev, (float)c1);

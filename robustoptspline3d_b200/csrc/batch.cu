@@ -113,7 +113,7 @@ __global__ void k_bf2d(long long total, const float* __restrict__ a, double* __r
 
 // FP32 Krylov recurrence of the batch (reliable-update PCG, as solve_pcg_k32):
 // r -= alpha_b q in FP32 with per-system sums of r.r, per-system a.b of FP32
-// vectors, x (FP64) += alpha_b p (FP32) and p = z + beta_b p
+// vectors; the steps x (FP64) += alpha_b p (FP32) and p = z + beta_b p below
 __global__ void __launch_bounds__(BR_THREADS) k_bresid32(long long n, const double* __restrict__ s,
                                                          const float* __restrict__ q, float* __restrict__ r,
                                                          double* __restrict__ part) {
@@ -137,22 +137,46 @@ __global__ void __launch_bounds__(BR_THREADS) k_bdot32(long long n, const float*
   acc = b_block_sum(acc);
   if (threadIdx.x == 0) part[blockIdx.y * BR_BLOCKS + blockIdx.x] = acc;
 }
-template <bool DIR_ONLY>
-__global__ void k_bstep_dir32(long long n, long long total, const double* __restrict__ s, const float* __restrict__ z,
-                              float* __restrict__ p, double* __restrict__ x) {
+// Deferred steps of the batch (as in solve_pcg_k32): each new direction goes
+// to the next slot of a ring of three FP32 slabs (the two halves of p's
+// memory and the half of q's the FP32 q leaves free), each system's step
+// size beside it, and x takes the waiting steps in their order at a
+// replacement or when the ring is full: the FP64 operations of the
+// per-iteration step in the same order, so x is bit-identical.
+constexpr int kBRing = 3;
+struct BRing {
+  const float* p[kBRing];
+};
+__global__ void k_balpha_keep(int k, double* s, const int* __restrict__ done, double* __restrict__ keep) {
+  const int b = threadIdx.x;
+  if (b >= k) return;
+  const double pq = s[b * KS + 1];
+  const double a = (done[b] || pq == 0.0) ? 0.0 : s[b * KS + 0] / pq;
+  s[b * KS + 2] = a;
+  keep[b] = a;
+}
+__global__ void k_bflush(long long n, long long total, int k, const double* __restrict__ alpha, const BRing R, int cnt,
+                         double* __restrict__ x) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= total) return;
   const long long b = i / n;
-  const float pi = p[i];
-  if (!DIR_ONLY) x[i] += s[b * KS + 2] * pi;
-  p[i] = z[i] + (float)s[b * KS + 4] * pi;
+  double xi = x[i];
+#pragma unroll
+  for (int j = 0; j < kBRing; j++) {
+    if (j >= cnt) break;
+    xi += alpha[j * k + b] * R.p[j][i];
+  }
+  x[i] = xi;
 }
-__global__ void k_bstep32(long long n, long long total, const double* __restrict__ s, const float* __restrict__ p,
-                          double* __restrict__ x) {
+// p_out = z + beta_b p_in (p_out may be p_in)
+__global__ void k_bdir32(long long n, long long total, const double* __restrict__ s, const float* __restrict__ z,
+                         const float* p_in, float* p_out) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= total) return;
-  x[i] += s[(i / n) * KS + 2] * p[i];
+  const long long b = i / n;
+  p_out[i] = z[i] + (float)s[b * KS + 4] * p_in[i];
 }
+
 // r32 = r for the systems whose bit is set in mask (k <= 64)
 __global__ void k_bd2f_sel(long long n, long long total, const double* __restrict__ r, float* __restrict__ r32,
                            unsigned long long mask) {
@@ -169,7 +193,7 @@ static void batch_free(rso_handle* h) {
     for (double* p : *v) cudaFree(p);
   B.u32.clear(); B.f32.clear(); B.r32.clear(); B.t32.clear();
   B.u64.clear(); B.f64.clear(); B.r64.clear(); B.t64.clear();
-  for (double* p : {B.x, B.r, B.p, B.q, B.z, B.cf, B.red, B.fpart, B.xfer, B.scal}) cudaFree(p);
+  for (double* p : {B.x, B.r, B.p, B.q, B.z, B.cf, B.red, B.fpart, B.xfer, B.scal, B.ralpha}) cudaFree(p);
   if (B.h_scal) cudaFreeHost(B.h_scal);
   cudaFree(B.done);
   B = rso_handle::Batch();  // c_fb aliases B.cf, freed above
@@ -217,6 +241,7 @@ static rso_status batch_alloc(rso_handle* h, int k) {
   BALLOC(B.fpart, sizeof(double) * h->fpart_n * k);
   BALLOC(B.xfer, sizeof(double) * h->xfer_n * k);
   BALLOC(B.scal, sizeof(double) * KS * k);
+  BALLOC(B.ralpha, sizeof(double) * kBRing * k);
   BALLOC(B.done, sizeof(int) * k);
 #undef BALLOC
   if (cudaMallocHost((void**)&B.h_scal, sizeof(double) * KS * k) != cudaSuccess) {
@@ -340,14 +365,42 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
       // the operator writes interior nodes only: q's padding must be zero
       RSO_CHECK_CUDA(h, cudaMemsetAsync(q32, 0, sizeof(float) * tot, h->stream));
       k_bd2f<<<cdiv(tot, 256), 256, 0, h->stream>>>(tot, B.r, r32); rso::note_launch();
+      // r . z of every system from the V-cycle's last fine step (a post-smoothing
+      // Jacobi or Chebyshev step), as in single solves
+      const bool fuse = h->cfg.post >= 1;
+      struct ZdotReset {
+        rso_handle* h;
+        ~ZdotReset() {
+          h->vc_zdot = nullptr;
+          h->vc_zdot_stride = 1;
+        }
+      } zreset{h};
+      h->vc_zdot = fuse ? s + 0 : nullptr;
+      h->vc_zdot_stride = KS;
       RSO_TRY(vcycle_mixed(h));
       RSO_CHECK_CUDA(h, cudaMemcpyAsync(p32, l0.u32, sizeof(float) * tot, cudaMemcpyDeviceToDevice, h->stream));
-      k_bdot32<<<rg, BR_THREADS, 0, h->stream>>>(n3, r32, l0.u32, B.red); rso::note_launch();
-      k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 0); rso::note_launch();
+      if (!fuse) {
+        k_bdot32<<<rg, BR_THREADS, 0, h->stream>>>(n3, r32, l0.u32, B.red); rso::note_launch();
+        k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 0); rso::note_launch();
+      }
+      h->vc_zdot = fuse ? s + 3 : nullptr;
+      // the deferred steps' ring (see k_bflush)
+      float* ring[kBRing] = {p32, p32 + tot, q32 + tot};
+      int pend = 0;     // steps waiting: directions ring[0 .. pend), step sizes B.ralpha[0 .. pend)
+      float* pc = p32;  // the current direction, ring[pend] until its step sizes are known
+      auto flush = [&]() -> rso_status {
+        if (pend == 0) return RSO_OK;
+        BRing R;
+        for (int j = 0; j < kBRing; j++) R.p[j] = ring[j < pend ? j : 0];
+        k_bflush<<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, k, B.ralpha, R, pend, B.x); rso::note_launch();
+        pend = 0;
+        return launch_check(h, "batched pcg32 deferred steps");
+      };
       int iter = 0;
       while (true) {
-        RSO_TRY(fine_applyK_dot32(h, p32, q32, s + 1, KS));
-        k_balpha<<<1, 64, 0, h->stream>>>(k, s, B.done); rso::note_launch();
+        RSO_TRY(fine_applyK_dot32(h, pc, q32, s + 1, KS));
+        k_balpha_keep<<<1, 64, 0, h->stream>>>(k, s, B.done, B.ralpha + (long long)pend * k); rso::note_launch();
+        pend++;
         k_bresid32<<<rg, BR_THREADS, 0, h->stream>>>(n3, s, q32, r32, B.red); rso::note_launch();
         k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 5); rso::note_launch();
         RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.h_scal, s, sizeof(double) * KS * k, cudaMemcpyDeviceToHost, h->stream));
@@ -375,7 +428,7 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
           // direction update below then leaves x alone); the true FP64
           // residuals replace the recursive ones of the asking systems only,
           // so each system follows the sequence of its own single solve
-          k_bstep32<<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, s, p32, B.x); rso::note_launch();
+          RSO_TRY(flush());
           RSO_TRY(fine_residual<double>(h, B.x, fpad, B.r, h->rp64));
           k_bdot<double><<<rg, BR_THREADS, 0, h->stream>>>(n3, B.r, B.r, B.red); rso::note_launch();
           k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 5); rso::note_launch();
@@ -409,14 +462,15 @@ rso_status solve_pcg_batch(rso_handle* h, int k, const double* F, double* U, dou
           RSO_CHECK_CUDA(h, cudaMemcpyAsync(B.done, done.data(), sizeof(int) * k, cudaMemcpyHostToDevice, h->stream));
         }
         RSO_TRY(vcycle_mixed(h));
-        k_bdot32<<<rg, BR_THREADS, 0, h->stream>>>(n3, r32, l0.u32, B.red); rso::note_launch();
-        k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 3); rso::note_launch();
+        if (!fuse) {
+          k_bdot32<<<rg, BR_THREADS, 0, h->stream>>>(n3, r32, l0.u32, B.red); rso::note_launch();
+          k_bsum<<<k, BR_THREADS, 0, h->stream>>>(B.red, s, 3); rso::note_launch();
+        }
         k_bbeta<<<1, 64, 0, h->stream>>>(k, s, B.done); rso::note_launch();
-        if (replace)
-          k_bstep_dir32<true><<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, s, l0.u32, p32, B.x);
-        else
-          k_bstep_dir32<false><<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, s, l0.u32, p32, B.x);
-        rso::note_launch();
+        if (pend == kBRing) RSO_TRY(flush());
+        float* pn = ring[pend];  // pc itself right after a flush of one step
+        k_bdir32<<<cdiv(tot, 256), 256, 0, h->stream>>>(n3, tot, s, l0.u32, pc, pn); rso::note_launch();
+        pc = pn;
         RSO_TRY(launch_check(h, "batched pcg32"));
       }
     }

@@ -1424,20 +1424,22 @@ rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const
   return launch_fine<T, 2>(h, u_in, f, u_out, rp, omega, pcls<T>(PC_FINE_JAC32, PC_FINE_JAC64), "fine_jacobi", nullptr,
                            u_prev, c1);
 }
-// the FP32 step with dot_dev = f . u_out in the same pass (single system)
+// the FP32 step with dot_dev = f . u_out in the same pass; with several
+// systems, system b's sum goes to dot_dev[b * stride]
 rso_status fine_jacobi_dot32(rso_handle* h, const float* u_in, const float* f, float* u_out, double omega,
-                             const float* u_prev, double c1, double* dot_dev) {
+                             const float* u_prev, double c1, double* dot_dev, int stride) {
   const Level& l0 = h->L[0];
   const dim3 g = pair_grid(l0, fine_pty(h), fine_zc(h));
-  const long long nb = (long long)g.x * g.y * g.z;
-  if (l0.nb != 1 || nb > h->fpart_n) {
+  const long long nb = (long long)g.x * g.y * g.z;  // all systems
+  if (nb > h->fpart_n) {
     h->err = "fine partial-sum buffer smaller than the grid";
     return RSO_ERR_STATE;
   }
   const rso_status st = launch_fine<float, 2>(h, u_in, f, u_out, h->rp32, omega, PC_FINE_JAC32, "fine_jacobi_dot32",
                                               h->fpart, u_prev, c1);
   if (st != RSO_OK) return st;
-  return reduce_partials(h, h->fpart, (int)nb, dot_dev);
+  if (l0.nb == 1) return reduce_partials(h, h->fpart, (int)nb, dot_dev);
+  return reduce_partials_batch(h, h->fpart, (int)(nb / l0.nb), l0.nb, dot_dev, stride);
 }
 template <typename T>
 rso_status fine_jacobi0(rso_handle* h, const T* f, T* u_out, const T* rp, double omega) {

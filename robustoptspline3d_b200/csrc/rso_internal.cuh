@@ -121,6 +121,7 @@ struct rso_handle {
     double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr;  // fine FP64, cap * 3 NP
     double *cf = nullptr, *red = nullptr, *fpart = nullptr, *xfer = nullptr;
     double *scal = nullptr, *h_scal = nullptr;
+    double* ralpha = nullptr;                         // step sizes of the deferred steps, [ring slot][system]
     int* done = nullptr;
   } batch;
   double* c_fb = nullptr;             // coarsest right-hand sides of a batch (cap x 3 nc)
@@ -199,6 +200,7 @@ struct rso_handle {
   // when set, the FP32 V-cycle's last fine sweep also sums f . u into this
   // device scalar (the CG step's r . z; solver.cu)
   double* vc_zdot = nullptr;
+  int vc_zdot_stride = 1;             // its spacing between systems (batched solves)
   void* surf = nullptr;                            // surface-point self-support state (surface.cu)
 };
 
@@ -312,7 +314,7 @@ rso_status fine_jacobi(rso_handle* h, const T* u_in, const T* f, T* u_out, const
                        const T* u_prev = nullptr, double c1 = 0.0);
 // the FP32 Jacobi / Chebyshev step with dot_dev = f . u_out from the same pass
 rso_status fine_jacobi_dot32(rso_handle* h, const float* u_in, const float* f, float* u_out, double omega,
-                             const float* u_prev, double c1, double* dot_dev);
+                             const float* u_prev, double c1, double* dot_dev, int stride = 1);
 // the FP64 residual with its FP32 copy and r . r from the same pass
 rso_status fine_residual64_rr(rso_handle* h, const double* u, const double* f, double* r, float* r32,
                               double* dot_dev);

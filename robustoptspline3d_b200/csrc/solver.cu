@@ -88,7 +88,8 @@ static rso_status smooth(rso_handle* h, int li, int sweeps, int reverse, bool ze
     if (li == 0 && zero && s == 0) RSO_TRY(fine_jacobi0<T>(h, LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om[0]));
     else if (dot_here) {
       if constexpr (sizeof(T) == 4)
-        RSO_TRY(fine_jacobi_dot32(h, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), om[s], prev, c1[s], last_dot));
+        RSO_TRY(fine_jacobi_dot32(h, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), om[s], prev, c1[s], last_dot,
+                                  h->vc_zdot_stride));
     } else if (li == 0) RSO_TRY(fine_jacobi<T>(h, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), LV<T>::rp(h), om[s], prev, c1[s]));
     else RSO_TRY(coarse_jacobi<T>(h, li, LV<T>::u(l), LV<T>::f(l), LV<T>::t(l), om[s], prev, c1[s]));
     if (cheb) {  // previous <- current <- next
@@ -140,7 +141,7 @@ rso_status vcycle_levels(rso_handle* h, int pre, int post, int symmetric, bool u
   }
   // up-sweep from the level above the coarsest (or above the cluster kernel's levels)
   // the FP32 V-cycle's last fine step may also sum f . u (h->vc_zdot)
-  double* zdot = sizeof(T) == 4 && h->L[0].nb == 1 ? h->vc_zdot : nullptr;
+  double* zdot = sizeof(T) == 4 ? h->vc_zdot : nullptr;
   for (int li = lb > 0 ? lb - 1 : nl - 2; li >= 0; li--) {
     RSO_TRY(prolong<T>(h, li + 1, LV<T>::u(h->L[li + 1]), LV<T>::u(h->L[li])));
     RSO_TRY(smooth<T>(h, li, post, symmetric ? 1 : 0, false, li == 0 ? zdot : nullptr));
@@ -269,7 +270,7 @@ std::vector<uint64_t> vc_key(const rso_handle* h, bool rotating = true) {
   push_bits(k, h->rp32); push_bits(k, h->xfer); push_bits(k, h->xfer_n);
   push_bits(k, h->c_K); push_bits(k, h->c_nodes); push_bits(k, h->c_f); push_bits(k, h->c_fb); push_bits(k, h->nc);
   push_bits(k, h->cfg.smoother); push_bits(k, h->cfg.pre); push_bits(k, h->cfg.post);
-  push_bits(k, h->cfg.omega); push_bits(k, h->cfg.cheb_lower); push_bits(k, h->prof_on); push_bits(k, h->vc_zdot);
+  push_bits(k, h->cfg.omega); push_bits(k, h->cfg.cheb_lower); push_bits(k, h->prof_on); push_bits(k, h->vc_zdot); push_bits(k, h->vc_zdot_stride);
   push_bits(k, h->tune.fine_rows); push_bits(k, h->tune.fine_zc); push_bits(k, h->tune.bottom);
   for (int r : h->tune.rowsplit) push_bits(k, r);
   return k;

@@ -357,7 +357,10 @@ rso_status vcycle_mixed(rso_handle* h);
 void batch_release(rso_handle* h);
 rso_status solve_pcg_batch(rso_handle* h, int k, const double* F_dense, double* U_dense, double tol, int max_iter,
                            rso_solve_info* infos);
-rso_status solve_pcg(rso_handle* h, const double* f, double* u, double tol, int max_iter, rso_solve_info* info);
+// u_zero: the caller set u to zero, so the first residual is f itself (the
+// FP64 operator pass on zero is skipped; the same values)
+rso_status solve_pcg(rso_handle* h, const double* f, double* u, double tol, int max_iter, rso_solve_info* info,
+                     bool u_zero = false);
 // the FP32 recurrence stalls when a replacement's true residual is not below
 // this fraction of the previous one (claimed: the recursive residual's reduction)
 double stall_ratio(double factor, double claimed);

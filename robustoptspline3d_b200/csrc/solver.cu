@@ -811,7 +811,7 @@ static rso_status pcg32_graph(rso_handle* h, const double* f, double* x, double 
 }
 
 static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, double tol, int max_iter,
-                                rso_solve_info* info, bool* stalled, int* used) {
+                                rso_solve_info* info, bool* stalled, int* used, bool x_zero) {
   Level& l0 = h->L[0];
   const long long n3 = 3 * l0.NP, n4 = n3 / 4;
   double* s = h->scal;  // s[0]=rz, s[1]=pq, s[2]=alpha, s[3]=rz_new, s[4]=beta, s[5]=rr
@@ -840,7 +840,10 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
   };
   double fn2 = 0, rn2 = 0;
   RSO_TRY(dot_host(h, f, f, n3, &fn2));
-  RSO_TRY(true_residual(&rn2));
+  // from a zero iterate the residual is f (the operator pass would give f
+  // exactly: K 0 = 0 at every node); h->r is first needed at a replacement
+  if (x_zero) rn2 = fn2;
+  else RSO_TRY(true_residual(&rn2));
   const double fn = std::sqrt(fn2);
   int it = 0;
   double rel = fn > 0 ? std::sqrt(rn2) / fn : 0.0;
@@ -856,7 +859,7 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
     // the operator writes interior nodes only: the padding of q (an FP64
     // buffer seen as FP32, so old doubles split across its entries) must be zero
     RSO_CHECK_CUDA(h, cudaMemsetAsync(q32, 0, sizeof(float) * n3, h->stream));
-    k_d2f<<<cdiv(n3, 256), 256, 0, h->stream>>>(h->r, r32, n3); rso::note_launch();
+    k_d2f<<<cdiv(n3, 256), 256, 0, h->stream>>>(x_zero ? f : h->r, r32, n3); rso::note_launch();
     // r . z comes out of the V-cycle's last fine step when it is a Jacobi or
     // Chebyshev step (after a post-smoothing), else from its own pass
     const bool fuse = h->cfg.smoother != RSO_SMOOTH_GS && h->cfg.post >= 1;
@@ -973,14 +976,15 @@ static rso_status solve_pcg_k32(rso_handle* h, const double* f, double* x, doubl
 // residual z stays FP32 (it only enters r.z and the direction update), the
 // FP32 copy of r is written by the fused residual update, and the norm of r
 // comes out of the same pass.
-rso_status solve_pcg(rso_handle* h, const double* f, double* x, double tol, int max_iter, rso_solve_info* info) {
+rso_status solve_pcg(rso_handle* h, const double* f, double* x, double tol, int max_iter, rso_solve_info* info,
+                     bool x_zero) {
   Level& l0 = h->L[0];
   const long long n3 = 3 * l0.NP;
   const bool mixed = h->cfg.precision == RSO_MIXED;
   int used = 0;  // iterations of an FP32 recurrence that stalled
   if (mixed && h->krylov32 > 0 && l0.nb == 1) {
     bool stalled = false;
-    const rso_status st = solve_pcg_k32(h, f, x, tol, max_iter, info, &stalled, &used);
+    const rso_status st = solve_pcg_k32(h, f, x, tol, max_iter, info, &stalled, &used, x_zero);
     if (st != RSO_OK || !stalled) return st;
     max_iter -= used;  // the FP64 recurrence from the current iterate for the rest
   }

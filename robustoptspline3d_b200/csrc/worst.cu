@@ -212,7 +212,7 @@ rso_status worst_case(rso_handle* h, int steps, int cf, double tol, uint64_t see
     RSO_CHECK_CUDA(h, cudaMemsetAsync(u, 0, sizeof(double) * n3, h->stream));
     rso_solve_info si = {0, 0, 0};
     // high-contrast designs (void at rho_min^p = 1e-9) can need hundreds of CG steps
-    RSO_TRY(solve_pcg(h, h->w, u, tol, 4000, &si));
+    RSO_TRY(solve_pcg(h, h->w, u, tol, 4000, &si, true));
     total_it += si.iterations;
     k_gather_load<<<cdiv(nl, 128), 128, 0, h->stream>>>(u, l0.NP, h->load_nodes, h->load_normals, nl, cf, wv); rso::note_launch();
     RSO_TRY(rigid_project_load(h, wv, cf));

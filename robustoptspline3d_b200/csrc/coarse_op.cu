@@ -501,6 +501,58 @@ __global__ void __launch_bounds__(256) k_restrict_z_v4(const Level Fl, int nZ, c
   for (int c = 0; c < 3; c++) *reinterpret_cast<float4*>(t + c * comp + Z * pxy + off) = s[c];
 }
 
+// FP32, single system: the xy filter of the padded-plane t as two separable
+// passes, y into ty[c][Z][Yc][px] (16-byte vectors along x) and x into the
+// coarse nodes, 7 + 7 loads per output where the fused pass makes 49 (the
+// sums grouped by axis, so the last bits may differ from k_restrict_xy)
+template <int F>
+__global__ void __launch_bounds__(256) k_restrict_y_v4(const Level Fl, const Level C, const float* __restrict__ t,
+                                                       float* __restrict__ ty) {
+  const int ng = Fl.px / 4;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x, Z = blockIdx.y;
+  if (idx >= ng * C.ny) return;
+  const int Yc = idx / ng, g = idx - Yc * ng;
+  const long long plane = (long long)Fl.px * Fl.py, comp = plane * C.nz;
+  const long long ocomp = (long long)C.nz * C.ny * Fl.px;
+  float4 acc[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) acc[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+  for (int dy = -F + 1; dy < F; dy++) {
+    const int y = F * Yc + dy;
+    if (y < 0 || y >= Fl.ny) continue;
+    const float w = (float)(F - (dy < 0 ? -dy : dy)) / (float)F;
+    const float* src = t + (long long)Z * plane + (long long)(y + 1) * Fl.px + 4 * g;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float4 v = *reinterpret_cast<const float4*>(src + c * comp);
+      acc[c].x += w * v.x; acc[c].y += w * v.y; acc[c].z += w * v.z; acc[c].w += w * v.w;
+    }
+  }
+  float* dst = ty + ((long long)Z * C.ny + Yc) * Fl.px + 4 * g;
+#pragma unroll
+  for (int c = 0; c < 3; c++) *reinterpret_cast<float4*>(dst + c * ocomp) = acc[c];
+}
+template <int F>
+__global__ void k_restrict_x(const Level Fl, const Level C, const float* __restrict__ ty, float* __restrict__ fc) {
+  const int X = blockIdx.x * 32 + threadIdx.x, Y = blockIdx.y * 8 + threadIdx.y, Z = blockIdx.z;
+  if (X >= C.nx || Y >= C.ny) return;
+  const long long nC = C.nidx(X, Y, Z);
+  const long long ocomp = (long long)C.nz * C.ny * Fl.px;
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+  if (C.vclass[nC] & NC_ACTIVE) {
+    const float* row = ty + ((long long)Z * C.ny + Y) * Fl.px + 1;  // padded x: fine x + 1
+#pragma unroll
+    for (int dx = -F + 1; dx < F; dx++) {
+      const int x = F * X + dx;
+      if (x < 0 || x >= Fl.nx) continue;
+      const float w = (float)(F - (dx < 0 ? -dx : dx)) / (float)F;
+      s0 += w * row[x]; s1 += w * row[x + ocomp]; s2 += w * row[x + 2 * ocomp];
+    }
+  }
+  fc[nC] = s0; fc[nC + C.NP] = s1; fc[nC + 2 * C.NP] = s2;
+}
+
 // PAD: t laid out like the fine level's padded planes, t[c][Z][py][px] (the
 // layout k_restrict_z_v4 writes)
 template <typename T, int F, bool PAD = false>
@@ -1734,12 +1786,27 @@ rso_status restrict_(rso_handle* h, int cl, const T* rf, T* fc) {
       (size_t)3 * f.px * f.py * c.nz <= 2 * h->xfer_n) {
     const dim3 g4((unsigned)cdiv((long long)f.px * f.py / 4, 256), c.nz);
     float* t4 = reinterpret_cast<float*>(h->xfer);
+    // the y-filtered planes after t when the scratch holds both
+    const size_t tn = (size_t)3 * f.px * f.py * c.nz, tyn = (size_t)3 * c.nz * c.ny * f.px;
+    float* ty = tn + tyn <= 2 * h->xfer_n ? t4 + tn : nullptr;
+    const dim3 gy((unsigned)cdiv((long long)(f.px / 4) * c.ny, 256), c.nz);
+    const dim3 gx(cdiv(c.nx, 32), cdiv(c.ny, 8), c.nz);
     if (c.factor == 4) {
       k_restrict_z_v4<4><<<g4, 256, 0, h->stream>>>(f, c.nz, (const float*)rf, t4); rso::note_launch();
-      k_restrict_xy<float, 4, true><<<node_grid(c), dim3(32, 8), 0, h->stream>>>(f, c, t4, (float*)fc); rso::note_launch();
+      if (ty) {
+        k_restrict_y_v4<4><<<gy, 256, 0, h->stream>>>(f, c, t4, ty); rso::note_launch();
+        k_restrict_x<4><<<gx, dim3(32, 8), 0, h->stream>>>(f, c, ty, (float*)fc); rso::note_launch();
+      } else {
+        k_restrict_xy<float, 4, true><<<node_grid(c), dim3(32, 8), 0, h->stream>>>(f, c, t4, (float*)fc); rso::note_launch();
+      }
     } else {
       k_restrict_z_v4<2><<<g4, 256, 0, h->stream>>>(f, c.nz, (const float*)rf, t4); rso::note_launch();
-      k_restrict_xy<float, 2, true><<<node_grid(c), dim3(32, 8), 0, h->stream>>>(f, c, t4, (float*)fc); rso::note_launch();
+      if (ty) {
+        k_restrict_y_v4<2><<<gy, 256, 0, h->stream>>>(f, c, t4, ty); rso::note_launch();
+        k_restrict_x<2><<<gx, dim3(32, 8), 0, h->stream>>>(f, c, ty, (float*)fc); rso::note_launch();
+      } else {
+        k_restrict_xy<float, 2, true><<<node_grid(c), dim3(32, 8), 0, h->stream>>>(f, c, t4, (float*)fc); rso::note_launch();
+      }
     }
     return launch_check(h, "restrict");
   }
